@@ -1,0 +1,2 @@
+#include "suite.cuh"
+__device__ void suite::jacobi2d_main(int pe) { if (threadIdx.x == 0 && pe == 0) charm::end(); }

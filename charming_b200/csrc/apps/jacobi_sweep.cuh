@@ -1,0 +1,324 @@
+// Jacobi sweep of one chare block, executed inside an entry method by all
+// threads of the PE block.
+//
+// Arithmetic (reference examples/jacobi2d/jacobi2d.cu:327-334):
+//   new = (c + l + r + u + d) * 0.2, added left to right in T, one multiply
+//   by the double 0.2 (float grids: float sum, double multiply, rounded to
+//   float). Written with _rn intrinsics so no contraction can change it.
+//
+// Block layout in HBM (per chare, two buffers): rows 0..h+1 (0 and h+1 are
+// ghost rows), row pitch `pitch` elements (a multiple of 128 bytes); column
+// c in 0..w+1 sits at element OFF-1+c, so the first interior column starts
+// on a 128-byte boundary (OFF = 128 / sizeof(T)).
+//
+// Two implementations with identical results:
+//   sweep_direct: every thread loads its 5 points from global memory.
+//   sweep_tma:    rows stream through a ring of shared-memory slots filled
+//                 by cp.async.bulk (TMA 1-D bulk copies, no multicast), one
+//                 mbarrier per slot; each input row is read from HBM once
+//                 per column tile, so the compulsory traffic is one read and
+//                 one write per point (16 B/LUP FP64, 8 B/LUP FP32).
+#pragma once
+
+#include "suite.cuh"
+
+namespace jac {
+
+template <typename T> struct traits;
+template <> struct traits<double> {
+  static constexpr int VEC = 2;   // elements per 16-byte vector
+  static constexpr int OFF = 16;  // element offset of interior column 1
+  static constexpr int TW_MAX = 1024;
+};
+template <> struct traits<float> {
+  static constexpr int VEC = 4;
+  static constexpr int OFF = 32;
+  static constexpr int TW_MAX = 2048;
+};
+
+__device__ __forceinline__ double stencil(double c, double l, double r, double u, double d) {
+  return __dmul_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(c, l), r), u), d), 0.2);
+}
+__device__ __forceinline__ float stencil(float c, float l, float r, float u, float d) {
+  float s = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(c, l), r), u), d);
+  return __double2float_rn(__dmul_rn((double)s, 0.2));
+}
+// Residual term (S(u) - u)^2 with S in FP64.
+template <typename T>
+__device__ __forceinline__ double resid2(T c, T l, T r, T u, T d) {
+  double s = __dmul_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn((double)c, (double)l), (double)r),
+                                           (double)u), (double)d), 0.2);
+  double e = __dsub_rn(s, (double)c);
+  return __dmul_rn(e, e);
+}
+
+template <typename T>
+struct block_view {
+  T* base;      // element (row 0, column 0 of the pitched layout)
+  int pitch;    // elements
+  __device__ __forceinline__ T* row(int r) const { return base + (size_t)r * pitch; }
+  // pointer to column c (0..w+1) of row r
+  __device__ __forceinline__ T* at(int r, int c) const {
+    return base + (size_t)r * pitch + traits<T>::OFF - 1 + c;
+  }
+};
+
+// Computes VEC outputs of one row from the 5 input vectors and stores the
+// valid ones. mid points at interior column j0 of the row (vector aligned),
+// left/right are the scalars at j0-1 and j0+VEC. Returns the residual sum.
+template <typename T, bool RESID>
+__device__ __forceinline__ double compute_vec(const T* up, const T* mid, const T* dn, T left,
+    T right, T* out, int nvalid) {
+  constexpr int V = traits<T>::VEC;
+  T u[V], m[V], d[V], o[V];
+  if (V == 2) {
+    double2 a = *reinterpret_cast<const double2*>(up);
+    double2 b = *reinterpret_cast<const double2*>(mid);
+    double2 c = *reinterpret_cast<const double2*>(dn);
+    u[0] = (T)a.x; u[1] = (T)a.y; m[0] = (T)b.x; m[1] = (T)b.y; d[0] = (T)c.x; d[1] = (T)c.y;
+  } else {
+    float4 a = *reinterpret_cast<const float4*>(up);
+    float4 b = *reinterpret_cast<const float4*>(mid);
+    float4 c = *reinterpret_cast<const float4*>(dn);
+    u[0] = (T)a.x; u[1] = (T)a.y; u[2] = (T)a.z; u[3] = (T)a.w;
+    m[0] = (T)b.x; m[1] = (T)b.y; m[2] = (T)b.z; m[3] = (T)b.w;
+    d[0] = (T)c.x; d[1] = (T)c.y; d[2] = (T)c.z; d[3] = (T)c.w;
+  }
+  double acc = 0.0;
+#pragma unroll
+  for (int k = 0; k < V; k++) {
+    T l = (k == 0) ? left : m[k - 1];
+    T r = (k == V - 1) ? right : m[k + 1];
+    o[k] = stencil(m[k], l, r, u[k], d[k]);
+    if (RESID && k < nvalid) acc += resid2<T>(m[k], l, r, u[k], d[k]);
+  }
+  if (nvalid == V) {
+    if (V == 2) {
+      *reinterpret_cast<double2*>(out) = make_double2((double)o[0], (double)o[1]);
+    } else {
+      *reinterpret_cast<float4*>(out) = make_float4((float)o[0], (float)o[1], (float)o[2], (float)o[3]);
+    }
+  } else {
+    for (int k = 0; k < nvalid; k++) out[k] = o[k];
+  }
+  return acc;
+}
+
+// ---------------------------------------------------------------------------
+// Direct-load sweep: thread i of the block handles vectors i, i+n, ... of
+// the (h rows x ceil(w/VEC) vectors) output.
+// ---------------------------------------------------------------------------
+template <typename T, bool RESID>
+__device__ double sweep_direct(block_view<T> in, block_view<T> out, int w, int h) {
+  constexpr int V = traits<T>::VEC;
+  const int nv = (w + V - 1) / V;
+  const long long total = (long long)nv * h;
+  double acc = 0.0;
+  for (long long x = threadIdx.x; x < total; x += blockDim.x) {
+    int r = (int)(x / nv) + 1;
+    int v = (int)(x % nv);
+    int j0 = 1 + v * V;
+    const T* mid = in.at(r, j0);
+    int nvalid = min(V, w - v * V);
+    acc += compute_vec<T, RESID>(in.at(r - 1, j0), mid, in.at(r + 1, j0), mid[-1], mid[V],
+                                 out.at(r, j0), nvalid);
+  }
+  return acc;
+}
+
+// ---------------------------------------------------------------------------
+// TMA row pipeline.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_inval(unsigned long long* b) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" :: "r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(b)),
+               "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done) : "r"(smem_u32(b)), "r"(parity) : "memory");
+  return done != 0;
+}
+// 1-D bulk copy global -> shared, completion counted on the mbarrier.
+// Both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
+    unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_global() {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+struct tma_plan {
+  int ntiles;     // column tiles
+  int tws;        // tile stride (columns), multiple of VEC
+  int tpr;        // threads per output row (vectors per tile row)
+  int G;          // rows per band
+  int NS;         // ring slots
+  int slot_elems; // elements per slot
+};
+
+// Smem needed by a plan with NS slots.
+template <typename T>
+__host__ __device__ inline size_t tma_slot_bytes(int tws) {
+  size_t e = (size_t)tws + 2 * traits<T>::VEC;
+  return (e * sizeof(T) + 127) / 128 * 128;
+}
+
+template <typename T>
+__device__ bool make_plan(int w, int nthreads, size_t smem_bytes, int tile_w_opt, tma_plan* p) {
+  constexpr int V = traits<T>::VEC;
+  int twmax = tile_w_opt > 0 ? tile_w_opt : traits<T>::TW_MAX;
+  twmax = (twmax + V - 1) / V * V;
+  p->ntiles = (w + twmax - 1) / twmax;
+  int tw = (w + p->ntiles - 1) / p->ntiles;
+  p->tws = (tw + V - 1) / V * V;
+  p->tpr = p->tws / V;
+  p->G = p->tpr >= nthreads ? 1 : nthreads / p->tpr;
+  size_t sb = tma_slot_bytes<T>(p->tws);
+  p->slot_elems = (int)(sb / sizeof(T));
+  size_t avail = smem_bytes > 1024 ? smem_bytes - 1024 : 0;  // mbarriers
+  long ns = (long)(avail / sb);
+  if (ns > 32) ns = 32;
+  p->NS = (int)ns;
+  return p->NS >= p->G + 2;
+}
+
+// Returns false (error recorded) when a pipeline wait ran out.
+template <typename T, bool RESID>
+__device__ bool sweep_tma(block_view<T> in, block_view<T> out, int w, int h, void* smem,
+    size_t smem_bytes, const tma_plan& P, double* acc_out) {
+  constexpr int V = traits<T>::VEC;
+  constexpr int H = V;  // halo elements each side of a slot row (16 bytes)
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem);
+  T* slots = reinterpret_cast<T*>(reinterpret_cast<char*>(smem) + 1024);
+  const int rows = h + 2;
+  const long long total_items = (long long)P.ntiles * rows;
+  __shared__ long long s_issued;
+  __shared__ int s_fail;
+
+  // Generic-proxy writes to `in` (previous sweep, halo unpack) must be
+  // visible to the bulk copies.
+  fence_proxy_async_global();
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < P.NS; s++) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+    s_issued = 0;
+    s_fail = 0;
+  }
+  __syncthreads();
+
+  auto issue_upto = [&](long long limit) {
+    // thread 0 only
+    if (limit > total_items) limit = total_items;
+    if (s_issued < limit) fence_proxy_async_smem();
+    while (s_issued < limit) {
+      long long j = s_issued;
+      int t = (int)(j / rows), r = (int)(j % rows);
+      int c0 = t * P.tws;
+      int tw = min(P.tws, w - c0);
+      unsigned bytes = (unsigned)(((size_t)(tw + 2 * H) * sizeof(T) + 15) / 16 * 16);
+      const T* src = in.row(r) + traits<T>::OFF + c0 - H;
+      int s = (int)(j % P.NS);
+      mbar_expect_tx(&bars[s], bytes);
+      bulk_g2s(slots + (size_t)s * P.slot_elems, src, bytes, &bars[s]);
+      s_issued = j + 1;
+    }
+  };
+
+  if (threadIdx.x == 0) issue_upto(P.NS);
+  __syncthreads();
+
+  double acc = 0.0;
+  const int g = threadIdx.x / P.tpr;     // row within band
+  const int lane = threadIdx.x % P.tpr;  // vector within tile row
+  const bool row_thread = P.tpr >= (int)blockDim.x || g < P.G;
+
+  for (int t = 0; t < P.ntiles; t++) {
+    const int c0 = t * P.tws;
+    const int tw = min(P.tws, w - c0);
+    const int nvec = (tw + V - 1) / V;
+    const long long ibase = (long long)t * rows;
+    for (int rb = 1; rb <= h; rb += P.G) {
+      const int r = rb + (P.tpr >= (int)blockDim.x ? 0 : g);
+      if (row_thread && r <= h && !s_fail) {
+        // wait for input rows r-1, r, r+1 of this tile
+        bool ok = true;
+        for (int q = -1; q <= 1 && ok; q++) {
+          long long j = ibase + r + q;
+          unsigned parity = (unsigned)((j / P.NS) & 1);
+          unsigned long long* b = &bars[j % P.NS];
+          unsigned spins = 0;
+          while (!mbar_try_wait(b, parity)) {
+            if (++spins > (1u << 26)) {
+              ok = false;
+              break;
+            }
+          }
+        }
+        if (!ok) {
+          atomicExch(&s_fail, 1);
+        } else {
+          const T* up = slots + (size_t)((ibase + r - 1) % P.NS) * P.slot_elems;
+          const T* mid = slots + (size_t)((ibase + r) % P.NS) * P.slot_elems;
+          const T* dn = slots + (size_t)((ibase + r + 1) % P.NS) * P.slot_elems;
+          for (int v = lane; v < nvec; v += P.tpr) {
+            int s = H + v * V;  // slot index of interior column c0 + v*V
+            int nvalid = min(V, tw - v * V);
+            acc += compute_vec<T, RESID>(up + s, mid + s, dn + s, mid[s - 1], mid[s + V],
+                                         out.at(r, 1 + c0 + v * V), nvalid);
+          }
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0 && !s_fail) {
+        int rmax = min(rb + P.G - 1, h);
+        long long freed = (rmax == h) ? ibase + rows : ibase + rmax;
+        issue_upto(freed + P.NS);
+      }
+      __syncthreads();
+    }
+  }
+
+  // All issued copies were waited on (or the run failed): retire barriers.
+  bool fail = s_fail != 0;
+  if (threadIdx.x == 0) {
+    if (fail) {
+      // Drain copies still in flight before the barriers are reused: wait
+      // (bounded) for every issued item's phase.
+      for (long long j = (s_issued > P.NS ? s_issued - P.NS : 0); j < s_issued; j++) {
+        unsigned spins = 0;
+        while (!mbar_try_wait(&bars[j % P.NS], (unsigned)((j / P.NS) & 1)) && ++spins < (1u << 24)) {
+        }
+      }
+      charm::detail::report_error(CHARMING_ERR_PIPELINE, (int)s_issued, h);
+    }
+    for (int s = 0; s < P.NS; s++) mbar_inval(&bars[s]);
+  }
+  // Outputs written by generic stores feed the next sweep's bulk copies.
+  fence_proxy_async_global();
+  __syncthreads();
+  *acc_out = acc;
+  return !fail;
+}
+
+}  // namespace jac

@@ -1,0 +1,379 @@
+// Messaging microbenchmarks: pingpong (examples/pingpong/pingpong.cu:17-217)
+// and a seeded fan-out with refnums.
+#include "suite.cuh"
+#include "../host.cuh"
+#include <vector>
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Pingpong: chares on PE 0 and PE n_pes/2 exchange messages of each size;
+// chare 0 times round trips after a warm-up (pingpong.cu:121-217).
+// g_app: a[0] n_sizes, a[1] round trips, a[2] warmup, a[3] seed, a[4] verify;
+//        p[0] sizes (u64[n_sizes]), p[1] results (u64[n_sizes][4]:
+//        total ns, total cycles, checksum errors, 0), p[2] u32[2] SM ids,
+//        p[3] u64[2][n_sizes] expected checksums (for the host's check).
+// ---------------------------------------------------------------------------
+struct PingChare : charm::chare {
+  int peer;
+  int init_cnt;
+  int size_idx;
+  int iter;
+  unsigned char* data;
+  unsigned long long* expect;  // checksum of the peer's prefix for each size
+  unsigned long long errors;
+  unsigned long long t_start, c_start;
+  __device__ PingChare() : peer(-1), init_cnt(0), size_idx(0), iter(0), data(nullptr),
+      expect(nullptr), errors(0), t_start(0), c_start(0) {}
+};
+
+__shared__ charm::chare_proxy<PingChare>* ping_proxy;
+
+__device__ unsigned long long prefix_checksum(unsigned long long seed, int who,
+    unsigned long long n) {
+  unsigned long long nw = (n + 7) / 8, acc = 0;
+  for (unsigned long long i = threadIdx.x; i < nw; i += blockDim.x) {
+    unsigned long long w = suite::gen_word(seed, (unsigned long long)who, i);
+    unsigned long long valid = n - 8 * i;
+    if (valid < 8) w &= (1ULL << (8 * valid)) - 1;
+    acc += suite::checksum_word(w, i);
+  }
+  return suite::block_sum_u64(acc) ^ n;
+}
+
+__device__ void ping_send(PingChare& c) {
+  const unsigned long long* sizes = reinterpret_cast<const unsigned long long*>(g_app.p[0]);
+  int warmup = (int)g_app.a[2];
+  if (c.i == 0 && c.iter == warmup && threadIdx.x == 0) {
+    c.t_start = charm::now_ns();
+    c.c_start = clock64();
+  }
+  __syncthreads();
+  ping_proxy->invoke(c.peer, 2, c.data, sizes[c.size_idx]);
+}
+
+__device__ void ping_init(PingChare& c, void* arg) {
+  const unsigned long long* sizes = reinterpret_cast<const unsigned long long*>(g_app.p[0]);
+  int n_sizes = (int)g_app.a[0];
+  unsigned long long seed = (unsigned long long)g_app.a[3];
+  unsigned long long max_size = 0;
+  for (int s = 0; s < n_sizes; s++) max_size = sizes[s] > max_size ? sizes[s] : max_size;
+  __shared__ unsigned char* s_data;
+  __shared__ unsigned long long* s_exp;
+  if (threadIdx.x == 0) {
+    c.peer = (c.i == 0) ? 1 : 0;
+    s_data = new unsigned char[max_size + 8];
+    s_exp = new unsigned long long[n_sizes];
+    c.data = s_data;
+    c.expect = s_exp;
+    if (!s_data || !s_exp) charm::detail::report_error(CHARMING_ERR_NO_MEMORY, 0, 0);
+    reinterpret_cast<unsigned int*>(g_app.p[2])[c.i] = charm::smid();
+  }
+  __syncthreads();
+  if (!s_data || !s_exp) return;
+  unsigned long long nw = (max_size + 7) / 8;
+  for (unsigned long long i = threadIdx.x; i < nw; i += blockDim.x) {
+    reinterpret_cast<unsigned long long*>(s_data)[i] = suite::gen_word(seed, (unsigned long long)c.i, i);
+  }
+  for (int s = 0; s < n_sizes; s++) {
+    unsigned long long cs = prefix_checksum(seed, c.peer, sizes[s]);
+    if (threadIdx.x == 0) {
+      s_exp[s] = cs;
+      reinterpret_cast<unsigned long long*>(g_app.p[3])[(size_t)c.peer * n_sizes + s] = cs;
+    }
+  }
+  __syncthreads();
+  ping_proxy->invoke(0, 1);
+}
+
+__device__ void ping_init_done(PingChare& c, void* arg) {
+  if (threadIdx.x == 0) c.init_cnt++;
+  __syncthreads();
+  if (c.init_cnt == 2) ping_send(c);
+}
+
+__device__ void ping_recv(PingChare& c, void* arg) {
+  const unsigned long long* sizes = reinterpret_cast<const unsigned long long*>(g_app.p[0]);
+  int n_sizes = (int)g_app.a[0];
+  int n_iters = (int)g_app.a[1];
+  int warmup = (int)g_app.a[2];
+  unsigned long long size = sizes[c.size_idx];
+  if (g_app.a[4]) {
+    unsigned long long cs = suite::checksum_block(arg, size);
+    if (threadIdx.x == 0 && cs != c.expect[c.size_idx]) c.errors++;
+  }
+  __shared__ int s_done;
+  if (threadIdx.x == 0) {
+    s_done = 0;
+    if (c.i == 0) {
+      if (++c.iter == n_iters + warmup) {
+        unsigned long long t = charm::now_ns();
+        unsigned long long cy = clock64();
+        unsigned long long* out = reinterpret_cast<unsigned long long*>(g_app.p[1]) + 4 * c.size_idx;
+        out[0] = t - c.t_start;
+        out[1] = cy - c.c_start;
+        out[2] = c.errors;
+        c.errors = 0;
+        c.iter = 0;
+        if (++c.size_idx == n_sizes) s_done = 1;
+      }
+    }
+  }
+  __syncthreads();
+  if (s_done) {
+    charm::end();
+    return;
+  }
+  if (c.i == 0) {
+    ping_send(c);
+  } else {
+    ping_proxy->invoke(c.peer, 2, c.data, size);
+    if (threadIdx.x == 0) {
+      if (++c.iter == n_iters + warmup) {
+        unsigned long long* out = reinterpret_cast<unsigned long long*>(g_app.p[1]) + 4 * c.size_idx;
+        out[3] = c.errors;
+        c.errors = 0;
+        c.iter = 0;
+        c.size_idx++;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Fan-out. g_app: a[0] n_chares, a[1] msgs per chare, a[2] payload bytes,
+// a[3] seed, a[4] mode (0: refnum -1, 1: message k carries refnum k),
+// a[5] log capacity (records); p[0] log (u32[cap][8]), p[1] counters
+// (u64[2]: log index, delivered), p[2] expected counts (int[n][msgs]).
+// Destination of message k of chare s: mix64(seed ^ ((s*msgs+k+1)*G)) % n.
+// Payload: {u32 src, u32 k, u32 refnum, u32 0} then gen_word(seed, s*msgs+k, j).
+// ---------------------------------------------------------------------------
+struct FanChare : charm::chare {
+  int cur_ref;      // refnum being received (mode 1)
+  int got_at_ref;   // deliveries at cur_ref
+  int seq;          // deliveries so far
+  __device__ FanChare() : cur_ref(0), got_at_ref(0), seq(0) {}
+};
+
+__shared__ charm::chare_proxy<FanChare>* fan_proxy;
+
+__device__ __forceinline__ int fan_dst(unsigned long long seed, long long s, long long k,
+    long long msgs, long long n) {
+  unsigned long long id = (unsigned long long)(s * msgs + k);
+  return (int)(suite::mix64(seed ^ ((id + 1) * 0x9E3779B97F4A7C15ULL)) % (unsigned long long)n);
+}
+
+// Thread 0: next refnum >= r with a non-zero expected count (msgs if none).
+__device__ int fan_next_ref(int chare, int r) {
+  const int* expected = reinterpret_cast<const int*>(g_app.p[2]);
+  int msgs = (int)g_app.a[1];
+  while (r < msgs && expected[(size_t)chare * msgs + r] == 0) r++;
+  return r;
+}
+
+__device__ void fan_start(FanChare& c, void* arg) {
+  int n = (int)g_app.a[0], msgs = (int)g_app.a[1], payload = (int)g_app.a[2];
+  unsigned long long seed = (unsigned long long)g_app.a[3];
+  int mode = (int)g_app.a[4];
+  size_t scratch_bytes = 0;
+  unsigned char* buf = reinterpret_cast<unsigned char*>(charm::smem_scratch(&scratch_bytes));
+  for (int k = 0; k < msgs; k++) {
+    unsigned long long id = (unsigned long long)c.i * msgs + k;
+    int nw = (payload + 7) / 8;
+    for (int j = threadIdx.x; j < nw; j += blockDim.x) {
+      unsigned long long w = suite::gen_word(seed, id, (unsigned long long)j);
+      if (j == 0) w = (unsigned long long)(unsigned)c.i | ((unsigned long long)(unsigned)k << 32);
+      if (j == 1) w = (unsigned long long)(unsigned)(mode ? k : -1);
+      reinterpret_cast<unsigned long long*>(buf)[j] = w;
+    }
+    __syncthreads();
+    int dst = fan_dst(seed, c.i, k, msgs, n);
+    fan_proxy->invoke(dst, 1, buf, (size_t)payload, mode ? k : -1);
+  }
+}
+
+__device__ void fan_recv(FanChare& c, void* arg) {
+  int n = (int)g_app.a[0], msgs = (int)g_app.a[1], payload = (int)g_app.a[2];
+  int mode = (int)g_app.a[4];
+  unsigned long long cs = suite::checksum_block(arg, (unsigned long long)payload);
+  __shared__ int s_end;
+  if (threadIdx.x == 0) {
+    const unsigned int* h = reinterpret_cast<const unsigned int*>(arg);
+    unsigned long long* ctr = reinterpret_cast<unsigned long long*>(g_app.p[1]);
+    unsigned long long slot = atomicAdd(&ctr[0], 1ULL);
+    if (slot < (unsigned long long)g_app.a[5]) {
+      unsigned int* rec = reinterpret_cast<unsigned int*>(g_app.p[0]) + 8 * slot;
+      rec[0] = (unsigned)c.i;
+      rec[1] = h[0];
+      rec[2] = h[1];
+      rec[3] = h[2];
+      rec[4] = (unsigned)c.seq;
+      rec[5] = (unsigned)(cs & 0xffffffffULL);
+      rec[6] = (unsigned)(cs >> 32);
+      rec[7] = mode ? (unsigned)c.cur_ref : 0xffffffffu;
+    }
+    c.seq++;
+    if (mode) {
+      const int* expected = reinterpret_cast<const int*>(g_app.p[2]);
+      if (++c.got_at_ref == expected[(size_t)c.i * msgs + c.cur_ref]) {
+        c.got_at_ref = 0;
+        c.cur_ref = fan_next_ref(c.i, c.cur_ref + 1);
+        fan_proxy->set_refnum(c.i, c.cur_ref);
+      }
+    }
+    unsigned long long done = atomicAdd(&ctr[1], 1ULL) + 1;
+    s_end = (done == (unsigned long long)n * msgs) ? 1 : 0;
+  }
+  __syncthreads();
+  if (s_end) charm::end();
+}
+
+}  // namespace
+
+__device__ void suite::pingpong_main(int pe) {
+  if (threadIdx.x == 0) {
+    ping_proxy = new charm::chare_proxy<PingChare>();
+    ping_proxy->add_entry_method<&ping_init>();
+    ping_proxy->add_entry_method<&ping_init_done>();
+    ping_proxy->add_entry_method<&ping_recv>();
+    int n = charm::n_pes();
+    int* block_map = new int[n];
+    for (int i = 0; i < n; i++) block_map[i] = 0;
+    block_map[0] += 1;
+    block_map[n / 2] += 1;
+    ping_proxy->create(2, block_map);
+    delete[] block_map;
+  }
+  __syncthreads();
+  charm::barrier();
+  if (pe == 0) ping_proxy->invoke_all(0);
+}
+
+__device__ void suite::fanout_main(int pe) {
+  int n = (int)g_app.a[0], msgs = (int)g_app.a[1];
+  unsigned long long seed = (unsigned long long)g_app.a[3];
+  int mode = (int)g_app.a[4];
+  if (threadIdx.x == 0) {
+    fan_proxy = new charm::chare_proxy<FanChare>();
+    fan_proxy->add_entry_method<&fan_start>();
+    fan_proxy->add_entry_method<&fan_recv>();
+    fan_proxy->create(n);
+  }
+  __syncthreads();
+  int lo = fan_proxy->start_idx, hi = fan_proxy->end_idx;
+  int* expected = reinterpret_cast<int*>(g_app.p[2]);
+  long long total = (long long)n * msgs;
+  for (long long x = threadIdx.x; x < total; x += blockDim.x) {
+    long long s = x / msgs, k = x % msgs;
+    int d = fan_dst(seed, s, k, msgs, n);
+    if (d >= lo && d <= hi) atomicAdd(&expected[(size_t)d * msgs + k], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && mode) {
+    for (int c = lo; c <= hi && fan_proxy->n_local > 0; c++) {
+      FanChare* ch = fan_proxy->local(c);
+      ch->cur_ref = fan_next_ref(c, 0);
+      fan_proxy->set_refnum(c, ch->cur_ref);
+    }
+  }
+  __syncthreads();
+  if (fan_proxy->n_local > 0) {
+    for (int c = lo; c <= hi; c++) fan_proxy->invoke(c, 0);
+  }
+}
+
+extern "C" int charming_pingpong(const uint64_t* sizes, int n_sizes, int round_trips,
+    int warmup, uint64_t seed, int verify, charming_pingpong_result* out, int* sm_pair) {
+  int rc = charm_host::ensure_init();
+  if (rc) return rc;
+  if (n_sizes <= 0 || round_trips <= 0 || warmup < 0 || !sizes || !out) return CHARMING_ERR_CONFIG;
+  for (int i = 0; i < n_sizes; i++) {
+    if (sizes[i] + 48 > charm_host::info().max_msg_bytes) return CHARMING_ERR_MSG_TOO_LARGE;
+  }
+  unsigned long long* d = nullptr;
+  size_t bytes = 8 * (size_t)n_sizes * (1 + 4 + 2) + 64;
+  cudaError_t e = cudaMalloc(&d, bytes);
+  if (e != cudaSuccess) return charm_host::cuda_fail(e, "pingpong buffers");
+  cudaMemset(d, 0, bytes);
+  cudaMemcpy(d, sizes, 8 * n_sizes, cudaMemcpyHostToDevice);
+  suite::app_params p{};
+  p.id = suite::APP_PINGPONG;
+  p.a[0] = n_sizes;
+  p.a[1] = round_trips;
+  p.a[2] = warmup;
+  p.a[3] = (long long)seed;
+  p.a[4] = verify;
+  p.p[0] = d;
+  p.p[1] = d + n_sizes;
+  p.p[2] = d + 5 * (size_t)n_sizes;
+  p.p[3] = d + 5 * (size_t)n_sizes + 8;
+  rc = suite_run(p);
+  std::vector<unsigned long long> h(bytes / 8);
+  cudaMemcpy(h.data(), d, bytes, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  for (int i = 0; i < n_sizes; i++) {
+    const unsigned long long* r = &h[n_sizes + 4 * (size_t)i];
+    out[i].size = sizes[i];
+    out[i].oneway_us = r[0] * 1e-3 / (2.0 * round_trips);
+    out[i].oneway_cycles = (double)r[1] / (2.0 * round_trips);
+    out[i].checksum_errors = r[2] + r[3];
+  }
+  if (sm_pair) {
+    const unsigned int* sm = reinterpret_cast<const unsigned int*>(&h[5 * (size_t)n_sizes]);
+    sm_pair[0] = (int)sm[0];
+    sm_pair[1] = (int)sm[1];
+  }
+  return rc;
+}
+
+extern "C" int charming_fanout(int n_chares, int msgs_per_chare, int payload_bytes,
+    uint64_t seed, int mode, uint32_t* log, uint64_t log_capacity, uint64_t* n_logged,
+    double* out_ms) {
+  int rc = charm_host::ensure_init();
+  if (rc) return rc;
+  if (n_chares <= 0 || msgs_per_chare <= 0 || payload_bytes < 16 || (payload_bytes % 8) ||
+      !log || (mode != 0 && mode != 1))
+    return CHARMING_ERR_CONFIG;
+  if ((size_t)payload_bytes > (size_t)charm_host::info().smem_scratch_bytes)
+    return CHARMING_ERR_CONFIG;
+  size_t total = (size_t)n_chares * msgs_per_chare;
+  unsigned int* d_log = nullptr;
+  unsigned long long* d_ctr = nullptr;
+  int* d_exp = nullptr;
+  cudaError_t e = cudaMalloc(&d_log, 32 * (size_t)log_capacity + 32);
+  if (e == cudaSuccess) e = cudaMalloc(&d_ctr, 64);
+  if (e == cudaSuccess) e = cudaMalloc(&d_exp, sizeof(int) * total);
+  if (e != cudaSuccess) {
+    cudaFree(d_log);
+    cudaFree(d_ctr);
+    cudaFree(d_exp);
+    return charm_host::cuda_fail(e, "fanout buffers");
+  }
+  cudaMemset(d_ctr, 0, 64);
+  cudaMemset(d_exp, 0, sizeof(int) * total);
+  suite::app_params p{};
+  p.id = suite::APP_FANOUT;
+  p.a[0] = n_chares;
+  p.a[1] = msgs_per_chare;
+  p.a[2] = payload_bytes;
+  p.a[3] = (long long)seed;
+  p.a[4] = mode;
+  p.a[5] = (long long)log_capacity;
+  p.p[0] = d_log;
+  p.p[1] = d_ctr;
+  p.p[2] = d_exp;
+  rc = suite_run(p);
+  unsigned long long ctr[2] = {0, 0};
+  cudaMemcpy(ctr, d_ctr, 16, cudaMemcpyDeviceToHost);
+  unsigned long long n_rec = ctr[0] < log_capacity ? ctr[0] : log_capacity;
+  cudaMemcpy(log, d_log, 32 * n_rec, cudaMemcpyDeviceToHost);
+  if (n_logged) *n_logged = ctr[0];
+  charming_stats st;
+  charming_last_stats(&st);
+  if (out_ms) *out_ms = st.loop_ms;
+  cudaFree(d_log);
+  cudaFree(d_ctr);
+  cudaFree(d_exp);
+  return rc;
+}

@@ -1,0 +1,53 @@
+// Process main() of libcharming.a: programs that define charm::main (and
+// optionally charm::main_host) link against the library and get this entry
+// point, as with the reference (src/charming.cu:50-263).
+//
+// Environment overrides: CHARMING_PES_PER_SM, CHARMING_RING_BYTES,
+// CHARMING_DEADLINE_S, CHARMING_IDLE_TIMEOUT_S, CHARMING_HEAP_BYTES,
+// CHARMING_QUIET (suppress the [INFO] lines).
+#include <cstdio>
+#include <cstdlib>
+#include "../../include/charming_c.h"
+
+namespace charm {
+// Weak: programs without a host main still link (the reference requires one).
+__attribute__((weak)) void main_host(int argc, char** argv);
+}
+
+static unsigned long long env_u64(const char* name, unsigned long long dflt) {
+  const char* s = getenv(name);
+  return s ? strtoull(s, nullptr, 0) : dflt;
+}
+
+int main(int argc, char** argv) {
+  if (charm::main_host) charm::main_host(argc, argv);
+
+  charming_config cfg;
+  charming_default_config(&cfg);
+  cfg.pes_per_sm = (int)env_u64("CHARMING_PES_PER_SM", (unsigned long long)cfg.pes_per_sm);
+  cfg.ring_bytes = env_u64("CHARMING_RING_BYTES", cfg.ring_bytes);
+  cfg.heap_bytes = env_u64("CHARMING_HEAP_BYTES", cfg.heap_bytes);
+  bool quiet = getenv("CHARMING_QUIET") != nullptr;
+  cfg.verbose = quiet ? 0 : 1;
+
+  int rc = charming_init(&cfg);
+  if (rc != CHARMING_OK) {
+    fprintf(stderr, "[ERROR] charming_init: %s (%s)\n", charming_status_string(rc),
+        charming_last_error());
+    return rc;
+  }
+  rc = charming_run(argc, argv);
+  charming_stats st;
+  charming_last_stats(&st);
+  if (rc != CHARMING_OK) {
+    fprintf(stderr, "[ERROR] run ended with status %d: %s (pe %d, info %d %d) %s\n", rc,
+        charming_status_string(rc), st.err_pe, st.err_info0, st.err_info1, charming_last_error());
+  }
+  if (!quiet) {
+    printf("[INFO] Exiting CharminG: %llu messages delivered, %.3f ms\n",
+        (unsigned long long)st.delivered, st.kernel_ms);
+  }
+  fflush(stdout);
+  charming_fini();
+  return rc;
+}

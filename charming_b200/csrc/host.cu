@@ -1,0 +1,410 @@
+// Host runtime: device setup, buffer allocation, the scheduler launch and the
+// core C ABI (charming_init / run / fini / stats).
+//
+// Replaces the reference's process main (src/charming.cu:50-263) and
+// comm_init_host / comm_fini_host (src/comm/get/get.cu:69-169) for one GPU:
+// no NVSHMEM or MPI bootstrap, plain cudaMalloc'd HBM for the inbox rings,
+// and a cooperative launch so that every PE block is resident.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#include <string>
+#include "host.cuh"
+
+__global__ void charming_scheduler_kernel(int argc, char** argv, size_t* argvs);
+__global__ void charming_reset_kernel();
+
+using namespace charm::rt;
+
+namespace {
+
+struct HostRuntime {
+  bool inited = false;
+  charming_config cfg{};
+  charming_info inf{};
+  cudaDeviceProp prop{};
+  device_state ds{};
+  std::vector<void*> dev_allocs;
+  int* h_stop = nullptr;
+  int* d_stop = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  charming_stats last{};
+  char* d_args = nullptr;
+  size_t d_args_cap = 0;
+};
+
+HostRuntime g;
+std::string g_err;
+
+template <typename T>
+int dev_alloc(T** p, size_t bytes, const char* what) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, bytes);
+  if (e != cudaSuccess) return charm_host::cuda_fail(e, what);
+  e = cudaMemset(q, 0, bytes);
+  if (e != cudaSuccess) {
+    cudaFree(q);
+    return charm_host::cuda_fail(e, what);
+  }
+  g.dev_allocs.push_back(q);
+  g.inf.device_bytes += bytes;
+  *p = reinterpret_cast<T*>(q);
+  return CHARMING_OK;
+}
+
+bool is_pow2(uint64_t v) { return v && !(v & (v - 1)); }
+
+double env_double(const char* name, double dflt) {
+  const char* s = getenv(name);
+  return s ? atof(s) : dflt;
+}
+
+}  // namespace
+
+namespace charm_host {
+
+int cuda_fail(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return CHARMING_OK;
+  g_err = std::string(what) + ": " + cudaGetErrorString(e);
+  return CHARMING_ERR_CUDA;
+}
+void set_error_text(const std::string& s) { g_err = s; }
+bool initialised() { return g.inited; }
+cudaStream_t stream() { return g.stream; }
+const charming_info& info() { return g.inf; }
+
+int ensure_init() {
+  if (g.inited) return CHARMING_OK;
+  charming_config cfg;
+  charming_default_config(&cfg);
+  return charming_init(&cfg);
+}
+
+void request_stop(int value) {
+  if (g.h_stop) {
+    *reinterpret_cast<volatile int*>(g.h_stop) = value;
+  }
+}
+
+int enqueue_scheduler(cudaStream_t s) {
+  if (!g.inited) return CHARMING_ERR_NOT_INIT;
+  int nb = (g.inf.n_pes + 255) / 256;
+  charming_reset_kernel<<<nb, 256, 0, s>>>();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "reset kernel launch");
+  int argc = 0;
+  char** argv = nullptr;
+  size_t* argvs = nullptr;
+  void* args[] = {&argc, &argv, &argvs};
+  cudaLaunchConfig_t lc{};
+  lc.gridDim = dim3(g.inf.n_pes);
+  lc.blockDim = dim3(g.inf.threads_per_pe);
+  lc.dynamicSmemBytes = g.inf.smem_bytes_per_pe;
+  lc.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  lc.attrs = attr;
+  lc.numAttrs = 1;
+  e = cudaLaunchKernelExC(&lc, (const void*)charming_scheduler_kernel, args);
+  if (e != cudaSuccess) return cuda_fail(e, "scheduler launch");
+  return CHARMING_OK;
+}
+
+int collect_run(double kernel_ms) {
+  int ctrl_h[CTRL_WORDS];
+  cudaError_t e = cudaMemcpy(ctrl_h, g.ds.ctrl, sizeof(ctrl_h), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "read status");
+  std::vector<unsigned long long> st((size_t)g.inf.n_pes * N_STATS), tm((size_t)g.inf.n_pes * 2);
+  e = cudaMemcpy(st.data(), g.ds.pe_stats, st.size() * 8, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(tm.data(), g.ds.pe_times, tm.size() * 8, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "read stats");
+  charming_stats s{};
+  unsigned long long tmin = ~0ULL, tmax = 0;
+  for (int p = 0; p < g.inf.n_pes; p++) {
+    const unsigned long long* q = &st[(size_t)p * N_STATS];
+    s.delivered += q[ST_DELIVERED];
+    s.sent += q[ST_SENT];
+    s.stashed += q[ST_STASHED];
+    s.revived += q[ST_REVIVED];
+    s.bytes_sent += q[ST_BYTES_SENT];
+    s.idle_polls += q[ST_IDLE_POLLS];
+    s.space_waits += q[ST_SPACE_WAITS];
+    if (tm[2 * p] && tm[2 * p] < tmin) tmin = tm[2 * p];
+    if (tm[2 * p + 1] > tmax) tmax = tm[2 * p + 1];
+  }
+  s.loop_ms = (tmax > tmin && tmin != ~0ULL) ? (tmax - tmin) * 1e-6 : 0.0;
+  s.kernel_ms = kernel_ms;
+  s.status = ctrl_h[CTRL_STATUS];
+  s.err_pe = ctrl_h[CTRL_ERR_PE];
+  s.err_info0 = ctrl_h[CTRL_ERR_I0];
+  s.err_info1 = ctrl_h[CTRL_ERR_I1];
+  g.last = s;
+  return s.status;
+}
+
+int run_scheduler(int argc, char** argv) {
+  if (!g.inited) return CHARMING_ERR_NOT_INIT;
+  // Arguments into device memory (reference: managed memory,
+  // src/charming.cu:146-169).
+  size_t total = (size_t)argc * (sizeof(char*) + sizeof(size_t)) + 16;
+  for (int i = 0; i < argc; i++) total += strlen(argv[i]) + 1;
+  if (total > g.d_args_cap) {
+    if (g.d_args) cudaFree(g.d_args);
+    g.d_args = nullptr;
+    size_t cap = total < 4096 ? 4096 : total * 2;
+    cudaError_t e = cudaMalloc(&g.d_args, cap);
+    if (e != cudaSuccess) return cuda_fail(e, "argv buffer");
+    g.d_args_cap = cap;
+  }
+  std::vector<char> blob(total, 0);
+  char** h_argv = reinterpret_cast<char**>(blob.data());
+  size_t* h_argvs = reinterpret_cast<size_t*>(blob.data() + (size_t)argc * sizeof(char*));
+  size_t off = (size_t)argc * (sizeof(char*) + sizeof(size_t));
+  for (int i = 0; i < argc; i++) {
+    size_t n = strlen(argv[i]);
+    memcpy(blob.data() + off, argv[i], n + 1);
+    h_argv[i] = g.d_args + off;
+    h_argvs[i] = n;
+    off += n + 1;
+  }
+  cudaError_t e = cudaMemcpyAsync(g.d_args, blob.data(), total, cudaMemcpyHostToDevice, g.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "argv copy");
+  *reinterpret_cast<volatile int*>(g.h_stop) = 0;
+
+  int nb = (g.inf.n_pes + 255) / 256;
+  charming_reset_kernel<<<nb, 256, 0, g.stream>>>();
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "reset kernel launch");
+
+  char** d_argv = reinterpret_cast<char**>(g.d_args);
+  size_t* d_argvs = reinterpret_cast<size_t*>(g.d_args + (size_t)argc * sizeof(char*));
+  void* args[] = {&argc, &d_argv, &d_argvs};
+  cudaEventRecord(g.ev0, g.stream);
+  e = cudaLaunchCooperativeKernel((const void*)charming_scheduler_kernel, dim3(g.inf.n_pes),
+      dim3(g.inf.threads_per_pe), args, (size_t)g.inf.smem_bytes_per_pe, g.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "scheduler launch");
+  cudaEventRecord(g.ev1, g.stream);
+  e = cudaStreamSynchronize(g.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "scheduler run");
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, g.ev0, g.ev1);
+  return collect_run(ms);
+}
+
+}  // namespace charm_host
+
+using namespace charm_host;
+
+extern "C" {
+
+void charming_default_config(charming_config* cfg) {
+  memset(cfg, 0, sizeof(*cfg));
+  cfg->device = 0;
+  cfg->pes_per_sm = 1;
+  cfg->threads_per_pe = 512;
+  cfg->n_pes = 0;
+  cfg->ring_bytes = 4ull << 20;
+  cfg->max_msg_bytes = (1ull << 20) + 64;
+  cfg->stash_bytes = 4ull << 20;
+  cfg->stash_entries = 4096;
+  cfg->heap_bytes = 1ull << 30;
+  cfg->stack_bytes = 8192;
+  cfg->deadline_s = env_double("CHARMING_DEADLINE_S", 120.0);
+  cfg->idle_timeout_s = env_double("CHARMING_IDLE_TIMEOUT_S", 10.0);
+  cfg->free_chares_at_exit = 1;
+  cfg->verbose = 0;
+}
+
+int charming_init(const charming_config* cfg_in) {
+  if (g.inited) return CHARMING_OK;
+  charming_config cfg = *cfg_in;
+  g.inf = charming_info{};
+  cudaError_t e = cudaSetDevice(cfg.device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+  e = cudaGetDeviceProperties(&g.prop, cfg.device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceProperties");
+  if (!g.prop.cooperativeLaunch) {
+    set_error_text("device does not support cooperative launch");
+    return CHARMING_ERR_CONFIG;
+  }
+  if (cfg.pes_per_sm < 1 || cfg.pes_per_sm > 4 || cfg.threads_per_pe < 32 ||
+      cfg.threads_per_pe > MAX_THREADS || (cfg.threads_per_pe % 32) ||
+      !is_pow2(cfg.ring_bytes) || cfg.ring_bytes < 4096 ||
+      cfg.max_msg_bytes < 64 || cfg.max_msg_bytes > cfg.ring_bytes / 2 ||
+      cfg.stash_entries < 16 || cfg.stash_bytes < cfg.max_msg_bytes ||
+      cfg.deadline_s <= 0) {
+    set_error_text("invalid charming_config");
+    return CHARMING_ERR_CONFIG;
+  }
+  int n_sms = g.prop.multiProcessorCount;
+  int n_pes = cfg.n_pes > 0 ? cfg.n_pes : n_sms * cfg.pes_per_sm;
+
+  // Device limits (reference: src/charming.cu:197-203).
+  e = cudaDeviceSetLimit(cudaLimitMallocHeapSize, cfg.heap_bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "heap limit");
+  e = cudaDeviceSetLimit(cudaLimitStackSize, cfg.stack_bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "stack limit");
+
+  cudaFuncAttributes fa;
+  e = cudaFuncGetAttributes(&fa, (const void*)charming_scheduler_kernel);
+  if (e != cudaSuccess) return cuda_fail(e, "scheduler attributes");
+  int smem_state = (int)((sizeof(pe_state) + 8ull * n_pes + 127) / 128 * 128);
+  long per_block = (long)g.prop.sharedMemPerBlockOptin - (long)fa.sharedSizeBytes;
+  long per_sm = (long)g.prop.sharedMemPerMultiprocessor / cfg.pes_per_sm -
+                (long)fa.sharedSizeBytes - (long)g.prop.reservedSharedMemPerBlock;
+  long smem_total = per_block < per_sm ? per_block : per_sm;
+  smem_total = smem_total / 128 * 128;
+  if (smem_total < smem_state + 1024) {
+    set_error_text("not enough shared memory per PE");
+    return CHARMING_ERR_CONFIG;
+  }
+  e = cudaFuncSetAttribute((const void*)charming_scheduler_kernel,
+      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_total);
+  if (e != cudaSuccess) return cuda_fail(e, "smem attribute");
+  int per_sm_blocks = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_blocks,
+      (const void*)charming_scheduler_kernel, cfg.threads_per_pe, (size_t)smem_total);
+  if (e != cudaSuccess) return cuda_fail(e, "occupancy");
+  if ((long)per_sm_blocks * n_sms < n_pes) {
+    char buf[256];
+    snprintf(buf, sizeof(buf), "%d PEs cannot be co-resident (%d blocks/SM x %d SMs)",
+        n_pes, per_sm_blocks, n_sms);
+    set_error_text(buf);
+    return CHARMING_ERR_CONFIG;
+  }
+
+  g.cfg = cfg;
+  g.inf.n_pes = n_pes;
+  g.inf.n_sms = n_sms;
+  g.inf.threads_per_pe = cfg.threads_per_pe;
+  g.inf.smem_bytes_per_pe = (int)smem_total;
+  g.inf.smem_scratch_bytes = (int)smem_total - smem_state;
+  g.inf.regs_per_thread = fa.numRegs;
+  g.inf.ring_bytes = cfg.ring_bytes;
+  g.inf.max_msg_bytes = (cfg.max_msg_bytes + 15) / 16 * 16;
+
+  device_state& ds = g.ds;
+  ds = device_state{};
+  ds.n_pes = n_pes;
+  ds.threads = cfg.threads_per_pe;
+  ds.ring_cells = cfg.ring_bytes / CELL;
+  ds.max_msg = (cfg.max_msg_bytes + 15) / 16 * 16;
+  ds.ring_stride = cfg.ring_bytes + (ds.max_msg + CELL - 1) / CELL * CELL + 128;
+  ds.stash_bytes = (cfg.stash_bytes + 127) / 128 * 128;
+  ds.stash_entries = cfg.stash_entries;
+  ds.smem_state_bytes = smem_state;
+  ds.smem_total = (unsigned long long)smem_total;
+  ds.deadline_ns = (unsigned long long)(cfg.deadline_s * 1e9);
+  ds.idle_timeout_ns = (unsigned long long)(cfg.idle_timeout_s * 1e9);
+  ds.free_chares_at_exit = cfg.free_chares_at_exit;
+
+  int rc;
+  if ((rc = dev_alloc(&ds.tail, sizeof(line_u64) * n_pes, "inbox tails"))) return rc;
+  if ((rc = dev_alloc(&ds.head, sizeof(line_u64) * n_pes, "inbox heads"))) return rc;
+  if ((rc = dev_alloc(&ds.flags, 8ull * ds.ring_cells * n_pes, "inbox flags"))) return rc;
+  if ((rc = dev_alloc(&ds.ring, ds.ring_stride * n_pes, "inbox rings"))) return rc;
+  if ((rc = dev_alloc(&ds.stash_keys, sizeof(stash_key) * (size_t)ds.stash_entries * n_pes, "stash keys"))) return rc;
+  if ((rc = dev_alloc(&ds.stash_data, ds.stash_bytes * n_pes, "stash arena"))) return rc;
+  if ((rc = dev_alloc(&ds.proxy_tables, sizeof(charm::chare_proxy_table) * n_pes, "proxy tables"))) return rc;
+  if ((rc = dev_alloc(&ds.ctrl, sizeof(int) * CTRL_WORDS, "control words"))) return rc;
+  if ((rc = dev_alloc(&ds.progress, 8ull * n_pes, "progress"))) return rc;
+  if ((rc = dev_alloc(&ds.pe_stats, 8ull * N_STATS * n_pes, "stats"))) return rc;
+  if ((rc = dev_alloc(&ds.pe_times, 16ull * n_pes, "times"))) return rc;
+  e = cudaHostAlloc(&g.h_stop, 64, cudaHostAllocMapped);
+  if (e != cudaSuccess) return cuda_fail(e, "host stop word");
+  *g.h_stop = 0;
+  e = cudaHostGetDevicePointer(&g.d_stop, g.h_stop, 0);
+  if (e != cudaSuccess) return cuda_fail(e, "host stop pointer");
+  ds.host_stop = g.d_stop;
+
+  int one = 1, zero = 0;
+  e = cudaMemcpyToSymbol(c_n_sms, &n_sms, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_my_dev, &zero, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_my_dev_node, &zero, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_n_devs, &one, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_n_devs_node, &one, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_n_nodes, &one, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_n_pes, &n_pes, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_n_pes_node, &n_pes, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_rt, &ds, sizeof(ds));
+  if (e != cudaSuccess) return cuda_fail(e, "constants");
+  e = cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&g.ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&g.ev1);
+  if (e != cudaSuccess) return cuda_fail(e, "stream/events");
+  e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cuda_fail(e, "init sync");
+  g.inited = true;
+  if (cfg.verbose) {
+    PINFO("Initiating CharminG (B200 runtime)\n");
+    PINFO("PEs: %d (%d per SM), SMs: %d, threads per PE: %d, regs/thread: %d\n", n_pes,
+        cfg.pes_per_sm, n_sms, cfg.threads_per_pe, fa.numRegs);
+    PINFO("Dynamic smem per PE: %ld B (scratch %d B), ring %llu B per PE\n", smem_total,
+        g.inf.smem_scratch_bytes, (unsigned long long)cfg.ring_bytes);
+  }
+  return CHARMING_OK;
+}
+
+int charming_run(int argc, char** argv) { return run_scheduler(argc, argv); }
+
+int charming_fini(void) {
+  if (!g.inited) return CHARMING_OK;
+  cudaDeviceSynchronize();
+  for (void* p : g.dev_allocs) cudaFree(p);
+  g.dev_allocs.clear();
+  if (g.d_args) cudaFree(g.d_args);
+  g.d_args = nullptr;
+  g.d_args_cap = 0;
+  if (g.h_stop) cudaFreeHost(g.h_stop);
+  g.h_stop = nullptr;
+  if (g.ev0) cudaEventDestroy(g.ev0);
+  if (g.ev1) cudaEventDestroy(g.ev1);
+  if (g.stream) cudaStreamDestroy(g.stream);
+  g.ev0 = g.ev1 = nullptr;
+  g.stream = nullptr;
+  g.inited = false;
+  return CHARMING_OK;
+}
+
+int charming_get_info(charming_info* out) {
+  if (!g.inited) return CHARMING_ERR_NOT_INIT;
+  *out = g.inf;
+  return CHARMING_OK;
+}
+
+int charming_last_stats(charming_stats* out) {
+  *out = g.last;
+  return CHARMING_OK;
+}
+
+const char* charming_status_string(int code) {
+  switch (code) {
+    case CHARMING_OK: return "ok";
+    case CHARMING_ERR_RING_FULL: return "inbox ring full (no space within the wait limit)";
+    case CHARMING_ERR_STASH_FULL: return "refnum stash full";
+    case CHARMING_ERR_BAD_TARGET: return "invalid chare array, index or entry method";
+    case CHARMING_ERR_BARRIER_TIMEOUT: return "barrier timeout";
+    case CHARMING_ERR_IDLE_TIMEOUT: return "idle timeout (nothing delivered; missing end()?)";
+    case CHARMING_ERR_DEADLINE: return "run deadline exceeded";
+    case CHARMING_ERR_BAD_MSG: return "malformed message";
+    case CHARMING_ERR_MSG_TOO_LARGE: return "message larger than max_msg_bytes";
+    case CHARMING_ERR_HOST_STOP: return "stopped by host";
+    case CHARMING_ERR_TOO_MANY_TYPES: return "too many chare types on a PE";
+    case CHARMING_ERR_TOO_MANY_EMS: return "too many entry methods";
+    case CHARMING_ERR_PIPELINE: return "bulk-copy pipeline wait ran out";
+    case CHARMING_ERR_LAUNCH: return "scheduler launch failed";
+    case CHARMING_ERR_CONFIG: return "invalid configuration";
+    case CHARMING_ERR_CUDA: return "CUDA error";
+    case CHARMING_ERR_NOT_INIT: return "runtime not initialised";
+    case CHARMING_ERR_NO_MEMORY: return "out of memory";
+    case CHARMING_ERR_APP: return "program reported a failure";
+    default: return "unknown status";
+  }
+}
+
+const char* charming_last_error(void) { return g_err.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,182 @@
+// Internal device-runtime definitions shared by the scheduler, the transport
+// and the built-in programs. Not part of the public API.
+//
+// Memory layout in HBM (one GPU, n_pes PE thread blocks):
+//   tail[pe], head[pe]      ticket counters of PE pe's inbox ring, one 128-B
+//                           line each (senders atomicAdd tail; the owner
+//                           publishes head with st.release)
+//   flags[pe][C]            per-cell sequence word: ticket+1 of the message
+//                           that starts in that cell, stored with st.release
+//   ring[pe]                C cells of CELL bytes + an overhang of max_msg
+//                           bytes, so that a message never wraps: one whose
+//                           cells run past the end continues in the overhang
+//   stash_keys[pe][S]       descriptors of messages whose refnum mismatched
+//   stash_data[pe]          byte arena holding those messages
+// Cell and flag indices are (ticket mod C); C is a power of two.
+#pragma once
+
+#include <charming.h>
+#include "../../include/charming_c.h"
+
+namespace charm {
+namespace rt {
+
+constexpr int CELL = 32;                 // ring cell, bytes
+constexpr int HDR = 32;                  // envelope (16) + regular_msg (16)
+constexpr int MAX_THREADS = 512;         // launch bound of the scheduler
+
+struct alignas(128) line_u64 {
+  unsigned long long v;
+  unsigned long long pad[15];
+};
+
+// Stash descriptor, 32 B.
+struct stash_key {
+  int chare_id;
+  int chare_idx;
+  int refnum;
+  int state;                    // 0 consumed, 1 waiting, 2 ready
+  unsigned long long data_off;  // virtual byte offset in the PE's arena
+  unsigned int bytes;
+  int src_pe;
+};
+
+enum : int { KEY_FREE = 0, KEY_WAIT = 1, KEY_READY = 2 };
+
+enum : int {
+  ST_DELIVERED = 0,   // entry methods run
+  ST_SENT,            // messages sent
+  ST_STASHED,         // messages parked on refnum mismatch
+  ST_REVIVED,         // stashed messages made ready
+  ST_BYTES_SENT,      // payload bytes sent
+  ST_IDLE_POLLS,      // empty inbox polls
+  ST_SPACE_WAITS,     // sends that waited for ring space
+  ST_LOOP_NS,         // ns spent in the scheduler loop
+  N_STATS = 8
+};
+
+// Device-wide runtime description, copied to __constant__ memory before each
+// launch.
+struct device_state {
+  int n_pes;
+  int threads;
+  unsigned long long ring_cells;       // C (power of two)
+  unsigned long long ring_stride;      // bytes per PE ring region
+  unsigned long long max_msg;          // bytes, envelope included
+  unsigned long long stash_bytes;      // arena bytes per PE
+  int stash_entries;                   // descriptors per PE
+  int smem_state_bytes;                // bytes of dynamic smem the runtime keeps
+  unsigned long long smem_total;       // dynamic smem bytes per PE
+  unsigned long long deadline_ns;      // run limit, relative to kernel start
+  unsigned long long idle_timeout_ns;  // no delivery anywhere for this long
+  line_u64* tail;
+  line_u64* head;
+  unsigned long long* flags;
+  unsigned char* ring;
+  stash_key* stash_keys;
+  unsigned char* stash_data;
+  chare_proxy_table* proxy_tables;
+  int* ctrl;                           // see CTRL_* below
+  unsigned long long* progress;        // [n_pes] last delivery (globaltimer)
+  unsigned long long* pe_stats;        // [n_pes][N_STATS]
+  unsigned long long* pe_times;        // [n_pes][2] loop start / end
+  volatile int* host_stop;             // mapped host word, may be null
+  int free_chares_at_exit;
+};
+
+// Words of device_state::ctrl (each on its own 128-B line).
+enum : int {
+  CTRL_TERM = 0,        // termination request
+  CTRL_STATUS = 32,     // first error code
+  CTRL_ERR_PE = 33,
+  CTRL_ERR_I0 = 34,
+  CTRL_ERR_I1 = 35,
+  CTRL_BAR_COUNT = 64,
+  CTRL_BAR_GEN = 96,
+  CTRL_WORDS = 128
+};
+
+extern __constant__ device_state c_rt;
+
+// Per-PE scheduler state at the start of dynamic shared memory.
+struct pe_state {
+  int my_pe;
+  int term;                 // this PE leaves its loop
+  int sent_term;
+  int revive_pending;
+  unsigned long long head;  // next inbox ticket to consume
+  unsigned long long t0;    // kernel start (globaltimer)
+  // stash
+  unsigned long long key_head, key_tail;
+  unsigned long long arena_head, arena_tail;
+  int n_waiting, n_ready;
+  // block-collective broadcast slots
+  void* b_ptr0;
+  const void* b_ptr1;
+  unsigned long long b_u0, b_u1;
+  int b_i0, b_i1, b_i2, b_i3, b_i4, b_i5;
+  int red_i[4];
+  unsigned long long red_u[4];
+  unsigned long long stats[N_STATS];
+  unsigned long long idle_polls_since_check;
+  // followed by head_cache[n_pes] (unsigned long long), then scratch
+};
+
+__device__ __forceinline__ pe_state* pes() { return reinterpret_cast<pe_state*>(s_mem); }
+__device__ __forceinline__ unsigned long long* head_cache() {
+  return reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(s_mem) + sizeof(pe_state));
+}
+
+// ---- PTX helpers ----------------------------------------------------------
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned int* p, unsigned int v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ int ld_relaxed_s32(const int* p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ int ld_sys_s32(const volatile int* p) {
+  int v;
+  asm volatile("ld.relaxed.sys.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ int* ctrl(int w) { return c_rt.ctrl + w; }
+
+// Error path: first error wins; every PE stops.
+__device__ void set_error(int code, int info0, int info1);
+__device__ __forceinline__ bool terminated() { return ld_relaxed_s32(ctrl(CTRL_TERM)) != 0; }
+
+// Deadline check for bounded waits (thread-local view).
+__device__ __forceinline__ bool past_deadline() {
+  return globaltimer() - pes()->t0 > c_rt.deadline_ns;
+}
+
+__device__ void grid_barrier();
+
+// Message bytes -> ring cells.
+__host__ __device__ __forceinline__ unsigned int cells_for(unsigned long long bytes) {
+  return (unsigned int)((bytes + CELL - 1) / CELL);
+}
+
+} // namespace rt
+} // namespace charm

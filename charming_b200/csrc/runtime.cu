@@ -1,0 +1,649 @@
+// Device runtime: the persistent scheduler kernel, the intra-GPU inbox rings,
+// the refnum stash, barriers and termination.
+//
+// Reference counterparts:
+//   scheduler kernel / loop      src/sched/scheduler.cu:183-234, :165-171
+//   message dispatch             src/sched/scheduler.cu:23-76
+//   send                         src/comm/get/get.cu:728-781, :864-914
+//   receive + stash              src/comm/get/get.cu:374-465
+//   revive                       src/comm/get/get.cu:1316-1345
+//   termination                  src/charming.cu:265-267, get.cu:916-988
+//   barriers                     src/sched/scheduler.cu:336-350
+// What is different, and why:
+//   * Each PE owns one multi-producer inbox ring. A sender takes a ticket with
+//     one atomicAdd on the ring's tail, writes header and payload straight
+//     into the ring, and publishes the ticket with a release store into the
+//     cell's sequence word. The receiver consumes tickets in order with
+//     acquire loads, so messages from one sender to one receiver are
+//     delivered in send order. (The reference picks the lowest free slot of
+//     4 per pair and the receiver the lowest occupied index, which reorders.)
+//   * The receiver never scans: it polls one sequence word at its head.
+//   * A refnum mismatch copies the message to a per-PE stash and frees the
+//     ring cells at once, so a parked message never blocks the ring.
+//   * Every wait is bounded by the run deadline (%globaltimer); a run that
+//     cannot progress ends with an error status instead of spinning forever.
+#include "rt.cuh"
+
+// Execution-environment constants (see include/common.h).
+__constant__ int c_n_sms;
+__constant__ int c_my_dev;
+__constant__ int c_my_dev_node;
+__constant__ int c_n_devs;
+__constant__ int c_n_devs_node;
+__constant__ int c_n_nodes;
+__constant__ int c_n_pes;
+__constant__ int c_n_pes_node;
+
+namespace charm {
+namespace rt {
+__constant__ device_state c_rt;
+}
+}
+
+using namespace charm;
+using namespace charm::rt;
+
+// ---------------------------------------------------------------------------
+// Errors and termination
+// ---------------------------------------------------------------------------
+__device__ void charm::rt::set_error(int code, int info0, int info1) {
+  int prev = atomicCAS(ctrl(CTRL_STATUS), 0, code);
+  if (prev == 0) {
+    atomicExch(ctrl(CTRL_ERR_PE), (int)blockIdx.x);
+    atomicExch(ctrl(CTRL_ERR_I0), info0);
+    atomicExch(ctrl(CTRL_ERR_I1), info1);
+  }
+  __threadfence();
+  atomicExch(ctrl(CTRL_TERM), 1);
+}
+
+__device__ void charm::detail::report_error(int code, int info0, int info1) {
+  set_error(code, info0, info1);
+}
+
+__device__ chare_proxy_table& charm::detail::my_proxy_table() {
+  return c_rt.proxy_tables[blockIdx.x];
+}
+
+__device__ void charm::end() {
+  if (!terminated()) atomicExch(ctrl(CTRL_TERM), 1);
+}
+
+__device__ void charm::send_begin_term_msg() { charm::end(); }
+
+__device__ void charm::abort() {
+  // Stops the calling PE only (reference: src/charming.cu:270-277).
+  if (threadIdx.x == 0) pes()->term = 1;
+  __syncthreads();
+}
+
+__device__ int charm::my_pe() { return (int)blockIdx.x; }
+__device__ int charm::n_pes() { return c_n_pes; }
+__device__ int charm::my_pe_node() { return (int)blockIdx.x; }
+__device__ int charm::n_pes_node() { return c_n_pes_node; }
+__device__ int charm::n_nodes() { return c_n_nodes; }
+
+__device__ int charm::device_atoi(const char* str, int strlen) {
+  int v = 0;
+  for (int i = 0; i < strlen; i++) v = v * 10 + (str[i] - '0');
+  return v;
+}
+
+__device__ void* charm::smem_scratch(size_t* bytes) {
+  size_t off = (size_t)c_rt.smem_state_bytes;
+  if (bytes) *bytes = (size_t)c_rt.smem_total - off;
+  return reinterpret_cast<char*>(s_mem) + off;
+}
+
+__device__ uint64_t charm::now_ns() { return globaltimer(); }
+
+__device__ unsigned int charm::smid() {
+  unsigned int r;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
+  return r;
+}
+
+// ---------------------------------------------------------------------------
+// Grid barrier (sense by generation counter), bounded by the deadline.
+// All PE blocks are co-resident: the host launches cooperatively.
+// ---------------------------------------------------------------------------
+__device__ void charm::rt::grid_barrier() {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int* count = reinterpret_cast<unsigned int*>(ctrl(CTRL_BAR_COUNT));
+    unsigned int* gen = reinterpret_cast<unsigned int*>(ctrl(CTRL_BAR_GEN));
+    unsigned int g = ld_acquire_u32(gen);
+    __threadfence();
+    unsigned int arrived = atomicAdd(count, 1u);
+    if (arrived == (unsigned int)c_rt.n_pes - 1) {
+      atomicExch(count, 0u);
+      __threadfence();
+      st_release_u32(gen, g + 1);
+    } else {
+      // Leaves early when the run is ending (an error or end() elsewhere).
+      unsigned int spins = 0;
+      while (ld_acquire_u32(gen) == g) {
+        if ((++spins & 1023) == 0) {
+          if (terminated()) break;
+          if (past_deadline()) {
+            set_error(CHARMING_ERR_BARRIER_TIMEOUT, (int)arrived, 0);
+            break;
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+__device__ void charm::barrier() { grid_barrier(); }
+__device__ void charm::barrier_local() { grid_barrier(); }
+
+// ---------------------------------------------------------------------------
+// Transport
+// ---------------------------------------------------------------------------
+namespace {
+
+__device__ __forceinline__ unsigned char* ring_cell(int pe, unsigned long long ticket) {
+  return c_rt.ring + (unsigned long long)pe * c_rt.ring_stride +
+         (ticket & (c_rt.ring_cells - 1)) * CELL;
+}
+__device__ __forceinline__ unsigned long long* ring_flag(int pe, unsigned long long ticket) {
+  return c_rt.flags + (unsigned long long)pe * c_rt.ring_cells + (ticket & (c_rt.ring_cells - 1));
+}
+
+// Thread 0 only. Reserves `bytes` in dst's inbox; returns the message start
+// or nullptr (error recorded, or the run is ending).
+__device__ unsigned char* reserve(int dst, unsigned long long bytes, unsigned long long* ticket) {
+  pe_state* ps = pes();
+  if (dst < 0 || dst >= c_rt.n_pes) {
+    set_error(CHARMING_ERR_BAD_TARGET, -1, dst);
+    return nullptr;
+  }
+  if (bytes > c_rt.max_msg) {
+    set_error(CHARMING_ERR_MSG_TOO_LARGE, dst, (int)(bytes > 0x7fffffffULL ? 0x7fffffff : bytes));
+    return nullptr;
+  }
+  const unsigned long long C = c_rt.ring_cells;
+  unsigned int cells = cells_for(bytes);
+  unsigned long long t = atomicAdd(&c_rt.tail[dst].v, (unsigned long long)cells);
+  unsigned long long* hc = head_cache();
+  if (t + cells - hc[dst] > C) {
+    ps->stats[ST_SPACE_WAITS]++;
+    unsigned long long start = globaltimer();
+    // A receiver that frees nothing for the idle timeout is taken as stuck.
+    unsigned long long limit = c_rt.idle_timeout_ns ? c_rt.idle_timeout_ns : c_rt.deadline_ns;
+    unsigned int spins = 0;
+    while (true) {
+      unsigned long long h = ld_acquire_u64(&c_rt.head[dst].v);
+      hc[dst] = h;
+      if (t + cells - h <= C) break;
+      if ((++spins & 255) == 0) {
+        if (terminated()) return nullptr;
+        unsigned long long now = globaltimer();
+        if (now - start > limit || now - ps->t0 > c_rt.deadline_ns) {
+          set_error(CHARMING_ERR_RING_FULL, dst, (int)cells);
+          return nullptr;
+        }
+      }
+      __nanosleep(100);
+    }
+  }
+  *ticket = t;
+  return ring_cell(dst, t);
+}
+
+__device__ __forceinline__ void publish(int dst, unsigned long long ticket) {
+  __threadfence();
+  st_release_u64(ring_flag(dst, ticket), ticket + 1);
+}
+
+} // namespace
+
+__device__ void charm::send_reg_msg(int chare_id, int chare_idx, int ep_id, void* buf,
+    size_t payload_size, int dst_pe, int refnum) {
+  pe_state* ps = pes();
+  if (threadIdx.x == 0) {
+    unsigned long long bytes = envelope::alloc_size(msgtype::regular, payload_size);
+    unsigned long long t = 0;
+    unsigned char* m = reserve(dst_pe, bytes, &t);
+    if (m) {
+      envelope* env = reinterpret_cast<envelope*>(m);
+      env->type = msgtype::regular;
+      env->src_pe = (int)blockIdx.x;
+      env->size = bytes;
+      regular_msg* rm = reinterpret_cast<regular_msg*>(m + sizeof(envelope));
+      rm->chare_id = chare_id;
+      rm->chare_idx = chare_idx;
+      rm->ep_id = ep_id;
+      rm->refnum = refnum;
+      ps->stats[ST_SENT]++;
+      ps->stats[ST_BYTES_SENT] += payload_size;
+    }
+    ps->b_ptr0 = m;
+    ps->b_ptr1 = buf;
+    ps->b_u0 = (m && buf) ? payload_size : 0;
+    ps->b_u1 = t;
+    ps->b_i0 = (buf != nullptr && __isLocal(buf)) ? 1 : 0;
+    ps->b_i1 = dst_pe;
+  }
+  __syncthreads();
+  unsigned char* m = reinterpret_cast<unsigned char*>(ps->b_ptr0);
+  if (m == nullptr) {
+    __syncthreads();
+    return;
+  }
+  size_t n = ps->b_u0;
+  if (n > 0) {
+    if (ps->b_i0) {
+      // A thread-local buffer is only addressable by the thread that owns it.
+      if (threadIdx.x == 0) copy_cooperative(m + HDR, ps->b_ptr1, n, 0, 1);
+    } else {
+      copy_cooperative(m + HDR, ps->b_ptr1, n, threadIdx.x, blockDim.x);
+    }
+  }
+  unsigned long long t = ps->b_u1;
+  int dst = ps->b_i1;
+  __syncthreads();
+  if (threadIdx.x == 0) publish(dst, t);
+}
+
+__device__ bool charm::alloc_user_msg(message& msg, int dst_pe, size_t payload_size) {
+  pe_state* ps = pes();
+  if (threadIdx.x == 0) {
+    unsigned long long bytes = envelope::alloc_size(msgtype::user, payload_size);
+    unsigned long long t = 0;
+    unsigned char* m = reserve(dst_pe, bytes, &t);
+    ps->b_ptr0 = m;
+    ps->b_u0 = bytes;
+    ps->b_u1 = t;
+  }
+  __syncthreads();
+  msg.env = reinterpret_cast<envelope*>(ps->b_ptr0);
+  msg.offset = ps->b_u1;
+  msg.dst_pe = dst_pe;
+  msg.cells = (int)cells_for(ps->b_u0);
+  msg.capacity = msg.env ? (size_t)(ps->b_u0 - HDR) : 0;
+  __syncthreads();
+  return msg.env != nullptr;
+}
+
+__device__ void charm::send_user_msg(int chare_id, int chare_idx, int ep_id,
+    message& msg, size_t payload_size, int refnum) {
+  if (msg.env == nullptr) return;
+  pe_state* ps = pes();
+  __syncthreads();  // payload writes of all threads are done
+  if (threadIdx.x == 0) {
+    unsigned char* m = reinterpret_cast<unsigned char*>(msg.env);
+    envelope* env = msg.env;
+    env->type = msgtype::user;
+    env->src_pe = (int)blockIdx.x;
+    // The ring advances by the reserved size, whatever part was filled.
+    env->size = (size_t)msg.capacity + HDR;
+    regular_msg* rm = reinterpret_cast<regular_msg*>(m + sizeof(envelope));
+    rm->chare_id = chare_id;
+    rm->chare_idx = chare_idx;
+    rm->ep_id = ep_id;
+    rm->refnum = refnum;
+    if (payload_size > msg.capacity) set_error(CHARMING_ERR_MSG_TOO_LARGE, msg.dst_pe, (int)payload_size);
+    ps->stats[ST_SENT]++;
+    ps->stats[ST_BYTES_SENT] += payload_size;
+    publish(msg.dst_pe, msg.offset);
+  }
+  __syncthreads();
+  msg.env = nullptr;
+}
+
+__device__ void charm::revive_mismatches(int chare_id, int chare_idx, int refnum) {
+  pes()->revive_pending = 1;
+}
+
+// ---------------------------------------------------------------------------
+// Stash (refnum mismatches)
+// ---------------------------------------------------------------------------
+namespace {
+
+__device__ __forceinline__ stash_key* keys_of(int pe) {
+  return c_rt.stash_keys + (unsigned long long)pe * c_rt.stash_entries;
+}
+__device__ __forceinline__ unsigned char* arena_of(int pe) {
+  return c_rt.stash_data + (unsigned long long)pe * c_rt.stash_bytes;
+}
+
+// Block-collective: copy the message at env (bytes long) into the stash.
+__device__ void stash_put(const unsigned char* env, unsigned long long bytes,
+    int chare_id, int chare_idx, int refnum, int src_pe) {
+  pe_state* ps = pes();
+  if (threadIdx.x == 0) {
+    const unsigned long long S = (unsigned long long)c_rt.stash_entries;
+    const unsigned long long A = c_rt.stash_bytes;
+    bool ok = ps->key_tail - ps->key_head < S;
+    unsigned long long v = ps->arena_tail;
+    unsigned long long p = v % A;
+    if (p + bytes > A) v += A - p;
+    if (v + bytes - ps->arena_head > A) ok = false;
+    if (!ok) {
+      set_error(CHARMING_ERR_STASH_FULL, (int)(ps->key_tail - ps->key_head), (int)bytes);
+      ps->b_ptr0 = nullptr;
+    } else {
+      stash_key* k = keys_of(blockIdx.x) + (ps->key_tail % S);
+      k->chare_id = chare_id;
+      k->chare_idx = chare_idx;
+      k->refnum = refnum;
+      k->state = KEY_WAIT;
+      k->data_off = v;
+      k->bytes = (unsigned int)bytes;
+      k->src_pe = src_pe;
+      if (ps->key_tail == ps->key_head) ps->arena_head = v;
+      ps->arena_tail = v + bytes;
+      ps->key_tail++;
+      ps->n_waiting++;
+      ps->stats[ST_STASHED]++;
+      ps->b_ptr0 = arena_of(blockIdx.x) + (v % A);
+    }
+  }
+  __syncthreads();
+  unsigned char* dst = reinterpret_cast<unsigned char*>(ps->b_ptr0);
+  if (dst) copy_cooperative(dst, env, bytes, threadIdx.x, blockDim.x);
+  __syncthreads();
+}
+
+// Thread 0: drop consumed descriptors at the head and release arena bytes.
+__device__ void stash_retire() {
+  pe_state* ps = pes();
+  const unsigned long long S = (unsigned long long)c_rt.stash_entries;
+  stash_key* keys = keys_of(blockIdx.x);
+  while (ps->key_head < ps->key_tail && keys[ps->key_head % S].state == KEY_FREE) ps->key_head++;
+  ps->arena_head = (ps->key_head < ps->key_tail) ? keys[ps->key_head % S].data_off : ps->arena_tail;
+}
+
+// Block-collective: waiting messages whose refnum now matches become ready.
+__device__ void stash_revive() {
+  pe_state* ps = pes();
+  const unsigned long long S = (unsigned long long)c_rt.stash_entries;
+  stash_key* keys = keys_of(blockIdx.x);
+  chare_proxy_table& tb = c_rt.proxy_tables[blockIdx.x];
+  unsigned long long kh = ps->key_head, kt = ps->key_tail;
+  if (threadIdx.x == 0) {
+    ps->red_i[0] = 0;
+    ps->revive_pending = 0;
+  }
+  __syncthreads();
+  if (ps->n_waiting > 0) {
+    int cnt = 0;
+    for (unsigned long long i = kh + threadIdx.x; i < kt; i += blockDim.x) {
+      stash_key* k = keys + (i % S);
+      if (k->state == KEY_WAIT) {
+        chare_proxy_base* p = tb.proxies[k->chare_id];
+        if (p->refnum_matches(k->chare_idx, k->refnum)) {
+          k->state = KEY_READY;
+          cnt++;
+        }
+      }
+    }
+    if (cnt) atomicAdd_block(&ps->red_i[0], cnt);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int c = ps->red_i[0];
+    ps->n_ready += c;
+    ps->n_waiting -= c;
+    ps->stats[ST_REVIVED] += c;
+  }
+  __syncthreads();
+}
+
+// Block-collective: deliver the oldest ready stashed message.
+__device__ void stash_dispatch_ready() {
+  pe_state* ps = pes();
+  const unsigned long long S = (unsigned long long)c_rt.stash_entries;
+  const unsigned long long A = c_rt.stash_bytes;
+  stash_key* keys = keys_of(blockIdx.x);
+  unsigned long long kh = ps->key_head, kt = ps->key_tail;
+  if (threadIdx.x == 0) ps->red_u[0] = ~0ULL;
+  __syncthreads();
+  for (unsigned long long i = kh + threadIdx.x; i < kt; i += blockDim.x) {
+    if (keys[i % S].state == KEY_READY) {
+      atomicMin(&ps->red_u[0], i);
+      break;
+    }
+  }
+  __syncthreads();
+  unsigned long long idx = ps->red_u[0];
+  if (idx == ~0ULL) {
+    if (threadIdx.x == 0) ps->n_ready = 0;
+    __syncthreads();
+    return;
+  }
+  stash_key* k = keys + (idx % S);
+  unsigned char* env = arena_of(blockIdx.x) + (k->data_off % A);
+  chare_proxy_base* p = c_rt.proxy_tables[blockIdx.x].proxies[k->chare_id];
+  if (threadIdx.x == 0) ps->b_i0 = p->refnum_matches(k->chare_idx, k->refnum) ? 1 : 0;
+  __syncthreads();
+  int go = ps->b_i0;
+  if (go) {
+    const regular_msg* rm = reinterpret_cast<const regular_msg*>(env + sizeof(envelope));
+    p->call(k->chare_idx, rm->ep_id, env + HDR, k->refnum);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ps->n_ready--;
+    if (go) {
+      k->state = KEY_FREE;
+      ps->stats[ST_DELIVERED]++;
+      c_rt.progress[blockIdx.x] = globaltimer();
+      stash_retire();
+    } else {
+      k->state = KEY_WAIT;
+      ps->n_waiting++;
+    }
+  }
+  __syncthreads();
+}
+
+// Thread 0 of PE 0: stop the run when no PE has delivered anything for
+// idle_timeout_ns (e.g. a program that never calls end()).
+__device__ void check_idle_timeout(unsigned long long now) {
+  if (c_rt.idle_timeout_ns == 0) return;
+  unsigned long long latest = pes()->t0;
+  for (int p = 0; p < c_rt.n_pes; p++) {
+    unsigned long long v = *((volatile unsigned long long*)&c_rt.progress[p]);
+    if (v > latest) latest = v;
+  }
+  if (now > latest && now - latest > c_rt.idle_timeout_ns) {
+    set_error(CHARMING_ERR_IDLE_TIMEOUT, 0, 0);
+  }
+}
+
+// Thread 0: wait for the message at the inbox head. Returns 1 when it has
+// arrived, 0 when this PE must leave the loop.
+__device__ int poll_inbox() {
+  pe_state* ps = pes();
+  const int me = blockIdx.x;
+  unsigned long long h = ps->head;
+  const unsigned long long* f = ring_flag(me, h);
+  unsigned int spins = 0;
+  while (true) {
+    if (ld_acquire_u64(f) == h + 1) return 1;
+    if (ps->term || terminated()) return 0;
+    ++spins;
+    if ((spins & 255) == 0) {
+      unsigned long long now = globaltimer();
+      if (now - ps->t0 > c_rt.deadline_ns) {
+        set_error(CHARMING_ERR_DEADLINE, 0, 0);
+        return 0;
+      }
+      if ((spins & 4095) == 0) {
+        if (c_rt.host_stop) {
+          int hs = ld_sys_s32(c_rt.host_stop);
+          if (hs == 1) {
+            atomicExch(ctrl(CTRL_TERM), 1);
+            return 0;
+          } else if (hs > 1) {
+            set_error(CHARMING_ERR_HOST_STOP, hs, 0);
+            return 0;
+          }
+        }
+        if (me == 0 && (spins & 65535) == 0) check_idle_timeout(now);
+      }
+      ps->stats[ST_IDLE_POLLS] += 256;
+    }
+  }
+}
+
+// Block-collective: deliver or stash the message at the inbox head, then
+// release its cells to the senders.
+__device__ void dispatch_inbox() {
+  pe_state* ps = pes();
+  const int me = blockIdx.x;
+  unsigned char* m = ring_cell(me, ps->head);
+  if (threadIdx.x == 0) {
+    const envelope* env = reinterpret_cast<const envelope*>(m);
+    const regular_msg* rm = reinterpret_cast<const regular_msg*>(m + sizeof(envelope));
+    unsigned long long size = env->size;
+    int type = (int)env->type;
+    int action = 2;  // 0 deliver, 1 stash, 2 skip
+    chare_proxy_base* p = nullptr;
+    if (size < HDR || size > c_rt.max_msg || (size & (ALIGN_SIZE - 1))) {
+      set_error(CHARMING_ERR_BAD_MSG, env->src_pe, (int)type);
+      size = CELL;
+    } else if (type == (int)msgtype::regular || type == (int)msgtype::user) {
+      chare_proxy_table& tb = c_rt.proxy_tables[me];
+      int cid = rm->chare_id;
+      if (cid < 0 || cid >= tb.count || (p = tb.proxies[cid]) == nullptr ||
+          !p->valid_target(rm->chare_idx, rm->ep_id)) {
+        set_error(CHARMING_ERR_BAD_TARGET, cid, rm->chare_idx);
+      } else {
+        action = p->refnum_matches(rm->chare_idx, rm->refnum) ? 0 : 1;
+      }
+    } else if (type == (int)msgtype::do_terminate || type == (int)msgtype::begin_terminate) {
+      atomicExch(ctrl(CTRL_TERM), 1);
+    } else {
+      set_error(CHARMING_ERR_BAD_MSG, env->src_pe, type);
+    }
+    ps->b_ptr0 = p;
+    ps->b_i0 = action;
+    ps->b_i1 = rm->chare_idx;
+    ps->b_i2 = rm->ep_id;
+    ps->b_i3 = rm->refnum;
+    ps->b_i4 = rm->chare_id;
+    ps->b_i5 = env->src_pe;
+    ps->b_u0 = size;
+  }
+  __syncthreads();
+  int action = ps->b_i0;
+  unsigned long long size = ps->b_u0;
+  if (action == 0) {
+    chare_proxy_base* p = reinterpret_cast<chare_proxy_base*>(ps->b_ptr0);
+    int idx = ps->b_i1, ep = ps->b_i2, ref = ps->b_i3;
+    p->call(idx, ep, m + HDR, ref);
+  } else if (action == 1) {
+    stash_put(m, size, ps->b_i4, ps->b_i1, ps->b_i3, ps->b_i5);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ps->head += cells_for(size);
+    st_release_u64(&c_rt.head[me].v, ps->head);
+    if (action == 0) {
+      ps->stats[ST_DELIVERED]++;
+      c_rt.progress[me] = globaltimer();
+    }
+  }
+}
+
+__device__ void scheduler_loop() {
+  pe_state* ps = pes();
+  while (true) {
+    if (ps->revive_pending) stash_revive();
+    if (ps->n_ready > 0) {
+      stash_dispatch_ready();
+      if (threadIdx.x == 0 && terminated()) ps->term = 1;
+      __syncthreads();
+      if (ps->term) break;
+      continue;
+    }
+    if (threadIdx.x == 0) ps->b_i0 = poll_inbox();
+    __syncthreads();
+    int got = ps->b_i0;
+    if (!got) {
+      if (threadIdx.x == 0) ps->term = 1;
+      __syncthreads();
+      break;
+    }
+    __syncthreads();
+    dispatch_inbox();
+  }
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// The persistent scheduler kernel (one launch per run, one block per PE).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(MAX_THREADS, 1)
+charming_scheduler_kernel(int argc, char** argv, size_t* argvs) {
+  pe_state* ps = pes();
+  const int me = blockIdx.x;
+  if (threadIdx.x == 0) {
+    ps->my_pe = me;
+    ps->term = 0;
+    ps->sent_term = 0;
+    ps->revive_pending = 0;
+    ps->head = c_rt.head[me].v;
+    ps->t0 = globaltimer();
+    ps->key_head = ps->key_tail = 0;
+    ps->arena_head = ps->arena_tail = 0;
+    ps->n_waiting = ps->n_ready = 0;
+    for (int i = 0; i < N_STATS; i++) ps->stats[i] = 0;
+    ps->idle_polls_since_check = 0;
+  }
+  for (int i = threadIdx.x; i < c_rt.n_pes; i += blockDim.x) head_cache()[i] = c_rt.head[i].v;
+  __syncthreads();
+
+  grid_barrier();
+  charm::main(argc, argv, argvs, me);
+  grid_barrier();
+
+  unsigned long long loop_t0 = globaltimer();
+  if (!terminated() && !ps->term) scheduler_loop();
+  unsigned long long loop_t1 = globaltimer();
+
+  if (threadIdx.x == 0) {
+    ps->stats[ST_LOOP_NS] = loop_t1 - loop_t0;
+    for (int i = 0; i < N_STATS; i++) c_rt.pe_stats[(unsigned long long)me * N_STATS + i] = ps->stats[i];
+    c_rt.pe_times[2 * me] = loop_t0;
+    c_rt.pe_times[2 * me + 1] = loop_t1;
+    if (c_rt.free_chares_at_exit) {
+      chare_proxy_table& tb = c_rt.proxy_tables[me];
+      for (int i = tb.count - 1; i >= 0; i--) {
+        chare_proxy_base* p = tb.proxies[i];
+        if (p) {
+          p->release_all();
+          delete p;
+        }
+        tb.proxies[i] = nullptr;
+      }
+      tb.count = 0;
+    }
+  }
+}
+
+// Resets per-run control words: every inbox restarts at its current tail
+// (messages left over from an earlier run are dropped), proxy tables empty.
+__global__ void charming_reset_kernel() {
+  int n = c_rt.n_pes;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    unsigned long long t = c_rt.tail[i].v;
+    c_rt.head[i].v = t;
+    c_rt.progress[i] = 0;
+    c_rt.proxy_tables[i].count = 0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    c_rt.ctrl[CTRL_TERM] = 0;
+    c_rt.ctrl[CTRL_STATUS] = 0;
+    c_rt.ctrl[CTRL_ERR_PE] = -1;
+    c_rt.ctrl[CTRL_ERR_I0] = 0;
+    c_rt.ctrl[CTRL_ERR_I1] = 0;
+    c_rt.ctrl[CTRL_BAR_COUNT] = 0;
+  }
+}

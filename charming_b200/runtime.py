@@ -1,0 +1,134 @@
+"""Host-side interface of the runtime (Python mirror of include/charming_c.h).
+
+The reference's host interface is its process ``main()``
+(src/charming.cu:50-263): bootstrap, one launch of the persistent scheduler,
+teardown.  ``Runtime`` exposes the same life cycle (``init`` / ``run`` /
+``fini``) plus the built-in programs, over the C ABI of
+``libcharming_b200.so``.  Every call goes to the GPU; errors raise
+``CharmingError`` with the runtime's status code.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+DEFAULTS = dict(device=0, pes_per_sm=1, threads_per_pe=512, n_pes=0, ring_bytes=4 << 20,
+                max_msg_bytes=(1 << 20) + 64, stash_bytes=4 << 20, stash_entries=4096,
+                heap_bytes=1 << 30, stack_bytes=8192, deadline_s=120.0, idle_timeout_s=10.0,
+                free_chares_at_exit=1, verbose=0)
+
+
+@dataclass
+class RunStats:
+    delivered: int
+    sent: int
+    stashed: int
+    revived: int
+    bytes_sent: int
+    idle_polls: int
+    space_waits: int
+    kernel_ms: float
+    loop_ms: float
+    status: int
+
+
+class Runtime:
+    """One initialised runtime on one GPU (process-wide, like the reference)."""
+
+    _active: "Runtime | None" = None
+
+    def __init__(self, **overrides):
+        self.lib = _lib.load()
+        cfg = _lib.Config()
+        self.lib.charming_default_config(C.byref(cfg))
+        for k, v in overrides.items():
+            if not hasattr(cfg, k):
+                raise KeyError(f"unknown config field {k}")
+            setattr(cfg, k, v)
+        if Runtime._active is not None:
+            Runtime._active.fini()
+        check(self.lib.charming_init(C.byref(cfg)), "charming_init")
+        Runtime._active = self
+        self.config = cfg
+        inf = _lib.Info()
+        check(self.lib.charming_get_info(C.byref(inf)), "charming_get_info")
+        self.info = {f: getattr(inf, f) for f, _ in _lib.Info._fields_}
+
+    # ---- life cycle --------------------------------------------------------
+    def fini(self) -> None:
+        if Runtime._active is self:
+            self.lib.charming_fini()
+            Runtime._active = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.fini()
+
+    @property
+    def n_pes(self) -> int:
+        return self.info["n_pes"]
+
+    def last_stats(self) -> RunStats:
+        st = _lib.Stats()
+        self.lib.charming_last_stats(C.byref(st))
+        return RunStats(st.delivered, st.sent, st.stashed, st.revived, st.bytes_sent,
+                        st.idle_polls, st.space_waits, st.kernel_ms, st.loop_ms, st.status)
+
+    # ---- built-in programs ---------------------------------------------------
+    def hello(self) -> np.ndarray:
+        n = 2 * self.n_pes
+        out = (C.c_int * n)()
+        nch = C.c_int(0)
+        check(self.lib.charming_hello(out, n, C.byref(nch)), "charming_hello")
+        return np.frombuffer(out, dtype=np.int32).copy()
+
+    def refnum(self, reversed_order: bool = False) -> list[int]:
+        out = (C.c_int * 2)()
+        nd = C.c_int(0)
+        fn = self.lib.charming_refnum_reversed if reversed_order else self.lib.charming_refnum
+        check(fn(out, 2, C.byref(nd)), "charming_refnum")
+        return [out[i] for i in range(nd.value)]
+
+    def pingpong(self, sizes, round_trips: int, warmup: int = 10, seed: int = 1,
+                 verify: bool = True):
+        sizes = [int(s) for s in sizes]
+        arr = (C.c_uint64 * len(sizes))(*sizes)
+        res = (_lib.PingpongResult * len(sizes))()
+        sm = (C.c_int * 2)()
+        check(self.lib.charming_pingpong(arr, len(sizes), round_trips, warmup, seed,
+                                         1 if verify else 0, res, sm), "charming_pingpong")
+        rows = [dict(size=r.size, oneway_us=r.oneway_us, oneway_cycles=r.oneway_cycles,
+                     checksum_errors=r.checksum_errors) for r in res]
+        return rows, (sm[0], sm[1])
+
+    def fanout(self, n_chares: int, msgs: int, payload: int, seed: int, mode: int):
+        cap = n_chares * msgs
+        log = np.zeros((cap, 8), dtype=np.uint32)
+        n_logged = C.c_uint64(0)
+        ms = C.c_double(0.0)
+        check(self.lib.charming_fanout(n_chares, msgs, payload, seed, mode,
+                                       log.ctypes.data_as(C.POINTER(C.c_uint32)), cap,
+                                       C.byref(n_logged), C.byref(ms)), "charming_fanout")
+        return log[: min(n_logged.value, cap)], ms.value
+
+    def jacobi1d(self, n_chares: int, width: int, sweeps: int):
+        out = np.zeros(n_chares * width + 4, dtype=np.float64)
+        ms = C.c_double(0.0)
+        check(self.lib.charming_jacobi1d(n_chares, width, sweeps,
+                                         out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(ms)),
+              "charming_jacobi1d")
+        return out, ms.value
+
+
+def runtime(**overrides) -> Runtime:
+    """The process-wide runtime, created on first use with `overrides`."""
+    if Runtime._active is None:
+        return Runtime(**overrides)
+    return Runtime._active

@@ -1,0 +1,290 @@
+// charming-b200: chares, chare arrays (proxies) and entry methods.
+//
+// Source-compatible with the reference's include/chare.h:24-270: same
+// names, template signatures, placement rule and refnum rule, so that code
+// written against it (e.g. examples/hello, refnum, pingpong) compiles
+// unchanged. What differs is underneath: a mismatched message is copied into
+// a per-PE stash managed by the scheduler instead of a fixed 128-entry table
+// per chare type (include/chare.h:12, :51-58), and invalid targets are turned
+// into a runtime error status instead of an assert.
+#ifndef _CHARE_H_
+#define _CHARE_H_
+
+#include "common.h"
+#include "message.h"
+#include "kernel.h"
+
+#define CHARE_TYPE_CNT_MAX 1024 // Maximum number of chare types per PE
+#define EM_CNT_MAX 128          // Maximum number of entry methods per chare type
+#define ASYNC_WAIT_MAX 16       // Kept for source compatibility
+#define MISMATCH_MAX 128        // Kept for source compatibility (stash is per PE)
+
+namespace charm {
+
+struct chare {
+  int i;
+  int n;
+
+  __device__ chare() : i(-1), n(0) {}
+};
+
+template <class C>
+struct entry_method_base {
+  __device__ virtual void operator()(C& chare, void* arg) = 0;
+  __device__ virtual ~entry_method_base() {}
+};
+
+template <class C, void Func(C&, void*)>
+struct entry_method : entry_method_base<C> {
+  __device__ virtual void operator()(C& chare, void* arg) { Func(chare, arg); }
+};
+
+struct async_wait_t {
+  bool valid;
+  uint64_t* ivars;
+  size_t nelems;
+  int cmp;
+  uint64_t cmp_value;
+  int idx;
+  int ep;
+};
+
+struct mismatch_t {
+  int found_idx;
+  uint64_t comp;
+  int chare_idx;
+  int refnum;
+
+  __device__ mismatch_t() : found_idx(-1) {}
+};
+
+struct chare_proxy_base {
+  int id;        // Chare array ID (registration order on this PE)
+
+  int n_local;   // Number of local chares
+  int n_total;   // Total number of chares
+  int start_idx; // Starting index of local chares
+  int end_idx;   // Ending index of local chares
+
+  int* loc_map;  // Chare -> PE location map
+
+  int em_count;  // Number of registered entry methods
+
+  async_wait_t* async_waits;
+
+  int* refnum;   // Reference numbers of local chares
+  mismatch_t* mismatches;
+
+  __device__ chare_proxy_base() : id(-1), n_local(0), n_total(0), start_idx(-1),
+  end_idx(-1), loc_map(nullptr), em_count(0), async_waits(nullptr),
+  refnum(nullptr), mismatches(nullptr) {}
+
+  // Returns false without running the entry method when the message refnum
+  // is not -1 and differs from the chare's (include/chare.h:181-195).
+  __device__ virtual bool call(int idx, int ep, void* arg, int ref) = 0;
+  // Frees the local chares and tables (the runtime calls it when a run ends
+  // and then deletes the proxy).
+  __device__ virtual void release_all() {}
+  __device__ virtual ~chare_proxy_base() {}
+
+  // Target validity, checked by the scheduler before call().
+  __device__ bool valid_target(int idx, int ep) const {
+    return idx >= start_idx && idx <= end_idx && n_local > 0 && ep >= 0 && ep < em_count;
+  }
+  __device__ bool refnum_matches(int idx, int ref) const {
+    return ref == -1 || ref == refnum[idx - start_idx];
+  }
+};
+
+struct chare_proxy_table {
+  chare_proxy_base* proxies[CHARE_TYPE_CNT_MAX];
+  int count;
+
+  __host__ __device__ chare_proxy_table() : count(0) {}
+};
+
+namespace detail {
+// This PE's proxy table (one per PE thread block).
+__device__ chare_proxy_table& my_proxy_table();
+// Record a runtime error; the scheduler stops all PEs and the host call
+// returns `code` (see charming_c.h for the codes).
+__device__ void report_error(int code, int info0, int info1);
+enum : int {
+  ERR_BAD_TARGET = 3,
+  ERR_TOO_MANY_TYPES = 10,
+  ERR_TOO_MANY_EMS = 11,
+  ERR_NO_MEMORY = 17,
+};
+} // namespace detail
+
+__device__ int my_pe();
+
+template <typename C>
+struct chare_proxy : chare_proxy_base {
+  C** objects;                           // Local chare objects
+  entry_method_base<C>** entry_methods;  // Entry method table
+
+  // Registers this proxy in the calling PE's table (single-threaded).
+  __device__ chare_proxy()
+    : chare_proxy_base(), objects(nullptr), entry_methods(nullptr) {
+    chare_proxy_table& table = detail::my_proxy_table();
+    if (table.count >= CHARE_TYPE_CNT_MAX) {
+      detail::report_error(detail::ERR_TOO_MANY_TYPES, table.count, 0);
+      return;
+    }
+    id = table.count++;
+    table.proxies[id] = this;
+    entry_methods = new entry_method_base<C>*[EM_CNT_MAX];
+    if (entry_methods == nullptr) detail::report_error(detail::ERR_NO_MEMORY, id, 0);
+  }
+
+  // Add entry method to table (single-threaded)
+  template <void Func(C&, void*)>
+  __device__ void add_entry_method() {
+    if (entry_methods == nullptr || em_count >= EM_CNT_MAX) {
+      detail::report_error(detail::ERR_TOO_MANY_EMS, id, em_count);
+      return;
+    }
+    entry_method_base<C>* em = new entry_method<C, Func>();
+    if (em == nullptr) {
+      detail::report_error(detail::ERR_NO_MEMORY, id, em_count);
+      return;
+    }
+    entry_methods[em_count++] = em;
+  }
+
+  // Create the chare array on every PE (single-threaded; called by each PE).
+  // Default block mapping: n / n_pes per PE, the first n % n_pes PEs get one
+  // more; with block_map, block_map[pe] chares go to PE pe, in order
+  // (include/chare.h:125-177).
+  __device__ void create(int n_chares, int* block_map) {
+    int n_pes_ = c_n_pes;
+    int me = charm::my_pe();
+
+    loc_map = new int[n_chares > 0 ? n_chares : 1];
+    if (loc_map == nullptr) {
+      detail::report_error(detail::ERR_NO_MEMORY, id, n_chares);
+      return;
+    }
+    n_total = n_chares;
+
+    int n_chares_pe = n_chares / n_pes_;
+    int rem = n_chares % n_pes_;
+    int start = 0;
+    for (int pe = 0; pe < n_pes_; pe++) {
+      int n_cur = block_map ? block_map[pe] : n_chares_pe;
+      if (!block_map && pe < rem) n_cur++;
+      int end = start + n_cur - 1;
+
+      if (pe == me) {
+        n_local = n_cur;
+        start_idx = start;
+        end_idx = end;
+        objects = (n_local > 0) ? new C*[n_local] : nullptr;
+        refnum = (n_local > 0) ? new int[n_local] : nullptr;
+        if (n_local > 0 && (objects == nullptr || refnum == nullptr)) {
+          detail::report_error(detail::ERR_NO_MEMORY, id, n_local);
+          n_local = 0;
+        }
+        for (int k = 0; k < n_local; k++) {
+          objects[k] = new C;
+          if (objects[k] == nullptr) {
+            detail::report_error(detail::ERR_NO_MEMORY, id, k);
+            n_local = k;
+            break;
+          }
+          objects[k]->i = start_idx + k;
+          objects[k]->n = n_total;
+          refnum[k] = -1;
+        }
+      }
+      for (int i = start; i <= end && i < n_chares; i++) loc_map[i] = pe;
+      start += n_cur;
+    }
+  }
+
+  inline __device__ void create(int n_chares) { create(n_chares, nullptr); }
+
+  __device__ virtual bool call(int idx, int ep, void* arg, int ref) {
+    int local_idx = idx - start_idx;
+    if (ref != -1 && ref != refnum[local_idx]) return false;
+    (*(entry_methods[ep]))(*(objects[local_idx]), arg);
+    return true;
+  }
+
+  __device__ virtual void release_all() {
+    for (int k = 0; k < n_local; k++) delete objects[k];
+    delete[] objects;
+    delete[] refnum;
+    delete[] loc_map;
+    if (entry_methods) {
+      for (int e = 0; e < em_count; e++) delete entry_methods[e];
+      delete[] entry_methods;
+    }
+    objects = nullptr;
+    refnum = nullptr;
+    loc_map = nullptr;
+    entry_methods = nullptr;
+    n_local = 0;
+    em_count = 0;
+  }
+
+  // Local object of chare idx, or nullptr if it lives on another PE.
+  __device__ C* local(int idx) const {
+    return (idx >= start_idx && idx <= end_idx) ? objects[idx - start_idx] : nullptr;
+  }
+
+  // Block-collective sends (include/chare.h:197-210). `buf` is copied before
+  // the call returns and may be reused at once.
+  inline __device__ void invoke(int idx, int ep) { invoke(idx, ep, nullptr, 0); }
+  inline __device__ void invoke(int idx, int ep, void* buf, size_t size) {
+    invoke(idx, ep, buf, size, -1);
+  }
+  inline __device__ void invoke(int idx, int ep, void* buf, size_t size, int ref) {
+    if (idx < 0 || idx >= n_total) {
+      if (threadIdx.x == 0) detail::report_error(detail::ERR_BAD_TARGET, id, idx);
+      return;
+    }
+    send_reg_msg(id, idx, ep, buf, size, loc_map[idx], ref);
+  }
+
+  inline __device__ void invoke_all(int ep) { invoke_all(ep, nullptr, 0); }
+  inline __device__ void invoke_all(int ep, void* buf, size_t size) {
+    for (int i = 0; i < n_total; i++) invoke(i, ep, buf, size);
+  }
+
+  // Zero-copy messages (the reference's TODO user-message API,
+  // include/chare.h:255-269). Block-collective.
+  inline __device__ bool alloc_msg(message& msg, int idx, size_t size) {
+    if (idx < 0 || idx >= n_total) {
+      if (threadIdx.x == 0) detail::report_error(detail::ERR_BAD_TARGET, id, idx);
+      return false;
+    }
+    return alloc_user_msg(msg, loc_map[idx], size);
+  }
+  inline __device__ void invoke(int idx, int ep, message& msg) {
+    send_user_msg(id, idx, ep, msg, msg.capacity, -1);
+  }
+  inline __device__ void invoke(int idx, int ep, message& msg, size_t size) {
+    send_user_msg(id, idx, ep, msg, size, -1);
+  }
+  inline __device__ void invoke(int idx, int ep, message& msg, size_t size, int ref) {
+    send_user_msg(id, idx, ep, msg, size, ref);
+  }
+  inline __device__ void free_msg(message& msg) {}
+
+  // Single-threaded (include/chare.h:243-253)
+  inline __device__ void set_refnum(int idx, int val) {
+    if (idx < start_idx || idx > end_idx) {
+      detail::report_error(detail::ERR_BAD_TARGET, id, idx);
+      return;
+    }
+    refnum[idx - start_idx] = val;
+    revive_mismatches(id, idx, val);
+  }
+  inline __device__ int get_refnum(int idx) const { return refnum[idx - start_idx]; }
+};
+
+} // namespace charm
+
+#endif // _CHARE_H_

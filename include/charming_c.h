@@ -1,0 +1,256 @@
+/* charming-b200 C ABI.
+ *
+ * Plain C entry points over the single-GPU runtime: plain pointers and sizes,
+ * no CUDA or torch types. Every function returns an int status
+ * (CHARMING_OK == 0) unless stated otherwise.
+ *
+ * The reference (minitu/charming) has no C ABI: its only host entry is the
+ * process main() in src/charming.cu:50-263 that every example links, so
+ * each entry point below names the part of that function (or of the example
+ * programs) it replaces.
+ */
+#ifndef CHARMING_C_H_
+#define CHARMING_C_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (device error words and host failures) ---------------- */
+enum {
+  CHARMING_OK = 0,
+  CHARMING_ERR_RING_FULL = 1,       /* no inbox space within the wait limit   */
+  CHARMING_ERR_STASH_FULL = 2,      /* refnum stash out of descriptors/bytes  */
+  CHARMING_ERR_BAD_TARGET = 3,      /* invalid chare array / index / entry    */
+  CHARMING_ERR_BARRIER_TIMEOUT = 4, /* a PE did not reach a barrier in time   */
+  CHARMING_ERR_IDLE_TIMEOUT = 5,    /* nothing delivered anywhere for too long*/
+  CHARMING_ERR_DEADLINE = 6,        /* run exceeded its deadline              */
+  CHARMING_ERR_BAD_MSG = 7,         /* malformed message in an inbox          */
+  CHARMING_ERR_MSG_TOO_LARGE = 8,   /* message larger than max_msg_bytes      */
+  CHARMING_ERR_HOST_STOP = 9,       /* stopped by the host                    */
+  CHARMING_ERR_TOO_MANY_TYPES = 10, /* > CHARE_TYPE_CNT_MAX proxies on a PE   */
+  CHARMING_ERR_TOO_MANY_EMS = 11,   /* > EM_CNT_MAX entry methods             */
+  CHARMING_ERR_PIPELINE = 12,       /* bulk-copy pipeline wait ran out        */
+  CHARMING_ERR_LAUNCH = 13,         /* scheduler launch failed                */
+  CHARMING_ERR_CONFIG = 14,         /* invalid configuration or argument      */
+  CHARMING_ERR_CUDA = 15,           /* CUDA runtime error (see last_error)    */
+  CHARMING_ERR_NOT_INIT = 16,       /* charming_init() not called             */
+  CHARMING_ERR_NO_MEMORY = 17,      /* allocation or HBM budget exhausted     */
+  CHARMING_ERR_APP = 18             /* built-in program reported a failure    */
+};
+
+/* ---- runtime ------------------------------------------------------------ */
+
+/* Runtime configuration. Replaces the constants and limits fixed in the
+ * reference's main (src/charming.cu:85-100 topology, :197-203 limits,
+ * :207-209 grid) and transport (src/comm/get/get.cu:20-32 buffer sizes). */
+typedef struct charming_config {
+  int device;               /* CUDA device ordinal                           */
+  int pes_per_sm;           /* PE thread blocks per SM (1 or 2)              */
+  int threads_per_pe;       /* threads per PE block, multiple of 32, <= 512  */
+  int n_pes;                /* 0: SMs * pes_per_sm                           */
+  uint64_t ring_bytes;      /* inbox ring bytes per PE (power of two)        */
+  uint64_t max_msg_bytes;   /* largest message incl. 32-byte header          */
+  uint64_t stash_bytes;     /* refnum stash arena bytes per PE               */
+  int stash_entries;        /* refnum stash descriptors per PE               */
+  uint64_t heap_bytes;      /* device malloc heap (chare objects)            */
+  uint64_t stack_bytes;     /* per-thread stack                              */
+  double deadline_s;        /* hard limit on one scheduler run               */
+  double idle_timeout_s;    /* stop if no message is delivered for this long */
+  int free_chares_at_exit;  /* delete proxies/chares when a run ends         */
+  int verbose;              /* print the configuration (PINFO) on init       */
+} charming_config;
+
+/* Fills *cfg with defaults (148 PEs on a B200, 512 threads, 4 MiB rings). */
+void charming_default_config(charming_config* cfg);
+
+/* Device setup, buffer allocation, constants. Replaces src/charming.cu:50-231
+ * (NVSHMEM/MPI init, proxy tables, limits, comm_init_host). */
+int charming_init(const charming_config* cfg);
+
+/* Runs charm::main on every PE and then the scheduler until charm::end(),
+ * an error, or a limit. One cooperative launch of the persistent scheduler
+ * kernel. Replaces src/charming.cu:146-169 (argv to device) and :234-244
+ * (collective launch + sync). */
+int charming_run(int argc, char** argv);
+
+/* Releases everything charming_init allocated (src/charming.cu:250-261). */
+int charming_fini(void);
+
+/* Effective configuration after init (n_pes, threads, smem bytes). */
+typedef struct charming_info {
+  int n_pes;
+  int n_sms;
+  int threads_per_pe;
+  int smem_bytes_per_pe;     /* dynamic shared memory per PE block       */
+  int smem_scratch_bytes;    /* of which available to entry methods      */
+  int regs_per_thread;       /* of the scheduler kernel                  */
+  uint64_t ring_bytes;
+  uint64_t max_msg_bytes;    /* largest message incl. 32-byte header     */
+  uint64_t device_bytes;     /* runtime buffers on the device            */
+} charming_info;
+int charming_get_info(charming_info* out);
+
+/* Statistics of the last run, summed over PEs. */
+typedef struct charming_stats {
+  uint64_t delivered;        /* entry methods run                        */
+  uint64_t sent;             /* messages sent                            */
+  uint64_t stashed;          /* messages parked on refnum mismatch       */
+  uint64_t revived;          /* parked messages made deliverable         */
+  uint64_t bytes_sent;       /* payload bytes                            */
+  uint64_t idle_polls;       /* empty inbox polls                        */
+  uint64_t space_waits;      /* sends that waited for ring space         */
+  double kernel_ms;          /* CUDA-event time of the scheduler launch  */
+  double loop_ms;            /* max over PEs of time in the loop         */
+  int status;                /* status code of the run                   */
+  int err_pe, err_info0, err_info1;
+} charming_stats;
+int charming_last_stats(charming_stats* out);
+
+/* Message for a status code (static string). */
+const char* charming_status_string(int code);
+/* Last host-side CUDA error text (static buffer, may be empty). */
+const char* charming_last_error(void);
+
+/* ---- built-in programs (libcharming_b200.so) ---------------------------- */
+enum { CHARMING_F64 = 0, CHARMING_F32 = 1 };
+
+/* One Dirichlet problem on an (ny+2) x (nx+2) grid whose outer ring holds
+ * fixed boundary values. Replaces the parameters of the reference's
+ * examples/jacobi2d/jacobi2d.cu:26-85 (grid size, chare count, iterations). */
+typedef struct charming_jacobi_problem {
+  int nx, ny;          /* interior columns, rows                            */
+  int px, py;          /* chares along x (columns) and y (rows); 0: auto    */
+  int max_sweeps;      /* sweeps to run (cap when tol > 0)                  */
+  int check_every;     /* residual check period in sweeps (0: none)         */
+  double tol;          /* stop when ||r_k|| / ||r_0|| <= tol (0: never)      */
+  double bc[4];        /* boundary values: top, bottom, left, right         */
+} charming_jacobi_problem;
+
+typedef struct charming_jacobi_options {
+  int dtype;           /* CHARMING_F64, or CHARMING_F32 sweeps with an FP64
+                          residual                                          */
+  int chare_side;      /* auto decomposition: target chare side (0: 256)    */
+  int tile_w;          /* sweep tile width in elements (0: default)         */
+  int pipeline;        /* 1: TMA bulk-copy row pipeline, 0: direct loads    */
+  int use_graph;       /* 1: replay each run from a captured CUDA graph     */
+  int balance;         /* 1: place chares by work (greedy), 0: block map    */
+} charming_jacobi_options;
+
+typedef struct charming_jacobi_result {
+  int sweeps;          /* sweeps performed                                  */
+  int checks;          /* residual checks performed                         */
+  double res0;         /* ||S(u_0) - u_0||_2 (FP64)                          */
+  double res_last;     /* last checked residual norm                        */
+} charming_jacobi_result;
+
+typedef struct charming_jacobi_info {
+  int n_problems;
+  int n_chares;
+  int max_chares_per_pe;
+  uint64_t interior_points;   /* sum of nx*ny                              */
+  uint64_t grid_bytes;        /* device bytes of all chare grids           */
+  uint64_t halo_msgs_per_sweep;
+  double last_run_ms;         /* CUDA-event time of the last run           */
+} charming_jacobi_info;
+
+/* Decomposes the problems into chares (reference decomposition:
+ * examples/jacobi2d/jacobi2d.cu:37-65) and allocates their grids. */
+int charming_jacobi2d_create(const charming_jacobi_problem* probs, int n,
+    const charming_jacobi_options* opt, void** handle);
+/* Device-side initial state: boundary ring from bc[], interior 0. */
+int charming_jacobi2d_init(void* handle);
+/* Host grid ((ny+2)*(nx+2) values of the problem's dtype, row-major with the
+ * boundary ring) -> chare blocks on the device. */
+int charming_jacobi2d_load(void* handle, int prob, const void* host_grid);
+/* Runs every problem to completion in one persistent scheduler launch. The
+ * chare logic follows examples/jacobi2d/jacobi2d.cu:93-279 with halos tagged
+ * refnum = sweep. */
+int charming_jacobi2d_run(void* handle);
+/* Chare blocks -> host grid (same layout as load). */
+int charming_jacobi2d_store(void* handle, int prob, void* host_grid);
+int charming_jacobi2d_result(void* handle, int prob, charming_jacobi_result* out);
+int charming_jacobi2d_get_info(void* handle, charming_jacobi_info* out);
+int charming_jacobi2d_destroy(void* handle);
+
+/* 1-D Jacobi chares (examples/jacobi1d/jacobi1d.cu:62-170): n_chares blocks
+ * of `width` points, 5-point window sum/5, boundary 10 and interior 0 as in
+ * that example; result is the (n_chares*width + 4)-point array. */
+int charming_jacobi1d(int n_chares, int width, int sweeps, double* host_out,
+    double* out_ms);
+
+/* Pingpong between chares on PEs 0 and n_pes/2 (examples/pingpong/
+ * pingpong.cu:17-217). Payload bytes are a seeded SplitMix64 stream; with
+ * verify=1 every received payload is checksummed and compared. */
+typedef struct charming_pingpong_result {
+  uint64_t size;
+  double oneway_us;          /* mean one-way latency                     */
+  double oneway_cycles;      /* same, in SM clock cycles                 */
+  uint64_t checksum_errors;
+} charming_pingpong_result;
+int charming_pingpong(const uint64_t* sizes, int n_sizes, int round_trips,
+    int warmup, uint64_t seed, int verify, charming_pingpong_result* out,
+    int* sm_pair);
+
+/* Fan-out: n_chares chares each send msgs_per_chare messages of payload_bytes
+ * to seeded destinations. mode 0: refnum -1 (plain FIFO); mode 1: message k
+ * carries refnum k and receivers advance their refnum after the expected
+ * count. log receives one record per delivery: {dst, src, k, refnum,
+ * seq_at_dst, checksum_lo, checksum_hi, pad} (8 x uint32). */
+int charming_fanout(int n_chares, int msgs_per_chare, int payload_bytes,
+    uint64_t seed, int mode, uint32_t* log, uint64_t log_capacity,
+    uint64_t* n_logged, double* out_ms);
+
+/* Hello chain (examples/hello/hello.cu): 2*n_pes chares pass an int along;
+ * out[i] = value received by chare i. */
+int charming_hello(int* out, int n_out, int* n_chares);
+
+/* Refnum scenario (examples/refnum/refnum.cu:27-53, made to terminate):
+ * out receives the refnums in the order chare 1 delivered them. */
+int charming_refnum(int* out, int n_out, int* n_delivered);
+/* Same with the two sends swapped: the refnum-0 message arrives first and is
+ * parked in the stash until chare 1 moves to refnum 0. Expected out: 1, 0. */
+int charming_refnum_reversed(int* out, int n_out, int* n_delivered);
+
+/* ---- serving ------------------------------------------------------------ */
+typedef struct charming_serve_config {
+  uint64_t hbm_budget_bytes; /* grids admitted at once must fit in this    */
+  int max_inflight;          /* device problem slots                       */
+  int workers_per_pe;        /* solver chares per PE                       */
+  int chare_side;            /* requests are cut into chares of this side  */
+  int dtype;                 /* CHARMING_F32 (FP64 residual) or F64        */
+  double deadline_s;         /* server lifetime limit                      */
+} charming_serve_config;
+
+typedef struct charming_serve_completion {
+  uint64_t tag;
+  int status;
+  int sweeps;
+  double res0, res_last;
+  double submit_s, admit_s, done_s;   /* host clock (seconds)             */
+} charming_serve_completion;
+
+typedef struct charming_serve_stats {
+  uint64_t submitted, admitted, completed;
+  uint64_t peak_bytes;
+  int peak_inflight;
+  double busy_s;
+} charming_serve_stats;
+
+int charming_serve_start(const charming_serve_config* cfg, void** server);
+int charming_serve_submit(void* server, const charming_jacobi_problem* req,
+    uint64_t tag);
+int charming_serve_poll(void* server, charming_serve_completion* out,
+    int max_n, int* n_out);
+int charming_serve_fetch(void* server, uint64_t tag, void* host_grid);
+int charming_serve_release(void* server, uint64_t tag);
+int charming_serve_stop(void* server, charming_serve_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CHARMING_C_H_ */
