@@ -114,6 +114,8 @@ SIGNATURES = [
     ("charming_init", i32, [C.POINTER(Config)]),
     ("charming_run", i32, [i32, C.POINTER(C.c_char_p)]),
     ("charming_fini", i32, []),
+    ("charming_timer_start", i32, []),
+    ("charming_timer_stop", i32, [C.POINTER(f64)]),
     ("charming_get_info", i32, [C.POINTER(Info)]),
     ("charming_last_stats", i32, [C.POINTER(Stats)]),
     ("charming_status_string", C.c_char_p, [i32]),

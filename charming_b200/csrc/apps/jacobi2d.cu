@@ -1,2 +1,388 @@
+// Jacobi2d chares: the scenario of the reference's examples/jacobi2d
+// (jacobi2d.cu:93-279) on this runtime, for many problems at once.
+//
+// Per chare and sweep: receive one halo per neighbour (refnum = sweep, which
+// closes the reference's ghost race, jacobi2d.cu:171-190 / :222), sweep the
+// block (jacobi_sweep.cuh), then pack the new boundary rows/columns straight
+// into the neighbours' inbox rings (zero-copy messages) with refnum = sweep+1.
+// Optional FP64 residual every `check_every` sweeps: each chare's partial
+// goes up a binary tree over the problem's chares (fixed summation order, so
+// the norm is bit-reproducible) and the stop decision comes back down. The
+// decision for the check taken at sweep cK is applied at sweep (c+1)K, which
+// leaves K sweeps for the round trip.
 #include "suite.cuh"
-__device__ void suite::jacobi2d_main(int pe) { if (threadIdx.x == 0 && pe == 0) charm::end(); }
+#include "jacobi_types.cuh"
+#include "jacobi_sweep.cuh"
+
+namespace {
+
+enum : int { EP_START = 0, EP_HALO = 1, EP_CONT = 2, EP_PARTIAL = 3, EP_DECISION = 4 };
+
+// g_app fields of this program.
+struct japp {
+  __device__ static int n_chares() { return (int)g_app.a[0]; }
+  __device__ static int dtype() { return (int)g_app.a[2]; }
+  __device__ static int pipeline() { return (int)g_app.a[3]; }
+  __device__ static int tile_w() { return (int)g_app.a[4]; }
+  __device__ static const jac::chare_desc* chares() {
+    return reinterpret_cast<const jac::chare_desc*>(g_app.p[0]);
+  }
+  __device__ static const jac::prob_desc* probs() {
+    return reinterpret_cast<const jac::prob_desc*>(g_app.p[1]);
+  }
+  __device__ static jac::prob_result* results() {
+    return reinterpret_cast<jac::prob_result*>(g_app.p[2]);
+  }
+  __device__ static unsigned long long* done_counter() {
+    return reinterpret_cast<unsigned long long*>(g_app.p[3]);
+  }
+  __device__ static int* final_buf() { return reinterpret_cast<int*>(g_app.p[4]); }
+  __device__ static const int* block_map() { return reinterpret_cast<const int*>(g_app.p[5]); }
+};
+
+struct JBlock : charm::chare {
+  int iter;          // sweeps completed; buf[cur] holds u_iter
+  int cur;
+  int got;           // halos received for sweep `iter`
+  int nbr_count;
+  int done;
+  int waiting;       // parked until the decision of check iter/K - 1 arrives
+  // residual tree state for the check in progress
+  int have_own;
+  int child_got[2];
+  double own;
+  double child_val[2];
+  int decided;       // highest check with a known decision (-1: none)
+  int stop_check;    // check whose decision was "stop" (-1: none)
+  double res0, res_last;
+  int checks;
+  __device__ JBlock()
+      : iter(0), cur(0), got(0), nbr_count(0), done(0), waiting(0), have_own(0), own(0.0),
+        decided(-1), stop_check(-1), res0(0.0), res_last(0.0), checks(0) {
+    child_got[0] = child_got[1] = 0;
+    child_val[0] = child_val[1] = 0.0;
+  }
+};
+
+__shared__ charm::chare_proxy<JBlock>* jproxy;
+
+template <typename T>
+__device__ jac::block_view<T> view(const jac::chare_desc& d, int b) {
+  return jac::block_view<T>{reinterpret_cast<T*>(d.buf[b]), d.pitch};
+}
+
+// One sweep buf[cur] -> buf[cur^1]; returns the block's residual sum (FP64,
+// deterministic) when resid is set. All threads.
+template <typename T>
+__device__ double sweep_block(const jac::chare_desc& d, int cur, bool resid) {
+  jac::block_view<T> in = view<T>(d, cur), out = view<T>(d, cur ^ 1);
+  double acc = 0.0;
+  bool done = false;
+  if (japp::pipeline()) {
+    size_t sb = 0;
+    void* sm = charm::smem_scratch(&sb);
+    jac::tma_plan P;
+    if (jac::make_plan<T>(d.w, blockDim.x, sb, japp::tile_w(), &P)) {
+      if (resid) jac::sweep_tma<T, true>(in, out, d.w, d.h, sm, sb, P, &acc);
+      else jac::sweep_tma<T, false>(in, out, d.w, d.h, sm, sb, P, &acc);
+      done = true;
+    }
+  }
+  if (!done) {
+    __syncthreads();
+    acc = resid ? jac::sweep_direct<T, true>(in, out, d.w, d.h)
+                : jac::sweep_direct<T, false>(in, out, d.w, d.h);
+    __syncthreads();
+  }
+  return resid ? suite::block_sum_f64(acc) : 0.0;
+}
+
+// Packs the boundary of buf[cur] for direction dir into a zero-copy message
+// to the neighbour and sends it with refnum = iter. All threads.
+template <typename T>
+__device__ void send_halo(JBlock& c, const jac::chare_desc& d, int dir) {
+  int nbr = d.nbr[dir];
+  int len = (dir == jac::TOP || dir == jac::BOTTOM) ? d.w : d.h;
+  size_t bytes = sizeof(jac::halo_hdr) + (size_t)len * sizeof(T);
+  charm::message msg;
+  if (!jproxy->alloc_msg(msg, nbr, bytes)) return;
+  char* pl = reinterpret_cast<char*>(msg.payload());
+  T* vals = reinterpret_cast<T*>(pl + sizeof(jac::halo_hdr));
+  jac::block_view<T> g = view<T>(d, c.cur);
+  if (threadIdx.x == 0) {
+    jac::halo_hdr* hh = reinterpret_cast<jac::halo_hdr*>(pl);
+    hh->dir = jac::opposite(dir);
+    hh->len = len;
+    hh->iter = c.iter;
+    hh->pad = 0;
+  }
+  if (dir == jac::TOP || dir == jac::BOTTOM) {
+    int r = (dir == jac::TOP) ? 1 : d.h;
+    charm::copy_cooperative(vals, g.at(r, 1), (size_t)len * sizeof(T), threadIdx.x, blockDim.x);
+  } else {
+    int col = (dir == jac::LEFT) ? 1 : d.w;
+    for (int i = threadIdx.x; i < len; i += blockDim.x) vals[i] = *g.at(1 + i, col);
+  }
+  jproxy->invoke(nbr, EP_HALO, msg, bytes, c.iter);
+}
+
+template <typename T>
+__device__ void send_halos(JBlock& c, const jac::chare_desc& d) {
+  for (int dir = 0; dir < 4; dir++) {
+    if (d.nbr[dir] >= 0) send_halo<T>(c, d, dir);
+  }
+}
+
+template <typename T>
+__device__ void unpack_halo(JBlock& c, const jac::chare_desc& d, const void* arg) {
+  const jac::halo_hdr* hh = reinterpret_cast<const jac::halo_hdr*>(arg);
+  const T* vals = reinterpret_cast<const T*>(reinterpret_cast<const char*>(arg) + sizeof(jac::halo_hdr));
+  jac::block_view<T> g = view<T>(d, c.cur);
+  int dir = hh->dir, len = hh->len;
+  if (dir == jac::TOP || dir == jac::BOTTOM) {
+    int r = (dir == jac::TOP) ? 0 : d.h + 1;
+    charm::copy_cooperative(g.at(r, 1), vals, (size_t)len * sizeof(T), threadIdx.x, blockDim.x);
+  } else {
+    int col = (dir == jac::LEFT) ? 0 : d.w + 1;
+    for (int i = threadIdx.x; i < len; i += blockDim.x) *g.at(1 + i, col) = vals[i];
+  }
+}
+
+
+// All threads. Marks the chare done; the last chare of all problems ends the
+// run (the reference counts "end" messages at chare 0, jacobi2d.cu:274-279).
+__device__ void finish(JBlock& c, const jac::chare_desc& d) {
+  __shared__ int s_last;
+  if (threadIdx.x == 0) {
+    c.done = 1;
+    japp::final_buf()[c.i] = c.cur;
+    const jac::prob_desc& p = japp::probs()[d.prob];
+    if (p.root == c.i) {
+      jac::prob_result& r = japp::results()[d.prob];
+      r.sweeps = c.iter;
+      r.checks = c.checks;
+      r.res0 = c.res0;
+      r.res_last = c.res_last;
+    }
+    __threadfence();
+    unsigned long long n = atomicAdd(japp::done_counter(), 1ULL) + 1;
+    s_last = (n == (unsigned long long)japp::n_chares()) ? 1 : 0;
+  }
+  __syncthreads();
+  if (s_last) charm::end();
+}
+
+template <typename T>
+__device__ void proceed(JBlock& c, const jac::chare_desc& d);
+
+// All threads: record the decision of check `chk`, pass it down the tree,
+// and resume the chare if it was parked on it.
+template <typename T>
+__device__ void apply_decision(JBlock& c, const jac::chare_desc& d, const jac::decision_msg& m) {
+  __shared__ int s_resume;
+  if (threadIdx.x == 0) {
+    if (m.check > c.decided) c.decided = m.check;
+    if (m.stop && c.stop_check < 0) c.stop_check = m.check;
+    c.res0 = m.res0;
+    c.res_last = m.res;
+    c.checks = m.check + 1;
+    s_resume = c.waiting;
+  }
+  __syncthreads();
+  jac::decision_msg fwd = m;
+  for (int k = 0; k < 2; k++) {
+    if (d.child[k] >= 0) jproxy->invoke(d.child[k], EP_DECISION, &fwd, sizeof(fwd));
+  }
+  if (s_resume) proceed<T>(c, d);
+}
+
+// All threads: when this chare's partial and its children's are in, send
+// the sum up (fixed order: own, child 0, child 1) or decide at the root.
+template <typename T>
+__device__ void tree_try_forward(JBlock& c, const jac::chare_desc& d, int chk) {
+  __shared__ int s_act;
+  __shared__ double s_total;
+  if (threadIdx.x == 0) {
+    s_act = 0;
+    bool complete = c.have_own && (d.child[0] < 0 || c.child_got[0]) &&
+                    (d.child[1] < 0 || c.child_got[1]);
+    if (complete) {
+      double t = c.own;
+      if (d.child[0] >= 0) t += c.child_val[0];
+      if (d.child[1] >= 0) t += c.child_val[1];
+      s_total = t;
+      s_act = d.parent < 0 ? 2 : 1;
+      c.have_own = 0;
+      c.child_got[0] = c.child_got[1] = 0;
+    }
+  }
+  __syncthreads();
+  int act = s_act;
+  double total = s_total;
+  __syncthreads();
+  if (act == 1) {
+    jac::partial_msg pm;
+    pm.check = chk;
+    pm.slot = (d.rank - 1) % 2;
+    pm.value = total;
+    jproxy->invoke(d.parent, EP_PARTIAL, &pm, sizeof(pm));
+  } else if (act == 2) {
+    const jac::prob_desc& p = japp::probs()[d.prob];
+    jac::decision_msg m;
+    double nrm = sqrt(total);
+    m.check = chk;
+    m.res0 = (chk == 0) ? nrm : c.res0;
+    m.res = nrm;
+    m.stop = (p.tol > 0.0) && (m.res0 == 0.0 || nrm <= p.tol * m.res0) ? 1 : 0;
+    apply_decision<T>(c, d, m);
+  }
+}
+
+// All threads: after sweep `iter` completed (or on resume), stop, park, or
+// start the next sweep by sending halos (refnum = iter).
+template <typename T>
+__device__ void proceed(JBlock& c, const jac::chare_desc& d) {
+  const jac::prob_desc& p = japp::probs()[d.prob];
+  __shared__ int s_act;
+  enum { CONT = 0, WAIT = 1, FIN = 2 };
+  if (threadIdx.x == 0) {
+    int act = CONT;
+    int K = p.check_every;
+    if (c.iter >= p.max_sweeps) {
+      act = FIN;
+    } else if (K > 0 && c.iter >= K && c.iter % K == 0) {
+      int need = c.iter / K - 1;
+      if (c.decided < need) act = WAIT;
+      else if (c.stop_check >= 0 && c.stop_check <= need) act = FIN;
+    }
+    c.waiting = (act == WAIT) ? 1 : 0;
+    if (act == CONT && c.nbr_count > 0) jproxy->set_refnum(c.i, c.iter);
+    s_act = act;
+  }
+  __syncthreads();
+  int act = s_act;
+  __syncthreads();
+  if (act == FIN) {
+    finish(c, d);
+  } else if (act == CONT) {
+    if (c.nbr_count > 0) {
+      send_halos<T>(c, d);
+    } else {
+      int it = c.iter;
+      jproxy->invoke(c.i, EP_CONT, &it, sizeof(int));
+    }
+  }
+}
+
+// All threads: one sweep, then the residual tree and the next step.
+template <typename T>
+__device__ void advance(JBlock& c, const jac::chare_desc& d) {
+  const jac::prob_desc& p = japp::probs()[d.prob];
+  int K = p.check_every;
+  bool resid = K > 0 && (c.iter % K == 0);
+  double part = sweep_block<T>(d, c.cur, resid);
+  int chk = K > 0 ? c.iter / K : 0;
+  if (threadIdx.x == 0) {
+    c.cur ^= 1;
+    c.iter++;
+    c.got = 0;
+    if (resid) {
+      c.own = part;
+      c.have_own = 1;
+    }
+  }
+  __syncthreads();
+  if (resid) tree_try_forward<T>(c, d, chk);
+  if (!c.done && !c.waiting) proceed<T>(c, d);
+}
+
+template <typename T>
+__device__ void em_start_t(JBlock& c) {
+  const jac::chare_desc& d = japp::chares()[c.i];
+  if (threadIdx.x == 0) {
+    int n = 0;
+    for (int k = 0; k < 4; k++) n += d.nbr[k] >= 0;
+    c.nbr_count = n;
+    c.iter = 0;
+    c.cur = 0;
+    c.got = 0;
+  }
+  __syncthreads();
+  proceed<T>(c, d);
+}
+
+template <typename T>
+__device__ void em_halo_t(JBlock& c, void* arg) {
+  if (c.done) return;
+  const jac::chare_desc& d = japp::chares()[c.i];
+  unpack_halo<T>(c, d, arg);
+  __shared__ int s_go;
+  if (threadIdx.x == 0) {
+    c.got++;
+    s_go = (c.got == c.nbr_count) ? 1 : 0;
+  }
+  __syncthreads();
+  if (s_go) advance<T>(c, d);
+}
+
+template <typename T>
+__device__ void em_cont_t(JBlock& c) {
+  if (c.done) return;
+  advance<T>(c, japp::chares()[c.i]);
+}
+
+template <typename T>
+__device__ void em_partial_t(JBlock& c, void* arg) {
+  if (c.done) return;
+  const jac::chare_desc& d = japp::chares()[c.i];
+  const jac::partial_msg* pm = reinterpret_cast<const jac::partial_msg*>(arg);
+  int chk = pm->check;
+  if (threadIdx.x == 0) {
+    c.child_val[pm->slot] = pm->value;
+    c.child_got[pm->slot] = 1;
+  }
+  __syncthreads();
+  tree_try_forward<T>(c, d, chk);
+}
+
+template <typename T>
+__device__ void em_decision_t(JBlock& c, void* arg) {
+  if (c.done) return;
+  jac::decision_msg m = *reinterpret_cast<const jac::decision_msg*>(arg);
+  __syncthreads();
+  apply_decision<T>(c, japp::chares()[c.i], m);
+}
+
+__device__ void em_start(JBlock& c, void* arg) {
+  if (japp::dtype() == CHARMING_F32) em_start_t<float>(c); else em_start_t<double>(c);
+}
+__device__ void em_halo(JBlock& c, void* arg) {
+  if (japp::dtype() == CHARMING_F32) em_halo_t<float>(c, arg); else em_halo_t<double>(c, arg);
+}
+__device__ void em_cont(JBlock& c, void* arg) {
+  if (japp::dtype() == CHARMING_F32) em_cont_t<float>(c); else em_cont_t<double>(c);
+}
+__device__ void em_partial(JBlock& c, void* arg) {
+  if (japp::dtype() == CHARMING_F32) em_partial_t<float>(c, arg); else em_partial_t<double>(c, arg);
+}
+__device__ void em_decision(JBlock& c, void* arg) {
+  if (japp::dtype() == CHARMING_F32) em_decision_t<float>(c, arg); else em_decision_t<double>(c, arg);
+}
+
+}  // namespace
+
+__device__ void suite::jacobi2d_main(int pe) {
+  if (threadIdx.x == 0) {
+    jproxy = new charm::chare_proxy<JBlock>();
+    jproxy->add_entry_method<&em_start>();
+    jproxy->add_entry_method<&em_halo>();
+    jproxy->add_entry_method<&em_cont>();
+    jproxy->add_entry_method<&em_partial>();
+    jproxy->add_entry_method<&em_decision>();
+    jproxy->create(japp::n_chares(), const_cast<int*>(japp::block_map()));
+  }
+  __syncthreads();
+  if (jproxy->n_local > 0) {
+    for (int i = jproxy->start_idx; i <= jproxy->end_idx; i++) jproxy->invoke(i, EP_START);
+  }
+}

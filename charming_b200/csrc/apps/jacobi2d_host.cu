@@ -1,0 +1,464 @@
+// Host side of the Jacobi2d program: decomposition into chares, placement on
+// PEs, chare grids in HBM, init/load/store kernels and the run (optionally
+// replayed from a captured CUDA graph). C ABI: charming_jacobi2d_*.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <queue>
+#include <vector>
+#include "suite.cuh"
+#include "jacobi_types.cuh"
+#include "jacobi_sweep.cuh"
+#include "../host.cuh"
+
+namespace {
+
+struct JHandle {
+  std::vector<charming_jacobi_problem> probs;
+  charming_jacobi_options opt{};
+  int n_chares = 0;
+  size_t esz = 8;
+  std::vector<jac::chare_desc> chares;     // placed order
+  std::vector<int> block_map;              // chares per PE
+  std::vector<int> chare_of;               // [prob offset + cy*px + cx] -> chare
+  std::vector<size_t> chare_of_off;
+  std::vector<int> px, py;
+  jac::chare_desc* d_chares = nullptr;
+  jac::prob_desc* d_probs = nullptr;
+  jac::prob_result* d_results = nullptr;
+  unsigned long long* d_done = nullptr;
+  int* d_final = nullptr;
+  int* d_block_map = nullptr;
+  int* d_chare_of = nullptr;
+  char* d_grid = nullptr;
+  size_t grid_bytes = 0;
+  void* d_stage = nullptr;
+  size_t stage_bytes = 0;
+  suite::app_params* h_params = nullptr;   // pinned
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms = 0.0;
+  int max_per_pe = 0;
+  uint64_t points = 0, halo_msgs = 0;
+};
+
+template <typename T>
+__device__ __forceinline__ T* cell(const jac::chare_desc& d, int b, int r, int c) {
+  return reinterpret_cast<T*>(d.buf[b]) + (size_t)r * d.pitch + jac::traits<T>::OFF - 1 + c;
+}
+
+// Initial state: boundary ring from bc (top/bottom rows include the corners),
+// interior 0; written to both buffers. One block per chare.
+template <typename T>
+__global__ void init_kernel(const jac::chare_desc* ch, const jac::prob_desc* pr, const double* bc) {
+  const jac::chare_desc d = ch[blockIdx.x];
+  const jac::prob_desc p = pr[d.prob];
+  const double* b = bc + 4 * d.prob;
+  long long n = (long long)(d.h + 2) * (d.w + 2);
+  for (long long x = threadIdx.x; x < n; x += blockDim.x) {
+    int r = (int)(x / (d.w + 2)), c = (int)(x % (d.w + 2));
+    int gy = d.y0 + r, gx = d.x0 + c;
+    double v = 0.0;
+    if (gy == 0) v = b[0];
+    else if (gy == p.ny + 1) v = b[1];
+    else if (gx == 0) v = b[2];
+    else if (gx == p.nx + 1) v = b[3];
+    *cell<T>(d, 0, r, c) = (T)v;
+    *cell<T>(d, 1, r, c) = (T)v;
+  }
+}
+
+// Global grid (ny+2) x (nx+2) in `stage` -> blocks of one problem.
+template <typename T>
+__global__ void scatter_kernel(const jac::chare_desc* ch, const int* chare_of, int nx,
+    const T* stage) {
+  const jac::chare_desc d = ch[chare_of[blockIdx.x]];
+  long long n = (long long)(d.h + 2) * (d.w + 2);
+  for (long long x = threadIdx.x; x < n; x += blockDim.x) {
+    int r = (int)(x / (d.w + 2)), c = (int)(x % (d.w + 2));
+    T v = stage[(size_t)(d.y0 + r) * (nx + 2) + d.x0 + c];
+    *cell<T>(d, 0, r, c) = v;
+    *cell<T>(d, 1, r, c) = v;
+  }
+}
+
+// Blocks of one problem -> global grid: interior cells from their owner,
+// ring cells from the ghost ring of the edge chare next to them.
+template <typename T>
+__global__ void gather_kernel(const jac::chare_desc* ch, const int* chare_of, const int* final_buf,
+    int nx, int ny, int px, int py, T* stage) {
+  long long n = (long long)(nx + 2) * (ny + 2);
+  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < n;
+       x += (long long)gridDim.x * blockDim.x) {
+    int gy = (int)(x / (nx + 2)), gx = (int)(x % (nx + 2));
+    int iy = min(max(gy - 1, 0), ny - 1), ix = min(max(gx - 1, 0), nx - 1);
+    int cy = jac::split_owner(ny, py, iy), cx = jac::split_owner(nx, px, ix);
+    int k = chare_of[cy * px + cx];
+    const jac::chare_desc& d = ch[k];
+    stage[x] = *cell<T>(d, final_buf[k], gy - d.y0, gx - d.x0);
+  }
+}
+
+int fail(int code, const char* msg) {
+  charm_host::set_error_text(msg);
+  return code;
+}
+
+int check_cuda(cudaError_t e, const char* what) { return charm_host::cuda_fail(e, what); }
+
+}  // namespace
+
+extern "C" int charming_jacobi2d_create(const charming_jacobi_problem* probs, int n,
+    const charming_jacobi_options* opt, void** handle) {
+  int rc = charm_host::ensure_init();
+  if (rc) return rc;
+  if (!probs || n <= 0 || !opt || !handle) return fail(CHARMING_ERR_CONFIG, "jacobi2d: bad arguments");
+  if (opt->dtype != CHARMING_F64 && opt->dtype != CHARMING_F32)
+    return fail(CHARMING_ERR_CONFIG, "jacobi2d: dtype");
+  const int n_pes = charm_host::info().n_pes;
+  JHandle* h = new JHandle();
+  h->probs.assign(probs, probs + n);
+  h->opt = *opt;
+  h->esz = opt->dtype == CHARMING_F64 ? 8 : 4;
+  const int V = opt->dtype == CHARMING_F64 ? jac::traits<double>::VEC : jac::traits<float>::VEC;
+  const int OFF = opt->dtype == CHARMING_F64 ? jac::traits<double>::OFF : jac::traits<float>::OFF;
+  const int align_el = (int)(128 / h->esz);
+  const int side = opt->chare_side > 0 ? opt->chare_side : 256;
+
+  // 1. decomposition, problem order
+  std::vector<jac::chare_desc> raw;
+  std::vector<jac::prob_desc> pd(n);
+  std::vector<int> root_raw(n);
+  for (int p = 0; p < n; p++) {
+    const charming_jacobi_problem& q = probs[p];
+    if (q.nx < 1 || q.ny < 1 || q.max_sweeps < 0 || q.check_every < 0) {
+      delete h;
+      return fail(CHARMING_ERR_CONFIG, "jacobi2d: problem size");
+    }
+    int px = q.px > 0 ? q.px : (q.nx + side - 1) / side;
+    int py = q.py > 0 ? q.py : (q.ny + side - 1) / side;
+    if (px > q.nx || py > q.ny) {
+      delete h;
+      return fail(CHARMING_ERR_CONFIG, "jacobi2d: more chares than rows/columns");
+    }
+    h->px.push_back(px);
+    h->py.push_back(py);
+    int base = (int)raw.size();
+    root_raw[p] = base;
+    int nc = px * py;
+    for (int cy = 0; cy < py; cy++) {
+      for (int cx = 0; cx < px; cx++) {
+        jac::chare_desc d{};
+        d.prob = p;
+        d.cx = cx;
+        d.cy = cy;
+        d.x0 = jac::split_start(q.nx, px, cx);
+        d.y0 = jac::split_start(q.ny, py, cy);
+        d.w = jac::split_start(q.nx, px, cx + 1) - d.x0;
+        d.h = jac::split_start(q.ny, py, cy + 1) - d.y0;
+        d.pitch = (OFF + d.w + 2 * V + align_el - 1) / align_el * align_el;
+        int r = cy * px + cx;
+        d.nbr[jac::TOP] = cy > 0 ? base + r - px : -1;
+        d.nbr[jac::BOTTOM] = cy < py - 1 ? base + r + px : -1;
+        d.nbr[jac::LEFT] = cx > 0 ? base + r - 1 : -1;
+        d.nbr[jac::RIGHT] = cx < px - 1 ? base + r + 1 : -1;
+        d.rank = r;
+        d.parent = r > 0 ? base + (r - 1) / 2 : -1;
+        d.child[0] = 2 * r + 1 < nc ? base + 2 * r + 1 : -1;
+        d.child[1] = 2 * r + 2 < nc ? base + 2 * r + 2 : -1;
+        raw.push_back(d);
+        h->halo_msgs += (d.nbr[0] >= 0) + (d.nbr[1] >= 0) + (d.nbr[2] >= 0) + (d.nbr[3] >= 0);
+      }
+    }
+    pd[p].nx = q.nx;
+    pd[p].ny = q.ny;
+    pd[p].px = px;
+    pd[p].py = py;
+    pd[p].max_sweeps = q.max_sweeps;
+    pd[p].check_every = q.check_every;
+    pd[p].tol = q.tol;
+    pd[p].n_chares = nc;
+    h->points += (uint64_t)q.nx * q.ny;
+  }
+  const int nch = (int)raw.size();
+  h->n_chares = nch;
+
+  // 2. placement: chares -> PEs (work-balanced greedy, or the reference's
+  // default block map over problem order, include/chare.h:136-176)
+  std::vector<int> pe_of(nch);
+  h->block_map.assign(n_pes, 0);
+  if (opt->balance) {
+    std::vector<int> order(nch);
+    std::iota(order.begin(), order.end(), 0);
+    auto work = [&](int i) { return (double)raw[i].w * raw[i].h + 4096.0; };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
+    using item = std::pair<double, int>;
+    std::priority_queue<item, std::vector<item>, std::greater<item>> pq;
+    for (int pe = 0; pe < n_pes; pe++) pq.push({0.0, pe});
+    for (int i : order) {
+      item t = pq.top();
+      pq.pop();
+      pe_of[i] = t.second;
+      pq.push({t.first + work(i), t.second});
+    }
+  } else {
+    int per = nch / n_pes, rem = nch % n_pes, k = 0;
+    for (int pe = 0; pe < n_pes; pe++) {
+      int cnt = per + (pe < rem ? 1 : 0);
+      for (int j = 0; j < cnt; j++) pe_of[k++] = pe;
+    }
+  }
+  std::vector<int> perm(nch);  // placed index -> raw index
+  std::iota(perm.begin(), perm.end(), 0);
+  std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return pe_of[a] < pe_of[b]; });
+  std::vector<int> inv(nch);
+  for (int k = 0; k < nch; k++) inv[perm[k]] = k;
+  auto remap = [&](int x) { return x < 0 ? -1 : inv[x]; };
+  h->chares.resize(nch);
+  for (int k = 0; k < nch; k++) {
+    jac::chare_desc d = raw[perm[k]];
+    for (int q = 0; q < 4; q++) d.nbr[q] = remap(d.nbr[q]);
+    d.parent = remap(d.parent);
+    d.child[0] = remap(d.child[0]);
+    d.child[1] = remap(d.child[1]);
+    h->chares[k] = d;
+    h->block_map[pe_of[perm[k]]]++;
+  }
+  for (int p = 0; p < n; p++) pd[p].root = inv[root_raw[p]];
+  h->max_per_pe = *std::max_element(h->block_map.begin(), h->block_map.end());
+  for (int p = 0, off = 0; p < n; p++) {
+    h->chare_of_off.push_back(off);
+    for (int r = 0; r < h->px[p] * h->py[p]; r++) h->chare_of.push_back(inv[root_raw[p] + r]);
+    off += h->px[p] * h->py[p];
+  }
+
+  // 3. grids: two pitched buffers per chare, 256-byte aligned
+  size_t total = 0;
+  std::vector<size_t> off(nch);
+  for (int k = 0; k < nch; k++) {
+    size_t b = ((size_t)h->chares[k].pitch * (h->chares[k].h + 2) * h->esz + 255) / 256 * 256;
+    off[k] = total;
+    total += 2 * b;
+  }
+  h->grid_bytes = total;
+  cudaError_t e = cudaMalloc(&h->d_grid, total);
+  if (e != cudaSuccess) {
+    delete h;
+    return charm_host::cuda_fail(e, "jacobi2d grids");
+  }
+  for (int k = 0; k < nch; k++) {
+    size_t b = ((size_t)h->chares[k].pitch * (h->chares[k].h + 2) * h->esz + 255) / 256 * 256;
+    h->chares[k].buf[0] = h->d_grid + off[k];
+    h->chares[k].buf[1] = h->d_grid + off[k] + b;
+  }
+  e = cudaMalloc(&h->d_chares, sizeof(jac::chare_desc) * nch);
+  if (e == cudaSuccess) e = cudaMalloc(&h->d_probs, sizeof(jac::prob_desc) * n);
+  if (e == cudaSuccess) e = cudaMalloc(&h->d_results, sizeof(jac::prob_result) * n);
+  if (e == cudaSuccess) e = cudaMalloc(&h->d_done, 64);
+  if (e == cudaSuccess) e = cudaMalloc(&h->d_final, sizeof(int) * nch);
+  if (e == cudaSuccess) e = cudaMalloc(&h->d_block_map, sizeof(int) * n_pes);
+  if (e == cudaSuccess) e = cudaMalloc(&h->d_chare_of, sizeof(int) * h->chare_of.size());
+  if (e == cudaSuccess) e = cudaMemcpy(h->d_chares, h->chares.data(), sizeof(jac::chare_desc) * nch, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(h->d_probs, pd.data(), sizeof(jac::prob_desc) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(h->d_results, 0, sizeof(jac::prob_result) * n);
+  if (e == cudaSuccess) e = cudaMemset(h->d_final, 0, sizeof(int) * nch);
+  if (e == cudaSuccess) e = cudaMemcpy(h->d_block_map, h->block_map.data(), sizeof(int) * n_pes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(h->d_chare_of, h->chare_of.data(), sizeof(int) * h->chare_of.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaHostAlloc(&h->h_params, sizeof(suite::app_params), cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaEventCreate(&h->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&h->ev1);
+  if (e != cudaSuccess) {
+    rc = charm_host::cuda_fail(e, "jacobi2d descriptors");
+    charming_jacobi2d_destroy(h);
+    return rc;
+  }
+  suite::app_params& ap = *h->h_params;
+  memset(&ap, 0, sizeof(ap));
+  ap.id = suite::APP_JACOBI2D;
+  ap.a[0] = nch;
+  ap.a[1] = n;
+  ap.a[2] = opt->dtype;
+  ap.a[3] = opt->pipeline;
+  ap.a[4] = opt->tile_w;
+  ap.p[0] = h->d_chares;
+  ap.p[1] = h->d_probs;
+  ap.p[2] = h->d_results;
+  ap.p[3] = h->d_done;
+  ap.p[4] = h->d_final;
+  ap.p[5] = h->d_block_map;
+  *handle = h;
+  return charming_jacobi2d_init(h);
+}
+
+extern "C" int charming_jacobi2d_init(void* handle) {
+  JHandle* h = reinterpret_cast<JHandle*>(handle);
+  if (!h) return CHARMING_ERR_CONFIG;
+  int n = (int)h->probs.size();
+  std::vector<double> bc(4 * n);
+  for (int p = 0; p < n; p++)
+    for (int k = 0; k < 4; k++) bc[4 * p + k] = h->probs[p].bc[k];
+  double* d_bc = nullptr;
+  cudaError_t e = cudaMalloc(&d_bc, sizeof(double) * bc.size());
+  if (e == cudaSuccess) e = cudaMemcpy(d_bc, bc.data(), sizeof(double) * bc.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    if (h->esz == 8) init_kernel<double><<<h->n_chares, 256>>>(h->d_chares, h->d_probs, d_bc);
+    else init_kernel<float><<<h->n_chares, 256>>>(h->d_chares, h->d_probs, d_bc);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  cudaFree(d_bc);
+  if (e == cudaSuccess) e = cudaMemset(h->d_final, 0, sizeof(int) * h->n_chares);
+  return check_cuda(e, "jacobi2d init");
+}
+
+static int ensure_stage(JHandle* h, size_t bytes) {
+  if (h->stage_bytes >= bytes) return CHARMING_OK;
+  if (h->d_stage) cudaFree(h->d_stage);
+  h->d_stage = nullptr;
+  h->stage_bytes = 0;
+  cudaError_t e = cudaMalloc(&h->d_stage, bytes);
+  if (e != cudaSuccess) return check_cuda(e, "jacobi2d staging buffer");
+  h->stage_bytes = bytes;
+  return CHARMING_OK;
+}
+
+extern "C" int charming_jacobi2d_load(void* handle, int prob, const void* host_grid) {
+  JHandle* h = reinterpret_cast<JHandle*>(handle);
+  if (!h || prob < 0 || prob >= (int)h->probs.size() || !host_grid) return CHARMING_ERR_CONFIG;
+  const charming_jacobi_problem& q = h->probs[prob];
+  size_t bytes = (size_t)(q.nx + 2) * (q.ny + 2) * h->esz;
+  int rc = ensure_stage(h, bytes);
+  if (rc) return rc;
+  cudaStream_t s = charm_host::stream();
+  cudaError_t e = cudaMemcpyAsync(h->d_stage, host_grid, bytes, cudaMemcpyHostToDevice, s);
+  int nc = h->px[prob] * h->py[prob];
+  const int* co = h->d_chare_of + h->chare_of_off[prob];
+  if (e == cudaSuccess) {
+    if (h->esz == 8) scatter_kernel<double><<<nc, 256, 0, s>>>(h->d_chares, co, q.nx, (const double*)h->d_stage);
+    else scatter_kernel<float><<<nc, 256, 0, s>>>(h->d_chares, co, q.nx, (const float*)h->d_stage);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->d_final, 0, sizeof(int) * h->n_chares, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return check_cuda(e, "jacobi2d load");
+}
+
+extern "C" int charming_jacobi2d_store(void* handle, int prob, void* host_grid) {
+  JHandle* h = reinterpret_cast<JHandle*>(handle);
+  if (!h || prob < 0 || prob >= (int)h->probs.size() || !host_grid) return CHARMING_ERR_CONFIG;
+  const charming_jacobi_problem& q = h->probs[prob];
+  size_t cells = (size_t)(q.nx + 2) * (q.ny + 2);
+  size_t bytes = cells * h->esz;
+  int rc = ensure_stage(h, bytes);
+  if (rc) return rc;
+  cudaStream_t s = charm_host::stream();
+  const int* co = h->d_chare_of + h->chare_of_off[prob];
+  int blocks = (int)std::min<size_t>((cells + 255) / 256, 4096);
+  if (h->esz == 8)
+    gather_kernel<double><<<blocks, 256, 0, s>>>(h->d_chares, co, h->d_final, q.nx, q.ny,
+        h->px[prob], h->py[prob], (double*)h->d_stage);
+  else
+    gather_kernel<float><<<blocks, 256, 0, s>>>(h->d_chares, co, h->d_final, q.nx, q.ny,
+        h->px[prob], h->py[prob], (float*)h->d_stage);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(host_grid, h->d_stage, bytes, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return check_cuda(e, "jacobi2d store");
+}
+
+// Work of one run on stream s: counters, program parameters, scheduler.
+static int enqueue_run(JHandle* h, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(h->d_done, 0, 64, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->d_results, 0, sizeof(jac::prob_result) * h->probs.size(), s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyToSymbolAsync(g_app, h->h_params, sizeof(suite::app_params), 0,
+                                cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return check_cuda(e, "jacobi2d run setup");
+  return charm_host::enqueue_scheduler(s);
+}
+
+extern "C" int charming_jacobi2d_run(void* handle) {
+  JHandle* h = reinterpret_cast<JHandle*>(handle);
+  if (!h) return CHARMING_ERR_CONFIG;
+  cudaStream_t s = charm_host::stream();
+  charm_host::request_stop(0);
+  int rc;
+  cudaError_t e;
+  if (h->opt.use_graph) {
+    if (!h->graph_exec) {
+      e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) return check_cuda(e, "graph capture begin");
+      rc = enqueue_run(h, s);
+      e = cudaStreamEndCapture(s, &h->graph);
+      if (rc) return rc;
+      if (e != cudaSuccess) return check_cuda(e, "graph capture end");
+      e = cudaGraphInstantiate(&h->graph_exec, h->graph, 0);
+      if (e != cudaSuccess) return check_cuda(e, "graph instantiate");
+    }
+    cudaEventRecord(h->ev0, s);
+    e = cudaGraphLaunch(h->graph_exec, s);
+    if (e != cudaSuccess) return check_cuda(e, "graph launch");
+    cudaEventRecord(h->ev1, s);
+  } else {
+    cudaEventRecord(h->ev0, s);
+    rc = enqueue_run(h, s);
+    if (rc) return rc;
+    cudaEventRecord(h->ev1, s);
+  }
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return check_cuda(e, "jacobi2d run");
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  h->last_ms = ms;
+  return charm_host::collect_run(ms);
+}
+
+extern "C" int charming_jacobi2d_result(void* handle, int prob, charming_jacobi_result* out) {
+  JHandle* h = reinterpret_cast<JHandle*>(handle);
+  if (!h || !out || prob < 0 || prob >= (int)h->probs.size()) return CHARMING_ERR_CONFIG;
+  jac::prob_result r;
+  cudaError_t e = cudaMemcpy(&r, h->d_results + prob, sizeof(r), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return check_cuda(e, "jacobi2d result");
+  out->sweeps = r.sweeps;
+  out->checks = r.checks;
+  out->res0 = r.res0;
+  out->res_last = r.res_last;
+  return CHARMING_OK;
+}
+
+extern "C" int charming_jacobi2d_get_info(void* handle, charming_jacobi_info* out) {
+  JHandle* h = reinterpret_cast<JHandle*>(handle);
+  if (!h || !out) return CHARMING_ERR_CONFIG;
+  out->n_problems = (int)h->probs.size();
+  out->n_chares = h->n_chares;
+  out->max_chares_per_pe = h->max_per_pe;
+  out->interior_points = h->points;
+  out->grid_bytes = h->grid_bytes;
+  out->halo_msgs_per_sweep = h->halo_msgs;
+  out->last_run_ms = h->last_ms;
+  return CHARMING_OK;
+}
+
+extern "C" int charming_jacobi2d_destroy(void* handle) {
+  JHandle* h = reinterpret_cast<JHandle*>(handle);
+  if (!h) return CHARMING_OK;
+  cudaDeviceSynchronize();
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  cudaFree(h->d_grid);
+  cudaFree(h->d_chares);
+  cudaFree(h->d_probs);
+  cudaFree(h->d_results);
+  cudaFree(h->d_done);
+  cudaFree(h->d_final);
+  cudaFree(h->d_block_map);
+  cudaFree(h->d_chare_of);
+  cudaFree(h->d_stage);
+  if (h->h_params) cudaFreeHost(h->h_params);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  delete h;
+  return CHARMING_OK;
+}

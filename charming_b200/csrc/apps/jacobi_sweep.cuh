@@ -281,7 +281,8 @@ __device__ bool sweep_tma(block_view<T> in, block_view<T> out, int w, int h, voi
           const T* up = slots + (size_t)((ibase + r - 1) % P.NS) * P.slot_elems;
           const T* mid = slots + (size_t)((ibase + r) % P.NS) * P.slot_elems;
           const T* dn = slots + (size_t)((ibase + r + 1) % P.NS) * P.slot_elems;
-          for (int v = lane; v < nvec; v += P.tpr) {
+          const int vstride = P.tpr < (int)blockDim.x ? P.tpr : (int)blockDim.x;
+          for (int v = lane; v < nvec; v += vstride) {
             int s = H + v * V;  // slot index of interior column c0 + v*V
             int nvalid = min(V, tw - v * V);
             acc += compute_vec<T, RESID>(up + s, mid + s, dn + s, mid[s - 1], mid[s + V],

@@ -350,6 +350,29 @@ int charming_init(const charming_config* cfg_in) {
 
 int charming_run(int argc, char** argv) { return run_scheduler(argc, argv); }
 
+// Stream-ordered timer over any number of runs: CUDA events recorded on the
+// runtime's stream, so host time between runs counts as idle device time.
+static cudaEvent_t g_timer0 = nullptr, g_timer1 = nullptr;
+
+int charming_timer_start(void) {
+  if (!g.inited) return CHARMING_ERR_NOT_INIT;
+  cudaError_t e = cudaSuccess;
+  if (!g_timer0) e = cudaEventCreate(&g_timer0);
+  if (e == cudaSuccess && !g_timer1) e = cudaEventCreate(&g_timer1);
+  if (e == cudaSuccess) e = cudaEventRecord(g_timer0, g.stream);
+  return cuda_fail(e, "timer start");
+}
+
+int charming_timer_stop(double* ms) {
+  if (!g.inited || !g_timer0) return CHARMING_ERR_NOT_INIT;
+  cudaError_t e = cudaEventRecord(g_timer1, g.stream);
+  if (e == cudaSuccess) e = cudaEventSynchronize(g_timer1);
+  float f = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&f, g_timer0, g_timer1);
+  if (ms) *ms = f;
+  return cuda_fail(e, "timer stop");
+}
+
 int charming_fini(void) {
   if (!g.inited) return CHARMING_OK;
   cudaDeviceSynchronize();

@@ -80,6 +80,13 @@ int charming_run(int argc, char** argv);
 /* Releases everything charming_init allocated (src/charming.cu:250-261). */
 int charming_fini(void);
 
+/* Device time over several runs: CUDA events on the runtime's stream around
+ * everything enqueued between start and stop (the reference times with
+ * device-side clocks inside entry methods, examples/jacobi2d/jacobi2d.cu:
+ * 236-262). */
+int charming_timer_start(void);
+int charming_timer_stop(double* ms);
+
 /* Effective configuration after init (n_pes, threads, smem bytes). */
 typedef struct charming_info {
   int n_pes;
