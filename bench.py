@@ -141,6 +141,12 @@ def choose_decomposition(n_pes: int, nx: int, ny: int) -> tuple[int, int]:
     return (best[1], best[2]) if best else (1, n_pes)
 
 
+def set_workload(n: int, sweeps: int) -> None:
+    global NX, NY, SWEEPS
+    NX = NY = n
+    SWEEPS = sweeps
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -225,7 +231,13 @@ def main() -> int:
     ap.add_argument("--pipeline", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--nx", type=int, default=NX, help="grid size (profiling runs)")
+    ap.add_argument("--sweeps", type=int, default=SWEEPS)
+    ap.add_argument("--tile-w", type=int, default=0)
+    ap.add_argument("--small-buffers", action="store_true",
+                    help="1 MiB inbox rings and stashes (smaller device footprint for ncu)")
     args = ap.parse_args()
+    set_workload(args.nx, args.sweeps)
 
     dist, rank, local, world = dist_setup()
     if args.impl == "reference":
@@ -236,11 +248,15 @@ def main() -> int:
 
     from charming_b200 import runtime
     from charming_b200.jacobi import Jacobi2D, Problem, initial_grid
-    rt = runtime(device=local)
+    cfg = dict(device=local)
+    if args.small_buffers:
+        cfg.update(ring_bytes=1 << 20, stash_bytes=2 << 20, max_msg_bytes=(256 << 10))
+    rt = runtime(**cfg)
     n_pes = rt.n_pes
     px, py = (args.px, args.py) if args.px and args.py else choose_decomposition(n_pes, NX, NY)
     prob = Problem(NX, NY, SWEEPS, px=px, py=py, bc=(1.0, 0.0, 0.0, 0.0))
-    j = Jacobi2D([prob], dtype="f64", pipeline=bool(args.pipeline), balance=True)
+    j = Jacobi2D([prob], dtype="f64", pipeline=bool(args.pipeline), balance=True,
+                 tile_w=args.tile_w)
     lib = rt.lib
     import ctypes as C
 
@@ -310,8 +326,14 @@ def main() -> int:
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(args, (px, py)),
             "msgs_per_s": msgs_per_s, "halo_msgs_per_sweep": info["halo_msgs_per_sweep"],
+            "last_launch": {"ms": info["last_run_ms"], "sweep_ms_max_pe": info["sweep_ms_max"],
+                            "sweep_ms_mean_pe": info["sweep_ms_mean"], "main_ms": stats.main_ms,
+                            "loop_ms": stats.loop_ms, "stashed": stats.stashed,
+                            "delivered": stats.delivered},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": 2 * args.steps, "status": stats.status,
+            "runtime": {k: rt.info[k] for k in ("n_pes", "threads_per_pe", "smem_bytes_per_pe",
+                                                "smem_scratch_bytes", "regs_per_thread")},
         }
         print(json.dumps(line), flush=True)
     j.close()

@@ -12,7 +12,9 @@ import threading
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_DIR = os.path.join(_HERE, "lib")
-LIB_PATH = os.path.join(LIB_DIR, "libcharming_b200.so")
+# CHARMING_CHECKED=1 selects the build with invariant checks (make CHECKS=1).
+LIB_PATH = os.path.join(LIB_DIR, "libcharming_b200_checked.so"
+                        if os.environ.get("CHARMING_CHECKED") == "1" else "libcharming_b200.so")
 
 u64 = C.c_uint64
 i32 = C.c_int
@@ -43,7 +45,8 @@ class Info(C.Structure):
     _fields_ = [
         ("n_pes", i32), ("n_sms", i32), ("threads_per_pe", i32), ("smem_bytes_per_pe", i32),
         ("smem_scratch_bytes", i32), ("regs_per_thread", i32), ("ring_bytes", u64),
-        ("max_msg_bytes", u64), ("device_bytes", u64),
+        ("max_msg_bytes", u64), ("device_bytes", u64), ("stack_bytes", u64),
+        ("local_bytes", u64),
     ]
 
 
@@ -51,7 +54,7 @@ class Stats(C.Structure):
     _fields_ = [
         ("delivered", u64), ("sent", u64), ("stashed", u64), ("revived", u64),
         ("bytes_sent", u64), ("idle_polls", u64), ("space_waits", u64),
-        ("kernel_ms", f64), ("loop_ms", f64), ("status", i32), ("err_pe", i32),
+        ("kernel_ms", f64), ("loop_ms", f64), ("main_ms", f64), ("status", i32), ("err_pe", i32),
         ("err_info0", i32), ("err_info1", i32),
     ]
 
@@ -66,7 +69,7 @@ class JacobiProblem(C.Structure):
 class JacobiOptions(C.Structure):
     _fields_ = [
         ("dtype", i32), ("chare_side", i32), ("tile_w", i32), ("pipeline", i32),
-        ("use_graph", i32), ("balance", i32),
+        ("use_graph", i32), ("balance", i32), ("halo_mode", i32),
     ]
 
 
@@ -78,7 +81,7 @@ class JacobiInfo(C.Structure):
     _fields_ = [
         ("n_problems", i32), ("n_chares", i32), ("max_chares_per_pe", i32),
         ("interior_points", u64), ("grid_bytes", u64), ("halo_msgs_per_sweep", u64),
-        ("last_run_ms", f64),
+        ("last_run_ms", f64), ("sweep_ms_max", f64), ("sweep_ms_mean", f64),
     ]
 
 

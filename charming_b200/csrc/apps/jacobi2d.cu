@@ -24,6 +24,7 @@ struct japp {
   __device__ static int dtype() { return (int)g_app.a[2]; }
   __device__ static int pipeline() { return (int)g_app.a[3]; }
   __device__ static int tile_w() { return (int)g_app.a[4]; }
+  __device__ static int halo_mode() { return (int)g_app.a[5]; }
   __device__ static const jac::chare_desc* chares() {
     return reinterpret_cast<const jac::chare_desc*>(g_app.p[0]);
   }
@@ -38,12 +39,18 @@ struct japp {
   }
   __device__ static int* final_buf() { return reinterpret_cast<int*>(g_app.p[4]); }
   __device__ static const int* block_map() { return reinterpret_cast<const int*>(g_app.p[5]); }
+  // per-PE nanoseconds spent in sweeps during the run
+  __device__ static unsigned long long* sweep_ns() {
+    return reinterpret_cast<unsigned long long*>(g_app.p[6]);
+  }
 };
 
 struct JBlock : charm::chare {
-  int iter;          // sweeps completed; buf[cur] holds u_iter
+  int iter;          // sweeps completed; buf[cur] holds u_iter (cur == iter & 1)
   int cur;
-  int got;           // halos received for sweep `iter`
+  int sent;          // last sweep whose boundary went to the neighbours
+  int started;       // the start message has been processed
+  int got[2];        // halos received for the sweep of each parity
   int nbr_count;
   int done;
   int waiting;       // parked until the decision of check iter/K - 1 arrives
@@ -57,8 +64,9 @@ struct JBlock : charm::chare {
   double res0, res_last;
   int checks;
   __device__ JBlock()
-      : iter(0), cur(0), got(0), nbr_count(0), done(0), waiting(0), have_own(0), own(0.0),
+      : iter(0), cur(0), sent(-1), started(0), nbr_count(0), done(0), waiting(0), have_own(0), own(0.0),
         decided(-1), stop_check(-1), res0(0.0), res_last(0.0), checks(0) {
+    got[0] = got[1] = 0;
     child_got[0] = child_got[1] = 0;
     child_val[0] = child_val[1] = 0.0;
   }
@@ -78,6 +86,11 @@ __device__ double sweep_block(const jac::chare_desc& d, int cur, bool resid) {
   jac::block_view<T> in = view<T>(d, cur), out = view<T>(d, cur ^ 1);
   double acc = 0.0;
   bool done = false;
+  if (!CHARM_VERIFY(d.w > 0 && d.h > 0 && d.buf[0] && d.buf[1] && (cur == 0 || cur == 1),
+                    CHARMING_ERR_APP, 8000 + cur, d.w))
+    return 0.0;
+  unsigned long long t0 = charm::now_ns();
+#ifndef CHARMING_HOST_EMULATION  // the CPU check of the chare logic has no bulk copies
   if (japp::pipeline()) {
     size_t sb = 0;
     void* sm = charm::smem_scratch(&sb);
@@ -88,12 +101,14 @@ __device__ double sweep_block(const jac::chare_desc& d, int cur, bool resid) {
       done = true;
     }
   }
+#endif
   if (!done) {
     __syncthreads();
     acc = resid ? jac::sweep_direct<T, true>(in, out, d.w, d.h)
                 : jac::sweep_direct<T, false>(in, out, d.w, d.h);
     __syncthreads();
   }
+  if (threadIdx.x == 0) japp::sweep_ns()[blockIdx.x] += charm::now_ns() - t0;
   return resid ? suite::block_sum_f64(acc) : 0.0;
 }
 
@@ -123,7 +138,7 @@ __device__ void send_halo(JBlock& c, const jac::chare_desc& d, int dir) {
     int col = (dir == jac::LEFT) ? 1 : d.w;
     for (int i = threadIdx.x; i < len; i += blockDim.x) vals[i] = *g.at(1 + i, col);
   }
-  jproxy->invoke(nbr, EP_HALO, msg, bytes, c.iter);
+  jproxy->invoke(nbr, EP_HALO, msg, bytes, japp::halo_mode() == 1 ? c.iter : -1);
 }
 
 template <typename T>
@@ -137,7 +152,7 @@ template <typename T>
 __device__ void unpack_halo(JBlock& c, const jac::chare_desc& d, const void* arg) {
   const jac::halo_hdr* hh = reinterpret_cast<const jac::halo_hdr*>(arg);
   const T* vals = reinterpret_cast<const T*>(reinterpret_cast<const char*>(arg) + sizeof(jac::halo_hdr));
-  jac::block_view<T> g = view<T>(d, c.cur);
+  jac::block_view<T> g = view<T>(d, hh->iter & 1);  // ghost ring of the sweep it belongs to
   int dir = hh->dir, len = hh->len;
   if (dir == jac::TOP || dir == jac::BOTTOM) {
     int r = (dir == jac::TOP) ? 0 : d.h + 1;
@@ -172,186 +187,7 @@ __device__ void finish(JBlock& c, const jac::chare_desc& d) {
   if (s_last) charm::end();
 }
 
-template <typename T>
-__device__ void proceed(JBlock& c, const jac::chare_desc& d);
-
-// All threads: record the decision of check `chk`, pass it down the tree,
-// and resume the chare if it was parked on it.
-template <typename T>
-__device__ void apply_decision(JBlock& c, const jac::chare_desc& d, const jac::decision_msg& m) {
-  __shared__ int s_resume;
-  if (threadIdx.x == 0) {
-    if (m.check > c.decided) c.decided = m.check;
-    if (m.stop && c.stop_check < 0) c.stop_check = m.check;
-    c.res0 = m.res0;
-    c.res_last = m.res;
-    c.checks = m.check + 1;
-    s_resume = c.waiting;
-  }
-  __syncthreads();
-  jac::decision_msg fwd = m;
-  for (int k = 0; k < 2; k++) {
-    if (d.child[k] >= 0) jproxy->invoke(d.child[k], EP_DECISION, &fwd, sizeof(fwd));
-  }
-  if (s_resume) proceed<T>(c, d);
-}
-
-// All threads: when this chare's partial and its children's are in, send
-// the sum up (fixed order: own, child 0, child 1) or decide at the root.
-template <typename T>
-__device__ void tree_try_forward(JBlock& c, const jac::chare_desc& d, int chk) {
-  __shared__ int s_act;
-  __shared__ double s_total;
-  if (threadIdx.x == 0) {
-    s_act = 0;
-    bool complete = c.have_own && (d.child[0] < 0 || c.child_got[0]) &&
-                    (d.child[1] < 0 || c.child_got[1]);
-    if (complete) {
-      double t = c.own;
-      if (d.child[0] >= 0) t += c.child_val[0];
-      if (d.child[1] >= 0) t += c.child_val[1];
-      s_total = t;
-      s_act = d.parent < 0 ? 2 : 1;
-      c.have_own = 0;
-      c.child_got[0] = c.child_got[1] = 0;
-    }
-  }
-  __syncthreads();
-  int act = s_act;
-  double total = s_total;
-  __syncthreads();
-  if (act == 1) {
-    jac::partial_msg pm;
-    pm.check = chk;
-    pm.slot = (d.rank - 1) % 2;
-    pm.value = total;
-    jproxy->invoke(d.parent, EP_PARTIAL, &pm, sizeof(pm));
-  } else if (act == 2) {
-    const jac::prob_desc& p = japp::probs()[d.prob];
-    jac::decision_msg m;
-    double nrm = sqrt(total);
-    m.check = chk;
-    m.res0 = (chk == 0) ? nrm : c.res0;
-    m.res = nrm;
-    m.stop = (p.tol > 0.0) && (m.res0 == 0.0 || nrm <= p.tol * m.res0) ? 1 : 0;
-    apply_decision<T>(c, d, m);
-  }
-}
-
-// All threads: after sweep `iter` completed (or on resume), stop, park, or
-// start the next sweep by sending halos (refnum = iter).
-template <typename T>
-__device__ void proceed(JBlock& c, const jac::chare_desc& d) {
-  const jac::prob_desc& p = japp::probs()[d.prob];
-  __shared__ int s_act;
-  enum { CONT = 0, WAIT = 1, FIN = 2 };
-  if (threadIdx.x == 0) {
-    int act = CONT;
-    int K = p.check_every;
-    if (c.iter >= p.max_sweeps) {
-      act = FIN;
-    } else if (K > 0 && c.iter >= K && c.iter % K == 0) {
-      int need = c.iter / K - 1;
-      if (c.decided < need) act = WAIT;
-      else if (c.stop_check >= 0 && c.stop_check <= need) act = FIN;
-    }
-    c.waiting = (act == WAIT) ? 1 : 0;
-    if (act == CONT && c.nbr_count > 0) jproxy->set_refnum(c.i, c.iter);
-    s_act = act;
-  }
-  __syncthreads();
-  int act = s_act;
-  __syncthreads();
-  if (act == FIN) {
-    finish(c, d);
-  } else if (act == CONT) {
-    if (c.nbr_count > 0) {
-      send_halos<T>(c, d);
-    } else {
-      int it = c.iter;
-      jproxy->invoke(c.i, EP_CONT, &it, sizeof(int));
-    }
-  }
-}
-
-// All threads: one sweep, then the residual tree and the next step.
-template <typename T>
-__device__ void advance(JBlock& c, const jac::chare_desc& d) {
-  const jac::prob_desc& p = japp::probs()[d.prob];
-  int K = p.check_every;
-  bool resid = K > 0 && (c.iter % K == 0);
-  double part = sweep_block<T>(d, c.cur, resid);
-  int chk = K > 0 ? c.iter / K : 0;
-  if (threadIdx.x == 0) {
-    c.cur ^= 1;
-    c.iter++;
-    c.got = 0;
-    if (resid) {
-      c.own = part;
-      c.have_own = 1;
-    }
-  }
-  __syncthreads();
-  if (resid) tree_try_forward<T>(c, d, chk);
-  if (!c.done && !c.waiting) proceed<T>(c, d);
-}
-
-template <typename T>
-__device__ void em_start_t(JBlock& c) {
-  const jac::chare_desc& d = japp::chares()[c.i];
-  if (threadIdx.x == 0) {
-    int n = 0;
-    for (int k = 0; k < 4; k++) n += d.nbr[k] >= 0;
-    c.nbr_count = n;
-    c.iter = 0;
-    c.cur = 0;
-    c.got = 0;
-  }
-  __syncthreads();
-  proceed<T>(c, d);
-}
-
-template <typename T>
-__device__ void em_halo_t(JBlock& c, void* arg) {
-  if (c.done) return;
-  const jac::chare_desc& d = japp::chares()[c.i];
-  unpack_halo<T>(c, d, arg);
-  __shared__ int s_go;
-  if (threadIdx.x == 0) {
-    c.got++;
-    s_go = (c.got == c.nbr_count) ? 1 : 0;
-  }
-  __syncthreads();
-  if (s_go) advance<T>(c, d);
-}
-
-template <typename T>
-__device__ void em_cont_t(JBlock& c) {
-  if (c.done) return;
-  advance<T>(c, japp::chares()[c.i]);
-}
-
-template <typename T>
-__device__ void em_partial_t(JBlock& c, void* arg) {
-  if (c.done) return;
-  const jac::chare_desc& d = japp::chares()[c.i];
-  const jac::partial_msg* pm = reinterpret_cast<const jac::partial_msg*>(arg);
-  int chk = pm->check;
-  if (threadIdx.x == 0) {
-    c.child_val[pm->slot] = pm->value;
-    c.child_got[pm->slot] = 1;
-  }
-  __syncthreads();
-  tree_try_forward<T>(c, d, chk);
-}
-
-template <typename T>
-__device__ void em_decision_t(JBlock& c, void* arg) {
-  if (c.done) return;
-  jac::decision_msg m = *reinterpret_cast<const jac::decision_msg*>(arg);
-  __syncthreads();
-  apply_decision<T>(c, japp::chares()[c.i], m);
-}
+#include "jacobi_chare.cuh"
 
 __device__ void em_start(JBlock& c, void* arg) {
   if (japp::dtype() == CHARMING_F32) em_start_t<float>(c); else em_start_t<double>(c);

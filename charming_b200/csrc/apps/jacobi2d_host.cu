@@ -31,6 +31,7 @@ struct JHandle {
   int* d_final = nullptr;
   int* d_block_map = nullptr;
   int* d_chare_of = nullptr;
+  unsigned long long* d_sweep_ns = nullptr;
   char* d_grid = nullptr;
   size_t grid_bytes = 0;
   void* d_stage = nullptr;
@@ -260,6 +261,7 @@ extern "C" int charming_jacobi2d_create(const charming_jacobi_problem* probs, in
   if (e == cudaSuccess) e = cudaMalloc(&h->d_final, sizeof(int) * nch);
   if (e == cudaSuccess) e = cudaMalloc(&h->d_block_map, sizeof(int) * n_pes);
   if (e == cudaSuccess) e = cudaMalloc(&h->d_chare_of, sizeof(int) * h->chare_of.size());
+  if (e == cudaSuccess) e = cudaMalloc(&h->d_sweep_ns, 8 * (size_t)n_pes);
   if (e == cudaSuccess) e = cudaMemcpy(h->d_chares, h->chares.data(), sizeof(jac::chare_desc) * nch, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(h->d_probs, pd.data(), sizeof(jac::prob_desc) * n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(h->d_results, 0, sizeof(jac::prob_result) * n);
@@ -282,12 +284,14 @@ extern "C" int charming_jacobi2d_create(const charming_jacobi_problem* probs, in
   ap.a[2] = opt->dtype;
   ap.a[3] = opt->pipeline;
   ap.a[4] = opt->tile_w;
+  ap.a[5] = opt->halo_mode;
   ap.p[0] = h->d_chares;
   ap.p[1] = h->d_probs;
   ap.p[2] = h->d_results;
   ap.p[3] = h->d_done;
   ap.p[4] = h->d_final;
   ap.p[5] = h->d_block_map;
+  ap.p[6] = h->d_sweep_ns;
   *handle = h;
   return charming_jacobi2d_init(h);
 }
@@ -372,6 +376,7 @@ extern "C" int charming_jacobi2d_store(void* handle, int prob, void* host_grid) 
 static int enqueue_run(JHandle* h, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(h->d_done, 0, 64, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->d_results, 0, sizeof(jac::prob_result) * h->probs.size(), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->d_sweep_ns, 0, 8 * h->block_map.size(), s);
   if (e == cudaSuccess)
     e = cudaMemcpyToSymbolAsync(g_app, h->h_params, sizeof(suite::app_params), 0,
                                 cudaMemcpyHostToDevice, s);
@@ -438,6 +443,20 @@ extern "C" int charming_jacobi2d_get_info(void* handle, charming_jacobi_info* ou
   out->grid_bytes = h->grid_bytes;
   out->halo_msgs_per_sweep = h->halo_msgs;
   out->last_run_ms = h->last_ms;
+  std::vector<unsigned long long> ns(h->block_map.size());
+  cudaError_t e = cudaMemcpy(ns.data(), h->d_sweep_ns, 8 * ns.size(), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return check_cuda(e, "jacobi2d info");
+  double mx = 0, sum = 0;
+  int busy = 0;
+  for (size_t p = 0; p < ns.size(); p++) {
+    mx = std::max(mx, (double)ns[p]);
+    if (h->block_map[p] > 0) {
+      sum += (double)ns[p];
+      busy++;
+    }
+  }
+  out->sweep_ms_max = mx * 1e-6;
+  out->sweep_ms_mean = busy ? sum / busy * 1e-6 : 0.0;
   return CHARMING_OK;
 }
 
@@ -455,6 +474,7 @@ extern "C" int charming_jacobi2d_destroy(void* handle) {
   cudaFree(h->d_final);
   cudaFree(h->d_block_map);
   cudaFree(h->d_chare_of);
+  cudaFree(h->d_sweep_ns);
   cudaFree(h->d_stage);
   if (h->h_params) cudaFreeHost(h->h_params);
   if (h->ev0) cudaEventDestroy(h->ev0);

@@ -1,0 +1,236 @@
+// Jacobi2d chare state machine (included by jacobi2d.cu inside its
+// anonymous namespace; uses JBlock, japp, jproxy and the helpers above it).
+//
+// State of a chare: `iter` sweeps done (buf[iter & 1] holds u_iter), `sent`
+// = last sweep whose boundary was sent, got[p] = halos received for the
+// sweep of parity p. A halo for sweep k is unpacked into the ghost ring of
+// buf[k & 1] as soon as it arrives: sweep k-1 reads only buf[(k-1) & 1] and
+// writes only the interior of buf[k & 1], and a neighbour can be at most one
+// sweep ahead, so early halos need no stash (halo_mode 0). halo_mode 1 tags
+// halos with refnum = sweep instead, which parks early ones in the runtime's
+// stash as the reference's refnum pattern would.
+
+// Control flow is never re-entrant: pump() runs only at the top of an entry
+// method; apply_decision() and tree_try_forward() report "the chare was
+// parked and may continue" to their caller instead of resuming it
+// themselves, so the call depth stays fixed whatever the message order.
+
+// All threads: record the decision of check m.check and pass it down the
+// tree. Returns 1 when the chare was parked on a decision (the caller then
+// runs pump()).
+template <typename T>
+__device__ int apply_decision(JBlock& c, const jac::chare_desc& d, const jac::decision_msg& m) {
+  __shared__ int s_resume;
+  if (threadIdx.x == 0) {
+    if (m.check > c.decided) c.decided = m.check;
+    if (m.stop && c.stop_check < 0) c.stop_check = m.check;
+    c.res0 = m.res0;
+    c.res_last = m.res;
+    c.checks = m.check + 1;
+    s_resume = c.waiting;
+    c.waiting = 0;
+  }
+  __syncthreads();
+  int resume = s_resume;
+  __syncthreads();
+  jac::decision_msg fwd = m;
+  for (int k = 0; k < 2; k++) {
+    if (d.child[k] >= 0) jproxy->invoke(d.child[k], EP_DECISION, &fwd, sizeof(fwd));
+  }
+  return resume;
+}
+
+// All threads: when this chare's partial and its children's are in, send
+// the sum up (fixed order: own, child 0, child 1) or decide at the root.
+// Returns apply_decision()'s resume flag (0 when nothing was decided).
+template <typename T>
+__device__ int tree_try_forward(JBlock& c, const jac::chare_desc& d, int chk) {
+  __shared__ int s_act;
+  __shared__ double s_total;
+  if (threadIdx.x == 0) {
+    s_act = 0;
+    bool complete = c.have_own && (d.child[0] < 0 || c.child_got[0]) &&
+                    (d.child[1] < 0 || c.child_got[1]);
+    if (complete) {
+      double t = c.own;
+      if (d.child[0] >= 0) t += c.child_val[0];
+      if (d.child[1] >= 0) t += c.child_val[1];
+      s_total = t;
+      s_act = d.parent < 0 ? 2 : 1;
+      c.have_own = 0;
+      c.child_got[0] = c.child_got[1] = 0;
+    }
+  }
+  __syncthreads();
+  int act = s_act;
+  double total = s_total;
+  __syncthreads();
+  if (act == 1) {
+    jac::partial_msg pm;
+    pm.check = chk;
+    pm.slot = (d.rank - 1) % 2;
+    pm.value = total;
+    jproxy->invoke(d.parent, EP_PARTIAL, &pm, sizeof(pm));
+  } else if (act == 2) {
+    const jac::prob_desc& p = japp::probs()[d.prob];
+    jac::decision_msg m;
+    double nrm = sqrt(total);
+    m.check = chk;
+    m.res0 = (chk == 0) ? nrm : c.res0;
+    m.res = nrm;
+    m.stop = (p.tol > 0.0) && (m.res0 == 0.0 || nrm <= p.tol * m.res0) ? 1 : 0;
+    return apply_decision<T>(c, d, m);
+  }
+  return 0;
+}
+
+// All threads: one sweep buf[iter&1] -> buf[(iter+1)&1], then the residual
+// tree when this sweep carries a check.
+template <typename T>
+__device__ void advance(JBlock& c, const jac::chare_desc& d) {
+  const jac::prob_desc& p = japp::probs()[d.prob];
+  int K = p.check_every;
+  bool resid = K > 0 && (c.iter % K == 0);
+  double part = sweep_block<T>(d, c.cur, resid);
+  int chk = K > 0 ? c.iter / K : 0;
+  if (threadIdx.x == 0) {
+    c.got[c.iter & 1] = 0;
+    c.cur ^= 1;
+    c.iter++;
+    if (resid) {
+      c.own = part;
+      c.have_own = 1;
+    }
+  }
+  __syncthreads();
+  // A decision taken here (at the tree root) cannot find this chare parked:
+  // it is sweeping. pump()'s loop re-examines the state anyway.
+  if (resid) tree_try_forward<T>(c, d, chk);
+}
+
+// All threads: drive the chare as far as it can go without new messages:
+// decide (stop / park on a residual decision / continue), send the boundary
+// of u_iter once, and sweep whenever all halos of the current sweep are in.
+template <typename T>
+__device__ void pump(JBlock& c, const jac::chare_desc& d) {
+  const jac::prob_desc& p = japp::probs()[d.prob];
+  __shared__ int s_act;
+  enum { IDLE = 0, SEND = 1, FIN = 2, SWEEP = 3, SELF = 4 };
+  while (true) {
+    if (threadIdx.x == 0) {
+      int act = IDLE;
+      int K = p.check_every;
+      CHARM_VERIFY(c.cur == (c.iter & 1) && c.got[0] <= c.nbr_count && c.got[1] <= c.nbr_count,
+                   CHARMING_ERR_APP, 7000 + c.iter, c.i);
+      if (c.done || c.waiting) {
+        act = IDLE;
+      } else if (c.sent < c.iter) {
+        if (c.iter >= p.max_sweeps) {
+          act = FIN;
+        } else if (K > 0 && c.iter >= K && c.iter % K == 0 && c.decided < c.iter / K - 1) {
+          c.waiting = 1;
+          act = IDLE;
+        } else if (K > 0 && c.iter >= K && c.iter % K == 0 && c.stop_check >= 0 &&
+                   c.stop_check <= c.iter / K - 1) {
+          act = FIN;
+        } else {
+          act = c.nbr_count > 0 ? SEND : SELF;
+          c.sent = c.iter;
+          if (act == SEND && japp::halo_mode() == 1) jproxy->set_refnum(c.i, c.iter);
+        }
+      } else if (c.nbr_count > 0 && c.got[c.iter & 1] == c.nbr_count) {
+        act = SWEEP;
+      }
+      s_act = act;
+    }
+    __syncthreads();
+    int act = s_act;
+    __syncthreads();
+    if (act == IDLE) return;
+    if (act == FIN) {
+      finish(c, d);
+      return;
+    }
+    if (act == SEND) {
+      send_halos<T>(c, d);
+    } else if (act == SELF) {
+      // no neighbours: one sweep per message, so other chares of the PE run
+      // in between
+      int it = c.iter;
+      jproxy->invoke(c.i, EP_CONT, &it, sizeof(int));
+      return;
+    } else {
+      advance<T>(c, d);
+    }
+  }
+}
+
+template <typename T>
+__device__ void em_start_t(JBlock& c) {
+  const jac::chare_desc& d = japp::chares()[c.i];
+  if (threadIdx.x == 0) {
+    int n = 0;
+    for (int k = 0; k < 4; k++) n += d.nbr[k] >= 0;
+    c.nbr_count = n;
+    c.started = 1;
+  }
+  __syncthreads();
+  pump<T>(c, d);
+}
+
+template <typename T>
+__device__ void em_halo_t(JBlock& c, void* arg) {
+  if (c.done) return;
+  const jac::chare_desc& d = japp::chares()[c.i];
+  const jac::halo_hdr* hh = reinterpret_cast<const jac::halo_hdr*>(arg);
+  // checked build: direction, length and sweep of the halo are consistent
+  if (!CHARM_VERIFY(hh->dir >= 0 && hh->dir < 4 && d.nbr[hh->dir] >= 0, CHARMING_ERR_APP,
+                    1000 + hh->dir, c.i) ||
+      !CHARM_VERIFY(hh->len == ((hh->dir < 2) ? d.w : d.h), CHARMING_ERR_APP, 2000 + hh->dir,
+                    hh->len) ||
+      !CHARM_VERIFY(hh->iter == c.iter || hh->iter == c.iter + 1, CHARMING_ERR_APP,
+                    3000 + (hh->iter - c.iter), c.i))
+    return;
+  unpack_halo<T>(c, d, arg);
+  if (threadIdx.x == 0) {
+    c.got[hh->iter & 1]++;
+    CHARM_VERIFY(c.got[hh->iter & 1] <= 4, CHARMING_ERR_APP, 4000 + c.got[hh->iter & 1], c.i);
+  }
+  __syncthreads();
+  if (c.started) pump<T>(c, d);  // a halo may overtake the start message
+}
+
+template <typename T>
+__device__ void em_cont_t(JBlock& c) {
+  if (c.done) return;
+  const jac::chare_desc& d = japp::chares()[c.i];
+  advance<T>(c, d);
+  pump<T>(c, d);
+}
+
+template <typename T>
+__device__ void em_partial_t(JBlock& c, void* arg) {
+  if (c.done) return;
+  const jac::chare_desc& d = japp::chares()[c.i];
+  const jac::partial_msg* pm = reinterpret_cast<const jac::partial_msg*>(arg);
+  int chk = pm->check;
+  if (!CHARM_VERIFY(pm->slot == 0 || pm->slot == 1, CHARMING_ERR_APP, 5000 + pm->slot, c.i) ||
+      !CHARM_VERIFY(d.child[pm->slot] >= 0 && !c.child_got[pm->slot], CHARMING_ERR_APP,
+                    6000 + pm->slot, c.i))
+    return;
+  if (threadIdx.x == 0) {
+    c.child_val[pm->slot] = pm->value;
+    c.child_got[pm->slot] = 1;
+  }
+  __syncthreads();
+  if (tree_try_forward<T>(c, d, chk)) pump<T>(c, d);
+}
+
+template <typename T>
+__device__ void em_decision_t(JBlock& c, void* arg) {
+  if (c.done) return;
+  const jac::chare_desc& d = japp::chares()[c.i];
+  jac::decision_msg m = *reinterpret_cast<const jac::decision_msg*>(arg);
+  __syncthreads();
+  if (apply_decision<T>(c, d, m)) pump<T>(c, d);
+}

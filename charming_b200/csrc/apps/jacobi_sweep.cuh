@@ -168,16 +168,30 @@ __device__ __forceinline__ void fence_mbar_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(unsigned long long* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_test_wait(unsigned long long* b, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done) : "r"(smem_u32(b)), "r"(parity) : "memory");
+  return done != 0;
+}
+
+constexpr int MAX_SLOTS = 64;        // mbarrier pairs in the first 1 KiB
+constexpr int BAR_BYTES = 2 * MAX_SLOTS * 8;
+
+// Column tiling and ring size of one sweep. Each warp owns a strip of
+// 32 * VEC columns of the tile and walks all rows of it.
 struct tma_plan {
   int ntiles;     // column tiles
   int tws;        // tile stride (columns), multiple of VEC
-  int tpr;        // threads per output row (vectors per tile row)
-  int G;          // rows per band
-  int NS;         // ring slots
+  int NS;         // ring slots (rows in flight)
   int slot_elems; // elements per slot
 };
 
-// Smem needed by a plan with NS slots.
 template <typename T>
 __host__ __device__ inline size_t tma_slot_bytes(int tws) {
   size_t e = (size_t)tws + 2 * traits<T>::VEC;
@@ -187,136 +201,171 @@ __host__ __device__ inline size_t tma_slot_bytes(int tws) {
 template <typename T>
 __device__ bool make_plan(int w, int nthreads, size_t smem_bytes, int tile_w_opt, tma_plan* p) {
   constexpr int V = traits<T>::VEC;
-  int twmax = tile_w_opt > 0 ? tile_w_opt : traits<T>::TW_MAX;
+  int twmax = (nthreads / 32) * 32 * V;  // one vector per lane
+  if (tile_w_opt > 0 && tile_w_opt < twmax) twmax = tile_w_opt;
   twmax = (twmax + V - 1) / V * V;
   p->ntiles = (w + twmax - 1) / twmax;
   int tw = (w + p->ntiles - 1) / p->ntiles;
   p->tws = (tw + V - 1) / V * V;
-  p->tpr = p->tws / V;
-  p->G = p->tpr >= nthreads ? 1 : nthreads / p->tpr;
   size_t sb = tma_slot_bytes<T>(p->tws);
   p->slot_elems = (int)(sb / sizeof(T));
-  size_t avail = smem_bytes > 1024 ? smem_bytes - 1024 : 0;  // mbarriers
+  size_t avail = smem_bytes > (size_t)BAR_BYTES ? smem_bytes - BAR_BYTES : 0;
   long ns = (long)(avail / sb);
-  if (ns > 32) ns = 32;
+  if (ns > MAX_SLOTS) ns = MAX_SLOTS;
   p->NS = (int)ns;
-  return p->NS >= p->G + 2;
+  return p->NS >= 4;
 }
 
-// Returns false (error recorded) when a pipeline wait ran out.
+// One sweep in -> out. Row segments (tile columns + 16-byte halo each side)
+// stream through NS shared-memory slots. full[s] completes when the bulk
+// copy into slot s landed; empty[s] when every warp is done with it. Lane 0
+// of warp 0 issues copies whenever a slot is empty (it also polls while
+// waiting, so it never blocks the pipeline it feeds). Returns false (error
+// recorded) if a wait ran out.
 template <typename T, bool RESID>
 __device__ bool sweep_tma(block_view<T> in, block_view<T> out, int w, int h, void* smem,
     size_t smem_bytes, const tma_plan& P, double* acc_out) {
   constexpr int V = traits<T>::VEC;
   constexpr int H = V;  // halo elements each side of a slot row (16 bytes)
-  unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem);
-  T* slots = reinterpret_cast<T*>(reinterpret_cast<char*>(smem) + 1024);
+  constexpr unsigned FULL = 0xffffffffu;
+  unsigned long long* full = reinterpret_cast<unsigned long long*>(smem);
+  unsigned long long* empty = full + MAX_SLOTS;
+  T* slots = reinterpret_cast<T*>(reinterpret_cast<char*>(smem) + BAR_BYTES);
   const int rows = h + 2;
-  const long long total_items = (long long)P.ntiles * rows;
-  __shared__ long long s_issued;
+  const long long total = (long long)P.ntiles * rows;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nw = blockDim.x >> 5;
   __shared__ int s_fail;
+  __shared__ long long s_issued;
 
-  // Generic-proxy writes to `in` (previous sweep, halo unpack) must be
-  // visible to the bulk copies.
-  fence_proxy_async_global();
+  fence_proxy_async_global();  // earlier generic writes to `in` -> bulk copies
   if (threadIdx.x == 0) {
-    for (int s = 0; s < P.NS; s++) mbar_init(&bars[s], 1);
+    for (int s = 0; s < P.NS; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], (unsigned)nw);
+    }
     fence_mbar_init();
-    s_issued = 0;
     s_fail = 0;
   }
   __syncthreads();
 
-  auto issue_upto = [&](long long limit) {
-    // thread 0 only
-    if (limit > total_items) limit = total_items;
-    if (s_issued < limit) fence_proxy_async_smem();
-    while (s_issued < limit) {
-      long long j = s_issued;
+  long long issued = 0;  // producer state (lane 0 of warp 0)
+  auto try_issue = [&]() {
+    while (issued < total) {
+      long long j = issued;
+      int s = (int)(j % P.NS);
+      long long u = j / P.NS;
+      if (u > 0 && !mbar_test_wait(&empty[s], (unsigned)((u - 1) & 1))) break;
       int t = (int)(j / rows), r = (int)(j % rows);
       int c0 = t * P.tws;
       int tw = min(P.tws, w - c0);
       unsigned bytes = (unsigned)(((size_t)(tw + 2 * H) * sizeof(T) + 15) / 16 * 16);
-      const T* src = in.row(r) + traits<T>::OFF + c0 - H;
-      int s = (int)(j % P.NS);
-      mbar_expect_tx(&bars[s], bytes);
-      bulk_g2s(slots + (size_t)s * P.slot_elems, src, bytes, &bars[s]);
-      s_issued = j + 1;
+      // checked build: 16-byte aligned source, copy fits its slot
+      if (!CHARM_VERIFY(((reinterpret_cast<uintptr_t>(in.row(r) + traits<T>::OFF + c0 - H) & 15) == 0) &&
+                        bytes <= (unsigned)(P.slot_elems * sizeof(T)),
+                        CHARMING_ERR_PIPELINE, (int)j, (int)bytes))
+        break;
+      mbar_expect_tx(&full[s], bytes);
+      bulk_g2s(slots + (size_t)s * P.slot_elems, in.row(r) + traits<T>::OFF + c0 - H, bytes,
+               &full[s]);
+      issued = j + 1;
     }
   };
-
-  if (threadIdx.x == 0) issue_upto(P.NS);
-  __syncthreads();
+  const bool producer = (warp == 0 && lane == 0);
+  if (producer) {
+    fence_proxy_async_smem();
+    try_issue();
+  }
+  __syncwarp();
 
   double acc = 0.0;
-  const int g = threadIdx.x / P.tpr;     // row within band
-  const int lane = threadIdx.x % P.tpr;  // vector within tile row
-  const bool row_thread = P.tpr >= (int)blockDim.x || g < P.G;
-
-  for (int t = 0; t < P.ntiles; t++) {
+  bool fail = false;
+  for (int t = 0; t < P.ntiles && !fail; t++) {
     const int c0 = t * P.tws;
     const int tw = min(P.tws, w - c0);
-    const int nvec = (tw + V - 1) / V;
     const long long ibase = (long long)t * rows;
-    for (int rb = 1; rb <= h; rb += P.G) {
-      const int r = rb + (P.tpr >= (int)blockDim.x ? 0 : g);
-      if (row_thread && r <= h && !s_fail) {
-        // wait for input rows r-1, r, r+1 of this tile
-        bool ok = true;
-        for (int q = -1; q <= 1 && ok; q++) {
-          long long j = ibase + r + q;
-          unsigned parity = (unsigned)((j / P.NS) & 1);
-          unsigned long long* b = &bars[j % P.NS];
-          unsigned spins = 0;
-          while (!mbar_try_wait(b, parity)) {
-            if (++spins > (1u << 26)) {
-              ok = false;
-              break;
-            }
-          }
+    const int v = warp * 32 + lane;      // vector of the tile row this lane owns
+    const bool active = v * V < tw;
+    const bool next_active = (v + 1) * V < tw;
+    const int nvalid = active ? min(V, tw - v * V) : 0;
+    const int s_off = H + v * V;         // slot element of interior column c0 + v*V
+    for (int r = 0; r < rows; r++) {
+      const long long j = ibase + r;
+      const unsigned parity = (unsigned)((j / P.NS) & 1);
+      unsigned long long* fb = &full[j % P.NS];
+      unsigned spins = 0;
+      while (true) {
+        // The producer's warp must not be suspended inside try_wait while
+        // copies wait to be issued: it polls with the non-blocking test.
+        bool ok = (warp == 0) ? mbar_test_wait(fb, parity) : mbar_try_wait(fb, parity);
+        if (__all_sync(FULL, ok)) break;
+        if (producer) try_issue();
+        __syncwarp();
+        if (++spins > (1u << 22) || *reinterpret_cast<volatile int*>(&s_fail)) {
+          fail = true;
+          break;
         }
-        if (!ok) {
-          atomicExch(&s_fail, 1);
+      }
+      if (fail) break;
+      if (r >= 2) {
+        const T* up = slots + (size_t)((j - 2) % P.NS) * P.slot_elems;
+        const T* mid = slots + (size_t)((j - 1) % P.NS) * P.slot_elems;
+        const T* dn = slots + (size_t)(j % P.NS) * P.slot_elems;
+        T m[V];
+        if (active) {
+          if (V == 2) {
+            double2 b = *reinterpret_cast<const double2*>(mid + s_off);
+            m[0] = (T)b.x;
+            m[1] = (T)b.y;
+          } else {
+            float4 b = *reinterpret_cast<const float4*>(mid + s_off);
+            m[0] = (T)b.x; m[1] = (T)b.y; m[2] = (T)b.z; m[3] = (T)b.w;
+          }
         } else {
-          const T* up = slots + (size_t)((ibase + r - 1) % P.NS) * P.slot_elems;
-          const T* mid = slots + (size_t)((ibase + r) % P.NS) * P.slot_elems;
-          const T* dn = slots + (size_t)((ibase + r + 1) % P.NS) * P.slot_elems;
-          const int vstride = P.tpr < (int)blockDim.x ? P.tpr : (int)blockDim.x;
-          for (int v = lane; v < nvec; v += vstride) {
-            int s = H + v * V;  // slot index of interior column c0 + v*V
-            int nvalid = min(V, tw - v * V);
-            acc += compute_vec<T, RESID>(up + s, mid + s, dn + s, mid[s - 1], mid[s + V],
-                                         out.at(r, 1 + c0 + v * V), nvalid);
-          }
+#pragma unroll
+          for (int k = 0; k < V; k++) m[k] = (T)0;
         }
+        T left = __shfl_up_sync(FULL, m[V - 1], 1);
+        T right = __shfl_down_sync(FULL, m[0], 1);
+        if (active) {
+          if (lane == 0) left = mid[s_off - 1];
+          if (lane == 31 || !next_active) right = mid[s_off + V];
+          acc += compute_vec<T, RESID>(up + s_off, mid + s_off, dn + s_off, left, right,
+                                       out.at(r - 1, 1 + c0 + v * V), nvalid);
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[(j - 2) % P.NS]);
+        if (producer) try_issue();
       }
-      __syncthreads();
-      if (threadIdx.x == 0 && !s_fail) {
-        int rmax = min(rb + P.G - 1, h);
-        long long freed = (rmax == h) ? ibase + rows : ibase + rmax;
-        issue_upto(freed + P.NS);
+    }
+    if (!fail) {
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(&empty[(ibase + h) % P.NS]);
+        mbar_arrive(&empty[(ibase + h + 1) % P.NS]);
       }
-      __syncthreads();
     }
   }
-
-  // All issued copies were waited on (or the run failed): retire barriers.
-  bool fail = s_fail != 0;
+  if (fail) atomicExch(&s_fail, 1);
+  if (producer) s_issued = issued;
+  __syncthreads();
+  fail = s_fail != 0;
   if (threadIdx.x == 0) {
     if (fail) {
-      // Drain copies still in flight before the barriers are reused: wait
-      // (bounded) for every issued item's phase.
+      // Let copies still in flight land before the slots are reused.
       for (long long j = (s_issued > P.NS ? s_issued - P.NS : 0); j < s_issued; j++) {
         unsigned spins = 0;
-        while (!mbar_try_wait(&bars[j % P.NS], (unsigned)((j / P.NS) & 1)) && ++spins < (1u << 24)) {
+        while (!mbar_try_wait(&full[j % P.NS], (unsigned)((j / P.NS) & 1)) && ++spins < (1u << 20)) {
         }
       }
       charm::detail::report_error(CHARMING_ERR_PIPELINE, (int)s_issued, h);
     }
-    for (int s = 0; s < P.NS; s++) mbar_inval(&bars[s]);
+    for (int s = 0; s < P.NS; s++) {
+      mbar_inval(&full[s]);
+      mbar_inval(&empty[s]);
+    }
   }
-  // Outputs written by generic stores feed the next sweep's bulk copies.
-  fence_proxy_async_global();
+  fence_proxy_async_global();  // outputs (generic stores) -> next sweep's copies
   __syncthreads();
   *acc_out = acc;
   return !fail;

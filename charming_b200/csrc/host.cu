@@ -117,13 +117,15 @@ int collect_run(double kernel_ms) {
   int ctrl_h[CTRL_WORDS];
   cudaError_t e = cudaMemcpy(ctrl_h, g.ds.ctrl, sizeof(ctrl_h), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_fail(e, "read status");
-  std::vector<unsigned long long> st((size_t)g.inf.n_pes * N_STATS), tm((size_t)g.inf.n_pes * 2);
+  std::vector<unsigned long long> st((size_t)g.inf.n_pes * N_STATS), tm((size_t)g.inf.n_pes * 3);
   e = cudaMemcpy(st.data(), g.ds.pe_stats, st.size() * 8, cudaMemcpyDeviceToHost);
   if (e == cudaSuccess) e = cudaMemcpy(tm.data(), g.ds.pe_times, tm.size() * 8, cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_fail(e, "read stats");
   charming_stats s{};
-  unsigned long long tmin = ~0ULL, tmax = 0;
+  unsigned long long tmin = ~0ULL, tmax = 0, main_max = 0;
   for (int p = 0; p < g.inf.n_pes; p++) {
+    const unsigned long long* t = &tm[3 * (size_t)p];
+    if (t[1] > t[0] && t[1] - t[0] > main_max) main_max = t[1] - t[0];
     const unsigned long long* q = &st[(size_t)p * N_STATS];
     s.delivered += q[ST_DELIVERED];
     s.sent += q[ST_SENT];
@@ -132,10 +134,11 @@ int collect_run(double kernel_ms) {
     s.bytes_sent += q[ST_BYTES_SENT];
     s.idle_polls += q[ST_IDLE_POLLS];
     s.space_waits += q[ST_SPACE_WAITS];
-    if (tm[2 * p] && tm[2 * p] < tmin) tmin = tm[2 * p];
-    if (tm[2 * p + 1] > tmax) tmax = tm[2 * p + 1];
+    if (t[1] && t[1] < tmin) tmin = t[1];
+    if (t[2] > tmax) tmax = t[2];
   }
   s.loop_ms = (tmax > tmin && tmin != ~0ULL) ? (tmax - tmin) * 1e-6 : 0.0;
+  s.main_ms = main_max * 1e-6;
   s.kernel_ms = kernel_ms;
   s.status = ctrl_h[CTRL_STATUS];
   s.err_pe = ctrl_h[CTRL_ERR_PE];
@@ -247,6 +250,9 @@ int charming_init(const charming_config* cfg_in) {
   if (e != cudaSuccess) return cuda_fail(e, "heap limit");
   e = cudaDeviceSetLimit(cudaLimitStackSize, cfg.stack_bytes);
   if (e != cudaSuccess) return cuda_fail(e, "stack limit");
+  size_t stack_eff = 0;
+  e = cudaDeviceGetLimit(&stack_eff, cudaLimitStackSize);
+  if (e != cudaSuccess) return cuda_fail(e, "stack limit query");
 
   cudaFuncAttributes fa;
   e = cudaFuncGetAttributes(&fa, (const void*)charming_scheduler_kernel);
@@ -283,6 +289,8 @@ int charming_init(const charming_config* cfg_in) {
   g.inf.smem_bytes_per_pe = (int)smem_total;
   g.inf.smem_scratch_bytes = (int)smem_total - smem_state;
   g.inf.regs_per_thread = fa.numRegs;
+  g.inf.stack_bytes = (uint64_t)stack_eff;
+  g.inf.local_bytes = (uint64_t)fa.localSizeBytes;
   g.inf.ring_bytes = cfg.ring_bytes;
   g.inf.max_msg_bytes = (cfg.max_msg_bytes + 15) / 16 * 16;
 
@@ -312,7 +320,7 @@ int charming_init(const charming_config* cfg_in) {
   if ((rc = dev_alloc(&ds.ctrl, sizeof(int) * CTRL_WORDS, "control words"))) return rc;
   if ((rc = dev_alloc(&ds.progress, 8ull * n_pes, "progress"))) return rc;
   if ((rc = dev_alloc(&ds.pe_stats, 8ull * N_STATS * n_pes, "stats"))) return rc;
-  if ((rc = dev_alloc(&ds.pe_times, 16ull * n_pes, "times"))) return rc;
+  if ((rc = dev_alloc(&ds.pe_times, 24ull * n_pes, "times"))) return rc;
   e = cudaHostAlloc(&g.h_stop, 64, cudaHostAllocMapped);
   if (e != cudaSuccess) return cuda_fail(e, "host stop word");
   *g.h_stop = 0;

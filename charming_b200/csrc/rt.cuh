@@ -173,6 +173,19 @@ __device__ __forceinline__ bool past_deadline() {
 
 __device__ void grid_barrier();
 
+// Invariant checks of the checked build (-DCHARMING_CHECKS): a failed check
+// records CHARMING_ERR_APP (or the given code) with two values, and the
+// caller skips the access. In the normal build the checks compile away.
+#ifdef CHARMING_CHECKS
+__device__ __forceinline__ bool verify(bool ok, int code, int a, int b) {
+  if (!ok) set_error(code, a, b);
+  return ok;
+}
+#define CHARM_VERIFY(cond, code, a, b) (::charm::rt::verify((cond), (code), (int)(a), (int)(b)))
+#else
+#define CHARM_VERIFY(cond, code, a, b) (true)
+#endif
+
 // Message bytes -> ring cells.
 __host__ __device__ __forceinline__ unsigned int cells_for(unsigned long long bytes) {
   return (unsigned int)((bytes + CELL - 1) / CELL);

@@ -611,8 +611,9 @@ charming_scheduler_kernel(int argc, char** argv, size_t* argvs) {
   if (threadIdx.x == 0) {
     ps->stats[ST_LOOP_NS] = loop_t1 - loop_t0;
     for (int i = 0; i < N_STATS; i++) c_rt.pe_stats[(unsigned long long)me * N_STATS + i] = ps->stats[i];
-    c_rt.pe_times[2 * me] = loop_t0;
-    c_rt.pe_times[2 * me + 1] = loop_t1;
+    c_rt.pe_times[3 * me] = ps->t0;
+    c_rt.pe_times[3 * me + 1] = loop_t0;
+    c_rt.pe_times[3 * me + 2] = loop_t1;
     if (c_rt.free_chares_at_exit) {
       chare_proxy_table& tb = c_rt.proxy_tables[me];
       for (int i = tb.count - 1; i >= 0; i--) {

@@ -34,6 +34,7 @@ class RunStats:
     space_waits: int
     kernel_ms: float
     loop_ms: float
+    main_ms: float
     status: int
 
 
@@ -79,7 +80,8 @@ class Runtime:
         st = _lib.Stats()
         self.lib.charming_last_stats(C.byref(st))
         return RunStats(st.delivered, st.sent, st.stashed, st.revived, st.bytes_sent,
-                        st.idle_polls, st.space_waits, st.kernel_ms, st.loop_ms, st.status)
+                        st.idle_polls, st.space_waits, st.kernel_ms, st.loop_ms, st.main_ms,
+                        st.status)
 
     # ---- built-in programs ---------------------------------------------------
     def hello(self) -> np.ndarray:

@@ -98,6 +98,8 @@ typedef struct charming_info {
   uint64_t ring_bytes;
   uint64_t max_msg_bytes;    /* largest message incl. 32-byte header     */
   uint64_t device_bytes;     /* runtime buffers on the device            */
+  uint64_t stack_bytes;      /* per-thread stack limit in effect         */
+  uint64_t local_bytes;      /* scheduler kernel's static local memory   */
 } charming_info;
 int charming_get_info(charming_info* out);
 
@@ -111,7 +113,9 @@ typedef struct charming_stats {
   uint64_t idle_polls;       /* empty inbox polls                        */
   uint64_t space_waits;      /* sends that waited for ring space         */
   double kernel_ms;          /* CUDA-event time of the scheduler launch  */
-  double loop_ms;            /* max over PEs of time in the loop         */
+  double loop_ms;            /* first loop start to last loop end        */
+  double main_ms;            /* max over PEs: kernel start to loop start
+                                (charm::main, chare creation, barriers)  */
   int status;                /* status code of the run                   */
   int err_pe, err_info0, err_info1;
 } charming_stats;
@@ -145,6 +149,9 @@ typedef struct charming_jacobi_options {
   int pipeline;        /* 1: TMA bulk-copy row pipeline, 0: direct loads    */
   int use_graph;       /* 1: replay each run from a captured CUDA graph     */
   int balance;         /* 1: place chares by work (greedy), 0: block map    */
+  int halo_mode;       /* 0: halos land in the ghost ring of the sweep they
+                          belong to (parity buffers); 1: halos carry refnum
+                          = sweep and early ones wait in the stash          */
 } charming_jacobi_options;
 
 typedef struct charming_jacobi_result {
@@ -162,6 +169,8 @@ typedef struct charming_jacobi_info {
   uint64_t grid_bytes;        /* device bytes of all chare grids           */
   uint64_t halo_msgs_per_sweep;
   double last_run_ms;         /* CUDA-event time of the last run           */
+  double sweep_ms_max;        /* last run: max over PEs of time in sweeps  */
+  double sweep_ms_mean;       /* last run: mean over busy PEs              */
 } charming_jacobi_info;
 
 /* Decomposes the problems into chares (reference decomposition:

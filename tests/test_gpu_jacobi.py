@@ -143,3 +143,27 @@ def test_jacobi1d_bit_exact(rt):
     lib = oracle_lib()
     lib.oracle_jacobi1d_f64(a.ctypes.data_as(C.POINTER(C.c_double)), n * w, sweeps)
     assert np.array_equal(out.view(np.uint64), a.view(np.uint64))
+
+
+@pytest.mark.parametrize("pipeline", [True, False])
+def test_halo_refnum_mode_bit_exact(rt, pipeline):
+    """halo_mode 1: halos tagged refnum = sweep, early ones parked in the stash."""
+    g = seeded_grid(200, 150, 12)
+    p = Problem(200, 150, 21, px=4, py=3)
+    with Jacobi2D([p], pipeline=pipeline, halo_mode=1) as j:
+        j.load(0, g)
+        j.run()
+        out = j.store(0)
+    assert np.array_equal(bits(out), bits(jac64(g, 21)))
+
+
+def test_many_chares_per_pe(rt):
+    """Over-decomposition: several chares per PE, uneven placement."""
+    g = seeded_grid(700, 610, 99)
+    p = Problem(700, 610, 15, px=23, py=19)
+    with Jacobi2D([p], balance=False) as j:
+        j.load(0, g)
+        j.run()
+        out = j.store(0)
+        assert j.info()["max_chares_per_pe"] >= 2
+    assert np.array_equal(bits(out), bits(jac64(g, 15)))
