@@ -24,6 +24,8 @@ def _run(cmd: str, cwd: str) -> None:
 
 def build_runtime(jobs: int = 8) -> None:
     _run(f"make -j{jobs}", CSRC)
+    # the same runtime with invariant checks (CHARMING_CHECKED=1 selects it)
+    _run(f"make -j{jobs} CHECKS=1", CSRC)
 
 
 def build_oracle() -> None:

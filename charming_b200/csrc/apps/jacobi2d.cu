@@ -90,7 +90,7 @@ __device__ double sweep_block(const jac::chare_desc& d, int cur, bool resid) {
                     CHARMING_ERR_APP, 8000 + cur, d.w))
     return 0.0;
   unsigned long long t0 = charm::now_ns();
-#ifndef CHARMING_HOST_EMULATION  // the CPU check of the chare logic has no bulk copies
+#if !defined(CHARMING_HOST_EMULATION) || defined(CHARMING_HOST_EMULATION_TMA)
   if (japp::pipeline()) {
     size_t sb = 0;
     void* sm = charm::smem_scratch(&sb);

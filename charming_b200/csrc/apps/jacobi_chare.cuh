@@ -42,11 +42,14 @@ __device__ int apply_decision(JBlock& c, const jac::chare_desc& d, const jac::de
 
 // All threads: when this chare's partial and its children's are in, send
 // the sum up (fixed order: own, child 0, child 1) or decide at the root.
-// Returns apply_decision()'s resume flag (0 when nothing was decided).
+// Thread 0 alone reads and writes the chare and builds the message; the
+// others only see it through shared memory. Returns apply_decision()'s
+// resume flag (0 when nothing was decided).
 template <typename T>
 __device__ int tree_try_forward(JBlock& c, const jac::chare_desc& d, int chk) {
   __shared__ int s_act;
-  __shared__ double s_total;
+  __shared__ jac::partial_msg s_pm;
+  __shared__ jac::decision_msg s_dm;
   if (threadIdx.x == 0) {
     s_act = 0;
     bool complete = c.have_own && (d.child[0] < 0 || c.child_got[0]) &&
@@ -55,31 +58,33 @@ __device__ int tree_try_forward(JBlock& c, const jac::chare_desc& d, int chk) {
       double t = c.own;
       if (d.child[0] >= 0) t += c.child_val[0];
       if (d.child[1] >= 0) t += c.child_val[1];
-      s_total = t;
-      s_act = d.parent < 0 ? 2 : 1;
       c.have_own = 0;
       c.child_got[0] = c.child_got[1] = 0;
+      if (d.parent >= 0) {
+        s_pm.check = chk;
+        s_pm.slot = (d.rank - 1) % 2;
+        s_pm.value = t;
+        s_act = 1;
+      } else {
+        const jac::prob_desc& p = japp::probs()[d.prob];
+        double nrm = sqrt(t);
+        s_dm.check = chk;
+        s_dm.res0 = (chk == 0) ? nrm : c.res0;
+        s_dm.res = nrm;
+        s_dm.stop = (p.tol > 0.0) && (s_dm.res0 == 0.0 || nrm <= p.tol * s_dm.res0) ? 1 : 0;
+        s_act = 2;
+      }
     }
   }
   __syncthreads();
   int act = s_act;
-  double total = s_total;
+  jac::partial_msg pm = s_pm;
+  jac::decision_msg dm = s_dm;
   __syncthreads();
   if (act == 1) {
-    jac::partial_msg pm;
-    pm.check = chk;
-    pm.slot = (d.rank - 1) % 2;
-    pm.value = total;
     jproxy->invoke(d.parent, EP_PARTIAL, &pm, sizeof(pm));
   } else if (act == 2) {
-    const jac::prob_desc& p = japp::probs()[d.prob];
-    jac::decision_msg m;
-    double nrm = sqrt(total);
-    m.check = chk;
-    m.res0 = (chk == 0) ? nrm : c.res0;
-    m.res = nrm;
-    m.stop = (p.tol > 0.0) && (m.res0 == 0.0 || nrm <= p.tol * m.res0) ? 1 : 0;
-    return apply_decision<T>(c, d, m);
+    return apply_decision<T>(c, d, dm);
   }
   return 0;
 }
@@ -90,9 +95,10 @@ template <typename T>
 __device__ void advance(JBlock& c, const jac::chare_desc& d) {
   const jac::prob_desc& p = japp::probs()[d.prob];
   int K = p.check_every;
-  bool resid = K > 0 && (c.iter % K == 0);
+  // read before thread 0 advances the chare below
+  const bool resid = K > 0 && (c.iter % K == 0);
+  const int chk = K > 0 ? c.iter / K : 0;
   double part = sweep_block<T>(d, c.cur, resid);
-  int chk = K > 0 ? c.iter / K : 0;
   if (threadIdx.x == 0) {
     c.got[c.iter & 1] = 0;
     c.cur ^= 1;
@@ -214,15 +220,23 @@ __device__ void em_partial_t(JBlock& c, void* arg) {
   const jac::chare_desc& d = japp::chares()[c.i];
   const jac::partial_msg* pm = reinterpret_cast<const jac::partial_msg*>(arg);
   int chk = pm->check;
-  if (!CHARM_VERIFY(pm->slot == 0 || pm->slot == 1, CHARMING_ERR_APP, 5000 + pm->slot, c.i) ||
-      !CHARM_VERIFY(d.child[pm->slot] >= 0 && !c.child_got[pm->slot], CHARMING_ERR_APP,
-                    6000 + pm->slot, c.i))
-    return;
+  // Thread 0 checks and records the partial; the others learn the outcome
+  // after the barrier (reading child_got themselves would race with it).
+  __shared__ int s_ok;
   if (threadIdx.x == 0) {
-    c.child_val[pm->slot] = pm->value;
-    c.child_got[pm->slot] = 1;
+    bool ok = CHARM_VERIFY(pm->slot == 0 || pm->slot == 1, CHARMING_ERR_APP, 5000 + pm->slot, c.i) &&
+              CHARM_VERIFY(d.child[pm->slot] >= 0 && !c.child_got[pm->slot], CHARMING_ERR_APP,
+                           6000 + pm->slot, c.i);
+    if (ok) {
+      c.child_val[pm->slot] = pm->value;
+      c.child_got[pm->slot] = 1;
+    }
+    s_ok = ok ? 1 : 0;
   }
   __syncthreads();
+  int ok = s_ok;
+  __syncthreads();
+  if (!ok) return;
   if (tree_try_forward<T>(c, d, chk)) pump<T>(c, d);
 }
 

@@ -129,6 +129,7 @@ __device__ double sweep_direct(block_view<T> in, block_view<T> out, int w, int h
 // ---------------------------------------------------------------------------
 // TMA row pipeline.
 // ---------------------------------------------------------------------------
+#ifndef CHARMING_HOST_EMULATION
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
@@ -179,6 +180,19 @@ __device__ __forceinline__ bool mbar_test_wait(unsigned long long* b, unsigned p
       : "=r"(done) : "r"(smem_u32(b)), "r"(parity) : "memory");
   return done != 0;
 }
+#else
+// The CPU check of the chare code models these (tests/emu).
+void mbar_init(unsigned long long* b, unsigned count);
+void mbar_inval(unsigned long long* b);
+void mbar_expect_tx(unsigned long long* b, unsigned bytes);
+bool mbar_try_wait(unsigned long long* b, unsigned parity);
+bool mbar_test_wait(unsigned long long* b, unsigned parity);
+void mbar_arrive(unsigned long long* b);
+void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar);
+inline void fence_proxy_async_global() {}
+inline void fence_proxy_async_smem() {}
+inline void fence_mbar_init() {}
+#endif
 
 constexpr int MAX_SLOTS = 64;        // mbarrier pairs in the first 1 KiB
 constexpr int BAR_BYTES = 2 * MAX_SLOTS * 8;

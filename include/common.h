@@ -42,6 +42,8 @@ extern __constant__ int c_n_pes_node;
 
 // Dynamic shared memory of the scheduler kernel. The runtime keeps its
 // per-PE state at the front; charm::smem_scratch() hands out the rest.
+#ifndef CHARMING_HOST_EMULATION  // the CPU check of app code has no PE block memory
 extern __shared__ uint64_t s_mem[];
+#endif
 
 #endif // _COMMON_H_

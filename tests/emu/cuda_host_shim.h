@@ -1,12 +1,23 @@
 // Host-compilation shim for the Jacobi chare code (TEST INFRASTRUCTURE).
 //
 // Lets g++ compile charming_b200/csrc/apps/jacobi2d.cu for the CPU, so that
-// the exact C++ of the chare state machine, halo pack/unpack and direct
-// sweep can run under AddressSanitizer. Each emulated PE is one host thread
-// and its PE block has a single thread (blockDim.x == 1, threadIdx.x == 0):
-// block-level barriers become no-ops and block-static __shared__ variables
-// become thread_local. The TMA pipeline is excluded
-// (CHARMING_HOST_EMULATION); tests/emu/jacobi_emu.cpp provides the runtime.
+// the exact C++ of the chare state machine, halo pack/unpack and both
+// sweeps runs on host threads (tests/emu/jacobi_emu.cpp provides the
+// runtime). Two builds:
+//
+//   default  one host thread per PE, blockDim.x == 1; block-static
+//            __shared__ variables become thread_local (one per PE). Built
+//            with AddressSanitizer: catches out-of-bounds accesses of the
+//            chare logic across many PEs and message orders. Direct sweep.
+//   EMU_MT   one PE whose block has blockDim.x host threads; __shared__
+//            variables are plain statics shared by the block, and
+//            __syncthreads() is a real barrier that checks every thread
+//            arrives at the same call site (a barrier reached from
+//            different places aborts the run). Warp-level calls run the
+//            32 threads of a warp in lockstep, and the TMA sweep runs on a
+//            model of mbarriers and asynchronous bulk copies. Built with
+//            ThreadSanitizer: catches thread-0-writes / other-threads-read
+//            races that a one-thread block cannot show.
 #pragma once
 
 #include <atomic>
@@ -22,7 +33,11 @@
 #define __global__
 #define __forceinline__ inline
 #define __constant__
+#ifdef EMU_MT
+#define __shared__ static
+#else
 #define __shared__ thread_local
+#endif
 #define __launch_bounds__(...)
 #define __restrict__
 
@@ -34,15 +49,41 @@ extern thread_local emu_dim3 blockIdx;
 extern emu_dim3 blockDim;
 extern emu_dim3 gridDim;
 
-inline void __syncthreads() {}
+// Block barrier of the calling PE; `file`/`line` identify the call site.
+void emu_sync(const char* file, int line);
+#define __syncthreads() emu_sync(__FILE__, __LINE__)
+
+#ifdef EMU_MT
+// Warps of 32 host threads in lockstep at every warp-level call; the TMA
+// sweep runs on modelled mbarriers and bulk copies (jacobi_emu.cpp).
+#define CHARMING_HOST_EMULATION_TMA 1
+void emu_syncwarp(const char* file, int line);
+#define __syncwarp(...) emu_syncwarp(__FILE__, __LINE__)
+bool emu_all_sync(bool p);
+void emu_shfl(void* v, unsigned bytes, int mode, int arg);  // mode 0 up, 1 down, 2 xor
+inline bool __all_sync(unsigned, bool p) { return emu_all_sync(p); }
+template <typename T> inline T __shfl_up_sync(unsigned, T v, int d) {
+  emu_shfl(&v, sizeof(T), 0, d);
+  return v;
+}
+template <typename T> inline T __shfl_down_sync(unsigned, T v, int d) {
+  emu_shfl(&v, sizeof(T), 1, d);
+  return v;
+}
+template <typename T> inline T __shfl_xor_sync(unsigned, T v, int m) {
+  emu_shfl(&v, sizeof(T), 2, m);
+  return v;
+}
+#else
 inline void __syncwarp(unsigned = 0xffffffffu) {}
-inline void __threadfence() { std::atomic_thread_fence(std::memory_order_seq_cst); }
-inline void __nanosleep(unsigned) {}
-inline bool __isLocal(const void*) { return true; }
 inline bool __all_sync(unsigned, bool p) { return p; }
 template <typename T> inline T __shfl_xor_sync(unsigned, T v, int) { return v; }
 template <typename T> inline T __shfl_up_sync(unsigned, T v, int) { return v; }
 template <typename T> inline T __shfl_down_sync(unsigned, T v, int) { return v; }
+#endif
+inline void __threadfence() { std::atomic_thread_fence(std::memory_order_seq_cst); }
+inline void __nanosleep(unsigned) {}
+inline bool __isLocal(const void*) { return true; }
 inline long long clock64() { return 0; }
 
 template <typename T> inline T atomicAdd(T* p, T v) { return __atomic_fetch_add(p, v, __ATOMIC_SEQ_CST); }
@@ -53,8 +94,9 @@ template <typename T> inline T atomicCAS(T* p, T c, T v) {
   return c;
 }
 template <typename T> inline T atomicMin(T* p, T v) {
-  T old = *p;
-  if (v < old) *p = v;
+  T old = __atomic_load_n(p, __ATOMIC_SEQ_CST);
+  while (v < old && !__atomic_compare_exchange_n(p, &old, v, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST)) {
+  }
   return old;
 }
 
@@ -74,3 +116,6 @@ inline float4 make_float4(float a, float b, float c, float d) { return float4{a,
 using std::min;
 using std::max;
 inline size_t __cvta_generic_to_shared(const void* p) { return (size_t)p; }
+
+// Stand-in for the scheduler's dynamic shared memory (referenced, unused).
+extern uint64_t s_mem[];

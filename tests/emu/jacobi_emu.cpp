@@ -2,15 +2,18 @@
 //
 // Compiles charming_b200/csrc/apps/jacobi2d.cu for the host (see
 // cuda_host_shim.h) and runs it on an in-process stand-in for the device
-// runtime: one host thread per PE, per-PE FIFO inboxes, the refnum stash
-// with revive-in-arrival-order, end() as a global flag. Built with
-// AddressSanitizer, so any out-of-bounds access of the chare logic (halo
-// pack/unpack, tree slots, descriptors) aborts the run. The sweep is the
-// direct-load path; the final grid is compared bit for bit with the serial
-// oracle (oracle/jacobi_oracle.c).
+// runtime with the same block-collective contract: every thread of a PE
+// block runs the scheduler loop, thread 0 picks the next message, all
+// threads run the entry method, sends are collective (thread 0 enqueues
+// thread 0's buffer). Per-PE FIFO inboxes, the refnum stash with
+// revive-in-arrival-order, end() as a global flag. The final grid is
+// compared bit for bit with the serial oracle (oracle/jacobi_oracle.c).
 //
 // usage: jacobi_emu nx ny px py max_sweeps check_every tol dtype(0 f64|1 f32)
-//                   n_pes halo_mode [bc_top bc_bottom bc_left bc_right]
+//                   n_pes halo_mode [bc_top bc_bottom bc_left bc_right] [seed]
+//                   [threads_per_pe] [pipeline 0|1] [tile_w]
+// (the EMU_MT build takes n_pes == 1 and threads_per_pe >= 1, a multiple of
+// 32 with pipeline 1; the default build takes threads_per_pe == 1)
 // prints: status=<code> sweeps=<n> res0=<x> res_last=<x> exact=<0|1>
 #include "cuda_host_shim.h"
 #include <charming.h>
@@ -18,11 +21,12 @@
 #include "../../charming_b200/csrc/apps/jacobi_types.cuh"
 #include "../../charming_b200/csrc/apps/jacobi_sweep.cuh"
 
-#include <barrier>
 #include <chrono>
+#include <condition_variable>
 #include <deque>
 #include <mutex>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 extern "C" int oracle_jacobi2d_f64(double* grid, int nx, int ny, int sweeps);
@@ -33,7 +37,7 @@ thread_local emu_dim3 blockIdx{0, 0, 0};
 emu_dim3 blockDim{1, 1, 1};
 emu_dim3 gridDim{1, 1, 1};
 int c_n_sms, c_my_dev, c_my_dev_node, c_n_devs, c_n_devs_node, c_n_nodes, c_n_pes, c_n_pes_node;
-thread_local uint64_t s_mem[16];
+uint64_t s_mem[16];
 namespace charm { namespace rt { device_state c_rt; } }
 suite::app_params g_app;
 
@@ -46,11 +50,59 @@ struct Stashed {
   bool ready;
 };
 
+// Barrier of one PE block (or warp) that also checks that all threads
+// arrive from the same call site.
+struct SiteBarrier {
+  std::mutex m;
+  std::condition_variable cv;
+  int n = 1, count = 0;
+  unsigned long long gen = 0;
+  const char* file = nullptr;
+  int line = 0;
+  void sync(const char* f, int l) {
+    std::unique_lock<std::mutex> lk(m);
+    if (count == 0) {
+      file = f;
+      line = l;
+    } else if (l != line || strcmp(f, file) != 0) {
+      fprintf(stderr, "barrier divergence: thread %u at %s:%d, others at %s:%d\n", threadIdx.x, f,
+              l, file, line);
+      fflush(stderr);
+      _exit(3);
+    }
+    if (++count == n) {
+      count = 0;
+      gen++;
+      cv.notify_all();
+    } else {
+      unsigned long long g = gen;
+      cv.wait(lk, [&] { return gen != g; });
+    }
+  }
+};
+
 struct PE {
   std::mutex mu;
   std::deque<bytes_t> inbox;
   charm::chare_proxy_table table;
   std::deque<Stashed> stash;  // arrival order
+  SiteBarrier bar;
+  // broadcast slots of the block (written by thread 0 before a barrier)
+  bytes_t cur;
+  int action = 0;
+  unsigned char* ubuf = nullptr;
+  size_t ucap = 0;
+  std::vector<double> red;
+  int revive = 0;
+  alignas(128) unsigned char smem[1 << 16];  // charm::smem_scratch() of the block
+#ifdef EMU_MT
+  struct Warp {
+    SiteBarrier bar;
+    unsigned char slot[32][8];
+    bool flag[32];
+  };
+  std::vector<Warp*> warps;
+#endif
 };
 
 std::vector<PE*> g_pes;
@@ -58,9 +110,10 @@ std::atomic<int> g_term{0};
 std::atomic<int> g_status{0};
 std::atomic<long long> g_progress{0};
 int g_err_a = 0, g_err_b = 0;
-thread_local int tl_revive = 0;
-alignas(128) thread_local unsigned char tl_smem[1 << 16];
-std::barrier<>* g_barrier = nullptr;
+std::mutex g_err_mu;
+SiteBarrier g_grid;  // charm::barrier(): all threads of all PEs
+
+PE& me_pe() { return *g_pes[blockIdx.x]; }
 
 bytes_t make_msg(charm::msgtype type, int chare_id, int idx, int ep, int ref, const void* buf,
     size_t size) {
@@ -90,6 +143,161 @@ void push(int dst, bytes_t&& b) {
 
 }  // namespace
 
+void emu_sync(const char* file, int line) { me_pe().bar.sync(file, line); }
+
+#ifdef EMU_MT
+// ---- warps: the 32 threads of a warp meet at every warp-level call ----------
+namespace {
+PE::Warp& my_warp() { return *me_pe().warps[threadIdx.x / 32]; }
+}  // namespace
+void emu_syncwarp(const char* file, int line) { my_warp().bar.sync(file, line); }
+bool emu_all_sync(bool p) {
+  PE::Warp& w = my_warp();
+  unsigned lane = threadIdx.x & 31;
+  w.flag[lane] = p;
+  w.bar.sync("all_sync", 0);
+  bool r = true;
+  for (int i = 0; i < 32; i++) r = r && w.flag[i];
+  w.bar.sync("all_sync", 1);
+  return r;
+}
+void emu_shfl(void* v, unsigned bytes, int mode, int arg) {
+  PE::Warp& w = my_warp();
+  int lane = (int)(threadIdx.x & 31);
+  memcpy(w.slot[lane], v, bytes);
+  w.bar.sync("shfl", 0);
+  int src = lane;
+  if (mode == 0 && lane - arg >= 0) src = lane - arg;
+  if (mode == 1 && lane + arg < 32) src = lane + arg;
+  if (mode == 2) src = lane ^ arg;
+  memcpy(v, w.slot[src], bytes);
+  w.bar.sync("shfl", 1);
+}
+
+// ---- mbarriers and bulk copies ----------------------------------------------
+// An mbarrier completes its phase when all expected arrivals happened and
+// the transaction count is back to zero; bulk copies run on an engine
+// thread, after a random delay, and count their bytes down on completion.
+namespace {
+struct Mbar {
+  int expected = 0, pending = 0;
+  long long tx = 0;
+  unsigned phase = 0;
+  int in_flight = 0;
+};
+std::mutex g_mb_mu;
+std::unordered_map<void*, Mbar> g_mb;
+struct Copy {
+  void* dst;
+  const void* src;
+  unsigned bytes;
+  void* bar;
+};
+std::mutex g_q_mu;
+std::condition_variable g_q_cv;
+std::deque<Copy> g_q;
+bool g_q_stop = false;
+std::vector<std::pair<const unsigned char*, size_t>> g_src_ranges;  // readable grid buffers
+
+void tma_fail(const char* what, const void* p) {
+  fprintf(stderr, "tma model: %s (%p)\n", what, p);
+  fflush(stderr);
+  _exit(5);
+}
+Mbar& mb_locked(void* b) {
+  auto it = g_mb.find(b);
+  if (it == g_mb.end()) tma_fail("mbarrier used before init or after inval", b);
+  return it->second;
+}
+void mb_complete_locked(Mbar& m) {
+  if (m.pending == 0 && m.tx == 0) {
+    m.phase++;
+    m.pending = m.expected;
+  }
+}
+void engine() {
+  unsigned rng = 12345;
+  while (true) {
+    Copy c;
+    {
+      std::unique_lock<std::mutex> lk(g_q_mu);
+      g_q_cv.wait(lk, [] { return g_q_stop || !g_q.empty(); });
+      if (g_q.empty()) return;
+      c = g_q.front();
+      g_q.pop_front();
+    }
+    rng = rng * 1103515245u + 12345u;
+    if ((rng >> 16) % 3 == 0) std::this_thread::sleep_for(std::chrono::microseconds((rng >> 8) % 50));
+    memcpy(c.dst, c.src, c.bytes);
+    std::lock_guard<std::mutex> lk(g_mb_mu);
+    Mbar& m = mb_locked(c.bar);
+    m.tx -= c.bytes;
+    m.in_flight--;
+    if (m.tx < 0) tma_fail("more bytes completed than expected", c.bar);
+    mb_complete_locked(m);
+  }
+}
+}  // namespace
+
+namespace jac {
+void mbar_init(unsigned long long* b, unsigned count) {
+  std::lock_guard<std::mutex> lk(g_mb_mu);
+  if (g_mb.count(b)) tma_fail("mbarrier initialised twice without inval", b);
+  if (reinterpret_cast<uintptr_t>(b) & 7) tma_fail("mbarrier not 8-byte aligned", b);
+  Mbar m;
+  m.expected = m.pending = (int)count;
+  g_mb[b] = m;
+}
+void mbar_inval(unsigned long long* b) {
+  std::lock_guard<std::mutex> lk(g_mb_mu);
+  Mbar& m = mb_locked(b);
+  if (m.in_flight || m.tx) tma_fail("mbarrier invalidated with copies in flight", b);
+  g_mb.erase(b);
+}
+void mbar_expect_tx(unsigned long long* b, unsigned bytes) {
+  std::lock_guard<std::mutex> lk(g_mb_mu);
+  Mbar& m = mb_locked(b);
+  m.tx += bytes;
+  if (--m.pending < 0) tma_fail("more arrivals than expected", b);
+  mb_complete_locked(m);
+}
+void mbar_arrive(unsigned long long* b) {
+  std::lock_guard<std::mutex> lk(g_mb_mu);
+  Mbar& m = mb_locked(b);
+  if (--m.pending < 0) tma_fail("more arrivals than expected", b);
+  mb_complete_locked(m);
+}
+bool mbar_test_wait(unsigned long long* b, unsigned parity) {
+  std::lock_guard<std::mutex> lk(g_mb_mu);
+  return (mb_locked(b).phase & 1u) != (parity & 1u);
+}
+bool mbar_try_wait(unsigned long long* b, unsigned parity) {
+  bool ok = mbar_test_wait(b, parity);
+  if (!ok) std::this_thread::yield();
+  return ok;
+}
+void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  if ((reinterpret_cast<uintptr_t>(dst) & 15) || (reinterpret_cast<uintptr_t>(src) & 15) ||
+      (bytes & 15) || bytes == 0)
+    tma_fail("bulk copy not 16-byte aligned", src);
+  PE& pe = me_pe();
+  const unsigned char* d = static_cast<const unsigned char*>(dst);
+  if (d < pe.smem || d + bytes > pe.smem + sizeof(pe.smem)) tma_fail("bulk copy outside shared memory", dst);
+  const unsigned char* s = static_cast<const unsigned char*>(src);
+  bool ok = false;
+  for (auto& r : g_src_ranges) ok = ok || (s >= r.first && s + bytes <= r.first + r.second);
+  if (!ok) tma_fail("bulk copy source outside every grid buffer", src);
+  {
+    std::lock_guard<std::mutex> lk(g_mb_mu);
+    mb_locked(bar).in_flight++;
+  }
+  std::lock_guard<std::mutex> lk(g_q_mu);
+  g_q.push_back(Copy{dst, src, bytes, bar});
+  g_q_cv.notify_one();
+}
+}  // namespace jac
+#endif
+
 // ---- the runtime interface the chare code uses ------------------------------
 namespace charm {
 int my_pe() { return (int)blockIdx.x; }
@@ -105,10 +313,11 @@ uint64_t now_ns() {
 }
 unsigned int smid() { return blockIdx.x; }
 void* smem_scratch(size_t* bytes) {
-  if (bytes) *bytes = sizeof(tl_smem);
-  return tl_smem;
+  PE& pe = me_pe();
+  if (bytes) *bytes = sizeof(pe.smem);
+  return pe.smem;
 }
-void barrier() { g_barrier->arrive_and_wait(); }
+void barrier() { g_grid.sync("grid", 0); }
 void barrier_local() { barrier(); }
 int device_atoi(const char* s, int n) {
   int v = 0;
@@ -117,6 +326,7 @@ int device_atoi(const char* s, int n) {
 }
 namespace rt {
 void set_error(int code, int a, int b) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
   int z = 0;
   if (g_status.compare_exchange_strong(z, code)) {
     g_err_a = a;
@@ -126,65 +336,94 @@ void set_error(int code, int a, int b) {
 }
 }  // namespace rt
 namespace detail {
-chare_proxy_table& my_proxy_table() { return g_pes[blockIdx.x]->table; }
+chare_proxy_table& my_proxy_table() { return me_pe().table; }
 void report_error(int code, int a, int b) { rt::set_error(code, a, b); }
 }  // namespace detail
+
+// Block-collective, as on the device: thread 0's buffer is sent.
 void send_reg_msg(int chare_id, int chare_idx, int ep, void* buf, size_t size, int dst_pe,
     int refnum) {
-  push(dst_pe, make_msg(msgtype::regular, chare_id, chare_idx, ep, refnum, buf, size));
+  emu_sync(__FILE__, __LINE__);
+  if (threadIdx.x == 0) push(dst_pe, make_msg(msgtype::regular, chare_id, chare_idx, ep, refnum, buf, size));
+  emu_sync(__FILE__, __LINE__);
 }
 bool alloc_user_msg(message& msg, int dst_pe, size_t size) {
-  size_t total = envelope::alloc_size(msgtype::user, size);
-  unsigned char* p = new unsigned char[total]();
-  msg.env = reinterpret_cast<envelope*>(p);
+  PE& pe = me_pe();
+  if (threadIdx.x == 0) {
+    size_t total = envelope::alloc_size(msgtype::user, size);
+    pe.ubuf = new unsigned char[total]();
+    pe.ucap = total - 32;
+  }
+  emu_sync(__FILE__, __LINE__);
+  msg.env = reinterpret_cast<envelope*>(pe.ubuf);
   msg.offset = 0;
   msg.dst_pe = dst_pe;
   msg.cells = 0;
-  msg.capacity = total - 32;
-  return true;
+  msg.capacity = pe.ucap;
+  emu_sync(__FILE__, __LINE__);
+  return msg.env != nullptr;
 }
 void send_user_msg(int chare_id, int chare_idx, int ep, message& msg, size_t size, int refnum) {
   if (!msg.env) return;
-  if (size > msg.capacity) rt::set_error(CHARMING_ERR_MSG_TOO_LARGE, msg.dst_pe, (int)size);
-  unsigned char* p = reinterpret_cast<unsigned char*>(msg.env);
-  push(msg.dst_pe, make_msg(msgtype::user, chare_id, chare_idx, ep, refnum, p + 32, msg.capacity));
-  delete[] p;
+  emu_sync(__FILE__, __LINE__);  // payload writes of all threads are done
+  if (threadIdx.x == 0) {
+    if (size > msg.capacity) rt::set_error(CHARMING_ERR_MSG_TOO_LARGE, msg.dst_pe, (int)size);
+    unsigned char* p = reinterpret_cast<unsigned char*>(msg.env);
+    push(msg.dst_pe, make_msg(msgtype::user, chare_id, chare_idx, ep, refnum, p + 32, msg.capacity));
+    delete[] p;
+  }
+  emu_sync(__FILE__, __LINE__);
   msg.env = nullptr;
 }
-void revive_mismatches(int, int, int) { tl_revive = 1; }
+void revive_mismatches(int, int, int) { me_pe().revive = 1; }
 void send_begin_term_msg() { end(); }
 }  // namespace charm
 
 namespace suite {
-double block_sum_f64(double v) { return v; }
+// Fixed order (thread index) like the device's deterministic block sum.
+double block_sum_f64(double v) {
+  PE& pe = me_pe();
+  if (threadIdx.x == 0) pe.red.assign(blockDim.x, 0.0);
+  emu_sync(__FILE__, __LINE__);
+  pe.red[threadIdx.x] = v;
+  emu_sync(__FILE__, __LINE__);
+  double s = 0.0;
+  for (unsigned i = 0; i < blockDim.x; i++) s += pe.red[i];
+  emu_sync(__FILE__, __LINE__);
+  return s;
+}
 unsigned long long block_sum_u64(unsigned long long v) { return v; }
 unsigned long long checksum_block(const void*, unsigned long long n) { return n; }
 }  // namespace suite
 
 namespace {
 
-// Delivers one message on this PE: refnum check, entry method or stash.
-// Returns false when the message was parked.
-bool deliver(PE& pe, bytes_t& m) {
+enum { ACT_IDLE = 0, ACT_DELIVER = 1, ACT_STOP = 2 };
+
+// Thread 0: validates the message in pe.cur; returns ACT_DELIVER when its
+// refnum matches, else parks it in the stash (ACT_IDLE).
+int classify(PE& pe) {
+  bytes_t& m = pe.cur;
   auto* env = reinterpret_cast<charm::envelope*>(m.data());
   auto* rm = reinterpret_cast<charm::regular_msg*>(m.data() + sizeof(charm::envelope));
   if (env->size != m.size()) {
     charm::rt::set_error(CHARMING_ERR_BAD_MSG, (int)env->size, (int)m.size());
-    return true;
+    return ACT_IDLE;
   }
   if (rm->chare_id < 0 || rm->chare_id >= pe.table.count) {
     charm::rt::set_error(CHARMING_ERR_BAD_TARGET, rm->chare_id, -1);
-    return true;
+    return ACT_IDLE;
   }
   charm::chare_proxy_base* p = pe.table.proxies[rm->chare_id];
   if (!p->valid_target(rm->chare_idx, rm->ep_id)) {
     charm::rt::set_error(CHARMING_ERR_BAD_TARGET, rm->chare_id, rm->chare_idx);
-    return true;
+    return ACT_IDLE;
   }
-  if (!p->refnum_matches(rm->chare_idx, rm->refnum)) return false;
-  p->call(rm->chare_idx, rm->ep_id, m.data() + 32, rm->refnum);
-  g_progress++;
-  return true;
+  if (!p->refnum_matches(rm->chare_idx, rm->refnum)) {
+    pe.stash.push_back(Stashed{std::move(m), false});
+    return ACT_IDLE;
+  }
+  return ACT_DELIVER;
 }
 
 void revive(PE& pe) {
@@ -195,40 +434,59 @@ void revive(PE& pe) {
   }
 }
 
-void pe_main(int me, int seed) {
-  threadIdx = emu_dim3{0, 0, 0};
+// Thread 0: next action of the block (ready stash entries first, then the
+// inbox head).
+int next_action(PE& pe, unsigned& rng) {
+  if (g_term) return ACT_STOP;
+  if (pe.revive) {
+    pe.revive = 0;
+    revive(pe);
+  }
+  auto it = std::find_if(pe.stash.begin(), pe.stash.end(), [](const Stashed& s) { return s.ready; });
+  if (it != pe.stash.end()) {
+    pe.cur = std::move(it->msg);
+    pe.stash.erase(it);
+    return classify(pe);
+  }
+  {
+    std::lock_guard<std::mutex> lk(pe.mu);
+    if (!pe.inbox.empty()) {
+      pe.cur = std::move(pe.inbox.front());
+      pe.inbox.pop_front();
+    } else {
+      pe.cur.clear();
+    }
+  }
+  if (pe.cur.empty()) {
+    rng = rng * 1103515245u + 12345u;
+    if ((rng >> 16) % 4 == 0) std::this_thread::yield();
+    return ACT_IDLE;
+  }
+  return classify(pe);
+}
+
+void pe_thread(int me, int tid, int seed) {
+  threadIdx = emu_dim3{(unsigned)tid, 0, 0};
   blockIdx = emu_dim3{(unsigned)me, 0, 0};
   PE& pe = *g_pes[me];
   charm::barrier();
   suite::jacobi2d_main(me);
   charm::barrier();
   unsigned rng = 2654435761u * (unsigned)(me + 1) + (unsigned)seed;
-  while (!g_term) {
-    if (tl_revive) {
-      tl_revive = 0;
-      revive(pe);
+  while (true) {
+    if (tid == 0) pe.action = next_action(pe, rng);
+    emu_sync(__FILE__, __LINE__);
+    int act = pe.action;
+    if (act == ACT_STOP) break;
+    if (act == ACT_DELIVER) {
+      auto* rm = reinterpret_cast<charm::regular_msg*>(pe.cur.data() + sizeof(charm::envelope));
+      pe.table.proxies[rm->chare_id]->call(rm->chare_idx, rm->ep_id, pe.cur.data() + 32, rm->refnum);
     }
-    auto it = std::find_if(pe.stash.begin(), pe.stash.end(), [](const Stashed& s) { return s.ready; });
-    if (it != pe.stash.end()) {
-      bytes_t m = std::move(it->msg);
-      pe.stash.erase(it);
-      if (!deliver(pe, m)) pe.stash.push_back(Stashed{std::move(m), false});
-      continue;
+    emu_sync(__FILE__, __LINE__);
+    if (tid == 0 && act == ACT_DELIVER) {
+      g_progress++;
+      pe.cur.clear();
     }
-    bytes_t m;
-    {
-      std::lock_guard<std::mutex> lk(pe.mu);
-      if (!pe.inbox.empty()) {
-        m = std::move(pe.inbox.front());
-        pe.inbox.pop_front();
-      }
-    }
-    if (m.empty()) {
-      rng = rng * 1103515245u + 12345u;
-      if ((rng >> 16) % 4 == 0) std::this_thread::yield();
-      continue;
-    }
-    if (!deliver(pe, m)) pe.stash.push_back(Stashed{std::move(m), false});
   }
 }
 
@@ -250,7 +508,7 @@ void cell_init(const jac::chare_desc& d, const jac::prob_desc& p, const double* 
 
 template <typename T>
 int run(int nx, int ny, int px, int py, int max_sweeps, int K, double tol, int n_pes,
-    int halo_mode, const double bc[4], int seed) {
+    int halo_mode, const double bc[4], int seed, int threads, int pipeline, int tile_w) {
   constexpr int V = jac::traits<T>::VEC, OFF = jac::traits<T>::OFF;
   const int align_el = 128 / (int)sizeof(T);
   c_n_pes = c_n_pes_node = n_pes;
@@ -283,6 +541,9 @@ int run(int nx, int ny, int px, int py, int max_sweeps, int K, double tol, int n
         size_t bytes = ((size_t)d.pitch * (d.h + 2) * sizeof(T) + 255) / 256 * 256;
         d.buf[b] = aligned_alloc(256, bytes);
         memset(d.buf[b], 0, bytes);
+#ifdef EMU_MT
+        g_src_ranges.push_back({static_cast<const unsigned char*>(d.buf[b]), bytes});
+#endif
       }
     }
   }
@@ -306,8 +567,8 @@ int run(int nx, int ny, int px, int py, int max_sweeps, int K, double tol, int n
   g_app.a[0] = nc;
   g_app.a[1] = 1;
   g_app.a[2] = sizeof(T) == 8 ? CHARMING_F64 : CHARMING_F32;
-  g_app.a[3] = 0;
-  g_app.a[4] = 0;
+  g_app.a[3] = pipeline;
+  g_app.a[4] = tile_w;
   g_app.a[5] = halo_mode;
   g_app.p[0] = ch.data();
   g_app.p[1] = &pd;
@@ -317,12 +578,27 @@ int run(int nx, int ny, int px, int py, int max_sweeps, int K, double tol, int n
   g_app.p[5] = block_map.data();
   g_app.p[6] = sweep_ns.data();
 
-  for (int p = 0; p < n_pes; p++) g_pes.push_back(new PE());
-  std::barrier<> bar(n_pes);
-  g_barrier = &bar;
+  blockDim = emu_dim3{(unsigned)threads, 1, 1};
+  gridDim = emu_dim3{(unsigned)n_pes, 1, 1};
+  for (int p = 0; p < n_pes; p++) {
+    g_pes.push_back(new PE());
+    g_pes.back()->bar.n = threads;
+#ifdef EMU_MT
+    for (int w = 0; w < (threads + 31) / 32; w++) {
+      g_pes.back()->warps.push_back(new PE::Warp());
+      g_pes.back()->warps.back()->bar.n = 32;
+    }
+#endif
+  }
+  g_grid.n = n_pes * threads;
+#ifdef EMU_MT
+  std::thread tma_engine(engine);
+#endif
   std::vector<std::thread> th;
-  for (int p = 0; p < n_pes; p++) th.emplace_back(pe_main, p, seed);
-  // watchdog: stop when nothing was delivered for 3 s
+  for (int p = 0; p < n_pes; p++)
+    for (int t = 0; t < threads; t++) th.emplace_back(pe_thread, p, t, seed);
+  // watchdog: stop when nothing was delivered for 3 s; a block that does
+  // not leave its loop 5 s after that is stuck in a barrier
   long long last = -1;
   auto t_last = std::chrono::steady_clock::now();
   while (!g_term) {
@@ -335,7 +611,21 @@ int run(int nx, int ny, int px, int py, int max_sweeps, int K, double tol, int n
       charm::rt::set_error(CHARMING_ERR_IDLE_TIMEOUT, 0, 0);
     }
   }
+  std::thread([] {
+    std::this_thread::sleep_for(std::chrono::seconds(5));
+    fprintf(stderr, "blocks did not stop (stuck in a barrier)\n");
+    fflush(stderr);
+    _exit(4);
+  }).detach();
   for (auto& t : th) t.join();
+#ifdef EMU_MT
+  {
+    std::lock_guard<std::mutex> lk(g_q_mu);
+    g_q_stop = true;
+    g_q_cv.notify_all();
+  }
+  tma_engine.join();
+#endif
 
   // gather the final grid and compare with the serial oracle
   std::vector<T> grid((size_t)(nx + 2) * (ny + 2)), ref(grid.size());
@@ -380,6 +670,20 @@ int main(int argc, char** argv) {
   double bc[4] = {1.0, 0.0, 0.0, 0.0};
   if (argc >= 15) for (int k = 0; k < 4; k++) bc[k] = atof(argv[11 + k]);
   int seed = argc >= 16 ? atoi(argv[15]) : 1;
-  return dtype == 0 ? run<double>(nx, ny, px, py, ms, K, tol, n_pes, halo, bc, seed)
-                    : run<float>(nx, ny, px, py, ms, K, tol, n_pes, halo, bc, seed);
+  int threads = argc >= 17 ? atoi(argv[16]) : 1;
+  int pipeline = argc >= 18 ? atoi(argv[17]) : 0;
+  int tile_w = argc >= 19 ? atoi(argv[18]) : 0;
+#ifdef EMU_MT
+  if (n_pes != 1 || threads < 1 || (pipeline && threads % 32)) {
+    fprintf(stderr, "the threaded build runs one PE block (n_pes 1); the bulk-copy sweep needs whole warps\n");
+    return 2;
+  }
+#else
+  if (threads != 1 || pipeline) {
+    fprintf(stderr, "the default build runs one thread per PE and the direct sweep\n");
+    return 2;
+  }
+#endif
+  return dtype == 0 ? run<double>(nx, ny, px, py, ms, K, tol, n_pes, halo, bc, seed, threads, pipeline, tile_w)
+                    : run<float>(nx, ny, px, py, ms, K, tol, n_pes, halo, bc, seed, threads, pipeline, tile_w);
 }

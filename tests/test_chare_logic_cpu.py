@@ -1,8 +1,11 @@
 """CPU check of the Jacobi chare code: jacobi2d.cu compiled for the host
-(tests/emu) and run on an in-process stand-in for the runtime, one host
-thread per PE, under AddressSanitizer/UBSan; the grid must match the serial
-oracle bit for bit and the residual stop rule must stop where the oracle
-says."""
+(tests/emu) and run on an in-process stand-in for the runtime. Two builds:
+one host thread per PE under AddressSanitizer/UBSan (many PEs, random
+message orders), and one PE block of many host threads under
+ThreadSanitizer, with call-site-checked barriers, lockstep warps and a model
+of mbarriers and asynchronous bulk copies for the TMA sweep. The grid must
+match the serial oracle bit for bit and the residual stop rule must stop
+where the oracle says."""
 import os
 import subprocess
 
@@ -15,6 +18,7 @@ from oracle.jacobi_protocol import ProtocolError, Sim
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 EMU = os.path.join(ROOT, "build", "emu", "jacobi_emu")
+EMU_MT = os.path.join(ROOT, "build", "emu", "jacobi_emu_mt")
 
 
 @pytest.fixture(scope="module")
@@ -26,10 +30,11 @@ def emu():
     return EMU
 
 
-def run_emu(emu, nx, ny, px, py, max_sweeps, K, tol, dtype, n_pes, halo, bc, seed=1):
-    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0")
+def run_emu(emu, nx, ny, px, py, max_sweeps, K, tol, dtype, n_pes, halo, bc, seed=1,
+            threads=1, pipeline=0, tile_w=0):
+    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0", TSAN_OPTIONS="halt_on_error=1")
     args = [emu] + [str(x) for x in (nx, ny, px, py, max_sweeps, K, tol, dtype, n_pes, halo)]
-    args += [str(b) for b in bc] + [str(seed)]
+    args += [str(b) for b in bc] + [str(seed), str(threads), str(pipeline), str(tile_w)]
     r = subprocess.run(args, capture_output=True, text=True, timeout=300, env=env)
     line = r.stdout.strip().splitlines()[-1] if r.stdout.strip() else ""
     fields = dict(kv.split("=", 1) for kv in line.split())
@@ -81,3 +86,27 @@ def test_protocol_model_random_orders(px, py, K, mx, stop_at):
     for seed in range(25):
         ends.add(Sim(px, py, K, mx, stop_at, seed).run())
     assert len(ends) == 1
+
+
+@pytest.mark.parametrize("cfg", [
+    # nx, ny, px, py, max_sweeps, K, tol, dtype, halo_mode, threads, pipeline, tile_w
+    (96, 80, 3, 2, 3000, 10, 0.05, 0, 0, 64, 1, 0),     # the residual stop rule, TMA sweep
+    (96, 80, 3, 2, 3000, 10, 0.05, 1, 1, 32, 0, 0),
+    (200, 150, 4, 3, 60, 1, 0.2, 0, 0, 64, 1, 64),      # several column tiles
+    (333, 97, 2, 2, 13, 0, 0.0, 0, 1, 96, 1, 0),
+    (50, 70, 1, 3, 40, 3, 0.3, 1, 0, 32, 1, 0),
+    (64, 64, 1, 1, 25, 5, 0.1, 0, 0, 40, 0, 0),          # single chare, odd block size
+])
+def test_chare_code_threaded_block(emu, cfg):
+    """One PE block of many threads: barriers reached from different call
+    sites, races between thread 0 and the rest, and misuse of mbarriers or
+    bulk copies abort the run."""
+    nx, ny, px, py, ms, K, tol, dt, halo, thr, pl, tw = cfg
+    bc = (1.0, 0.25, 0.5, 0.0)
+    rc, f, err = run_emu(EMU_MT, nx, ny, px, py, ms, K, tol, dt, 1, halo, bc,
+                         threads=thr, pipeline=pl, tile_w=tw)
+    assert "ThreadSanitizer" not in err and "divergence" not in err, err[-3000:]
+    assert rc == 0 and f.get("status") == "0" and f.get("exact") == "1", (f, err[-2000:])
+    assert int(f["done"]) == px * py
+    if K > 0:
+        assert int(f["sweeps"]) == expected_stop(nx, ny, K, tol, ms, bc, dt)
