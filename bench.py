@@ -228,7 +228,7 @@ def main() -> int:
     ap.add_argument("--impl", default="charming", choices=["charming", "reference"])
     ap.add_argument("--px", type=int, default=0)
     ap.add_argument("--py", type=int, default=0)
-    ap.add_argument("--pipeline", type=int, default=1)
+    ap.add_argument("--pipeline", type=int, default=0, help="1: TMA row pipeline, 0: direct loads")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--nx", type=int, default=NX, help="grid size (profiling runs)")
