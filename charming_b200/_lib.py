@@ -131,6 +131,7 @@ SIGNATURES = [
     ("charming_jacobi2d_result", i32, [vp, i32, C.POINTER(JacobiResult)]),
     ("charming_jacobi2d_get_info", i32, [vp, C.POINTER(JacobiInfo)]),
     ("charming_jacobi2d_destroy", i32, [vp]),
+    ("charming_jacobi2d_sweeps_noalloc", i32, [i32, i32, i32, i32, vp, vp]),
     ("charming_jacobi1d", i32, [i32, i32, i32, C.POINTER(f64), C.POINTER(f64)]),
     ("charming_pingpong", i32, [C.POINTER(u64), i32, i32, i32, u64, i32, C.POINTER(PingpongResult), C.POINTER(i32)]),
     ("charming_fanout", i32, [i32, i32, i32, u64, i32, C.POINTER(C.c_uint32), u64, C.POINTER(u64), C.POINTER(f64)]),

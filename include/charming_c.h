@@ -192,6 +192,23 @@ int charming_jacobi2d_result(void* handle, int prob, charming_jacobi_result* out
 int charming_jacobi2d_get_info(void* handle, charming_jacobi_info* out);
 int charming_jacobi2d_destroy(void* handle);
 
+/* Sweeps one grid without allocating device memory (no counterpart in the
+ * reference). For callers that must not allocate: code that serves this
+ * library device buffers from its own pool and forbids other allocations,
+ * or that cannot afford the device synchronisation a cudaMalloc implies.
+ * dev_in and dev_out are device grids of (ny+2)*(nx+2) values of dtype,
+ * row-major with the boundary ring, not overlapping; dev_out receives the
+ * grid after `sweeps` sweeps, equal bit for bit to charming_jacobi2d_run's
+ * result with max_sweeps = sweeps and check_every = 0. The second grid
+ * lives in a 16 MiB scratch array inside the library (one per GPU, held
+ * until exit), so (nx+2)*(ny+2)*element size must be <= 16 MiB, else
+ * CHARMING_ERR_CONFIG. Works on the current device and the legacy default
+ * stream and returns when done. The first call on a device looks up the
+ * scratch's device address; make it before any stream capture. All calls
+ * share the scratch: calls that overlap on the GPU race. */
+int charming_jacobi2d_sweeps_noalloc(int dtype, int nx, int ny, int sweeps,
+    const void* dev_in, void* dev_out);
+
 /* 1-D Jacobi chares (examples/jacobi1d/jacobi1d.cu:62-170): n_chares blocks
  * of `width` points, 5-point window sum/5, boundary 10 and interior 0 as in
  * that example; result is the (n_chares*width + 4)-point array. */
