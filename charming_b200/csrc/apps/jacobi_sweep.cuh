@@ -12,7 +12,8 @@
 // on a 128-byte boundary (OFF = 128 / sizeof(T)).
 //
 // Two implementations with identical results:
-//   sweep_direct: every thread loads its 5 points from global memory.
+//   sweep_direct: warps walk column strips down the rows, keeping three
+//                 rows in registers (each input row loaded once per strip).
 //   sweep_tma:    rows stream through a ring of shared-memory slots filled
 //                 by cp.async.bulk (TMA 1-D bulk copies, no multicast), one
 //                 mbarrier per slot; each input row is read from HBM once
@@ -105,11 +106,12 @@ __device__ __forceinline__ double compute_vec(const T* up, const T* mid, const T
 }
 
 // ---------------------------------------------------------------------------
-// Direct-load sweep: thread i of the block handles vectors i, i+n, ... of
-// the (h rows x ceil(w/VEC) vectors) output.
+// Direct-load sweep, simple form: thread i of the block handles vectors
+// i, i+n, ... of the (h rows x ceil(w/VEC) vectors) output. Used for blocks
+// of fewer than 32 threads.
 // ---------------------------------------------------------------------------
 template <typename T, bool RESID>
-__device__ double sweep_direct(block_view<T> in, block_view<T> out, int w, int h) {
+__device__ double sweep_simple(block_view<T> in, block_view<T> out, int w, int h) {
   constexpr int V = traits<T>::VEC;
   const int nv = (w + V - 1) / V;
   const long long total = (long long)nv * h;
@@ -122,6 +124,159 @@ __device__ double sweep_direct(block_view<T> in, block_view<T> out, int w, int h
     int nvalid = min(V, w - v * V);
     acc += compute_vec<T, RESID>(in.at(r - 1, j0), mid, in.at(r + 1, j0), mid[-1], mid[V],
                                  out.at(r, j0), nvalid);
+  }
+  return acc;
+}
+
+// ---------------------------------------------------------------------------
+// Direct-load sweep, strip walker. The block's work is split into items: a
+// column strip of 32*J vectors (lane l of a warp owns vectors l, l+32, ...)
+// times a run of rows. A warp walks its rows top to bottom keeping the
+// rows above, at and below the output row in registers, so each input row
+// is loaded once per strip; it loads G rows ahead at a time, which keeps
+// G*J 16-byte loads per thread in flight. Left/right neighbours come from
+// the neighbouring lanes by shuffle; only the strip's two edge columns are
+// loaded as scalars. No block barrier inside the sweep.
+// ---------------------------------------------------------------------------
+template <typename T> struct vec_of;
+template <> struct vec_of<double> { using type = double2; };
+template <> struct vec_of<float> { using type = float4; };
+
+template <typename T, int J>
+struct walk_row {
+  typename vec_of<T>::type v[J];
+  T left, right;  // columns just outside the strip (same for all lanes)
+};
+
+template <typename T>
+__device__ __forceinline__ T vec_elem(const double2& x, int k) { return (T)(k == 0 ? x.x : x.y); }
+template <typename T>
+__device__ __forceinline__ T vec_elem(const float4& x, int k) {
+  return (T)(k == 0 ? x.x : k == 1 ? x.y : k == 2 ? x.z : x.w);
+}
+
+// Loads row r of a strip: vector v_j = vbase + lane + 32 j when v_j <= nv
+// (vector nv holds the right ghost column and padding, inside the pitched
+// row), plus the two edge scalars.
+template <typename T, int J>
+__device__ __forceinline__ void walk_load(walk_row<T, J>& R, const block_view<T>& in, int r,
+    int vbase, int nv, int lane, bool has_right) {
+  constexpr int V = traits<T>::VEC;
+  using VT = typename vec_of<T>::type;
+  const T* row = in.at(r, 1);
+#pragma unroll
+  for (int j = 0; j < J; j++) {
+    int v = vbase + lane + 32 * j;
+    if (v <= nv) R.v[j] = *reinterpret_cast<const VT*>(row + (size_t)v * V);
+    else R.v[j] = VT{};
+  }
+  R.left = row[(size_t)vbase * V - 1];
+  R.right = has_right ? row[(size_t)(vbase + 32 * J) * V] : (T)0;
+}
+
+template <typename T, bool RESID, int J>
+__device__ __forceinline__ double walk_compute(const walk_row<T, J>& U, const walk_row<T, J>& M,
+    const walk_row<T, J>& D, T* orow, int vbase, int w, int lane) {
+  constexpr int V = traits<T>::VEC;
+  constexpr unsigned FULL = 0xffffffffu;
+  using VT = typename vec_of<T>::type;
+  double acc = 0.0;
+  T first[J], last[J];
+#pragma unroll
+  for (int j = 0; j < J; j++) {
+    first[j] = vec_elem<T>(M.v[j], 0);
+    last[j] = vec_elem<T>(M.v[j], V - 1);
+  }
+#pragma unroll
+  for (int j = 0; j < J; j++) {
+    T up_last = __shfl_up_sync(FULL, last[j], 1);
+    T dn_first = __shfl_down_sync(FULL, first[j], 1);
+    T wrap_l = __shfl_sync(FULL, last[j > 0 ? j - 1 : 0], 31);
+    T wrap_r = __shfl_sync(FULL, first[j < J - 1 ? j + 1 : 0], 0);
+    T left = lane > 0 ? up_last : (j > 0 ? wrap_l : M.left);
+    T right = lane < 31 ? dn_first : (j < J - 1 ? wrap_r : M.right);
+    int v = vbase + lane + 32 * j;
+    int nvalid = w - v * V;
+    if (nvalid > 0) {
+      if (nvalid > V) nvalid = V;
+      T m[V], u[V], d[V], o[V];
+#pragma unroll
+      for (int k = 0; k < V; k++) {
+        m[k] = vec_elem<T>(M.v[j], k);
+        u[k] = vec_elem<T>(U.v[j], k);
+        d[k] = vec_elem<T>(D.v[j], k);
+      }
+#pragma unroll
+      for (int k = 0; k < V; k++) {
+        T l = (k == 0) ? left : m[k - 1];
+        T r = (k == V - 1) ? right : m[k + 1];
+        o[k] = stencil(m[k], l, r, u[k], d[k]);
+        if (RESID && k < nvalid) acc += resid2<T>(m[k], l, r, u[k], d[k]);
+      }
+      T* op = orow + (size_t)v * V;
+      if (nvalid == V) {
+        VT ov;
+        if constexpr (V == 2) ov = make_double2((double)o[0], (double)o[1]);
+        else ov = make_float4((float)o[0], (float)o[1], (float)o[2], (float)o[3]);
+        *reinterpret_cast<VT*>(op) = ov;
+      } else {
+        for (int k = 0; k < nvalid; k++) op[k] = o[k];
+      }
+    }
+  }
+  return acc;
+}
+
+// Rows r0..r1-1 of the strip starting at vector vbase (one warp).
+template <typename T, bool RESID, int J, int G>
+__device__ double walk_item(const block_view<T>& in, const block_view<T>& out, int w, int nv,
+    int vbase, int r0, int r1, int lane) {
+  const bool has_right = vbase + 32 * J <= nv;
+  walk_row<T, J> U, M, D[G];
+  walk_load<T, J>(U, in, r0 - 1, vbase, nv, lane, has_right);
+  walk_load<T, J>(M, in, r0, vbase, nv, lane, has_right);
+  double acc = 0.0;
+  for (int r = r0; r < r1; r += G) {
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+      if (r + 1 + g <= r1) walk_load<T, J>(D[g], in, r + 1 + g, vbase, nv, lane, has_right);
+    }
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+      if (r + g < r1) {
+        acc += walk_compute<T, RESID, J>(U, M, D[g], out.at(r + g, 1), vbase, w, lane);
+        U = M;
+        M = D[g];
+      }
+    }
+  }
+  return acc;
+}
+
+template <typename T> struct walk_shape;
+template <> struct walk_shape<double> { static constexpr int J = 2, G = 4; };
+template <> struct walk_shape<float> { static constexpr int J = 2, G = 4; };
+
+// Not inlined: the walker gets the whole register budget, whatever the
+// caller keeps live.
+template <typename T, bool RESID>
+__device__ __noinline__ double sweep_direct(block_view<T> in, block_view<T> out, int w, int h) {
+  if (blockDim.x < 32) return sweep_simple<T, RESID>(in, out, w, h);
+  constexpr int V = traits<T>::VEC, J = walk_shape<T>::J, G = walk_shape<T>::G;
+  const int nv = (w + V - 1) / V;
+  const int n_strips = (nv + 32 * J - 1) / (32 * J);
+  const int nw = (int)(blockDim.x / 32), warp = (int)(threadIdx.x / 32), lane = (int)(threadIdx.x & 31);
+  if (warp >= nw) return 0.0;  // threads of a partial warp (host emulation only)
+  // Enough row runs that every warp gets an item; runs of at least 8 rows.
+  int segs = (nw + n_strips - 1) / n_strips;
+  if (segs > (h + 7) / 8) segs = (h + 7) / 8;
+  if (segs < 1) segs = 1;
+  const int items = n_strips * segs;
+  double acc = 0.0;
+  for (int it = warp; it < items; it += nw) {
+    int s = it % n_strips, g = it / n_strips;
+    int r0 = 1 + (int)((long long)h * g / segs), r1 = 1 + (int)((long long)h * (g + 1) / segs);
+    acc += walk_item<T, RESID, J, G>(in, out, w, nv, s * 32 * J, r0, r1, lane);
   }
   return acc;
 }

@@ -32,6 +32,7 @@
 #define __host__
 #define __global__
 #define __forceinline__ inline
+#define __noinline__
 #define __constant__
 #ifdef EMU_MT
 #define __shared__ static
@@ -60,7 +61,7 @@ void emu_sync(const char* file, int line);
 void emu_syncwarp(const char* file, int line);
 #define __syncwarp(...) emu_syncwarp(__FILE__, __LINE__)
 bool emu_all_sync(bool p);
-void emu_shfl(void* v, unsigned bytes, int mode, int arg);  // mode 0 up, 1 down, 2 xor
+void emu_shfl(void* v, unsigned bytes, int mode, int arg);  // mode 0 up, 1 down, 2 xor, 3 index
 inline bool __all_sync(unsigned, bool p) { return emu_all_sync(p); }
 template <typename T> inline T __shfl_up_sync(unsigned, T v, int d) {
   emu_shfl(&v, sizeof(T), 0, d);
@@ -74,12 +75,17 @@ template <typename T> inline T __shfl_xor_sync(unsigned, T v, int m) {
   emu_shfl(&v, sizeof(T), 2, m);
   return v;
 }
+template <typename T> inline T __shfl_sync(unsigned, T v, int src) {
+  emu_shfl(&v, sizeof(T), 3, src);
+  return v;
+}
 #else
 inline void __syncwarp(unsigned = 0xffffffffu) {}
 inline bool __all_sync(unsigned, bool p) { return p; }
 template <typename T> inline T __shfl_xor_sync(unsigned, T v, int) { return v; }
 template <typename T> inline T __shfl_up_sync(unsigned, T v, int) { return v; }
 template <typename T> inline T __shfl_down_sync(unsigned, T v, int) { return v; }
+template <typename T> inline T __shfl_sync(unsigned, T v, int) { return v; }
 #endif
 inline void __threadfence() { std::atomic_thread_fence(std::memory_order_seq_cst); }
 inline void __nanosleep(unsigned) {}

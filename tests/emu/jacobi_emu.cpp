@@ -170,6 +170,7 @@ void emu_shfl(void* v, unsigned bytes, int mode, int arg) {
   if (mode == 0 && lane - arg >= 0) src = lane - arg;
   if (mode == 1 && lane + arg < 32) src = lane + arg;
   if (mode == 2) src = lane ^ arg;
+  if (mode == 3) src = arg & 31;
   memcpy(v, w.slot[src], bytes);
   w.bar.sync("shfl", 1);
 }
