@@ -69,7 +69,7 @@ class JacobiProblem(C.Structure):
 class JacobiOptions(C.Structure):
     _fields_ = [
         ("dtype", i32), ("chare_side", i32), ("tile_w", i32), ("pipeline", i32),
-        ("use_graph", i32), ("balance", i32), ("halo_mode", i32),
+        ("use_graph", i32), ("balance", i32), ("halo_mode", i32), ("depth", i32),
     ]
 
 

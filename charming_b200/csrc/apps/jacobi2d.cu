@@ -1,10 +1,15 @@
 // Jacobi2d chares: the scenario of the reference's examples/jacobi2d
 // (jacobi2d.cu:93-279) on this runtime, for many problems at once.
 //
-// Per chare and sweep: receive one halo per neighbour (refnum = sweep, which
-// closes the reference's ghost race, jacobi2d.cu:171-190 / :222), sweep the
-// block (jacobi_sweep.cuh), then pack the new boundary rows/columns straight
-// into the neighbours' inbox rings (zero-copy messages) with refnum = sweep+1.
+// Per chare and exchange ("pass"): receive one halo per neighbour, run the
+// pass's sweeps on the block (jacobi_sweep.cuh), then pack the new boundary
+// rows/columns straight into the neighbours' inbox rings (zero-copy
+// messages). Halos carry their pass number, which closes the reference's
+// ghost race (jacobi2d.cu:171-190 / :222): a halo of pass p lands in the
+// ghost zone of buffer p & 1. A pass is one sweep with ghost depth 1 (the
+// reference's scheme) or up to `depth` sweeps with a ghost zone that deep,
+// corners included (temporal blocking: same arithmetic per point, fewer
+// exchanges and one read + one write of the block per pass).
 // Optional FP64 residual every `check_every` sweeps: each chare's partial
 // goes up a binary tree over the problem's chares (fixed summation order, so
 // the norm is bit-reproducible) and the stop decision comes back down. The
@@ -46,11 +51,12 @@ struct japp {
 };
 
 struct JBlock : charm::chare {
-  int iter;          // sweeps completed; buf[cur] holds u_iter (cur == iter & 1)
+  int iter;          // sweeps completed; buf[cur] holds u_iter
+  int pass;          // passes completed (cur == pass & 1)
   int cur;
-  int sent;          // last sweep whose boundary went to the neighbours
+  int sent;          // last pass whose boundary went to the neighbours
   int started;       // the start message has been processed
-  int got[2];        // halos received for the sweep of each parity
+  int got[2];        // halos received for the pass of each parity
   int nbr_count;
   int done;
   int waiting;       // parked until the decision of check iter/K - 1 arrives
@@ -64,7 +70,7 @@ struct JBlock : charm::chare {
   double res0, res_last;
   int checks;
   __device__ JBlock()
-      : iter(0), cur(0), sent(-1), started(0), nbr_count(0), done(0), waiting(0), have_own(0), own(0.0),
+      : iter(0), pass(0), cur(0), sent(-1), started(0), nbr_count(0), done(0), waiting(0), have_own(0), own(0.0),
         decided(-1), stop_check(-1), res0(0.0), res_last(0.0), checks(0) {
     got[0] = got[1] = 0;
     child_got[0] = child_got[1] = 0;
@@ -79,19 +85,42 @@ __device__ jac::block_view<T> view(const jac::chare_desc& d, int b) {
   return jac::block_view<T>{reinterpret_cast<T*>(d.buf[b]), d.pitch};
 }
 
-// One sweep buf[cur] -> buf[cur^1]; returns the block's residual sum (FP64,
-// deterministic) when resid is set. All threads.
+// Sweeps per pass: the ghost depth, cut at the next residual check and at
+// max_sweeps, so checks fall on pass boundaries.
+__device__ int pass_len(const jac::chare_desc& d, const jac::prob_desc& p, int iter) {
+  int L = d.depth;
+  if (p.max_sweeps - iter < L) L = p.max_sweeps - iter;
+  if (p.check_every > 0) {
+    int to_check = p.check_every - iter % p.check_every;
+    if (to_check < L) L = to_check;
+  }
+  return L < 1 ? 1 : L;
+}
+
+// One pass of L sweeps buf[cur] -> buf[cur^1]; returns the block's residual
+// sum of the pass's first sweep (FP64, deterministic) when resid is set.
+// All threads.
 template <typename T>
-__device__ double sweep_block(const jac::chare_desc& d, int cur, bool resid) {
+__device__ double sweep_block(const jac::chare_desc& d, int cur, bool resid, int L) {
   jac::block_view<T> in = view<T>(d, cur), out = view<T>(d, cur ^ 1);
   double acc = 0.0;
   bool done = false;
-  if (!CHARM_VERIFY(d.w > 0 && d.h > 0 && d.buf[0] && d.buf[1] && (cur == 0 || cur == 1),
+  if (!CHARM_VERIFY(d.w > 0 && d.h > 0 && d.buf[0] && d.buf[1] && (cur == 0 || cur == 1) &&
+                        L >= 1 && L <= d.depth,
                     CHARMING_ERR_APP, 8000 + cur, d.w))
     return 0.0;
   unsigned long long t0 = charm::now_ns();
+  if (L > 1) {
+    int fixed = (d.nbr[jac::TOP] < 0 ? 1 : 0) | (d.nbr[jac::BOTTOM] < 0 ? 2 : 0) |
+                (d.nbr[jac::LEFT] < 0 ? 4 : 0) | (d.nbr[jac::RIGHT] < 0 ? 8 : 0);
+    __syncthreads();
+    acc = resid ? jac::sweep_deep<T, true>(in, out, d.w, d.h, L, fixed)
+                : jac::sweep_deep<T, false>(in, out, d.w, d.h, L, fixed);
+    __syncthreads();
+    done = true;
+  }
 #if !defined(CHARMING_HOST_EMULATION) || defined(CHARMING_HOST_EMULATION_TMA)
-  if (japp::pipeline()) {
+  if (!done && japp::pipeline()) {
     size_t sb = 0;
     void* sm = charm::smem_scratch(&sb);
     jac::tma_plan P;
@@ -112,12 +141,13 @@ __device__ double sweep_block(const jac::chare_desc& d, int cur, bool resid) {
   return resid ? suite::block_sum_f64(acc) : 0.0;
 }
 
-// Packs the boundary of buf[cur] for direction dir into a zero-copy message
-// to the neighbour and sends it with refnum = iter. All threads.
+// Packs the boundary region of buf[cur] for direction dir into a zero-copy
+// message to the neighbour there (refnum = pass in halo_mode 1). All threads.
 template <typename T>
 __device__ void send_halo(JBlock& c, const jac::chare_desc& d, int dir) {
   int nbr = d.nbr[dir];
-  int len = (dir == jac::TOP || dir == jac::BOTTOM) ? d.w : d.h;
+  jac::region e = jac::edge_region(dir, d.depth, d.w, d.h);
+  int len = e.nr * e.nc;
   size_t bytes = sizeof(jac::halo_hdr) + (size_t)len * sizeof(T);
   charm::message msg;
   if (!jproxy->alloc_msg(msg, nbr, bytes)) return;
@@ -128,38 +158,36 @@ __device__ void send_halo(JBlock& c, const jac::chare_desc& d, int dir) {
     jac::halo_hdr* hh = reinterpret_cast<jac::halo_hdr*>(pl);
     hh->dir = jac::opposite(dir);
     hh->len = len;
+    hh->pass = c.pass;
     hh->iter = c.iter;
-    hh->pad = 0;
   }
-  if (dir == jac::TOP || dir == jac::BOTTOM) {
-    int r = (dir == jac::TOP) ? 1 : d.h;
-    charm::copy_cooperative(vals, g.at(r, 1), (size_t)len * sizeof(T), threadIdx.x, blockDim.x);
+  if (e.nr == 1) {
+    charm::copy_cooperative(vals, g.at(e.r0, e.c0), (size_t)len * sizeof(T), threadIdx.x, blockDim.x);
   } else {
-    int col = (dir == jac::LEFT) ? 1 : d.w;
-    for (int i = threadIdx.x; i < len; i += blockDim.x) vals[i] = *g.at(1 + i, col);
+    for (int i = threadIdx.x; i < len; i += blockDim.x) vals[i] = *g.at(e.r0 + i / e.nc, e.c0 + i % e.nc);
   }
-  jproxy->invoke(nbr, EP_HALO, msg, bytes, japp::halo_mode() == 1 ? c.iter : -1);
+  jproxy->invoke(nbr, EP_HALO, msg, bytes, japp::halo_mode() == 1 ? c.pass : -1);
 }
 
 template <typename T>
 __device__ void send_halos(JBlock& c, const jac::chare_desc& d) {
-  for (int dir = 0; dir < 4; dir++) {
+  for (int dir = 0; dir < jac::N_DIRS; dir++) {
     if (d.nbr[dir] >= 0) send_halo<T>(c, d, dir);
   }
 }
 
+// Halo of pass hh->pass -> ghost zone of buf[pass & 1]. All threads.
 template <typename T>
 __device__ void unpack_halo(JBlock& c, const jac::chare_desc& d, const void* arg) {
   const jac::halo_hdr* hh = reinterpret_cast<const jac::halo_hdr*>(arg);
   const T* vals = reinterpret_cast<const T*>(reinterpret_cast<const char*>(arg) + sizeof(jac::halo_hdr));
-  jac::block_view<T> g = view<T>(d, hh->iter & 1);  // ghost ring of the sweep it belongs to
-  int dir = hh->dir, len = hh->len;
-  if (dir == jac::TOP || dir == jac::BOTTOM) {
-    int r = (dir == jac::TOP) ? 0 : d.h + 1;
-    charm::copy_cooperative(g.at(r, 1), vals, (size_t)len * sizeof(T), threadIdx.x, blockDim.x);
+  jac::block_view<T> g = view<T>(d, hh->pass & 1);
+  jac::region gr = jac::ghost_region(hh->dir, d.depth, d.w, d.h);
+  int len = gr.nr * gr.nc;
+  if (gr.nr == 1) {
+    charm::copy_cooperative(g.at(gr.r0, gr.c0), vals, (size_t)len * sizeof(T), threadIdx.x, blockDim.x);
   } else {
-    int col = (dir == jac::LEFT) ? 0 : d.w + 1;
-    for (int i = threadIdx.x; i < len; i += blockDim.x) *g.at(1 + i, col) = vals[i];
+    for (int i = threadIdx.x; i < len; i += blockDim.x) *g.at(gr.r0 + i / gr.nc, gr.c0 + i % gr.nc) = vals[i];
   }
 }
 

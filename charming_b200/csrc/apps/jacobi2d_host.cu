@@ -10,6 +10,7 @@
 #include "suite.cuh"
 #include "jacobi_types.cuh"
 #include "jacobi_sweep.cuh"
+#include "jacobi_layout.h"
 #include "../host.cuh"
 
 namespace {
@@ -51,16 +52,20 @@ __device__ __forceinline__ T* cell(const jac::chare_desc& d, int b, int r, int c
 }
 
 // Initial state: boundary ring from bc (top/bottom rows include the corners),
-// interior 0; written to both buffers. One block per chare.
+// interior 0; written to both buffers over the whole ghost zone wherever the
+// position lies on the global grid (ghost cells on the domain boundary must
+// hold boundary values for the multi-sweep pass). One block per chare.
 template <typename T>
 __global__ void init_kernel(const jac::chare_desc* ch, const jac::prob_desc* pr, const double* bc) {
   const jac::chare_desc d = ch[blockIdx.x];
   const jac::prob_desc p = pr[d.prob];
   const double* b = bc + 4 * d.prob;
-  long long n = (long long)(d.h + 2) * (d.w + 2);
+  const int D = d.depth, W = d.w + 2 * D;
+  long long n = (long long)(d.h + 2 * D) * W;
   for (long long x = threadIdx.x; x < n; x += blockDim.x) {
-    int r = (int)(x / (d.w + 2)), c = (int)(x % (d.w + 2));
+    int r = (int)(x / W) + 1 - D, c = (int)(x % W) + 1 - D;
     int gy = d.y0 + r, gx = d.x0 + c;
+    if (gy < 0 || gy > p.ny + 1 || gx < 0 || gx > p.nx + 1) continue;
     double v = 0.0;
     if (gy == 0) v = b[0];
     else if (gy == p.ny + 1) v = b[1];
@@ -71,15 +76,19 @@ __global__ void init_kernel(const jac::chare_desc* ch, const jac::prob_desc* pr,
   }
 }
 
-// Global grid (ny+2) x (nx+2) in `stage` -> blocks of one problem.
+// Global grid (ny+2) x (nx+2) in `stage` -> blocks of one problem (whole
+// ghost zone, as init_kernel).
 template <typename T>
-__global__ void scatter_kernel(const jac::chare_desc* ch, const int* chare_of, int nx,
+__global__ void scatter_kernel(const jac::chare_desc* ch, const int* chare_of, int nx, int ny,
     const T* stage) {
   const jac::chare_desc d = ch[chare_of[blockIdx.x]];
-  long long n = (long long)(d.h + 2) * (d.w + 2);
+  const int D = d.depth, W = d.w + 2 * D;
+  long long n = (long long)(d.h + 2 * D) * W;
   for (long long x = threadIdx.x; x < n; x += blockDim.x) {
-    int r = (int)(x / (d.w + 2)), c = (int)(x % (d.w + 2));
-    T v = stage[(size_t)(d.y0 + r) * (nx + 2) + d.x0 + c];
+    int r = (int)(x / W) + 1 - D, c = (int)(x % W) + 1 - D;
+    int gy = d.y0 + r, gx = d.x0 + c;
+    if (gy < 0 || gy > ny + 1 || gx < 0 || gx > nx + 1) continue;
+    T v = stage[(size_t)gy * (nx + 2) + gx];
     *cell<T>(d, 0, r, c) = v;
     *cell<T>(d, 1, r, c) = v;
   }
@@ -125,135 +134,42 @@ extern "C" int charming_jacobi2d_create(const charming_jacobi_problem* probs, in
   h->esz = opt->dtype == CHARMING_F64 ? 8 : 4;
   const int V = opt->dtype == CHARMING_F64 ? jac::traits<double>::VEC : jac::traits<float>::VEC;
   const int OFF = opt->dtype == CHARMING_F64 ? jac::traits<double>::OFF : jac::traits<float>::OFF;
-  const int align_el = (int)(128 / h->esz);
-  const int side = opt->chare_side > 0 ? opt->chare_side : 256;
 
-  // 1. decomposition, problem order
-  std::vector<jac::chare_desc> raw;
-  std::vector<jac::prob_desc> pd(n);
-  std::vector<int> root_raw(n);
-  for (int p = 0; p < n; p++) {
-    const charming_jacobi_problem& q = probs[p];
-    if (q.nx < 1 || q.ny < 1 || q.max_sweeps < 0 || q.check_every < 0) {
-      delete h;
-      return fail(CHARMING_ERR_CONFIG, "jacobi2d: problem size");
-    }
-    int px = q.px > 0 ? q.px : (q.nx + side - 1) / side;
-    int py = q.py > 0 ? q.py : (q.ny + side - 1) / side;
-    if (px > q.nx || py > q.ny) {
-      delete h;
-      return fail(CHARMING_ERR_CONFIG, "jacobi2d: more chares than rows/columns");
-    }
-    h->px.push_back(px);
-    h->py.push_back(py);
-    int base = (int)raw.size();
-    root_raw[p] = base;
-    int nc = px * py;
-    for (int cy = 0; cy < py; cy++) {
-      for (int cx = 0; cx < px; cx++) {
-        jac::chare_desc d{};
-        d.prob = p;
-        d.cx = cx;
-        d.cy = cy;
-        d.x0 = jac::split_start(q.nx, px, cx);
-        d.y0 = jac::split_start(q.ny, py, cy);
-        d.w = jac::split_start(q.nx, px, cx + 1) - d.x0;
-        d.h = jac::split_start(q.ny, py, cy + 1) - d.y0;
-        d.pitch = (OFF + d.w + 2 * V + align_el - 1) / align_el * align_el;
-        int r = cy * px + cx;
-        d.nbr[jac::TOP] = cy > 0 ? base + r - px : -1;
-        d.nbr[jac::BOTTOM] = cy < py - 1 ? base + r + px : -1;
-        d.nbr[jac::LEFT] = cx > 0 ? base + r - 1 : -1;
-        d.nbr[jac::RIGHT] = cx < px - 1 ? base + r + 1 : -1;
-        d.rank = r;
-        d.parent = r > 0 ? base + (r - 1) / 2 : -1;
-        d.child[0] = 2 * r + 1 < nc ? base + 2 * r + 1 : -1;
-        d.child[1] = 2 * r + 2 < nc ? base + 2 * r + 2 : -1;
-        raw.push_back(d);
-        h->halo_msgs += (d.nbr[0] >= 0) + (d.nbr[1] >= 0) + (d.nbr[2] >= 0) + (d.nbr[3] >= 0);
-      }
-    }
-    pd[p].nx = q.nx;
-    pd[p].ny = q.ny;
-    pd[p].px = px;
-    pd[p].py = py;
-    pd[p].max_sweeps = q.max_sweeps;
-    pd[p].check_every = q.check_every;
-    pd[p].tol = q.tol;
-    pd[p].n_chares = nc;
-    h->points += (uint64_t)q.nx * q.ny;
+  // decomposition, tree, neighbours, placement, grid offsets
+  jac::layout L;
+  std::string err;
+  if (!jac::build_layout(probs, n, opt->chare_side, opt->balance, opt->depth, opt->pipeline, n_pes,
+                         (int)h->esz, OFF, V, &L, &err)) {
+    delete h;
+    return fail(CHARMING_ERR_CONFIG, err.c_str());
   }
-  const int nch = (int)raw.size();
+  const int nch = (int)L.chares.size();
   h->n_chares = nch;
-
-  // 2. placement: chares -> PEs (work-balanced greedy, or the reference's
-  // default block map over problem order, include/chare.h:136-176)
-  std::vector<int> pe_of(nch);
-  h->block_map.assign(n_pes, 0);
-  if (opt->balance) {
-    std::vector<int> order(nch);
-    std::iota(order.begin(), order.end(), 0);
-    auto work = [&](int i) { return (double)raw[i].w * raw[i].h + 4096.0; };
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
-    using item = std::pair<double, int>;
-    std::priority_queue<item, std::vector<item>, std::greater<item>> pq;
-    for (int pe = 0; pe < n_pes; pe++) pq.push({0.0, pe});
-    for (int i : order) {
-      item t = pq.top();
-      pq.pop();
-      pe_of[i] = t.second;
-      pq.push({t.first + work(i), t.second});
-    }
-  } else {
-    int per = nch / n_pes, rem = nch % n_pes, k = 0;
-    for (int pe = 0; pe < n_pes; pe++) {
-      int cnt = per + (pe < rem ? 1 : 0);
-      for (int j = 0; j < cnt; j++) pe_of[k++] = pe;
-    }
-  }
-  std::vector<int> perm(nch);  // placed index -> raw index
-  std::iota(perm.begin(), perm.end(), 0);
-  std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return pe_of[a] < pe_of[b]; });
-  std::vector<int> inv(nch);
-  for (int k = 0; k < nch; k++) inv[perm[k]] = k;
-  auto remap = [&](int x) { return x < 0 ? -1 : inv[x]; };
-  h->chares.resize(nch);
-  for (int k = 0; k < nch; k++) {
-    jac::chare_desc d = raw[perm[k]];
-    for (int q = 0; q < 4; q++) d.nbr[q] = remap(d.nbr[q]);
-    d.parent = remap(d.parent);
-    d.child[0] = remap(d.child[0]);
-    d.child[1] = remap(d.child[1]);
-    h->chares[k] = d;
-    h->block_map[pe_of[perm[k]]]++;
-  }
-  for (int p = 0; p < n; p++) pd[p].root = inv[root_raw[p]];
-  h->max_per_pe = *std::max_element(h->block_map.begin(), h->block_map.end());
-  for (int p = 0, off = 0; p < n; p++) {
-    h->chare_of_off.push_back(off);
-    for (int r = 0; r < h->px[p] * h->py[p]; r++) h->chare_of.push_back(inv[root_raw[p] + r]);
-    off += h->px[p] * h->py[p];
-  }
-
-  // 3. grids: two pitched buffers per chare, 256-byte aligned
-  size_t total = 0;
-  std::vector<size_t> off(nch);
-  for (int k = 0; k < nch; k++) {
-    size_t b = ((size_t)h->chares[k].pitch * (h->chares[k].h + 2) * h->esz + 255) / 256 * 256;
-    off[k] = total;
-    total += 2 * b;
-  }
-  h->grid_bytes = total;
-  cudaError_t e = cudaMalloc(&h->d_grid, total);
+  h->px = L.px;
+  h->py = L.py;
+  h->block_map = L.block_map;
+  h->chare_of = L.chare_of;
+  h->chare_of_off = L.chare_of_off;
+  h->max_per_pe = L.max_per_pe;
+  h->points = L.points;
+  h->halo_msgs = L.halo_msgs;
+  h->grid_bytes = L.total_bytes;
+  std::vector<jac::prob_desc>& pd = L.probs;
+  cudaError_t e = cudaMalloc(&h->d_grid, L.total_bytes);
   if (e != cudaSuccess) {
     delete h;
     return charm_host::cuda_fail(e, "jacobi2d grids");
   }
-  for (int k = 0; k < nch; k++) {
-    size_t b = ((size_t)h->chares[k].pitch * (h->chares[k].h + 2) * h->esz + 255) / 256 * 256;
-    h->chares[k].buf[0] = h->d_grid + off[k];
-    h->chares[k].buf[1] = h->d_grid + off[k] + b;
+  // zero everything once: ghost cells beyond the boundary ring are read
+  // (never used) by the multi-sweep pass
+  e = cudaMemset(h->d_grid, 0, L.total_bytes);
+  if (e != cudaSuccess) {
+    cudaFree(h->d_grid);
+    delete h;
+    return charm_host::cuda_fail(e, "jacobi2d grids");
   }
+  jac::place_buffers(&L, h->d_grid, (int)h->esz);
+  h->chares = L.chares;
   e = cudaMalloc(&h->d_chares, sizeof(jac::chare_desc) * nch);
   if (e == cudaSuccess) e = cudaMalloc(&h->d_probs, sizeof(jac::prob_desc) * n);
   if (e == cudaSuccess) e = cudaMalloc(&h->d_results, sizeof(jac::prob_result) * n);
@@ -340,8 +256,8 @@ extern "C" int charming_jacobi2d_load(void* handle, int prob, const void* host_g
   int nc = h->px[prob] * h->py[prob];
   const int* co = h->d_chare_of + h->chare_of_off[prob];
   if (e == cudaSuccess) {
-    if (h->esz == 8) scatter_kernel<double><<<nc, 256, 0, s>>>(h->d_chares, co, q.nx, (const double*)h->d_stage);
-    else scatter_kernel<float><<<nc, 256, 0, s>>>(h->d_chares, co, q.nx, (const float*)h->d_stage);
+    if (h->esz == 8) scatter_kernel<double><<<nc, 256, 0, s>>>(h->d_chares, co, q.nx, q.ny, (const double*)h->d_stage);
+    else scatter_kernel<float><<<nc, 256, 0, s>>>(h->d_chares, co, q.nx, q.ny, (const float*)h->d_stage);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemsetAsync(h->d_final, 0, sizeof(int) * h->n_chares, s);

@@ -1,14 +1,16 @@
 // Jacobi2d chare state machine (included by jacobi2d.cu inside its
 // anonymous namespace; uses JBlock, japp, jproxy and the helpers above it).
 //
-// State of a chare: `iter` sweeps done (buf[iter & 1] holds u_iter), `sent`
-// = last sweep whose boundary was sent, got[p] = halos received for the
-// sweep of parity p. A halo for sweep k is unpacked into the ghost ring of
-// buf[k & 1] as soon as it arrives: sweep k-1 reads only buf[(k-1) & 1] and
-// writes only the interior of buf[k & 1], and a neighbour can be at most one
-// sweep ahead, so early halos need no stash (halo_mode 0). halo_mode 1 tags
-// halos with refnum = sweep instead, which parks early ones in the runtime's
-// stash as the reference's refnum pattern would.
+// State of a chare: `pass` exchanges done, `iter` sweeps done (buf[pass & 1]
+// holds u_iter), `sent` = last pass whose boundary was sent, got[p] = halos
+// received for the pass of parity p. A halo for pass k is unpacked into the
+// ghost zone of buf[k & 1] as soon as it arrives: pass k-1 reads only
+// buf[(k-1) & 1] and writes only the interior of buf[k & 1], and a neighbour
+// can be at most one pass ahead, so early halos need no stash (halo_mode 0).
+// halo_mode 1 tags halos with refnum = pass instead, which parks early ones
+// in the runtime's stash as the reference's refnum pattern would. Every
+// chare of a problem computes the same pass lengths (pass_len), so residual
+// checks fall on pass boundaries everywhere.
 
 // Control flow is never re-entrant: pump() runs only at the top of an entry
 // method; apply_decision() and tree_try_forward() report "the chare was
@@ -89,8 +91,8 @@ __device__ int tree_try_forward(JBlock& c, const jac::chare_desc& d, int chk) {
   return 0;
 }
 
-// All threads: one sweep buf[iter&1] -> buf[(iter+1)&1], then the residual
-// tree when this sweep carries a check.
+// All threads: one pass buf[pass&1] -> buf[(pass+1)&1], then the residual
+// tree when the pass starts at a check.
 template <typename T>
 __device__ void advance(JBlock& c, const jac::chare_desc& d) {
   const jac::prob_desc& p = japp::probs()[d.prob];
@@ -98,11 +100,13 @@ __device__ void advance(JBlock& c, const jac::chare_desc& d) {
   // read before thread 0 advances the chare below
   const bool resid = K > 0 && (c.iter % K == 0);
   const int chk = K > 0 ? c.iter / K : 0;
-  double part = sweep_block<T>(d, c.cur, resid);
+  const int L = pass_len(d, p, c.iter);
+  double part = sweep_block<T>(d, c.cur, resid, L);
   if (threadIdx.x == 0) {
-    c.got[c.iter & 1] = 0;
+    c.got[c.pass & 1] = 0;
     c.cur ^= 1;
-    c.iter++;
+    c.pass++;
+    c.iter += L;
     if (resid) {
       c.own = part;
       c.have_own = 1;
@@ -126,11 +130,11 @@ __device__ void pump(JBlock& c, const jac::chare_desc& d) {
     if (threadIdx.x == 0) {
       int act = IDLE;
       int K = p.check_every;
-      CHARM_VERIFY(c.cur == (c.iter & 1) && c.got[0] <= c.nbr_count && c.got[1] <= c.nbr_count,
-                   CHARMING_ERR_APP, 7000 + c.iter, c.i);
+      (void)CHARM_VERIFY(c.cur == (c.pass & 1) && c.got[0] <= c.nbr_count && c.got[1] <= c.nbr_count,
+                   CHARMING_ERR_APP, 7000 + c.pass, c.i);
       if (c.done || c.waiting) {
         act = IDLE;
-      } else if (c.sent < c.iter) {
+      } else if (c.sent < c.pass) {
         if (c.iter >= p.max_sweeps) {
           act = FIN;
         } else if (K > 0 && c.iter >= K && c.iter % K == 0 && c.decided < c.iter / K - 1) {
@@ -141,10 +145,10 @@ __device__ void pump(JBlock& c, const jac::chare_desc& d) {
           act = FIN;
         } else {
           act = c.nbr_count > 0 ? SEND : SELF;
-          c.sent = c.iter;
-          if (act == SEND && japp::halo_mode() == 1) jproxy->set_refnum(c.i, c.iter);
+          c.sent = c.pass;
+          if (act == SEND && japp::halo_mode() == 1) jproxy->set_refnum(c.i, c.pass);
         }
-      } else if (c.nbr_count > 0 && c.got[c.iter & 1] == c.nbr_count) {
+      } else if (c.nbr_count > 0 && c.got[c.pass & 1] == c.nbr_count) {
         act = SWEEP;
       }
       s_act = act;
@@ -162,7 +166,7 @@ __device__ void pump(JBlock& c, const jac::chare_desc& d) {
     } else if (act == SELF) {
       // no neighbours: one sweep per message, so other chares of the PE run
       // in between
-      int it = c.iter;
+      int it = c.pass;
       jproxy->invoke(c.i, EP_CONT, &it, sizeof(int));
       return;
     } else {
@@ -176,7 +180,7 @@ __device__ void em_start_t(JBlock& c) {
   const jac::chare_desc& d = japp::chares()[c.i];
   if (threadIdx.x == 0) {
     int n = 0;
-    for (int k = 0; k < 4; k++) n += d.nbr[k] >= 0;
+    for (int k = 0; k < jac::N_DIRS; k++) n += d.nbr[k] >= 0;
     c.nbr_count = n;
     c.started = 1;
   }
@@ -190,17 +194,18 @@ __device__ void em_halo_t(JBlock& c, void* arg) {
   const jac::chare_desc& d = japp::chares()[c.i];
   const jac::halo_hdr* hh = reinterpret_cast<const jac::halo_hdr*>(arg);
   // checked build: direction, length and sweep of the halo are consistent
-  if (!CHARM_VERIFY(hh->dir >= 0 && hh->dir < 4 && d.nbr[hh->dir] >= 0, CHARMING_ERR_APP,
+  if (!CHARM_VERIFY(hh->dir >= 0 && hh->dir < jac::N_DIRS && d.nbr[hh->dir] >= 0, CHARMING_ERR_APP,
                     1000 + hh->dir, c.i) ||
-      !CHARM_VERIFY(hh->len == ((hh->dir < 2) ? d.w : d.h), CHARMING_ERR_APP, 2000 + hh->dir,
-                    hh->len) ||
-      !CHARM_VERIFY(hh->iter == c.iter || hh->iter == c.iter + 1, CHARMING_ERR_APP,
-                    3000 + (hh->iter - c.iter), c.i))
+      !CHARM_VERIFY(hh->len == jac::ghost_region(hh->dir, d.depth, d.w, d.h).nr *
+                                   jac::ghost_region(hh->dir, d.depth, d.w, d.h).nc,
+                    CHARMING_ERR_APP, 2000 + hh->dir, hh->len) ||
+      !CHARM_VERIFY(hh->pass == c.pass || hh->pass == c.pass + 1, CHARMING_ERR_APP,
+                    3000 + (hh->pass - c.pass), c.i))
     return;
   unpack_halo<T>(c, d, arg);
   if (threadIdx.x == 0) {
-    c.got[hh->iter & 1]++;
-    CHARM_VERIFY(c.got[hh->iter & 1] <= 4, CHARMING_ERR_APP, 4000 + c.got[hh->iter & 1], c.i);
+    c.got[hh->pass & 1]++;
+    (void)CHARM_VERIFY(c.got[hh->pass & 1] <= jac::N_DIRS, CHARMING_ERR_APP, 4000 + c.got[hh->pass & 1], c.i);
   }
   __syncthreads();
   if (c.started) pump<T>(c, d);  // a halo may overtake the start message

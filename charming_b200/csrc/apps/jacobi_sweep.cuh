@@ -22,6 +22,7 @@
 #pragma once
 
 #include "suite.cuh"
+#include "jacobi_types.cuh"
 
 namespace jac {
 
@@ -104,6 +105,90 @@ __device__ __forceinline__ double compute_vec(const T* up, const T* mid, const T
   }
   return acc;
 }
+
+// ---------------------------------------------------------------------------
+// PTX helpers: mbarriers, bulk copies, per-thread async copies.
+// ---------------------------------------------------------------------------
+#ifndef CHARMING_HOST_EMULATION
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_inval(unsigned long long* b) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" :: "r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(b)),
+               "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done) : "r"(smem_u32(b)), "r"(parity) : "memory");
+  return done != 0;
+}
+// 1-D bulk copy global -> shared, completion counted on the mbarrier.
+// Both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
+    unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_global() {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(b)) : "memory");
+}
+// 16-byte asynchronous global -> shared copy (zero fill when src_bytes is 0),
+// committed per row; wait_group<N> waits until at most N groups are pending.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, unsigned src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" :: "r"(smem_u32(dst)), "l"(src),
+               "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
+__device__ __forceinline__ bool mbar_test_wait(unsigned long long* b, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done) : "r"(smem_u32(b)), "r"(parity) : "memory");
+  return done != 0;
+}
+#else
+// The CPU check of the chare code models these (tests/emu).
+void mbar_init(unsigned long long* b, unsigned count);
+void mbar_inval(unsigned long long* b);
+void mbar_expect_tx(unsigned long long* b, unsigned bytes);
+bool mbar_try_wait(unsigned long long* b, unsigned parity);
+bool mbar_test_wait(unsigned long long* b, unsigned parity);
+void mbar_arrive(unsigned long long* b);
+void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar);
+inline void fence_proxy_async_global() {}
+inline void fence_proxy_async_smem() {}
+inline void fence_mbar_init() {}
+// per-thread copies: done at once on the host
+inline void cp_async16(void* dst, const void* src, unsigned src_bytes) {
+  memset(dst, 0, 16);
+  if (src_bytes) memcpy(dst, src, src_bytes);
+}
+inline void cp_async_commit() {}
+template <int N> inline void cp_async_wait() {}
+#endif
 
 // ---------------------------------------------------------------------------
 // Direct-load sweep, simple form: thread i of the block handles vectors
@@ -282,72 +367,219 @@ __device__ __noinline__ double sweep_direct(block_view<T> in, block_view<T> out,
 }
 
 // ---------------------------------------------------------------------------
-// TMA row pipeline.
+// Multi-sweep pass (temporal blocking): L sweeps (2 <= L <= LMAX) from a
+// grid whose ghost zone is at least L deep, without writing the
+// intermediate sweeps. A warp owns a strip of 32 vectors (one per lane) and
+// streams level-0 rows down it; level l row r is computed when level l-1
+// row r+1 arrives, from a three-row register window per level, so the pass
+// is a wavefront L rows deep. Every level loses one valid column at each
+// strip edge (the neighbour value is in another warp), so strips overlap by
+// 2*ceil(L/VEC) vectors and each owns the 32 - 2*ceil(L/VEC) in the middle;
+// row runs overlap by 2L rows. Cells on the domain boundary (row 0 / h+1,
+// column 0 / w+1 of a chare without a neighbour there) keep their value at
+// every level; cells beyond it are never used by a stored result. Each
+// stored value is computed from the same five operands in the same order as
+// a single sweep, so L passes of one sweep give the same bits.
+// `fixed`: bit 0 top, 1 bottom, 2 left, 3 right side is the domain boundary.
 // ---------------------------------------------------------------------------
-#ifndef CHARMING_HOST_EMULATION
-__device__ __forceinline__ unsigned smem_u32(const void* p) {
-  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+template <typename T>
+__device__ __forceinline__ void vec_to(const typename vec_of<T>::type& x, T (&a)[traits<T>::VEC]) {
+#pragma unroll
+  for (int k = 0; k < traits<T>::VEC; k++) a[k] = vec_elem<T>(x, k);
 }
-__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(b)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_inval(unsigned long long* b) {
-  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" :: "r"(smem_u32(b)) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(b)),
-               "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, unsigned parity) {
-  unsigned done;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(done) : "r"(smem_u32(b)), "r"(parity) : "memory");
-  return done != 0;
-}
-// 1-D bulk copy global -> shared, completion counted on the mbarrier.
-// Both addresses 16-byte aligned, bytes a multiple of 16.
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
-    unsigned long long* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-      :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ void fence_proxy_async_global() {
-  asm volatile("fence.proxy.async.global;" ::: "memory");
-}
-__device__ __forceinline__ void fence_proxy_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void fence_mbar_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+__device__ __forceinline__ double2 vec_from(const double (&a)[2]) { return make_double2(a[0], a[1]); }
+__device__ __forceinline__ float4 vec_from(const float (&a)[4]) {
+  return make_float4(a[0], a[1], a[2], a[3]);
 }
 
-__device__ __forceinline__ void mbar_arrive(unsigned long long* b) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(b)) : "memory");
+// One level-l row of the wavefront at sub-step K (static slot rotation:
+// level-l row r lives in W[l][(r - qs) mod 3]).
+template <typename T, bool RESID, int LMAX, int K>
+__device__ __forceinline__ void deep_substep(typename vec_of<T>::type (&W)[LMAX][3], int q, int qs,
+    int L, int h, int w, int fixed, const bool (&fixc)[traits<T>::VEC], const bool (&inw)[traits<T>::VEC],
+    bool own, int v, int col0, int r0, int r1, const block_view<T>& out, double& acc) {
+  constexpr int V = traits<T>::VEC;
+  constexpr unsigned FULL = 0xffffffffu;
+  using VT = typename vec_of<T>::type;
+#pragma unroll
+  for (int l = 1; l <= LMAX; l++) {
+    if (l <= L && q >= qs + 2 * l) {
+      const int r = q - l;  // row of level l computed now
+      const int su = ((K - l - 1) % 3 + 6) % 3, sm = ((K - l) % 3 + 6) % 3, sd = ((K - l + 1) % 3 + 6) % 3;
+      T m[V], u[V], d[V], o[V];
+      vec_to<T>(W[l - 1][sm], m);
+      vec_to<T>(W[l - 1][su], u);
+      vec_to<T>(W[l - 1][sd], d);
+      T left = __shfl_up_sync(FULL, m[V - 1], 1);
+      T right = __shfl_down_sync(FULL, m[0], 1);
+      const bool fixr = (r == 0 && (fixed & 1)) || (r == h + 1 && (fixed & 2));
+#pragma unroll
+      for (int k = 0; k < V; k++) {
+        T lk = (k == 0) ? left : m[k - 1];
+        T rk = (k == V - 1) ? right : m[k + 1];
+        o[k] = (fixr || fixc[k]) ? m[k] : stencil(m[k], lk, rk, u[k], d[k]);
+        if (RESID && l == 1 && own && inw[k] && r >= r0 && r < r1)
+          acc += resid2<T>(m[k], lk, rk, u[k], d[k]);
+      }
+      if (l == L) {
+        if (own) {
+          T* op = out.at(r, col0);
+          int nvalid = w - v * V;
+          if (nvalid >= V) {
+            *reinterpret_cast<VT*>(op) = vec_from(o);
+          } else {
+            for (int k = 0; k < nvalid; k++) op[k] = o[k];
+          }
+        }
+      } else if (l < LMAX) {
+        W[l][sm] = vec_from(o);
+      }
+    }
+  }
 }
-__device__ __forceinline__ bool mbar_test_wait(unsigned long long* b, unsigned parity) {
-  unsigned done;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(done) : "r"(smem_u32(b)), "r"(parity) : "memory");
-  return done != 0;
+
+// One strip item: level-0 rows stream through this lane's private ring of P
+// 16-byte slots in shared memory (cp.async, P-1 rows ahead), the levels
+// through registers.
+template <typename T, bool RESID, int LMAX, int P>
+__device__ double deep_item(const block_view<T>& in, const block_view<T>& out, int w, int h,
+    int L, int fixed, int vbase, int own0, int nown, int r0, int r1, int lane,
+    typename vec_of<T>::type* ring) {
+  constexpr int V = traits<T>::VEC;
+  using VT = typename vec_of<T>::type;
+  const int v = vbase + lane;
+  const int col0 = 1 + v * V;                         // first column of this lane's vector
+  const long long e0 = (long long)traits<T>::OFF - 1 + col0;  // its element index in a row
+  const bool can_load = e0 >= 0 && e0 + V <= in.pitch;
+  const long long eo = can_load ? e0 : 0;
+  const unsigned nb = can_load ? 16u : 0u;
+  const bool own = v >= own0 && v < own0 + nown;
+  bool fixc[V], inw[V];
+#pragma unroll
+  for (int k = 0; k < V; k++) {
+    int c = col0 + k;
+    fixc[k] = (c == 0 && (fixed & 4)) || (c == w + 1 && (fixed & 8));
+    inw[k] = c >= 1 && c <= w;
+  }
+  const int qs = r0 - L, qe = r1 - 1 + L;             // level-0 rows streamed
+  // prologue: rows qs .. qs+P-2 into slots 0..P-2
+#pragma unroll
+  for (int k = 0; k < P - 1; k++) {
+    if (qs + k <= qe) cp_async16(&ring[k * 32 + lane], in.row(qs + k) + eo, nb);
+    cp_async_commit();
+  }
+  VT W[LMAX][3];
+  double acc = 0.0;
+  int slot = 0;                                       // ring slot of row q
+  for (int q0 = qs; q0 <= qe; q0 += 3) {
+#pragma unroll
+    for (int K = 0; K < 3; K++) {
+      const int q = q0 + K;
+      if (q <= qe) {
+        cp_async_wait<P - 2>();
+        W[0][K] = ring[slot * 32 + lane];
+        const int nslot = slot == 0 ? P - 1 : slot - 1;  // slot of row q-1, read last sub-step
+        if (q + P - 1 <= qe) cp_async16(&ring[nslot * 32 + lane], in.row(q + P - 1) + eo, nb);
+        cp_async_commit();
+        slot = slot + 1 == P ? 0 : slot + 1;
+        if (K == 0) deep_substep<T, RESID, LMAX, 0>(W, q, qs, L, h, w, fixed, fixc, inw, own, v, col0, r0, r1, out, acc);
+        else if (K == 1) deep_substep<T, RESID, LMAX, 1>(W, q, qs, L, h, w, fixed, fixc, inw, own, v, col0, r0, r1, out, acc);
+        else deep_substep<T, RESID, LMAX, 2>(W, q, qs, L, h, w, fixed, fixc, inw, own, v, col0, r0, r1, out, acc);
+      }
+    }
+  }
+  cp_async_wait<0>();
+  return acc;
 }
-#else
-// The CPU check of the chare code models these (tests/emu).
-void mbar_init(unsigned long long* b, unsigned count);
-void mbar_inval(unsigned long long* b);
-void mbar_expect_tx(unsigned long long* b, unsigned bytes);
-bool mbar_try_wait(unsigned long long* b, unsigned parity);
-bool mbar_test_wait(unsigned long long* b, unsigned parity);
-void mbar_arrive(unsigned long long* b);
-void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar);
-inline void fence_proxy_async_global() {}
-inline void fence_proxy_async_smem() {}
-inline void fence_mbar_init() {}
-#endif
+
+// The same pass, computed by thread 0 alone for blocks under one warp, with
+// levels 1..L-1 kept as three-row rings in the block's scratch.
+template <typename T, bool RESID>
+__device__ double sweep_deep_simple(block_view<T> in, block_view<T> out, int w, int h, int L,
+    int fixed) {
+  if (threadIdx.x != 0) return 0.0;
+  size_t cap = 0;
+  T* ring = reinterpret_cast<T*>(charm::smem_scratch(&cap));
+  const int W = w + 2 * L;  // columns 1-L .. w+L
+  if ((size_t)(L - 1) * 3 * W * sizeof(T) > cap) {
+    charm::detail::report_error(CHARMING_ERR_CONFIG, w, L);
+    return 0.0;
+  }
+  auto slot = [&](int l, int r) -> T* { return ring + ((size_t)(l - 1) * 3 + ((r % 3) + 3) % 3) * W; };
+  auto lv = [&](int l, int r, int c) -> T { return l == 0 ? *in.at(r, c) : slot(l, r)[c + L - 1]; };
+  double acc = 0.0;
+  for (int q = 1 - L; q <= h + L; q++) {
+    for (int l = 1; l <= L; l++) {
+      const int r = q - l, ext = L - l;
+      if (r < 1 - ext || r > h + ext) continue;
+      const bool fixr = (r == 0 && (fixed & 1)) || (r == h + 1 && (fixed & 2));
+      for (int c = 1 - ext; c <= w + ext; c++) {
+        const bool fixc = (c == 0 && (fixed & 4)) || (c == w + 1 && (fixed & 8));
+        T m = lv(l - 1, r, c), v = m;
+        if (!fixr && !fixc) {
+          T lc = lv(l - 1, r, c - 1), rc = lv(l - 1, r, c + 1);
+          T up = lv(l - 1, r - 1, c), dn = lv(l - 1, r + 1, c);
+          v = stencil(m, lc, rc, up, dn);
+          if (RESID && l == 1 && r >= 1 && r <= h && c >= 1 && c <= w)
+            acc += resid2<T>(m, lc, rc, up, dn);
+        }
+        if (l == L) {
+          if (r >= 1 && r <= h && c >= 1 && c <= w) *out.at(r, c) = v;
+        } else {
+          slot(l, r)[c + L - 1] = v;
+        }
+      }
+    }
+  }
+  return acc;
+}
+
+template <typename T, bool RESID>
+__device__ __noinline__ double sweep_deep(block_view<T> in, block_view<T> out, int w, int h, int L,
+    int fixed) {
+  if (blockDim.x < 32) return sweep_deep_simple<T, RESID>(in, out, w, h, L, fixed);
+  constexpr int V = traits<T>::VEC, LMAX = DEPTH_MAX, P = 8;
+  using VT = typename vec_of<T>::type;
+  const int E = (L + V - 1) / V;        // vectors lost per level set at each strip edge
+  const int SS = 32 - 2 * E;            // vectors a strip owns
+  const int nv = (w + V - 1) / V;
+  const int n_strips = (nv + SS - 1) / SS;
+  const int nw = (int)(blockDim.x / 32), warp = (int)(threadIdx.x / 32), lane = (int)(threadIdx.x & 31);
+  if (warp >= nw) return 0.0;
+  size_t sbytes = 0;
+  VT* rings = reinterpret_cast<VT*>(charm::smem_scratch(&sbytes));
+  if ((size_t)nw * P * 32 * sizeof(VT) > sbytes) {
+    if (threadIdx.x == 0) charm::detail::report_error(CHARMING_ERR_CONFIG, (int)sbytes, nw);
+    return 0.0;
+  }
+  VT* ring = rings + (size_t)warp * P * 32;
+  // row runs: balance items over warps; each run at least 4L rows
+  int segs = 1, best = 0x7fffffff;
+  for (int sg = 1; sg <= 8; sg++) {
+    if (sg > 1 && h / sg < 4 * L) break;
+    int rounds = (n_strips * sg + nw - 1) / nw;
+    int cost = rounds * ((h + sg - 1) / sg + 2 * L);
+    if (cost < best) {
+      best = cost;
+      segs = sg;
+    }
+  }
+  const int items = n_strips * segs;
+  double acc = 0.0;
+  for (int it = warp; it < items; it += nw) {
+    int s = it % n_strips, g = it / n_strips;
+    int r0 = 1 + (int)((long long)h * g / segs), r1 = 1 + (int)((long long)h * (g + 1) / segs);
+    int own0 = s * SS;
+    int nown = min(SS, nv - own0);
+    acc += deep_item<T, RESID, LMAX, P>(in, out, w, h, L, fixed, own0 - E, own0, nown, r0, r1, lane,
+                                        ring);
+  }
+  return acc;
+}
+
+// ---------------------------------------------------------------------------
+// TMA row pipeline.
+// ---------------------------------------------------------------------------
 
 constexpr int MAX_SLOTS = 64;        // mbarrier pairs in the first 1 KiB
 constexpr int BAR_BYTES = 2 * MAX_SLOTS * 8;

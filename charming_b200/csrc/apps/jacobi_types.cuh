@@ -3,8 +3,47 @@
 
 namespace jac {
 
-enum dir : int { TOP = 0, BOTTOM = 1, LEFT = 2, RIGHT = 3 };
+// Neighbour directions; opposite directions differ in bit 0. The corners are
+// used with ghost depth > 1 only.
+enum dir : int {
+  TOP = 0, BOTTOM = 1, LEFT = 2, RIGHT = 3,
+  TOP_LEFT = 4, BOTTOM_RIGHT = 5, TOP_RIGHT = 6, BOTTOM_LEFT = 7
+};
+constexpr int N_DIRS = 8;
+constexpr int DEPTH_MAX = 4;  // sweeps per halo exchange, at most
 __host__ __device__ inline int opposite(int d) { return d ^ 1; }
+__host__ __device__ inline bool dir_top(int d) { return d == TOP || d == TOP_LEFT || d == TOP_RIGHT; }
+__host__ __device__ inline bool dir_bottom(int d) {
+  return d == BOTTOM || d == BOTTOM_LEFT || d == BOTTOM_RIGHT;
+}
+__host__ __device__ inline bool dir_left(int d) { return d == LEFT || d == TOP_LEFT || d == BOTTOM_LEFT; }
+__host__ __device__ inline bool dir_right(int d) {
+  return d == RIGHT || d == TOP_RIGHT || d == BOTTOM_RIGHT;
+}
+
+// Rectangle of a chare's grid in its own coordinates (interior rows and
+// columns 1..h, 1..w).
+struct region {
+  int r0, c0, nr, nc;
+};
+// The ghost cells a halo from direction `d` fills (depth D).
+__host__ __device__ inline region ghost_region(int d, int D, int w, int h) {
+  region g;
+  g.r0 = dir_top(d) ? 1 - D : dir_bottom(d) ? h + 1 : 1;
+  g.nr = (dir_top(d) || dir_bottom(d)) ? D : h;
+  g.c0 = dir_left(d) ? 1 - D : dir_right(d) ? w + 1 : 1;
+  g.nc = (dir_left(d) || dir_right(d)) ? D : w;
+  return g;
+}
+// The boundary cells a chare sends to its neighbour in direction `d`.
+__host__ __device__ inline region edge_region(int d, int D, int w, int h) {
+  region e;
+  e.r0 = dir_top(d) ? 1 : dir_bottom(d) ? h - D + 1 : 1;
+  e.nr = (dir_top(d) || dir_bottom(d)) ? D : h;
+  e.c0 = dir_left(d) ? 1 : dir_right(d) ? w - D + 1 : 1;
+  e.nc = (dir_left(d) || dir_right(d)) ? D : w;
+  return e;
+}
 
 // One chare block of one problem (host-built, read-only on the device).
 struct chare_desc {
@@ -13,11 +52,13 @@ struct chare_desc {
   int x0, y0;          // first interior column / row of the block (0-based)
   int w, h;            // interior columns / rows of the block
   int pitch;           // row pitch, elements
-  int nbr[4];          // global chare index per direction, -1 at the boundary
+  int depth;           // ghost depth D: rows/columns 1-D..h+D / 1-D..w+D exist
+  int nbr[N_DIRS];     // global chare index per direction, -1 at the boundary
   int parent;          // residual tree: parent chare (-1 at the root)
   int child[2];        // residual tree: children (-1 if none)
   int rank;            // index within the problem (tree position; 0 = root)
-  void* buf[2];        // the two pitched grids (ghost ring included)
+  void* buf[2];        // the two pitched grids, pointing at row 0 (ghost rows
+                       // 1-D..0 lie before it)
 };
 
 struct prob_desc {
@@ -27,6 +68,7 @@ struct prob_desc {
   double tol;          // 0: never stop early
   int root;            // global chare index of the problem's tree root
   int n_chares;
+  int depth;           // ghost depth of the problem's chares
 };
 
 struct prob_result {
@@ -39,9 +81,9 @@ struct prob_result {
 // Payload header of a halo message; the values follow (16-byte aligned).
 struct halo_hdr {
   int dir;             // ghost side at the receiver
-  int len;             // values
-  int iter;            // sweep the values belong to
-  int pad;
+  int len;             // values (the ghost region, row-major)
+  int pass;            // exchange the values belong to (the sender's pass count)
+  int iter;            // sweep count of the values
 };
 
 struct partial_msg {

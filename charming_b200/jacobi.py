@@ -76,8 +76,8 @@ class Jacobi2D:
     """A set of problems decomposed into chares, resident on the GPU."""
 
     def __init__(self, problems, dtype: str = "f64", chare_side: int = 0, tile_w: int = 0,
-                 pipeline: bool = True, use_graph: bool = False, balance: bool = True,
-                 halo_mode: int = 0):
+                 pipeline: bool = False, use_graph: bool = False, balance: bool = True,
+                 halo_mode: int = 0, depth: int = 0):
         self.rt = runtime()
         self.lib = self.rt.lib
         self.problems = [p if isinstance(p, Problem) else Problem(**p) for p in problems]
@@ -88,6 +88,7 @@ class Jacobi2D:
         opt.chare_side, opt.tile_w = chare_side, tile_w
         opt.pipeline, opt.use_graph, opt.balance = int(pipeline), int(use_graph), int(balance)
         opt.halo_mode = halo_mode
+        opt.depth = depth
         h = C.c_void_p()
         check(self.lib.charming_jacobi2d_create(arr, len(self.problems), C.byref(opt), C.byref(h)),
               "charming_jacobi2d_create")

@@ -151,7 +151,12 @@ typedef struct charming_jacobi_options {
   int balance;         /* 1: place chares by work (greedy), 0: block map    */
   int halo_mode;       /* 0: halos land in the ghost ring of the sweep they
                           belong to (parity buffers); 1: halos carry refnum
-                          = sweep and early ones wait in the stash          */
+                          = exchange and early ones wait in the stash       */
+  int depth;           /* sweeps per halo exchange, 1..4, with ghost zones of
+                          that depth (corners from diagonal neighbours when
+                          > 1); 0: 4 for the direct sweep, 1 for the TMA
+                          pipeline; capped by the smallest chare side.
+                          The reference exchanges halos every sweep (1)     */
 } charming_jacobi_options;
 
 typedef struct charming_jacobi_result {
@@ -167,7 +172,7 @@ typedef struct charming_jacobi_info {
   int max_chares_per_pe;
   uint64_t interior_points;   /* sum of nx*ny                              */
   uint64_t grid_bytes;        /* device bytes of all chare grids           */
-  uint64_t halo_msgs_per_sweep;
+  uint64_t halo_msgs_per_sweep; /* halo messages per exchange (every `depth` sweeps) */
   double last_run_ms;         /* CUDA-event time of the last run           */
   double sweep_ms_max;        /* last run: max over PEs of time in sweeps  */
   double sweep_ms_mean;       /* last run: mean over busy PEs              */

@@ -11,7 +11,7 @@
 //
 // usage: jacobi_emu nx ny px py max_sweeps check_every tol dtype(0 f64|1 f32)
 //                   n_pes halo_mode [bc_top bc_bottom bc_left bc_right] [seed]
-//                   [threads_per_pe] [pipeline 0|1] [tile_w]
+//                   [threads_per_pe] [pipeline 0|1] [tile_w] [depth] [balance]
 // (the EMU_MT build takes n_pes == 1 and threads_per_pe >= 1, a multiple of
 // 32 with pipeline 1; the default build takes threads_per_pe == 1)
 // prints: status=<code> sweeps=<n> res0=<x> res_last=<x> exact=<0|1>
@@ -20,11 +20,13 @@
 #include "../../charming_b200/csrc/apps/suite.cuh"
 #include "../../charming_b200/csrc/apps/jacobi_types.cuh"
 #include "../../charming_b200/csrc/apps/jacobi_sweep.cuh"
+#include "../../charming_b200/csrc/apps/jacobi_layout.h"
 
 #include <chrono>
 #include <condition_variable>
 #include <deque>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -94,7 +96,7 @@ struct PE {
   size_t ucap = 0;
   std::vector<double> red;
   int revive = 0;
-  alignas(128) unsigned char smem[1 << 16];  // charm::smem_scratch() of the block
+  alignas(128) unsigned char smem[1 << 20];  // charm::smem_scratch() of the block
 #ifdef EMU_MT
   struct Warp {
     SiteBarrier bar;
@@ -491,74 +493,61 @@ void pe_thread(int me, int tid, int seed) {
   }
 }
 
+// Initial state as init_kernel: boundary values wherever the ghost zone
+// position lies on the global grid, interior 0, both buffers.
 template <typename T>
 void cell_init(const jac::chare_desc& d, const jac::prob_desc& p, const double* bc) {
-  for (int r = 0; r < d.h + 2; r++) {
-    for (int c = 0; c < d.w + 2; c++) {
+  const int D = d.depth;
+  for (int r = 1 - D; r <= d.h + D; r++) {
+    for (int c = 1 - D; c <= d.w + D; c++) {
       int gy = d.y0 + r, gx = d.x0 + c;
+      if (gy < 0 || gy > p.ny + 1 || gx < 0 || gx > p.nx + 1) continue;
       double v = 0.0;
       if (gy == 0) v = bc[0];
       else if (gy == p.ny + 1) v = bc[1];
       else if (gx == 0) v = bc[2];
       else if (gx == p.nx + 1) v = bc[3];
       for (int b = 0; b < 2; b++)
-        reinterpret_cast<T*>(d.buf[b])[(size_t)r * d.pitch + jac::traits<T>::OFF - 1 + c] = (T)v;
+        reinterpret_cast<T*>(d.buf[b])[(long long)r * d.pitch + jac::traits<T>::OFF - 1 + c] = (T)v;
     }
   }
 }
 
 template <typename T>
 int run(int nx, int ny, int px, int py, int max_sweeps, int K, double tol, int n_pes,
-    int halo_mode, const double bc[4], int seed, int threads, int pipeline, int tile_w) {
+    int halo_mode, const double bc[4], int seed, int threads, int pipeline, int tile_w, int depth,
+    int balance) {
   constexpr int V = jac::traits<T>::VEC, OFF = jac::traits<T>::OFF;
-  const int align_el = 128 / (int)sizeof(T);
   c_n_pes = c_n_pes_node = n_pes;
   c_n_sms = n_pes;
   c_n_nodes = c_n_devs = c_n_devs_node = 1;
-  int nc = px * py;
-  std::vector<jac::chare_desc> ch(nc);
-  for (int cy = 0; cy < py; cy++) {
-    for (int cx = 0; cx < px; cx++) {
-      int r = cy * px + cx;
-      jac::chare_desc& d = ch[r];
-      d = jac::chare_desc{};
-      d.prob = 0;
-      d.cx = cx;
-      d.cy = cy;
-      d.x0 = jac::split_start(nx, px, cx);
-      d.y0 = jac::split_start(ny, py, cy);
-      d.w = jac::split_start(nx, px, cx + 1) - d.x0;
-      d.h = jac::split_start(ny, py, cy + 1) - d.y0;
-      d.pitch = (OFF + d.w + 2 * V + align_el - 1) / align_el * align_el;
-      d.nbr[jac::TOP] = cy > 0 ? r - px : -1;
-      d.nbr[jac::BOTTOM] = cy < py - 1 ? r + px : -1;
-      d.nbr[jac::LEFT] = cx > 0 ? r - 1 : -1;
-      d.nbr[jac::RIGHT] = cx < px - 1 ? r + 1 : -1;
-      d.rank = r;
-      d.parent = r > 0 ? (r - 1) / 2 : -1;
-      d.child[0] = 2 * r + 1 < nc ? 2 * r + 1 : -1;
-      d.child[1] = 2 * r + 2 < nc ? 2 * r + 2 : -1;
-      for (int b = 0; b < 2; b++) {
-        size_t bytes = ((size_t)d.pitch * (d.h + 2) * sizeof(T) + 255) / 256 * 256;
-        d.buf[b] = aligned_alloc(256, bytes);
-        memset(d.buf[b], 0, bytes);
-#ifdef EMU_MT
-        g_src_ranges.push_back({static_cast<const unsigned char*>(d.buf[b]), bytes});
-#endif
-      }
-    }
+  // the decomposition and placement of charming_jacobi2d_create
+  charming_jacobi_problem q{};
+  q.nx = nx;
+  q.ny = ny;
+  q.px = px;
+  q.py = py;
+  q.max_sweeps = max_sweeps;
+  q.check_every = K;
+  q.tol = tol;
+  for (int k = 0; k < 4; k++) q.bc[k] = bc[k];
+  jac::layout L;
+  std::string err;
+  if (!jac::build_layout(&q, 1, 0, balance, depth, pipeline, n_pes, (int)sizeof(T), OFF, V, &L, &err)) {
+    fprintf(stderr, "layout: %s\n", err.c_str());
+    return 2;
   }
-  jac::prob_desc pd{};
-  pd.nx = nx; pd.ny = ny; pd.px = px; pd.py = py;
-  pd.max_sweeps = max_sweeps;
-  pd.check_every = K;
-  pd.tol = tol;
-  pd.root = 0;
-  pd.n_chares = nc;
+  const int nc = (int)L.chares.size();
+  char* grids = static_cast<char*>(aligned_alloc(256, L.total_bytes));
+  memset(grids, 0, L.total_bytes);
+#ifdef EMU_MT
+  g_src_ranges.push_back({reinterpret_cast<const unsigned char*>(grids), L.total_bytes});
+#endif
+  jac::place_buffers(&L, grids, (int)sizeof(T));
+  std::vector<jac::chare_desc>& ch = L.chares;
+  jac::prob_desc& pd = L.probs[0];
   for (auto& d : ch) cell_init<T>(d, pd, bc);
-  // default block map over PEs (include/chare.h placement rule)
-  std::vector<int> block_map(n_pes, nc / n_pes);
-  for (int p = 0; p < nc % n_pes; p++) block_map[p]++;
+  std::vector<int>& block_map = L.block_map;
   jac::prob_result res{};
   unsigned long long done = 0;
   std::vector<int> final_buf(nc, 0);
@@ -633,10 +622,10 @@ int run(int nx, int ny, int px, int py, int max_sweeps, int K, double tol, int n
   for (int gy = 0; gy < ny + 2; gy++) {
     for (int gx = 0; gx < nx + 2; gx++) {
       int iy = std::min(std::max(gy - 1, 0), ny - 1), ix = std::min(std::max(gx - 1, 0), nx - 1);
-      int k = jac::split_owner(ny, py, iy) * px + jac::split_owner(nx, px, ix);
+      int k = L.chare_of[jac::split_owner(ny, py, iy) * px + jac::split_owner(nx, px, ix)];
       const jac::chare_desc& d = ch[k];
       grid[(size_t)gy * (nx + 2) + gx] = reinterpret_cast<T*>(d.buf[final_buf[k]])
-          [(size_t)(gy - d.y0) * d.pitch + OFF - 1 + (gx - d.x0)];
+          [(long long)(gy - d.y0) * d.pitch + OFF - 1 + (gx - d.x0)];
       double v = 0.0;
       if (gy == 0) v = bc[0];
       else if (gy == ny + 1) v = bc[1];
@@ -650,10 +639,7 @@ int run(int nx, int ny, int px, int py, int max_sweeps, int K, double tol, int n
   int exact = memcmp(grid.data(), ref.data(), grid.size() * sizeof(T)) == 0;
   printf("status=%d err=%d,%d sweeps=%d checks=%d res0=%.17g res_last=%.17g exact=%d done=%llu\n",
       g_status.load(), g_err_a, g_err_b, res.sweeps, res.checks, res.res0, res.res_last, exact, done);
-  for (auto& d : ch) {
-    free(d.buf[0]);
-    free(d.buf[1]);
-  }
+  free(grids);
   return g_status.load() == 0 && exact ? 0 : 1;
 }
 
@@ -674,6 +660,8 @@ int main(int argc, char** argv) {
   int threads = argc >= 17 ? atoi(argv[16]) : 1;
   int pipeline = argc >= 18 ? atoi(argv[17]) : 0;
   int tile_w = argc >= 19 ? atoi(argv[18]) : 0;
+  int depth = argc >= 20 ? atoi(argv[19]) : 1;
+  int balance = argc >= 21 ? atoi(argv[20]) : 0;
 #ifdef EMU_MT
   if (n_pes != 1 || threads < 1 || (pipeline && threads % 32)) {
     fprintf(stderr, "the threaded build runs one PE block (n_pes 1); the bulk-copy sweep needs whole warps\n");
@@ -685,6 +673,6 @@ int main(int argc, char** argv) {
     return 2;
   }
 #endif
-  return dtype == 0 ? run<double>(nx, ny, px, py, ms, K, tol, n_pes, halo, bc, seed, threads, pipeline, tile_w)
-                    : run<float>(nx, ny, px, py, ms, K, tol, n_pes, halo, bc, seed, threads, pipeline, tile_w);
+  return dtype == 0 ? run<double>(nx, ny, px, py, ms, K, tol, n_pes, halo, bc, seed, threads, pipeline, tile_w, depth, balance)
+                    : run<float>(nx, ny, px, py, ms, K, tol, n_pes, halo, bc, seed, threads, pipeline, tile_w, depth, balance);
 }

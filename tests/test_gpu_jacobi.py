@@ -32,9 +32,10 @@ def bits(a):
 
 @pytest.mark.parametrize("pipeline", [True, False])
 def test_c1_512_fp64_bit_exact(rt, pipeline):
-    """C1: 512^2 interior, top 1 / others 0, 4x4 chares of 128^2, 100 sweeps."""
+    """C1: 512^2 interior, top 1 / others 0, 4x4 chares of 128^2, 100 sweeps,
+    one halo exchange per sweep as in the reference."""
     p = Problem(512, 512, 100, px=4, py=4, bc=(1.0, 0.0, 0.0, 0.0))
-    with Jacobi2D([p], pipeline=pipeline) as j:
+    with Jacobi2D([p], pipeline=pipeline, depth=1) as j:
         j.run()
         out = j.store(0)
         assert j.result(0).sweeps == 100
@@ -167,3 +168,47 @@ def test_many_chares_per_pe(rt):
         out = j.store(0)
         assert j.info()["max_chares_per_pe"] >= 2
     assert np.array_equal(bits(out), bits(jac64(g, 15)))
+
+
+@pytest.mark.parametrize("depth", [2, 3, 4])
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_multi_sweep_passes_bit_exact(rt, depth, dtype):
+    """depth sweeps per halo exchange (ghost zones of that depth, corner
+    halos from diagonal neighbours): the same bits as one sweep per
+    exchange. Sweep counts that are not multiples of the depth end with a
+    shorter pass."""
+    npdt = np.float64 if dtype == "f64" else np.float32
+    for (nx, ny, px, py, sweeps) in [(333, 201, 5, 3, 37), (1000, 77, 7, 2, 9), (50, 700, 1, 9, 11),
+                                     (2500, 40, 2, 1, 6), (300, 180, 3, 2, 40)]:
+        g = seeded_grid(nx, ny, nx * 7 + ny + depth).astype(npdt)
+        with Jacobi2D([Problem(nx, ny, sweeps, px=px, py=py)], dtype=dtype, depth=depth) as j:
+            j.load(0, g)
+            j.run()
+            out = j.store(0)
+            info = j.info()
+        ref = jac64(g, sweeps) if dtype == "f64" else jac32(g, sweeps)
+        assert np.array_equal(bits(out), bits(ref)), (nx, ny, px, py, sweeps)
+        corners = 4 * (px - 1) * (py - 1)
+        edges = 2 * (px - 1) * py + 2 * px * (py - 1)
+        assert info["halo_msgs_per_sweep"] == edges + corners
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_multi_sweep_residual_stop_rule(rt, dtype):
+    """Residual checks every 10 sweeps with passes of 4: passes 4, 4, 2 so
+    every check starts a pass; stops where one-sweep exchanges stop."""
+    nx, ny, K = 96, 80, 10
+    p = Problem(nx, ny, 3000, px=3, py=2, check_every=K, tol=0.05, bc=(1.0, 0.25, 0.5, 0.0))
+    npdt = np.float64 if dtype == "f64" else np.float32
+    with Jacobi2D([p], dtype=dtype, depth=4) as j:
+        j.run()
+        out = j.store(0)
+        r = j.result(0)
+    with Jacobi2D([p], dtype=dtype, depth=1) as j:
+        j.run()
+        r1 = j.result(0)
+    assert r.sweeps == r1.sweeps and r.sweeps % K == 0
+    g0 = initial_grid(nx, ny, p.bc, npdt)
+    ref = jac64(g0, r.sweeps) if dtype == "f64" else jac32(g0, r.sweeps)
+    assert np.array_equal(bits(out), bits(ref))
+    assert r.res0 == pytest.approx(r1.res0, rel=1e-12)
