@@ -8,7 +8,9 @@
 // 0 on delivery). The reference never terminates; here chare 1 calls end()
 // after its second delivery. out records the delivered refnums in order.
 #include "suite.cuh"
+#ifndef CHARMING_HOST_EMULATION  // the CPU check of the runtime has no CUDA API
 #include "../host.cuh"
+#endif
 
 namespace {
 
@@ -96,6 +98,7 @@ __device__ void suite::refnum_main(int pe) {
   if (pe == 0) ref_proxy->invoke(0, 0, nullptr, 0, 0);
 }
 
+#ifndef CHARMING_HOST_EMULATION
 extern "C" int charming_hello(int* out, int n_out, int* n_chares) {
   int rc = charm_host::ensure_init();
   if (rc) return rc;
@@ -149,3 +152,4 @@ extern "C" int charming_refnum(int* out, int n_out, int* n_delivered) {
 extern "C" int charming_refnum_reversed(int* out, int n_out, int* n_delivered) {
   return refnum_run(out, n_out, n_delivered, 1);
 }
+#endif

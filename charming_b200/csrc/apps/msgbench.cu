@@ -1,7 +1,9 @@
 // Messaging microbenchmarks: pingpong (examples/pingpong/pingpong.cu:17-217)
 // and a seeded fan-out with refnums.
 #include "suite.cuh"
+#ifndef CHARMING_HOST_EMULATION  // the CPU check of the runtime has no CUDA API
 #include "../host.cuh"
+#endif
 #include <vector>
 
 namespace {
@@ -283,6 +285,7 @@ __device__ void suite::fanout_main(int pe) {
   }
 }
 
+#ifndef CHARMING_HOST_EMULATION
 extern "C" int charming_pingpong(const uint64_t* sizes, int n_sizes, int round_trips,
     int warmup, uint64_t seed, int verify, charming_pingpong_result* out, int* sm_pair) {
   int rc = charm_host::ensure_init();
@@ -377,3 +380,4 @@ extern "C" int charming_fanout(int n_chares, int msgs_per_chare, int payload_byt
   cudaFree(d_exp);
   return rc;
 }
+#endif

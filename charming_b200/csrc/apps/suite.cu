@@ -1,6 +1,8 @@
 // charm::main of libcharming_b200.so and helpers shared by the programs.
 #include "suite.cuh"
+#ifndef CHARMING_HOST_EMULATION  // the CPU check of the runtime has no CUDA API
 #include "../host.cuh"
+#endif
 
 __device__ suite::app_params g_app;
 
@@ -68,6 +70,7 @@ __device__ unsigned long long suite::checksum_block(const void* data, unsigned l
   return block_sum_u64(acc) ^ n;
 }
 
+#ifndef CHARMING_HOST_EMULATION
 int suite_run(const suite::app_params& p) {
   int rc = charm_host::ensure_init();
   if (rc) return rc;
@@ -77,3 +80,4 @@ int suite_run(const suite::app_params& p) {
   char* argv[] = {name, nullptr};
   return charm_host::run_scheduler(1, argv);
 }
+#endif

@@ -321,6 +321,12 @@ int charming_init(const charming_config* cfg_in) {
   if ((rc = dev_alloc(&ds.progress, 8ull * n_pes, "progress"))) return rc;
   if ((rc = dev_alloc(&ds.pe_stats, 8ull * N_STATS * n_pes, "stats"))) return rc;
   if ((rc = dev_alloc(&ds.pe_times, 24ull * n_pes, "times"))) return rc;
+  // per-PE arena for proxy tables and chare objects (reset every run; the
+  // device heap takes over when a PE needs more)
+  ds.arena_bytes = 256ull << 10;
+  if (const char* ev = getenv("CHARMING_ARENA_BYTES")) ds.arena_bytes = strtoull(ev, nullptr, 10);
+  ds.arena = nullptr;
+  if (ds.arena_bytes && (rc = dev_alloc(&ds.arena, ds.arena_bytes * n_pes, "arena"))) return rc;
   e = cudaHostAlloc(&g.h_stop, 64, cudaHostAllocMapped);
   if (e != cudaSuccess) return cuda_fail(e, "host stop word");
   *g.h_stop = 0;

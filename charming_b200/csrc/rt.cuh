@@ -82,6 +82,8 @@ struct device_state {
   unsigned long long* pe_times;        // [n_pes][2] loop start / end
   volatile int* host_stop;             // mapped host word, may be null
   int free_chares_at_exit;
+  unsigned char* arena;                // [n_pes][arena_bytes]: per-run bump allocator
+  unsigned long long arena_bytes;      // per PE
 };
 
 // Words of device_state::ctrl (each on its own 128-B line).
@@ -119,6 +121,7 @@ struct pe_state {
   unsigned long long red_u[4];
   unsigned long long stats[N_STATS];
   unsigned long long idle_polls_since_check;
+  unsigned long long arena_top;        // bytes of this PE's arena handed out this run
   // followed by head_cache[n_pes] (unsigned long long), then scratch
 };
 
@@ -128,6 +131,7 @@ __device__ __forceinline__ unsigned long long* head_cache() {
 }
 
 // ---- PTX helpers ----------------------------------------------------------
+#ifndef CHARMING_HOST_EMULATION
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
   unsigned long long v;
   asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
@@ -154,11 +158,31 @@ __device__ __forceinline__ int ld_sys_s32(const volatile int* p) {
   asm volatile("ld.relaxed.sys.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
+}
 __device__ __forceinline__ unsigned long long globaltimer() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
+#else
+// The CPU check of the runtime (tests/emu) maps these onto C++ atomics.
+inline unsigned long long ld_acquire_u64(const unsigned long long* p) { return __atomic_load_n(p, __ATOMIC_ACQUIRE); }
+inline void st_release_u64(unsigned long long* p, unsigned long long v) { __atomic_store_n(p, v, __ATOMIC_RELEASE); }
+inline unsigned int ld_acquire_u32(const unsigned int* p) { return __atomic_load_n(p, __ATOMIC_ACQUIRE); }
+inline void st_release_u32(unsigned int* p, unsigned int v) { __atomic_store_n(p, v, __ATOMIC_RELEASE); }
+inline int ld_relaxed_s32(const int* p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
+inline int ld_sys_s32(const volatile int* p) { return __atomic_load_n(const_cast<const int*>(p), __ATOMIC_RELAXED); }
+inline unsigned long long ld_relaxed_u64(const unsigned long long* p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
+inline void st_relaxed_u64(unsigned long long* p, unsigned long long v) { __atomic_store_n(p, v, __ATOMIC_RELAXED); }
+unsigned long long globaltimer();
+#endif
 
 __device__ __forceinline__ int* ctrl(int w) { return c_rt.ctrl + w; }
 

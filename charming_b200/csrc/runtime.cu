@@ -61,6 +61,20 @@ __device__ void charm::detail::report_error(int code, int info0, int info1) {
   set_error(code, info0, info1);
 }
 
+__device__ void* charm::detail::pe_alloc(size_t bytes) {
+  if (!c_rt.arena) return nullptr;
+  pe_state* ps = pes();
+  unsigned long long at = (ps->arena_top + 15) & ~15ULL;
+  if (at + bytes > c_rt.arena_bytes) return nullptr;
+  ps->arena_top = at + bytes;
+  return c_rt.arena + (unsigned long long)blockIdx.x * c_rt.arena_bytes + at;
+}
+
+__device__ bool charm::detail::pe_owns(const void* p) {
+  const unsigned char* b = static_cast<const unsigned char*>(p);
+  return c_rt.arena && b >= c_rt.arena && b < c_rt.arena + (unsigned long long)c_rt.n_pes * c_rt.arena_bytes;
+}
+
 __device__ chare_proxy_table& charm::detail::my_proxy_table() {
   return c_rt.proxy_tables[blockIdx.x];
 }
@@ -98,9 +112,13 @@ __device__ void* charm::smem_scratch(size_t* bytes) {
 __device__ uint64_t charm::now_ns() { return globaltimer(); }
 
 __device__ unsigned int charm::smid() {
+#ifndef CHARMING_HOST_EMULATION
   unsigned int r;
   asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
   return r;
+#else
+  return blockIdx.x;
+#endif
 }
 
 // ---------------------------------------------------------------------------
@@ -364,10 +382,9 @@ __device__ void stash_revive() {
   stash_key* keys = keys_of(blockIdx.x);
   chare_proxy_table& tb = c_rt.proxy_tables[blockIdx.x];
   unsigned long long kh = ps->key_head, kt = ps->key_tail;
-  if (threadIdx.x == 0) {
-    ps->red_i[0] = 0;
-    ps->revive_pending = 0;
-  }
+  if (threadIdx.x == 0) ps->red_i[0] = 0;
+  // revive_pending is cleared below, after this barrier: every thread has
+  // read it (scheduler_loop) before it changes
   __syncthreads();
   if (ps->n_waiting > 0) {
     int cnt = 0;
@@ -386,6 +403,7 @@ __device__ void stash_revive() {
   __syncthreads();
   if (threadIdx.x == 0) {
     int c = ps->red_i[0];
+    ps->revive_pending = 0;
     ps->n_ready += c;
     ps->n_waiting -= c;
     ps->stats[ST_REVIVED] += c;
@@ -421,6 +439,9 @@ __device__ void stash_dispatch_ready() {
   if (threadIdx.x == 0) ps->b_i0 = p->refnum_matches(k->chare_idx, k->refnum) ? 1 : 0;
   __syncthreads();
   int go = ps->b_i0;
+  // The entry method may send at once, and a send reuses the broadcast
+  // slots: every thread must have read them first.
+  __syncthreads();
   if (go) {
     const regular_msg* rm = reinterpret_cast<const regular_msg*>(env + sizeof(envelope));
     p->call(k->chare_idx, rm->ep_id, env + HDR, k->refnum);
@@ -431,7 +452,7 @@ __device__ void stash_dispatch_ready() {
     if (go) {
       k->state = KEY_FREE;
       ps->stats[ST_DELIVERED]++;
-      c_rt.progress[blockIdx.x] = globaltimer();
+      st_relaxed_u64(&c_rt.progress[blockIdx.x], globaltimer());
       stash_retire();
     } else {
       k->state = KEY_WAIT;
@@ -447,7 +468,7 @@ __device__ void check_idle_timeout(unsigned long long now) {
   if (c_rt.idle_timeout_ns == 0) return;
   unsigned long long latest = pes()->t0;
   for (int p = 0; p < c_rt.n_pes; p++) {
-    unsigned long long v = *((volatile unsigned long long*)&c_rt.progress[p]);
+    unsigned long long v = ld_relaxed_u64(&c_rt.progress[p]);
     if (v > latest) latest = v;
   }
   if (now > latest && now - latest > c_rt.idle_timeout_ns) {
@@ -531,14 +552,17 @@ __device__ void dispatch_inbox() {
     ps->b_u0 = size;
   }
   __syncthreads();
-  int action = ps->b_i0;
-  unsigned long long size = ps->b_u0;
+  const int action = ps->b_i0;
+  const unsigned long long size = ps->b_u0;
+  chare_proxy_base* p = reinterpret_cast<chare_proxy_base*>(ps->b_ptr0);
+  const int idx = ps->b_i1, ep = ps->b_i2, ref = ps->b_i3, cid = ps->b_i4, src = ps->b_i5;
+  // The entry method may send at once, and a send reuses the broadcast
+  // slots: every thread must have read them first.
+  __syncthreads();
   if (action == 0) {
-    chare_proxy_base* p = reinterpret_cast<chare_proxy_base*>(ps->b_ptr0);
-    int idx = ps->b_i1, ep = ps->b_i2, ref = ps->b_i3;
     p->call(idx, ep, m + HDR, ref);
   } else if (action == 1) {
-    stash_put(m, size, ps->b_i4, ps->b_i1, ps->b_i3, ps->b_i5);
+    stash_put(m, size, cid, idx, ref, src);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -546,7 +570,7 @@ __device__ void dispatch_inbox() {
     st_release_u64(&c_rt.head[me].v, ps->head);
     if (action == 0) {
       ps->stats[ST_DELIVERED]++;
-      c_rt.progress[me] = globaltimer();
+      st_relaxed_u64(&c_rt.progress[me], globaltimer());
     }
   }
 }
@@ -596,6 +620,7 @@ charming_scheduler_kernel(int argc, char** argv, size_t* argvs) {
     ps->n_waiting = ps->n_ready = 0;
     for (int i = 0; i < N_STATS; i++) ps->stats[i] = 0;
     ps->idle_polls_since_check = 0;
+    ps->arena_top = 0;
   }
   for (int i = threadIdx.x; i < c_rt.n_pes; i += blockDim.x) head_cache()[i] = c_rt.head[i].v;
   __syncthreads();

@@ -79,8 +79,11 @@ struct chare_proxy_base {
   end_idx(-1), loc_map(nullptr), em_count(0), async_waits(nullptr),
   refnum(nullptr), mismatches(nullptr) {}
 
-  // Returns false without running the entry method when the message refnum
-  // is not -1 and differs from the chare's (include/chare.h:181-195).
+  // Runs entry method ep of local chare idx on arg (all threads of the PE
+  // block). The scheduler decides the refnum match (refnum_matches, the
+  // rule of include/chare.h:181-195) in one thread before it calls: the
+  // entry method may change the chare's refnum at once, so the threads must
+  // not test it again here. Returns true.
   __device__ virtual bool call(int idx, int ep, void* arg, int ref) = 0;
   // Frees the local chares and tables (the runtime calls it when a run ends
   // and then deletes the proxy).
@@ -115,6 +118,33 @@ enum : int {
   ERR_TOO_MANY_EMS = 11,
   ERR_NO_MEMORY = 17,
 };
+// Per-PE bump allocator for the runtime's own objects (proxy tables, chare
+// objects): reset at every run, nothing freed one by one. Single-threaded.
+// Returns nullptr when the PE's arena is exhausted (callers fall back to the
+// device heap).
+__device__ void* pe_alloc(size_t bytes);
+// Whether p came from some PE's arena (then it is not handed to free()).
+__device__ bool pe_owns(const void* p);
+template <class T>
+__device__ T* pe_array(size_t n) {  // trivially constructible T
+  void* p = pe_alloc(n * sizeof(T));
+  return p ? static_cast<T*>(p) : new T[n];
+}
+template <class T>
+__device__ void pe_free_array(T* p) {
+  if (p && !pe_owns(p)) delete[] p;
+}
+template <class T>
+__device__ T* pe_make() {
+  void* p = pe_alloc(sizeof(T));
+  return p ? new (p) T() : new T();
+}
+template <class T>
+__device__ void pe_destroy(T* p) {
+  if (!p) return;
+  if (pe_owns(p)) p->~T();
+  else delete p;
+}
 } // namespace detail
 
 __device__ int my_pe();
@@ -134,7 +164,7 @@ struct chare_proxy : chare_proxy_base {
     }
     id = table.count++;
     table.proxies[id] = this;
-    entry_methods = new entry_method_base<C>*[EM_CNT_MAX];
+    entry_methods = detail::pe_array<entry_method_base<C>*>(EM_CNT_MAX);
     if (entry_methods == nullptr) detail::report_error(detail::ERR_NO_MEMORY, id, 0);
   }
 
@@ -145,7 +175,7 @@ struct chare_proxy : chare_proxy_base {
       detail::report_error(detail::ERR_TOO_MANY_EMS, id, em_count);
       return;
     }
-    entry_method_base<C>* em = new entry_method<C, Func>();
+    entry_method_base<C>* em = detail::pe_make<entry_method<C, Func>>();
     if (em == nullptr) {
       detail::report_error(detail::ERR_NO_MEMORY, id, em_count);
       return;
@@ -161,7 +191,7 @@ struct chare_proxy : chare_proxy_base {
     int n_pes_ = c_n_pes;
     int me = charm::my_pe();
 
-    loc_map = new int[n_chares > 0 ? n_chares : 1];
+    loc_map = detail::pe_array<int>(n_chares > 0 ? n_chares : 1);
     if (loc_map == nullptr) {
       detail::report_error(detail::ERR_NO_MEMORY, id, n_chares);
       return;
@@ -180,14 +210,14 @@ struct chare_proxy : chare_proxy_base {
         n_local = n_cur;
         start_idx = start;
         end_idx = end;
-        objects = (n_local > 0) ? new C*[n_local] : nullptr;
-        refnum = (n_local > 0) ? new int[n_local] : nullptr;
+        objects = (n_local > 0) ? detail::pe_array<C*>(n_local) : nullptr;
+        refnum = (n_local > 0) ? detail::pe_array<int>(n_local) : nullptr;
         if (n_local > 0 && (objects == nullptr || refnum == nullptr)) {
           detail::report_error(detail::ERR_NO_MEMORY, id, n_local);
           n_local = 0;
         }
         for (int k = 0; k < n_local; k++) {
-          objects[k] = new C;
+          objects[k] = detail::pe_make<C>();
           if (objects[k] == nullptr) {
             detail::report_error(detail::ERR_NO_MEMORY, id, k);
             n_local = k;
@@ -206,20 +236,20 @@ struct chare_proxy : chare_proxy_base {
   inline __device__ void create(int n_chares) { create(n_chares, nullptr); }
 
   __device__ virtual bool call(int idx, int ep, void* arg, int ref) {
+    (void)ref;
     int local_idx = idx - start_idx;
-    if (ref != -1 && ref != refnum[local_idx]) return false;
     (*(entry_methods[ep]))(*(objects[local_idx]), arg);
     return true;
   }
 
   __device__ virtual void release_all() {
-    for (int k = 0; k < n_local; k++) delete objects[k];
-    delete[] objects;
-    delete[] refnum;
-    delete[] loc_map;
+    for (int k = 0; k < n_local; k++) detail::pe_destroy(objects[k]);
+    detail::pe_free_array(objects);
+    detail::pe_free_array(refnum);
+    detail::pe_free_array(loc_map);
     if (entry_methods) {
-      for (int e = 0; e < em_count; e++) delete entry_methods[e];
-      delete[] entry_methods;
+      for (int e = 0; e < em_count; e++) detail::pe_destroy(entry_methods[e]);
+      detail::pe_free_array(entry_methods);
     }
     objects = nullptr;
     refnum = nullptr;

@@ -82,7 +82,9 @@ template <typename T> inline T __shfl_sync(unsigned, T v, int src) {
 #else
 inline void __syncwarp(unsigned = 0xffffffffu) {}
 inline bool __all_sync(unsigned, bool p) { return p; }
-template <typename T> inline T __shfl_xor_sync(unsigned, T v, int) { return v; }
+// one thread per block: the partner lane of a butterfly does not exist and
+// contributes nothing
+template <typename T> inline T __shfl_xor_sync(unsigned, T v, int o) { return o ? T(0) : v; }
 template <typename T> inline T __shfl_up_sync(unsigned, T v, int) { return v; }
 template <typename T> inline T __shfl_down_sync(unsigned, T v, int) { return v; }
 template <typename T> inline T __shfl_sync(unsigned, T v, int) { return v; }
@@ -123,5 +125,11 @@ using std::min;
 using std::max;
 inline size_t __cvta_generic_to_shared(const void* p) { return (size_t)p; }
 
-// Stand-in for the scheduler's dynamic shared memory (referenced, unused).
+// Stand-in for the scheduler's dynamic shared memory: one per PE thread for
+// the runtime check (EMU_RT), referenced but unused by the chare checks.
+#ifdef EMU_RT
+extern thread_local uint64_t* s_mem_of_pe;  // set by each PE thread
+#define s_mem s_mem_of_pe
+#else
 extern uint64_t s_mem[];
+#endif

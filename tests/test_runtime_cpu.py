@@ -1,0 +1,94 @@
+"""CPU check of the runtime itself: charming_b200/csrc/runtime.cu (scheduler
+loop, inbox rings, stash and revive, termination) and the message programs
+compiled for the host (tests/emu/rt_emu.cpp). Three builds: one host thread
+per PE under AddressSanitizer/UBSan and under ThreadSanitizer (many PEs,
+small rings that wrap), and one PE block of many threads under
+ThreadSanitizer with call-site-checked barriers and lockstep warps (the
+block-collective paths). Delivery logs are checked against the CPU model of
+the reference semantics (oracle/msgmodel.py): counts, per-pair order, the
+refnum ladder and payload checksums."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import msgmodel
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+OUT = os.path.join(ROOT, "build", "emu")
+
+
+@pytest.fixture(scope="module")
+def emus():
+    r = subprocess.run(["make", "-s"], cwd=os.path.join(ROOT, "tests", "emu"), capture_output=True,
+                       text=True)
+    if r.returncode != 0:
+        pytest.fail(r.stdout[-3000:] + r.stderr[-3000:])
+    return {k: os.path.join(OUT, k) for k in ("rt_emu", "rt_emu_tsan", "rt_emu_mt")}
+
+
+def run(exe, args, threads=1, timeout=600):
+    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0", TSAN_OPTIONS="halt_on_error=1",
+               RT_EMU_THREADS=str(threads))
+    r = subprocess.run([exe] + [str(a) for a in args], capture_output=True, text=True,
+                       timeout=timeout, env=env)
+    assert "ThreadSanitizer" not in r.stderr and "divergence" not in r.stderr, r.stderr[-3000:]
+    assert "runtime error" not in r.stderr, r.stderr[-3000:]
+    return r
+
+
+def fanout(exe, n_pes, ring, n, msgs, payload, seed, mode, threads=1):
+    r = run(exe, ["fanout", n_pes, ring, n, msgs, payload, seed, mode], threads)
+    head = r.stdout.splitlines()[0]
+    assert r.returncode == 0 and head.startswith("status=0"), (head, r.stderr[-2000:])
+    rows = [l.split()[1:] for l in r.stdout.splitlines() if l.startswith("L ")]
+    log = np.array([[int(x, 16) for x in row] for row in rows], dtype=np.uint32).reshape(-1, 8)
+    chk = msgmodel.check_fanout_log(log, n, msgs, payload, seed, mode)
+    assert chk.ok, chk.errors
+    assert chk.delivered == n * msgs
+
+
+@pytest.mark.parametrize("n_pes,ring,n,msgs,payload,mode", [
+    (16, 65536, 300, 16, 64, 0),      # rings wrap many times
+    (16, 262144, 300, 16, 64, 1),     # refnum ladder through the stash
+    (32, 1 << 20, 4096, 16, 64, 1),   # the C2b shape on 32 PEs
+    (24, 1 << 20, 512, 8, 1024, 1),   # larger payloads, stash arena use
+])
+def test_fanout_many_pes(emus, n_pes, ring, n, msgs, payload, mode):
+    fanout(emus["rt_emu"], n_pes, ring, n, msgs, payload, 0xC0FFEE + n + mode, mode)
+
+
+@pytest.mark.parametrize("n_pes,ring,n,msgs,payload,mode", [
+    (8, 65536, 200, 8, 64, 1),
+    (8, 65536, 120, 8, 64, 0),
+])
+def test_fanout_many_pes_threads_race_free(emus, n_pes, ring, n, msgs, payload, mode):
+    fanout(emus["rt_emu_tsan"], n_pes, ring, n, msgs, payload, 7 + mode, mode)
+
+
+@pytest.mark.parametrize("threads", [32, 96])
+@pytest.mark.parametrize("n,msgs,payload,mode,ring", [
+    (32, 16, 64, 1, 1 << 18),
+    (40, 8, 1024, 1, 1 << 20),
+    (48, 8, 256, 0, 1 << 18),
+])
+def test_fanout_block_collective_paths(emus, threads, n, msgs, payload, mode, ring):
+    fanout(emus["rt_emu_mt"], 1, ring, n, msgs, payload, 0xC0FFEE, mode, threads)
+
+
+@pytest.mark.parametrize("reversed_order", [0, 1])
+@pytest.mark.parametrize("exe,n_pes,threads", [("rt_emu", 6, 1), ("rt_emu_mt", 1, 64)])
+def test_refnum_scenario(emus, exe, n_pes, threads, reversed_order):
+    r = run(emus[exe], ["refnum", n_pes, 65536, reversed_order], threads)
+    assert r.returncode == 0
+    out = r.stdout.split("out=")[1].split(",")
+    assert [int(out[0]), int(out[1])] == msgmodel.refnum_scenario(bool(reversed_order)) == [1, 0]
+
+
+@pytest.mark.parametrize("exe,n_pes,threads", [("rt_emu", 5, 1), ("rt_emu_mt", 1, 32)])
+def test_hello_chain(emus, exe, n_pes, threads):
+    r = run(emus[exe], ["hello", n_pes, 65536], threads)
+    assert r.returncode == 0
+    out = [int(x) for x in r.stdout.split("out=")[1].strip().strip(",").split(",")]
+    assert out[: 2 * n_pes] == list(range(2 * n_pes))
