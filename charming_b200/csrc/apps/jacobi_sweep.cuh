@@ -21,6 +21,7 @@
 //                 one write per point (16 B/LUP FP64, 8 B/LUP FP32).
 #pragma once
 
+#include <climits>
 #include "suite.cuh"
 #include "jacobi_types.cuh"
 
@@ -392,48 +393,69 @@ __device__ __forceinline__ float4 vec_from(const float (&a)[4]) {
   return make_float4(a[0], a[1], a[2], a[3]);
 }
 
-// One level-l row of the wavefront at sub-step K (static slot rotation:
-// level-l row r lives in W[l][(r - qs) mod 3]).
-template <typename T, bool RESID, int LMAX, int K>
-__device__ __forceinline__ void deep_substep(typename vec_of<T>::type (&W)[LMAX][3], int q, int qs,
-    int L, int h, int w, int fixed, const bool (&fixc)[traits<T>::VEC], const bool (&inw)[traits<T>::VEC],
-    bool own, int v, int col0, int r0, int r1, const block_view<T>& out, double& acc) {
+// Per-lane constants of one strip item.
+template <typename T>
+struct deep_lane {
+  bool own;                        // this lane stores its vector / counts the residual
+  int v, col0;                     // vector index, its first column
+  bool fixc[traits<T>::VEC];       // column on the domain boundary (kept at every level)
+  bool inw[traits<T>::VEC];        // column inside the chare (1..w)
+  bool anyfix;                     // some fixc[k]
+  int fix_r0, fix_r1;              // rows kept at every level (0 / h+1), or INT_MIN
+};
+
+// All L levels of the wavefront at sub-step K of a three-step cycle (level-l
+// row r lives in W[l][(r - qs) mod 3], so every window index is static).
+// CHECK: a level runs only once its three input rows exist (the first 2L
+// steps of an item). Domain-boundary cells keep their value at every level:
+// a whole row by a warp-uniform branch, a column by a per-lane fix-up.
+template <typename T, bool RESID, int L, int K, bool CHECK>
+__device__ __forceinline__ void deep_step(typename vec_of<T>::type (&W)[L][3], int q, int qs, int w,
+    const deep_lane<T>& ln, int r0, int r1, const block_view<T>& out, double& acc) {
   constexpr int V = traits<T>::VEC;
   constexpr unsigned FULL = 0xffffffffu;
   using VT = typename vec_of<T>::type;
 #pragma unroll
-  for (int l = 1; l <= LMAX; l++) {
-    if (l <= L && q >= qs + 2 * l) {
-      const int r = q - l;  // row of level l computed now
-      const int su = ((K - l - 1) % 3 + 6) % 3, sm = ((K - l) % 3 + 6) % 3, sd = ((K - l + 1) % 3 + 6) % 3;
-      T m[V], u[V], d[V], o[V];
-      vec_to<T>(W[l - 1][sm], m);
-      vec_to<T>(W[l - 1][su], u);
-      vec_to<T>(W[l - 1][sd], d);
-      T left = __shfl_up_sync(FULL, m[V - 1], 1);
-      T right = __shfl_down_sync(FULL, m[0], 1);
-      const bool fixr = (r == 0 && (fixed & 1)) || (r == h + 1 && (fixed & 2));
+  for (int l = 1; l <= L; l++) {
+    if (CHECK && q < qs + 2 * l) continue;
+    const int r = q - l;  // row of level l computed now
+    const int su = ((K - l - 1) % 3 + 6) % 3, sm = ((K - l) % 3 + 6) % 3, sd = ((K - l + 1) % 3 + 6) % 3;
+    T m[V], u[V], d[V], o[V];
+    vec_to<T>(W[l - 1][sm], m);
+    vec_to<T>(W[l - 1][su], u);
+    vec_to<T>(W[l - 1][sd], d);
+    T left = __shfl_up_sync(FULL, m[V - 1], 1);
+    T right = __shfl_down_sync(FULL, m[0], 1);
+    if (r == ln.fix_r0 || r == ln.fix_r1) {  // domain-boundary row: kept (warp-uniform)
+#pragma unroll
+      for (int k = 0; k < V; k++) o[k] = m[k];
+    } else {
 #pragma unroll
       for (int k = 0; k < V; k++) {
         T lk = (k == 0) ? left : m[k - 1];
         T rk = (k == V - 1) ? right : m[k + 1];
-        o[k] = (fixr || fixc[k]) ? m[k] : stencil(m[k], lk, rk, u[k], d[k]);
-        if (RESID && l == 1 && own && inw[k] && r >= r0 && r < r1)
+        o[k] = stencil(m[k], lk, rk, u[k], d[k]);
+        if (RESID && l == 1 && ln.own && ln.inw[k] && r >= r0 && r < r1)
           acc += resid2<T>(m[k], lk, rk, u[k], d[k]);
       }
-      if (l == L) {
-        if (own) {
-          T* op = out.at(r, col0);
-          int nvalid = w - v * V;
-          if (nvalid >= V) {
-            *reinterpret_cast<VT*>(op) = vec_from(o);
-          } else {
-            for (int k = 0; k < nvalid; k++) op[k] = o[k];
-          }
-        }
-      } else if (l < LMAX) {
-        W[l][sm] = vec_from(o);
+      if (ln.anyfix) {  // the lane holding column 0 or w+1 of the domain
+#pragma unroll
+        for (int k = 0; k < V; k++)
+          if (ln.fixc[k]) o[k] = m[k];
       }
+    }
+    if (l == L) {
+      if (ln.own) {
+        T* op = out.at(r, ln.col0);
+        int nvalid = w - ln.v * V;
+        if (nvalid >= V) {
+          *reinterpret_cast<VT*>(op) = vec_from(o);
+        } else {
+          for (int k = 0; k < nvalid; k++) op[k] = o[k];
+        }
+      }
+    } else {
+      W[l][sm] = vec_from(o);
     }
   }
 }
@@ -441,51 +463,59 @@ __device__ __forceinline__ void deep_substep(typename vec_of<T>::type (&W)[LMAX]
 // One strip item: level-0 rows stream through this lane's private ring of P
 // 16-byte slots in shared memory (cp.async, P-1 rows ahead), the levels
 // through registers.
-template <typename T, bool RESID, int LMAX, int P>
-__device__ double deep_item(const block_view<T>& in, const block_view<T>& out, int w, int h,
-    int L, int fixed, int vbase, int own0, int nown, int r0, int r1, int lane,
-    typename vec_of<T>::type* ring) {
+template <typename T, int P>
+__device__ __forceinline__ void deep_fetch(typename vec_of<T>::type* ring, int lane, int& slot, int q,
+    int qe, const block_view<T>& in, long long eo, unsigned nb, typename vec_of<T>::type& x) {
+  cp_async_wait<P - 2>();
+  x = ring[slot * 32 + lane];
+  const int nslot = slot == 0 ? P - 1 : slot - 1;  // slot of row q-1, read last step
+  if (q + P - 1 <= qe) cp_async16(&ring[nslot * 32 + lane], in.row(q + P - 1) + eo, nb);
+  cp_async_commit();
+  slot = slot + 1 == P ? 0 : slot + 1;
+}
+
+template <typename T, bool RESID, int L, int P>
+__device__ __forceinline__ double deep_item(const block_view<T>& in, const block_view<T>& out, int w,
+    const deep_lane<T>& ln, int r0, int r1, int lane, typename vec_of<T>::type* ring) {
   constexpr int V = traits<T>::VEC;
   using VT = typename vec_of<T>::type;
-  const int v = vbase + lane;
-  const int col0 = 1 + v * V;                         // first column of this lane's vector
-  const long long e0 = (long long)traits<T>::OFF - 1 + col0;  // its element index in a row
+  const long long e0 = (long long)traits<T>::OFF - 1 + ln.col0;  // element index in a row
   const bool can_load = e0 >= 0 && e0 + V <= in.pitch;
   const long long eo = can_load ? e0 : 0;
   const unsigned nb = can_load ? 16u : 0u;
-  const bool own = v >= own0 && v < own0 + nown;
-  bool fixc[V], inw[V];
-#pragma unroll
-  for (int k = 0; k < V; k++) {
-    int c = col0 + k;
-    fixc[k] = (c == 0 && (fixed & 4)) || (c == w + 1 && (fixed & 8));
-    inw[k] = c >= 1 && c <= w;
-  }
   const int qs = r0 - L, qe = r1 - 1 + L;             // level-0 rows streamed
-  // prologue: rows qs .. qs+P-2 into slots 0..P-2
 #pragma unroll
   for (int k = 0; k < P - 1; k++) {
     if (qs + k <= qe) cp_async16(&ring[k * 32 + lane], in.row(qs + k) + eo, nb);
     cp_async_commit();
   }
-  VT W[LMAX][3];
+  VT W[L][3];
   double acc = 0.0;
   int slot = 0;                                       // ring slot of row q
-  for (int q0 = qs; q0 <= qe; q0 += 3) {
+  // fill: until every level has its three rows (checked steps)
+  constexpr int F = (2 * L + 2) / 3 * 3;
+  int q0 = qs;
+  for (; q0 < qs + F && q0 <= qe; q0 += 3) {
 #pragma unroll
     for (int K = 0; K < 3; K++) {
       const int q = q0 + K;
-      if (q <= qe) {
-        cp_async_wait<P - 2>();
-        W[0][K] = ring[slot * 32 + lane];
-        const int nslot = slot == 0 ? P - 1 : slot - 1;  // slot of row q-1, read last sub-step
-        if (q + P - 1 <= qe) cp_async16(&ring[nslot * 32 + lane], in.row(q + P - 1) + eo, nb);
-        cp_async_commit();
-        slot = slot + 1 == P ? 0 : slot + 1;
-        if (K == 0) deep_substep<T, RESID, LMAX, 0>(W, q, qs, L, h, w, fixed, fixc, inw, own, v, col0, r0, r1, out, acc);
-        else if (K == 1) deep_substep<T, RESID, LMAX, 1>(W, q, qs, L, h, w, fixed, fixc, inw, own, v, col0, r0, r1, out, acc);
-        else deep_substep<T, RESID, LMAX, 2>(W, q, qs, L, h, w, fixed, fixc, inw, own, v, col0, r0, r1, out, acc);
-      }
+      if (q > qe) break;
+      deep_fetch<T, P>(ring, lane, slot, q, qe, in, eo, nb, W[0][K]);
+      if (K == 0) deep_step<T, RESID, L, 0, true>(W, q, qs, w, ln, r0, r1, out, acc);
+      else if (K == 1) deep_step<T, RESID, L, 1, true>(W, q, qs, w, ln, r0, r1, out, acc);
+      else deep_step<T, RESID, L, 2, true>(W, q, qs, w, ln, r0, r1, out, acc);
+    }
+  }
+  // steady state: all levels every step
+  for (; q0 <= qe; q0 += 3) {
+#pragma unroll
+    for (int K = 0; K < 3; K++) {
+      const int q = q0 + K;
+      if (q > qe) break;
+      deep_fetch<T, P>(ring, lane, slot, q, qe, in, eo, nb, W[0][K]);
+      if (K == 0) deep_step<T, RESID, L, 0, false>(W, q, qs, w, ln, r0, r1, out, acc);
+      else if (K == 1) deep_step<T, RESID, L, 1, false>(W, q, qs, w, ln, r0, r1, out, acc);
+      else deep_step<T, RESID, L, 2, false>(W, q, qs, w, ln, r0, r1, out, acc);
     }
   }
   cp_async_wait<0>();
@@ -534,25 +564,15 @@ __device__ double sweep_deep_simple(block_view<T> in, block_view<T> out, int w, 
   return acc;
 }
 
-template <typename T, bool RESID>
-__device__ __noinline__ double sweep_deep(block_view<T> in, block_view<T> out, int w, int h, int L,
-    int fixed) {
-  if (blockDim.x < 32) return sweep_deep_simple<T, RESID>(in, out, w, h, L, fixed);
-  constexpr int V = traits<T>::VEC, LMAX = DEPTH_MAX, P = 8;
-  using VT = typename vec_of<T>::type;
-  const int E = (L + V - 1) / V;        // vectors lost per level set at each strip edge
-  const int SS = 32 - 2 * E;            // vectors a strip owns
+// The items of one pass of L sweeps (one warp); one register allocation per L.
+template <typename T, bool RESID, int L>
+__device__ __noinline__ double sweep_deep_items(block_view<T> in, block_view<T> out, int w, int h,
+    int fixed, typename vec_of<T>::type* ring, int nw, int warp, int lane) {
+  constexpr int V = traits<T>::VEC, P = 8;
+  constexpr int E = (L + V - 1) / V;    // vectors lost at each strip edge over L levels
+  constexpr int SS = 32 - 2 * E;        // vectors a strip owns
   const int nv = (w + V - 1) / V;
   const int n_strips = (nv + SS - 1) / SS;
-  const int nw = (int)(blockDim.x / 32), warp = (int)(threadIdx.x / 32), lane = (int)(threadIdx.x & 31);
-  if (warp >= nw) return 0.0;
-  size_t sbytes = 0;
-  VT* rings = reinterpret_cast<VT*>(charm::smem_scratch(&sbytes));
-  if ((size_t)nw * P * 32 * sizeof(VT) > sbytes) {
-    if (threadIdx.x == 0) charm::detail::report_error(CHARMING_ERR_CONFIG, (int)sbytes, nw);
-    return 0.0;
-  }
-  VT* ring = rings + (size_t)warp * P * 32;
   // row runs: balance items over warps; each run at least 4L rows
   int segs = 1, best = 0x7fffffff;
   for (int sg = 1; sg <= 8; sg++) {
@@ -571,10 +591,43 @@ __device__ __noinline__ double sweep_deep(block_view<T> in, block_view<T> out, i
     int r0 = 1 + (int)((long long)h * g / segs), r1 = 1 + (int)((long long)h * (g + 1) / segs);
     int own0 = s * SS;
     int nown = min(SS, nv - own0);
-    acc += deep_item<T, RESID, LMAX, P>(in, out, w, h, L, fixed, own0 - E, own0, nown, r0, r1, lane,
-                                        ring);
+    deep_lane<T> ln;
+    ln.v = own0 - E + lane;
+    ln.col0 = 1 + ln.v * V;
+    ln.own = ln.v >= own0 && ln.v < own0 + nown;
+    ln.anyfix = false;
+#pragma unroll
+    for (int k = 0; k < V; k++) {
+      int c = ln.col0 + k;
+      ln.fixc[k] = (c == 0 && (fixed & 4)) || (c == w + 1 && (fixed & 8));
+      ln.inw[k] = c >= 1 && c <= w;
+      ln.anyfix = ln.anyfix || ln.fixc[k];
+    }
+    ln.fix_r0 = (fixed & 1) ? 0 : INT_MIN;
+    ln.fix_r1 = (fixed & 2) ? h + 1 : INT_MIN;
+    acc += deep_item<T, RESID, L, P>(in, out, w, ln, r0, r1, lane, ring);
   }
   return acc;
+}
+
+template <typename T, bool RESID>
+__device__ __noinline__ double sweep_deep(block_view<T> in, block_view<T> out, int w, int h, int L,
+    int fixed) {
+  if (blockDim.x < 32) return sweep_deep_simple<T, RESID>(in, out, w, h, L, fixed);
+  constexpr int P = 8;
+  using VT = typename vec_of<T>::type;
+  const int nw = (int)(blockDim.x / 32), warp = (int)(threadIdx.x / 32), lane = (int)(threadIdx.x & 31);
+  if (warp >= nw) return 0.0;
+  size_t sbytes = 0;
+  VT* rings = reinterpret_cast<VT*>(charm::smem_scratch(&sbytes));
+  if ((size_t)nw * P * 32 * sizeof(VT) > sbytes) {
+    if (threadIdx.x == 0) charm::detail::report_error(CHARMING_ERR_CONFIG, (int)sbytes, nw);
+    return 0.0;
+  }
+  VT* ring = rings + (size_t)warp * P * 32;
+  if (L == 2) return sweep_deep_items<T, RESID, 2>(in, out, w, h, fixed, ring, nw, warp, lane);
+  if (L == 3) return sweep_deep_items<T, RESID, 3>(in, out, w, h, fixed, ring, nw, warp, lane);
+  return sweep_deep_items<T, RESID, 4>(in, out, w, h, fixed, ring, nw, warp, lane);
 }
 
 // ---------------------------------------------------------------------------

@@ -61,8 +61,10 @@ void emu_sync(const char* file, int line);
 void emu_syncwarp(const char* file, int line);
 #define __syncwarp(...) emu_syncwarp(__FILE__, __LINE__)
 bool emu_all_sync(bool p);
+bool emu_any_sync(bool p);
 void emu_shfl(void* v, unsigned bytes, int mode, int arg);  // mode 0 up, 1 down, 2 xor, 3 index
 inline bool __all_sync(unsigned, bool p) { return emu_all_sync(p); }
+inline bool __any_sync(unsigned, bool p) { return emu_any_sync(p); }
 template <typename T> inline T __shfl_up_sync(unsigned, T v, int d) {
   emu_shfl(&v, sizeof(T), 0, d);
   return v;
@@ -82,6 +84,7 @@ template <typename T> inline T __shfl_sync(unsigned, T v, int src) {
 #else
 inline void __syncwarp(unsigned = 0xffffffffu) {}
 inline bool __all_sync(unsigned, bool p) { return p; }
+inline bool __any_sync(unsigned, bool p) { return p; }
 // one thread per block: the partner lane of a butterfly does not exist and
 // contributes nothing
 template <typename T> inline T __shfl_xor_sync(unsigned, T v, int o) { return o ? T(0) : v; }

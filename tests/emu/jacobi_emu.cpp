@@ -163,6 +163,15 @@ bool emu_all_sync(bool p) {
   w.bar.sync("all_sync", 1);
   return r;
 }
+bool emu_any_sync(bool p) {
+  PE::Warp& w = my_warp();
+  w.flag[threadIdx.x & 31] = p;
+  w.bar.sync("any_sync", 0);
+  bool r = false;
+  for (int i = 0; i < 32; i++) r = r || w.flag[i];
+  w.bar.sync("any_sync", 1);
+  return r;
+}
 void emu_shfl(void* v, unsigned bytes, int mode, int arg) {
   PE::Warp& w = my_warp();
   int lane = (int)(threadIdx.x & 31);
