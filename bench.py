@@ -345,7 +345,9 @@ def main() -> int:
             "config": workload_config(args, (px, py)),
             "msgs_per_s": msgs_per_s, "halo_msgs_per_sweep": info["halo_msgs_per_sweep"],
             "last_launch": {"ms": info["last_run_ms"], "sweep_ms_max_pe": info["sweep_ms_max"],
-                            "sweep_ms_mean_pe": info["sweep_ms_mean"], "main_ms": stats.main_ms,
+                            "sweep_ms_mean_pe": info["sweep_ms_mean"],
+                            "send_ms_mean_pe": info["send_ms_mean"],
+                            "halo_em_ms_mean_pe": info["halo_ms_mean"], "main_ms": stats.main_ms,
                             "loop_ms": stats.loop_ms, "stashed": stats.stashed,
                             "delivered": stats.delivered},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,

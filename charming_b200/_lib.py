@@ -82,6 +82,7 @@ class JacobiInfo(C.Structure):
         ("n_problems", i32), ("n_chares", i32), ("max_chares_per_pe", i32),
         ("interior_points", u64), ("grid_bytes", u64), ("halo_msgs_per_sweep", u64),
         ("last_run_ms", f64), ("sweep_ms_max", f64), ("sweep_ms_mean", f64),
+        ("send_ms_mean", f64), ("halo_ms_mean", f64),
     ]
 
 

@@ -44,8 +44,9 @@ struct japp {
   }
   __device__ static int* final_buf() { return reinterpret_cast<int*>(g_app.p[4]); }
   __device__ static const int* block_map() { return reinterpret_cast<const int*>(g_app.p[5]); }
-  // per-PE nanoseconds spent in sweeps during the run
-  __device__ static unsigned long long* sweep_ns() {
+  // per-PE nanoseconds of the run: [4 * pe + k], k = 0 sweeps, 1 sending
+  // halos, 2 halo entry methods (unpack and what follows)
+  __device__ static unsigned long long* pe_ns() {
     return reinterpret_cast<unsigned long long*>(g_app.p[6]);
   }
 };
@@ -137,43 +138,70 @@ __device__ double sweep_block(const jac::chare_desc& d, int cur, bool resid, int
                 : jac::sweep_direct<T, false>(in, out, d.w, d.h);
     __syncthreads();
   }
-  if (threadIdx.x == 0) japp::sweep_ns()[blockIdx.x] += charm::now_ns() - t0;
+  if (threadIdx.x == 0) japp::pe_ns()[4 * blockIdx.x] += charm::now_ns() - t0;
   return resid ? suite::block_sum_f64(acc) : 0.0;
 }
 
-// Packs the boundary region of buf[cur] for direction dir into a zero-copy
-// message to the neighbour there (refnum = pass in halo_mode 1). All threads.
+// Copies a rectangle between a chare grid and a packed row-major buffer
+// (to_grid: buffer -> grid). Long rows go as whole-row vector copies by all
+// threads, short ones element by element. All threads.
 template <typename T>
-__device__ void send_halo(JBlock& c, const jac::chare_desc& d, int dir) {
-  int nbr = d.nbr[dir];
-  jac::region e = jac::edge_region(dir, d.depth, d.w, d.h);
-  int len = e.nr * e.nc;
-  size_t bytes = sizeof(jac::halo_hdr) + (size_t)len * sizeof(T);
-  charm::message msg;
-  if (!jproxy->alloc_msg(msg, nbr, bytes)) return;
-  char* pl = reinterpret_cast<char*>(msg.payload());
-  T* vals = reinterpret_cast<T*>(pl + sizeof(jac::halo_hdr));
-  jac::block_view<T> g = view<T>(d, c.cur);
-  if (threadIdx.x == 0) {
-    jac::halo_hdr* hh = reinterpret_cast<jac::halo_hdr*>(pl);
-    hh->dir = jac::opposite(dir);
-    hh->len = len;
-    hh->pass = c.pass;
-    hh->iter = c.iter;
-  }
-  if (e.nr == 1) {
-    charm::copy_cooperative(vals, g.at(e.r0, e.c0), (size_t)len * sizeof(T), threadIdx.x, blockDim.x);
+__device__ void copy_region(jac::block_view<T> g, jac::region e, T* buf, bool to_grid) {
+  if (e.nc >= 32) {
+    for (int r = 0; r < e.nr; r++) {
+      T* gp = g.at(e.r0 + r, e.c0);
+      T* bp = buf + (size_t)r * e.nc;
+      if (to_grid) charm::copy_cooperative(gp, bp, (size_t)e.nc * sizeof(T), threadIdx.x, blockDim.x);
+      else charm::copy_cooperative(bp, gp, (size_t)e.nc * sizeof(T), threadIdx.x, blockDim.x);
+    }
   } else {
-    for (int i = threadIdx.x; i < len; i += blockDim.x) vals[i] = *g.at(e.r0 + i / e.nc, e.c0 + i % e.nc);
+    const int len = e.nr * e.nc;
+    for (int i = threadIdx.x; i < len; i += blockDim.x) {
+      const int r = i / e.nc, c = i - r * e.nc;
+      T* gp = g.at(e.r0 + r, e.c0 + c);
+      if (to_grid) *gp = buf[i];
+      else buf[i] = *gp;
+    }
   }
-  jproxy->invoke(nbr, EP_HALO, msg, bytes, japp::halo_mode() == 1 ? c.pass : -1);
 }
 
+// Packs the boundary regions of buf[cur] for every neighbour straight into
+// their inbox rings (zero-copy) and publishes them together: the ring
+// reservations and the publishing fences of the messages overlap (refnum =
+// pass in halo_mode 1). All threads.
 template <typename T>
 __device__ void send_halos(JBlock& c, const jac::chare_desc& d) {
+  unsigned long long t0 = charm::now_ns();
+  int idx[jac::N_DIRS], dirs[jac::N_DIRS], refs[jac::N_DIRS];
+  size_t bytes[jac::N_DIRS];
+  int n = 0;
   for (int dir = 0; dir < jac::N_DIRS; dir++) {
-    if (d.nbr[dir] >= 0) send_halo<T>(c, d, dir);
+    if (d.nbr[dir] < 0) continue;
+    jac::region e = jac::edge_region(dir, d.depth, d.w, d.h);
+    idx[n] = d.nbr[dir];
+    dirs[n] = dir;
+    refs[n] = japp::halo_mode() == 1 ? c.pass : -1;
+    bytes[n] = sizeof(jac::halo_hdr) + (size_t)e.nr * e.nc * sizeof(T);
+    n++;
   }
+  charm::message msg[jac::N_DIRS];
+  if (n > 0 && jproxy->alloc_msgs(msg, idx, bytes, n)) {
+    jac::block_view<T> g = view<T>(d, c.cur);
+    for (int k = 0; k < n; k++) {
+      jac::region e = jac::edge_region(dirs[k], d.depth, d.w, d.h);
+      char* pl = reinterpret_cast<char*>(msg[k].payload());
+      if (threadIdx.x == 0) {
+        jac::halo_hdr* hh = reinterpret_cast<jac::halo_hdr*>(pl);
+        hh->dir = jac::opposite(dirs[k]);
+        hh->len = e.nr * e.nc;
+        hh->pass = c.pass;
+        hh->iter = c.iter;
+      }
+      copy_region<T>(g, e, reinterpret_cast<T*>(pl + sizeof(jac::halo_hdr)), false);
+    }
+    jproxy->invoke_msgs(idx, EP_HALO, msg, bytes, refs, n);
+  }
+  if (threadIdx.x == 0) japp::pe_ns()[4 * blockIdx.x + 1] += charm::now_ns() - t0;
 }
 
 // Halo of pass hh->pass -> ghost zone of buf[pass & 1]. All threads.
@@ -181,14 +209,8 @@ template <typename T>
 __device__ void unpack_halo(JBlock& c, const jac::chare_desc& d, const void* arg) {
   const jac::halo_hdr* hh = reinterpret_cast<const jac::halo_hdr*>(arg);
   const T* vals = reinterpret_cast<const T*>(reinterpret_cast<const char*>(arg) + sizeof(jac::halo_hdr));
-  jac::block_view<T> g = view<T>(d, hh->pass & 1);
   jac::region gr = jac::ghost_region(hh->dir, d.depth, d.w, d.h);
-  int len = gr.nr * gr.nc;
-  if (gr.nr == 1) {
-    charm::copy_cooperative(g.at(gr.r0, gr.c0), vals, (size_t)len * sizeof(T), threadIdx.x, blockDim.x);
-  } else {
-    for (int i = threadIdx.x; i < len; i += blockDim.x) *g.at(gr.r0 + i / gr.nc, gr.c0 + i % gr.nc) = vals[i];
-  }
+  copy_region<T>(view<T>(d, hh->pass & 1), gr, const_cast<T*>(vals), true);
 }
 
 

@@ -191,6 +191,7 @@ __device__ void em_start_t(JBlock& c) {
 template <typename T>
 __device__ void em_halo_t(JBlock& c, void* arg) {
   if (c.done) return;
+  const unsigned long long t_em = charm::now_ns();
   const jac::chare_desc& d = japp::chares()[c.i];
   const jac::halo_hdr* hh = reinterpret_cast<const jac::halo_hdr*>(arg);
   // checked build: direction, length and sweep of the halo are consistent
@@ -208,6 +209,7 @@ __device__ void em_halo_t(JBlock& c, void* arg) {
     (void)CHARM_VERIFY(c.got[hh->pass & 1] <= jac::N_DIRS, CHARMING_ERR_APP, 4000 + c.got[hh->pass & 1], c.i);
   }
   __syncthreads();
+  if (threadIdx.x == 0) japp::pe_ns()[4 * blockIdx.x + 2] += charm::now_ns() - t_em;
   if (c.started) pump<T>(c, d);  // a halo may overtake the start message
 }
 

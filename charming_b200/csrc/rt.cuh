@@ -122,6 +122,10 @@ struct pe_state {
   unsigned long long stats[N_STATS];
   unsigned long long idle_polls_since_check;
   unsigned long long arena_top;        // bytes of this PE's arena handed out this run
+  // batched sends (alloc_user_msgs): per message start, ticket, bytes
+  void* bm_ptr[MSG_BATCH_MAX];
+  unsigned long long bm_tick[MSG_BATCH_MAX];
+  unsigned long long bm_bytes[MSG_BATCH_MAX];
   // followed by head_cache[n_pes] (unsigned long long), then scratch
 };
 

@@ -187,14 +187,14 @@ __device__ unsigned char* reserve(int dst, unsigned long long bytes, unsigned lo
   unsigned long long t = atomicAdd(&c_rt.tail[dst].v, (unsigned long long)cells);
   unsigned long long* hc = head_cache();
   if (t + cells - hc[dst] > C) {
-    ps->stats[ST_SPACE_WAITS]++;
+    atomicAdd_block(&ps->stats[ST_SPACE_WAITS], 1ULL);
     unsigned long long start = globaltimer();
     // A receiver that frees nothing for the idle timeout is taken as stuck.
     unsigned long long limit = c_rt.idle_timeout_ns ? c_rt.idle_timeout_ns : c_rt.deadline_ns;
     unsigned int spins = 0;
     while (true) {
       unsigned long long h = ld_acquire_u64(&c_rt.head[dst].v);
-      hc[dst] = h;
+      atomicMax(&hc[dst], h);  // monotonic; several threads may reserve at once
       if (t + cells - h <= C) break;
       if ((++spins & 255) == 0) {
         if (terminated()) return nullptr;
@@ -310,6 +310,58 @@ __device__ void charm::send_user_msg(int chare_id, int chare_idx, int ep_id,
   }
   __syncthreads();
   msg.env = nullptr;
+}
+
+__device__ bool charm::alloc_user_msgs(message* msgs, const int* dst_pes,
+    const size_t* payload_sizes, int n) {
+  pe_state* ps = pes();
+  if (n > MSG_BATCH_MAX) n = MSG_BATCH_MAX;
+  const int k = (int)threadIdx.x;
+  if (k < n) {  // one reservation per thread: the ring atomics overlap
+    unsigned long long bytes = envelope::alloc_size(msgtype::user, payload_sizes[k]);
+    unsigned long long t = 0;
+    ps->bm_ptr[k] = reserve(dst_pes[k], bytes, &t);
+    ps->bm_tick[k] = t;
+    ps->bm_bytes[k] = bytes;
+  }
+  __syncthreads();
+  bool ok = true;
+  for (int j = 0; j < n; j++) {
+    msgs[j].env = reinterpret_cast<envelope*>(ps->bm_ptr[j]);
+    msgs[j].offset = ps->bm_tick[j];
+    msgs[j].dst_pe = dst_pes[j];
+    msgs[j].cells = (int)cells_for(ps->bm_bytes[j]);
+    msgs[j].capacity = msgs[j].env ? (size_t)(ps->bm_bytes[j] - HDR) : 0;
+    ok = ok && msgs[j].env != nullptr;
+  }
+  __syncthreads();
+  return ok;
+}
+
+__device__ void charm::send_user_msgs(int chare_id, const int* chare_idx, int ep_id,
+    message* msgs, const size_t* payload_sizes, const int* refnums, int n) {
+  pe_state* ps = pes();
+  if (n > MSG_BATCH_MAX) n = MSG_BATCH_MAX;
+  __syncthreads();  // payload writes of all threads are done
+  const int k = (int)threadIdx.x;
+  if (k < n && msgs[k].env) {  // one message per thread: the publishing fences overlap
+    unsigned char* m = reinterpret_cast<unsigned char*>(msgs[k].env);
+    envelope* env = msgs[k].env;
+    env->type = msgtype::user;
+    env->src_pe = (int)blockIdx.x;
+    env->size = (size_t)msgs[k].capacity + HDR;
+    regular_msg* rm = reinterpret_cast<regular_msg*>(m + sizeof(envelope));
+    rm->chare_id = chare_id;
+    rm->chare_idx = chare_idx[k];
+    rm->ep_id = ep_id;
+    rm->refnum = refnums ? refnums[k] : -1;
+    if (payload_sizes[k] > msgs[k].capacity) set_error(CHARMING_ERR_MSG_TOO_LARGE, msgs[k].dst_pe, (int)payload_sizes[k]);
+    atomicAdd_block(&ps->stats[ST_SENT], 1ULL);
+    atomicAdd_block(&ps->stats[ST_BYTES_SENT], (unsigned long long)payload_sizes[k]);
+    publish(msgs[k].dst_pe, msgs[k].offset);
+  }
+  __syncthreads();
+  for (int j = 0; j < n; j++) msgs[j].env = nullptr;
 }
 
 __device__ void charm::revive_mismatches(int chare_id, int chare_idx, int refnum) {

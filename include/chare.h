@@ -303,6 +303,24 @@ struct chare_proxy : chare_proxy_base {
   }
   inline __device__ void free_msg(message& msg) {}
 
+  // Batched zero-copy messages to chares idx[0..n) (extension, see
+  // alloc_user_msgs in message.h). Block-collective.
+  inline __device__ bool alloc_msgs(message* msgs, const int* idx, const size_t* sizes, int n) {
+    int pe[MSG_BATCH_MAX];
+    for (int k = 0; k < n; k++) {
+      if (k >= MSG_BATCH_MAX || idx[k] < 0 || idx[k] >= n_total) {
+        if (threadIdx.x == 0) detail::report_error(detail::ERR_BAD_TARGET, id, k < MSG_BATCH_MAX ? idx[k] : k);
+        return false;
+      }
+      pe[k] = loc_map[idx[k]];
+    }
+    return alloc_user_msgs(msgs, pe, sizes, n);
+  }
+  inline __device__ void invoke_msgs(const int* idx, int ep, message* msgs, const size_t* sizes,
+      const int* refnums, int n) {
+    send_user_msgs(id, idx, ep, msgs, sizes, refnums, n);
+  }
+
   // Single-threaded (include/chare.h:243-253)
   inline __device__ void set_refnum(int idx, int val) {
     if (idx < start_idx || idx > end_idx) {

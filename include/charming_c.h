@@ -176,6 +176,8 @@ typedef struct charming_jacobi_info {
   double last_run_ms;         /* CUDA-event time of the last run           */
   double sweep_ms_max;        /* last run: max over PEs of time in sweeps  */
   double sweep_ms_mean;       /* last run: mean over busy PEs              */
+  double send_ms_mean;        /* last run: mean time packing/sending halos */
+  double halo_ms_mean;        /* last run: mean time in halo entry methods */
 } charming_jacobi_info;
 
 /* Decomposes the problems into chares (reference decomposition:

@@ -120,6 +120,18 @@ __device__ bool alloc_user_msg(message& msg, int dst_pe, size_t payload_size);
 __device__ void send_user_msg(int chare_id, int chare_idx, int ep_id,
     message& msg, size_t payload_size, int refnum);
 
+// Several zero-copy messages at once (an extension; the reference sends one
+// at a time): n <= MSG_BATCH_MAX messages to PEs dst_pes[k] with
+// payload_sizes[k] bytes are reserved by n threads in parallel, and later
+// published in parallel, so their ring reservations and publishing fences
+// overlap. Block-collective; every thread passes the same arrays. Returns
+// false when a reservation failed (error recorded).
+constexpr int MSG_BATCH_MAX = 8;
+__device__ bool alloc_user_msgs(message* msgs, const int* dst_pes, const size_t* payload_sizes,
+    int n);
+__device__ void send_user_msgs(int chare_id, const int* chare_idx, int ep_id, message* msgs,
+    const size_t* payload_sizes, const int* refnums, int n);
+
 // Single-threaded (called under threadIdx.x == 0 by set_refnum). Marks the
 // PE's stash for re-examination; stashed messages whose refnum now matches
 // their chare are delivered, in arrival order, before new inbox messages

@@ -389,6 +389,15 @@ void send_user_msg(int chare_id, int chare_idx, int ep, message& msg, size_t siz
   emu_sync(__FILE__, __LINE__);
   msg.env = nullptr;
 }
+bool alloc_user_msgs(message* msgs, const int* dst_pes, const size_t* sizes, int n) {
+  bool ok = true;
+  for (int k = 0; k < n; k++) ok = alloc_user_msg(msgs[k], dst_pes[k], sizes[k]) && ok;
+  return ok;
+}
+void send_user_msgs(int chare_id, const int* chare_idx, int ep, message* msgs, const size_t* sizes,
+    const int* refnums, int n) {
+  for (int k = 0; k < n; k++) send_user_msg(chare_id, chare_idx[k], ep, msgs[k], sizes[k], refnums ? refnums[k] : -1);
+}
 void revive_mismatches(int, int, int) { me_pe().revive = 1; }
 void send_begin_term_msg() { end(); }
 }  // namespace charm
@@ -562,7 +571,7 @@ int run(int nx, int ny, int px, int py, int max_sweeps, int K, double tol, int n
   jac::prob_result res{};
   unsigned long long done = 0;
   std::vector<int> final_buf(nc, 0);
-  std::vector<unsigned long long> sweep_ns(n_pes, 0);
+  std::vector<unsigned long long> sweep_ns(4 * (size_t)n_pes, 0);
   g_app = suite::app_params{};
   g_app.id = suite::APP_JACOBI2D;
   g_app.a[0] = nc;
