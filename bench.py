@@ -2,9 +2,25 @@
 """Benchmark: Jacobi2d chares on one B200 (replicas on N GPUs).
 
 Headline workload: jacobi2d 8192 x 8192 FP64, one chare per PE (148 on a
-B200), halos exchanged as runtime messages every sweep, 100 sweeps per step
-(the reference's default iteration count, examples/jacobi2d/jacobi2d.cu:12).
+B200), halos exchanged as runtime messages, 100 sweeps per step (the
+reference's default iteration count, examples/jacobi2d/jacobi2d.cu:12).
 Metric: GLUP/s = interior points x sweeps / time.
+
+The same JSON line carries the other workloads of the metric (skipped with
+--headline-only):
+  messaging  pingpong 8 B..1 MiB (10,000 round trips per size, payloads
+             checksummed on the device) and fan-out 4096 chares x 16 x 64 B
+             with refnums 0..15 (msgs/s)
+  batched    64 uneven FP64 problems (sides log-uniform in [64, 2048]),
+             500 sweeps, one launch replayed from a CUDA graph, launch
+             configuration picked by the autotuner
+  precision  the batched set plus one 8192^2 problem in FP32 with the FP64
+             residual every 10 sweeps, stop at 1e-5 or 5000 sweeps; GLUP/s
+             against the plain FP64 headline and the max-abs error against
+             the FP64 grids after the same sweep counts
+  serving    Poisson arrivals at 200 req/s of FP32 solves (sides log-uniform
+             in [128, 4096], tol 1e-5, cap 5000 sweeps) into one running
+             scheduler under a 120 GB HBM budget; p50/p99 latency, solves/s
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -213,6 +229,163 @@ def run_reference_arm(args, rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def messaging_suite(seed: int = 0xC2) -> dict:
+    """C2a pingpong and C2b fan-out on the default runtime."""
+    from charming_b200.runtime import Runtime
+    rt = Runtime()
+    sizes = [1 << k for k in range(3, 21)]
+    rows, sm = rt.pingpong(sizes, 10000, warmup=200, seed=seed, verify=True)
+    st = rt.last_stats()
+    log, ms = rt.fanout(4096, 16, 64, seed, 1)
+    fst = rt.last_stats()
+    n = 4096 * 16
+    return {
+        "pingpong": {"sm_pair": list(sm), "round_trips": 10000,
+                     "oneway_ns": {str(r["size"]): round(r["oneway_us"] * 1e3, 1) for r in rows},
+                     "oneway_cycles": {str(r["size"]): round(r["oneway_cycles"], 1) for r in rows},
+                     "checksum_errors": int(sum(r["checksum_errors"] for r in rows)),
+                     "status": st.status},
+        "fanout": {"chares": 4096, "msgs_per_chare": 16, "payload_bytes": 64, "refnums": "0..15",
+                   "ms": ms, "msgs_per_s": n / (ms * 1e-3), "delivered": int(len(log)),
+                   "stashed": fst.stashed, "status": fst.status,
+                   "checked": "counts, per-pair FIFO and checksums against the CPU model in tests"},
+    }
+
+
+def batched_suite(steps: int = 3, warmup: int = 3) -> dict:
+    """C3: the 64-problem uneven FP64 set, 500 sweeps, CUDA graph, autotuned."""
+    from charming_b200.batch import autotune, uneven_set
+    from charming_b200.jacobi import Jacobi2D
+    probs = uneven_set(max_sweeps=500)
+    tune = autotune(probs, "f64")
+    best = tune.best
+    points = sum(p.nx * p.ny for p in probs)
+    with Jacobi2D(probs, dtype="f64", chare_side=best.chare_side, use_graph=True) as j:
+        for _ in range(warmup):
+            j.run()
+        ts = [j.run() for _ in range(steps)]
+        info = j.info()
+    ms = statistics.mean(ts)
+    return {"workload": "64 square FP64 problems, sides log-uniform in [64, 2048] (seed 0xC3), "
+                        "500 sweeps, one launch from a CUDA graph",
+            "glups": points * 500 / (ms * 1e-3) / 1e9, "ms_per_launch": ms, "launches": steps,
+            "points": points, "chares": info["n_chares"], "autotune": tune.as_dict()}
+
+
+def precision_suite(plain_fp64_glups: float, steps: int = 2, warmup: int = 1) -> dict:
+    """C4: the batched set plus 8192^2 in FP32 sweeps with the FP64 residual
+    (every 10 sweeps, stop at 1e-5 or 5000 sweeps); max-abs error against
+    FP64 grids after the same sweep counts (the FP64 path equals the serial
+    oracle bit for bit)."""
+    from charming_b200.batch import _uniform, autotune, default_candidates, uneven_set
+    from charming_b200.jacobi import Jacobi2D, Problem
+    bc = tuple(_uniform(0xC4, k) for k in range(4))
+    probs = uneven_set(max_sweeps=5000, check_every=10, tol=1e-5)
+    probs.append(Problem(8192, 8192, 5000, check_every=10, tol=1e-5, bc=bc))
+    proxy = [Problem(p.nx, p.ny, 100, check_every=10, tol=0.0, bc=p.bc) for p in probs]
+    cands = [c for c in default_candidates() if c.chare_side >= 128 and c.ring_bytes == (4 << 20)]
+    tune = autotune(proxy, "f32", candidates=cands)
+    side = tune.best.chare_side
+    with Jacobi2D(probs, dtype="f32", chare_side=side, use_graph=True) as j:
+        for _ in range(warmup):
+            j.run()
+        ts = [j.run() for _ in range(steps)]
+        res = [j.result(i) for i in range(len(probs))]
+        g32 = [j.store(i) for i in range(len(probs))]
+    ms = statistics.mean(ts)
+    lups = sum(p.nx * p.ny * r.sweeps for p, r in zip(probs, res))
+    ref = [Problem(p.nx, p.ny, r.sweeps, bc=p.bc) for p, r in zip(probs, res)]
+    err = 0.0
+    with Jacobi2D(ref, dtype="f64", chare_side=side) as j64:
+        j64.run()
+        for i in range(len(ref)):
+            g64 = j64.store(i)
+            err = max(err, float(np.max(np.abs(g32[i].astype(np.float64) - g64))))
+    glups = lups / (ms * 1e-3) / 1e9
+    sw = [r.sweeps for r in res]
+    return {"workload": "the batched set with 5000-sweep caps plus one 8192^2 problem, FP32 "
+                        "sweeps and storage, FP64 residual every 10 sweeps, tol 1e-5",
+            "glups": glups, "ms_per_launch": ms, "launches": steps,
+            "vs_plain_fp64": glups / plain_fp64_glups if plain_fp64_glups else None,
+            "target_vs_plain_fp64": 1.8, "max_abs_err_vs_fp64": err, "target_max_abs_err": 1e-5,
+            "sweeps_min": min(sw), "sweeps_max": max(sw),
+            "stopped_by_tol": sum(1 for p, r in zip(probs, res) if r.sweeps < p.max_sweeps),
+            "res_rel_8192": res[-1].res_last / res[-1].res0 if res[-1].res0 else None,
+            "reference": "FP64 grids from the FP64 path (bit-identical to the serial oracle) "
+                         "after each problem's FP32 sweep count",
+            "autotune": tune.as_dict()}
+
+
+def serving_suite(n_req: int, rate: float = 200.0, seed: int = 0xC5) -> dict:
+    """C5: Poisson arrivals of FP32 solves into one running scheduler."""
+    import torch
+    from charming_b200.batch import _uniform
+    from charming_b200.jacobi import Problem
+    from charming_b200.runtime import Runtime
+    from charming_b200.serve import Server
+    Runtime()
+    rng = np.random.default_rng(seed)
+    sides = np.exp(rng.uniform(np.log(128), np.log(4096), n_req)).round().astype(int)
+    gaps = rng.exponential(1.0 / rate, n_req)
+    arrive = np.cumsum(gaps) - gaps[0]
+    probs = [Problem(int(s), int(s), 5000, check_every=10, tol=1e-5,
+                     bc=tuple(float(v) for v in rng.uniform(0, 1, 4))) for s in sides]
+    out = torch.empty((4098 * 4098,), dtype=torch.float32, pin_memory=True).numpy()
+    budget = 120 * 10**9
+    lat, service, lups_done = [], [], 0
+    with Server(budget, max_inflight=64, workers_per_pe=16, chare_side=256, dtype="f32",
+                deadline_s=600) as srv:
+        t0 = time.monotonic()
+        nxt = 0
+        done = 0
+        while done < n_req:
+            now = time.monotonic() - t0
+            while nxt < n_req and arrive[nxt] <= now:
+                srv.submit(probs[nxt], nxt)
+                nxt += 1
+            for c in srv.poll():
+                p = probs[c.tag]
+                srv.fetch(c.tag, out[: (p.ny + 2) * (p.nx + 2)].reshape(p.ny + 2, p.nx + 2))
+                srv.release(c.tag)
+                lat.append(c.done_s - c.submit_s)
+                service.append(c.done_s - c.admit_s)
+                lups_done += p.nx * p.ny * c.sweeps
+                done += 1
+            if time.monotonic() - t0 > 900:
+                break
+            time.sleep(0.0001)
+        wall = time.monotonic() - t0
+        stats = srv.stop()
+    offered = sum(p.nx * p.ny * p.max_sweeps for p in probs) / max(arrive[-1], 1e-9)
+    return {"workload": f"{n_req} FP32 solve requests, Poisson {rate:.0f} req/s, sides log-uniform "
+                        "in [128, 4096], tol 1e-5 with the FP64 residual every 10 sweeps, cap 5000 "
+                        "sweeps, 120 GB HBM budget, each result fetched to the host",
+            "requests": n_req, "completed": done, "wall_s": wall,
+            "solves_per_s": done / wall, "p50_ms": float(np.percentile(lat, 50)) * 1e3,
+            "p99_ms": float(np.percentile(lat, 99)) * 1e3,
+            "service_p50_ms": float(np.percentile(service, 50)) * 1e3,
+            "service_p99_ms": float(np.percentile(service, 99)) * 1e3,
+            "offered_glups": offered / 1e9, "served_glups": lups_done / wall / 1e9,
+            "peak_inflight": stats.get("peak_inflight"), "peak_bytes": stats.get("peak_bytes")}
+
+
+def run_suites(args, headline_glups: float) -> dict:
+    out = {}
+    for name, fn in (("messaging", lambda: messaging_suite()),
+                     ("batched", lambda: batched_suite()),
+                     ("precision", lambda: precision_suite(headline_glups)),
+                     ("serving", lambda: serving_suite(args.serve_requests))):
+        if name in args.skip:
+            continue
+        t0 = time.perf_counter()
+        try:
+            out[name] = fn()
+        except Exception as e:  # report, keep the line
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        out[name]["suite_s"] = round(time.perf_counter() - t0, 1)
+    return out
+
+
 def exchange_depth(args) -> int:
     """Sweeps per halo exchange the run uses (the library's choice for 0)."""
     if args.pipeline:
@@ -248,6 +421,11 @@ def main() -> int:
                     help="sweeps per halo exchange (ghost depth), 0: 4 (direct) / 1 (TMA)")
     ap.add_argument("--small-buffers", action="store_true",
                     help="1 MiB inbox rings and stashes (smaller device footprint for ncu)")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="skip the messaging, batched, precision and serving workloads")
+    ap.add_argument("--skip", default="", help="comma-separated workloads to skip")
+    ap.add_argument("--serve-requests", type=int, default=2000,
+                    help="requests of the serving workload (the full stream is 20000)")
     args = ap.parse_args()
     set_workload(args.nx, args.sweeps)
 
@@ -334,9 +512,14 @@ def main() -> int:
         roof["effective"] = (f"achieved counts 16 B per lattice update per sweep; a pass of {dep} "
                              "sweeps reads and writes each block once, so DRAM moves about "
                              f"1/{dep} of that and frac can exceed 1 (effective bandwidth)")
+    j.close()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline()
+    suites = {}
+    if rank == 0 and world == 1 and not args.headline_only:
+        args.skip = [x for x in args.skip.split(",") if x]
+        suites = run_suites(args, value)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -355,8 +538,8 @@ def main() -> int:
             "runtime": {k: rt.info[k] for k in ("n_pes", "threads_per_pe", "smem_bytes_per_pe",
                                                 "smem_scratch_bytes", "regs_per_thread")},
         }
+        line.update(suites)
         print(json.dumps(line), flush=True)
-    j.close()
     if dist is not None:
         dist.destroy_process_group()
     return 0

@@ -15,6 +15,15 @@
 // the norm is bit-reproducible) and the stop decision comes back down. The
 // decision for the check taken at sweep cK is applied at sweep (c+1)K, which
 // leaves K sweeps for the round trip.
+//
+// Serving (g_app.a[6] != 0): the same chares form a pool of reusable
+// workers, created once for a long-lived scheduler run; a server chare on
+// PE 0 polls a request ring in mapped host memory and starts each admitted
+// request at its root worker (the start travels down the residual tree).
+// Every message carries the request's generation; the first one of a new
+// generation resets the worker, copies its descriptor from the host's
+// staging table and initialises its grids. The request's last chare to
+// finish writes a completion record into mapped host memory.
 #include "suite.cuh"
 #include "jacobi_types.cuh"
 #include "jacobi_sweep.cuh"
@@ -22,6 +31,7 @@
 namespace {
 
 enum : int { EP_START = 0, EP_HALO = 1, EP_CONT = 2, EP_PARTIAL = 3, EP_DECISION = 4 };
+enum : int { EP_POLL = 0 };  // server chare
 
 // g_app fields of this program.
 struct japp {
@@ -49,6 +59,25 @@ struct japp {
   __device__ static unsigned long long* pe_ns() {
     return reinterpret_cast<unsigned long long*>(g_app.p[6]);
   }
+  // serving
+  __device__ static bool serving() { return g_app.a[6] != 0; }
+  __device__ static int serve_q() { return (int)g_app.a[7]; }   // request ring entries
+  __device__ static int serve_cq() { return (int)g_app.a[8]; }  // completion ring entries
+  __device__ static jac::chare_desc* chares_rw() { return reinterpret_cast<jac::chare_desc*>(g_app.p[0]); }
+  __device__ static jac::prob_desc* probs_rw() { return reinterpret_cast<jac::prob_desc*>(g_app.p[1]); }
+  __device__ static jac::serve_req* serve_reqs() { return reinterpret_cast<jac::serve_req*>(g_app.p[7]); }
+  __device__ static const jac::chare_desc* stage_descs() {
+    return reinterpret_cast<const jac::chare_desc*>(g_app.p[8]);
+  }
+  __device__ static const jac::prob_desc* stage_probs() {
+    return reinterpret_cast<const jac::prob_desc*>(g_app.p[9]);
+  }
+  __device__ static jac::serve_comp* serve_comps() { return reinterpret_cast<jac::serve_comp*>(g_app.p[10]); }
+  // [0] requests started and not completed, [1] completion tickets
+  __device__ static unsigned long long* serve_ctr() { return reinterpret_cast<unsigned long long*>(g_app.p[11]); }
+  __device__ static unsigned int* serve_done() { return reinterpret_cast<unsigned int*>(g_app.p[12]); }
+  __device__ static const int* serve_ctl() { return reinterpret_cast<const int*>(g_app.p[13]); }  // [0] stop
+  __device__ static const int* server_map() { return reinterpret_cast<const int*>(g_app.p[14]); }
 };
 
 struct JBlock : charm::chare {
@@ -70,16 +99,31 @@ struct JBlock : charm::chare {
   int stop_check;    // check whose decision was "stop" (-1: none)
   double res0, res_last;
   int checks;
-  __device__ JBlock()
-      : iter(0), pass(0), cur(0), sent(-1), started(0), nbr_count(0), done(0), waiting(0), have_own(0), own(0.0),
-        decided(-1), stop_check(-1), res0(0.0), res_last(0.0), checks(0) {
+  unsigned gen;      // request generation (serving; 0 otherwise)
+  __device__ JBlock() { reset(0); }
+  __device__ void reset(unsigned g) {
+    iter = pass = cur = 0;
+    sent = -1;
+    started = nbr_count = done = waiting = have_own = 0;
+    own = 0.0;
+    decided = stop_check = -1;
+    res0 = res_last = 0.0;
+    checks = 0;
+    gen = g;
     got[0] = got[1] = 0;
     child_got[0] = child_got[1] = 0;
     child_val[0] = child_val[1] = 0.0;
   }
 };
 
+// The server chare of a serving run (one, on PE 0): next request ticket.
+struct JServer : charm::chare {
+  unsigned long long next;
+  __device__ JServer() : next(0) {}
+};
+
 __shared__ charm::chare_proxy<JBlock>* jproxy;
+__shared__ charm::chare_proxy<JServer>* sproxy;
 
 template <typename T>
 __device__ jac::block_view<T> view(const jac::chare_desc& d, int b) {
@@ -195,7 +239,7 @@ __device__ void send_halos(JBlock& c, const jac::chare_desc& d) {
         hh->dir = jac::opposite(dirs[k]);
         hh->len = e.nr * e.nc;
         hh->pass = c.pass;
-        hh->iter = c.iter;
+        hh->gen = c.gen;
       }
       copy_region<T>(g, e, reinterpret_cast<T*>(pl + sizeof(jac::halo_hdr)), false);
     }
@@ -214,11 +258,41 @@ __device__ void unpack_halo(JBlock& c, const jac::chare_desc& d, const void* arg
 }
 
 
+// Serving, thread 0 of the request's last chare: completion record into the
+// mapped host ring (fields first, then seq with a system-scope release).
+// The ring has as many entries as request slots and the host frees a slot
+// only after reading its record, so an entry is never overwritten unread.
+__device__ void serve_complete(const JBlock& c, const jac::chare_desc& d) {
+  using namespace charm::rt;
+  unsigned long long t = atomicAdd(&japp::serve_ctr()[1], 1ULL);
+  jac::serve_comp* r = japp::serve_comps() + t % (unsigned long long)japp::serve_cq();
+  r->slot = d.slot;
+  r->gen = c.gen;
+  r->sweeps = c.iter;
+  r->checks = c.checks;
+  r->final_buf = c.cur;
+  r->status = 0;
+  r->res0 = c.res0;
+  r->res_last = c.res_last;
+  r->t_ns = globaltimer();
+  __threadfence_system();
+  st_release_sys_u64(&r->seq, t + 1);
+  atomicAdd(&japp::serve_ctr()[0], ~0ULL);  // one request fewer in flight
+}
+
 // All threads. Marks the chare done; the last chare of all problems ends the
 // run (the reference counts "end" messages at chare 0, jacobi2d.cu:274-279).
+// Serving: the last chare of the request reports its completion instead.
 __device__ void finish(JBlock& c, const jac::chare_desc& d) {
   __shared__ int s_last;
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0 && japp::serving()) {
+    c.done = 1;
+    const jac::prob_desc& p = japp::probs()[d.prob];
+    __threadfence();
+    unsigned n = atomicAdd(&japp::serve_done()[d.slot], 1u) + 1;
+    if (n == (unsigned)p.n_chares) serve_complete(c, d);
+    s_last = 0;
+  } else if (threadIdx.x == 0) {
     c.done = 1;
     japp::final_buf()[c.i] = c.cur;
     const jac::prob_desc& p = japp::probs()[d.prob];
@@ -237,10 +311,129 @@ __device__ void finish(JBlock& c, const jac::chare_desc& d) {
   if (s_last) charm::end();
 }
 
+// Serving, all threads: the first message of a new request generation
+// resets the worker, copies its descriptor and its request's problem
+// descriptor from the host's staging tables (mapped host memory, read at
+// system scope) into the worker's own entries, and writes both grids: the
+// boundary ring where the block touches it, 0 everywhere else (ghost cells
+// beyond the ring included, so nothing of a previous request survives).
+// Generations grow with every admission. Returns 0 for a message of an
+// older generation, which the caller drops: with residual checks none can
+// arrive (a chare finishes only after the last decision of its tree, so
+// nothing of a completed request is in flight), without them a start that
+// went down the tree after its chare had finished can.
+template <typename T>
+__device__ int ensure_gen(JBlock& c, unsigned gen) {
+  using namespace charm::rt;
+  if (!japp::serving()) return 1;
+  __shared__ int s_new;
+  if (threadIdx.x == 0) s_new = gen > c.gen ? 1 : gen == c.gen ? 0 : -1;
+  __syncthreads();
+  const int fresh = s_new;
+  __syncthreads();
+  if (fresh <= 0) return fresh + 1;
+  static_assert(sizeof(jac::chare_desc) % 8 == 0 && sizeof(jac::prob_desc) % 8 == 0, "word copies");
+  constexpr int WD = sizeof(jac::chare_desc) / 8, WP = sizeof(jac::prob_desc) / 8;
+  {
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(japp::stage_descs() + c.i);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(japp::chares_rw() + c.i);
+    for (int k = threadIdx.x; k < WD; k += blockDim.x) dst[k] = ld_relaxed_sys_u64(src + k);
+  }
+  __syncthreads();
+  const jac::chare_desc& d = japp::chares()[c.i];
+  {
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(japp::stage_probs() + d.slot);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(japp::probs_rw() + d.prob);
+    for (int k = threadIdx.x; k < WP; k += blockDim.x) dst[k] = ld_relaxed_sys_u64(src + k);
+  }
+  __syncthreads();
+  const jac::prob_desc& p = japp::probs()[d.prob];
+  if (CHARM_VERIFY(d.w > 0 && d.h > 0 && d.depth >= 1 && d.depth <= jac::DEPTH_MAX && d.prob == c.i,
+                   CHARMING_ERR_APP, 9000 + d.depth, c.i)) {
+    const int D = d.depth, rows = d.h + 2 * D;
+    const long long n = (long long)rows * d.pitch;
+    for (int b = 0; b < 2; b++) {
+      T* base = reinterpret_cast<T*>(d.buf[b]) + (long long)(1 - D) * d.pitch;
+      for (long long x = threadIdx.x; x < n; x += blockDim.x) {
+        const int r = (int)(x / d.pitch) + 1 - D, col = (int)(x % d.pitch) - jac::traits<T>::OFF + 1;
+        const int gy = d.y0 + r, gx = d.x0 + col;
+        double v = 0.0;
+        if (gy >= 0 && gy <= p.ny + 1 && gx >= 0 && gx <= p.nx + 1) {
+          if (gy == 0) v = p.bc[0];
+          else if (gy == p.ny + 1) v = p.bc[1];
+          else if (gx == 0) v = p.bc[2];
+          else if (gx == p.nx + 1) v = p.bc[3];
+        }
+        base[x] = (T)v;
+      }
+    }
+  }
+  if (threadIdx.x == 0) {
+    c.reset(gen);
+    int nb = 0;
+    for (int k = 0; k < jac::N_DIRS; k++) nb += d.nbr[k] >= 0;
+    c.nbr_count = nb;
+    c.started = 1;
+  }
+  __syncthreads();
+  return 1;
+}
+
 #include "jacobi_chare.cuh"
 
+// Serving, server chare: takes up to 4 posted requests from the mapped ring
+// per call, starts each at its root worker, and calls itself again; ends the
+// run when the host asked to stop and no request is in flight. All threads.
+__device__ void em_poll(JServer& s, void* arg) {
+  using namespace charm::rt;
+  constexpr int MAXN = 4;
+  __shared__ int s_n, s_stop;
+  __shared__ jac::start_msg s_m[MAXN];
+  __shared__ int s_root[MAXN];
+  if (threadIdx.x == 0) {
+    int n = 0;
+    while (n < MAXN) {
+      jac::serve_req* q = japp::serve_reqs() + s.next % (unsigned long long)japp::serve_q();
+      if (ld_acquire_sys_u64(&q->seq) != s.next + 1) break;
+      unsigned long long w1 = ld_relaxed_sys_u64(reinterpret_cast<const unsigned long long*>(q) + 1);
+      unsigned long long w2 = ld_relaxed_sys_u64(reinterpret_cast<const unsigned long long*>(q) + 2);
+      s_m[n].slot = (int)(unsigned)(w1 & 0xffffffffu);
+      s_root[n] = (int)(unsigned)(w1 >> 32);
+      s_m[n].gen = (unsigned)(w2 & 0xffffffffu);
+      atomicExch(&japp::serve_done()[s_m[n].slot], 0u);
+      atomicAdd(&japp::serve_ctr()[0], 1ULL);
+      s.next++;
+      n++;
+    }
+    __threadfence();
+    s_n = n;
+    // 1: the host asked to stop and nothing is in flight; 2: the run is
+    // ending anyway (an error elsewhere, or past its deadline)
+    s_stop = n == 0 && ld_sys_s32(japp::serve_ctl()) != 0 &&
+             ld_relaxed_u64(&japp::serve_ctr()[0]) == 0;
+    if (terminated()) {
+      s_stop = 2;
+    } else if (past_deadline()) {
+      set_error(CHARMING_ERR_DEADLINE, 2, 0);
+      s_stop = 2;
+    }
+  }
+  __syncthreads();
+  const int n = s_n, stop = s_stop;
+  for (int k = 0; k < n; k++) {
+    jac::start_msg m = s_m[k];
+    jproxy->invoke(s_root[k], EP_START, &m, sizeof(m));
+  }
+  __syncthreads();
+  if (stop) {
+    if (stop == 1) charm::end();
+    return;
+  }
+  sproxy->invoke(0, EP_POLL);
+}
+
 __device__ void em_start(JBlock& c, void* arg) {
-  if (japp::dtype() == CHARMING_F32) em_start_t<float>(c); else em_start_t<double>(c);
+  if (japp::dtype() == CHARMING_F32) em_start_t<float>(c, arg); else em_start_t<double>(c, arg);
 }
 __device__ void em_halo(JBlock& c, void* arg) {
   if (japp::dtype() == CHARMING_F32) em_halo_t<float>(c, arg); else em_halo_t<double>(c, arg);
@@ -266,9 +459,16 @@ __device__ void suite::jacobi2d_main(int pe) {
     jproxy->add_entry_method<&em_partial>();
     jproxy->add_entry_method<&em_decision>();
     jproxy->create(japp::n_chares(), const_cast<int*>(japp::block_map()));
+    if (japp::serving()) {
+      sproxy = new charm::chare_proxy<JServer>();
+      sproxy->add_entry_method<&em_poll>();
+      sproxy->create(1, const_cast<int*>(japp::server_map()));
+    }
   }
   __syncthreads();
-  if (jproxy->n_local > 0) {
+  if (japp::serving()) {
+    if (pe == 0) sproxy->invoke(0, EP_POLL);
+  } else if (jproxy->n_local > 0) {
     for (int i = jproxy->start_idx; i <= jproxy->end_idx; i++) jproxy->invoke(i, EP_START);
   }
 }

@@ -65,12 +65,16 @@ __device__ int tree_try_forward(JBlock& c, const jac::chare_desc& d, int chk) {
       if (d.parent >= 0) {
         s_pm.check = chk;
         s_pm.slot = (d.rank - 1) % 2;
+        s_pm.gen = c.gen;
+        s_pm.pad = 0;
         s_pm.value = t;
         s_act = 1;
       } else {
         const jac::prob_desc& p = japp::probs()[d.prob];
         double nrm = sqrt(t);
         s_dm.check = chk;
+        s_dm.gen = c.gen;
+        s_dm.pad = 0;
         s_dm.res0 = (chk == 0) ? nrm : c.res0;
         s_dm.res = nrm;
         s_dm.stop = (p.tol > 0.0) && (s_dm.res0 == 0.0 || nrm <= p.tol * s_dm.res0) ? 1 : 0;
@@ -136,7 +140,15 @@ __device__ void pump(JBlock& c, const jac::chare_desc& d) {
         act = IDLE;
       } else if (c.sent < c.pass) {
         if (c.iter >= p.max_sweeps) {
-          act = FIN;
+          // finish only after the decision of the last residual check: the
+          // result reports that check's norm, and no message of the problem
+          // is left in flight (a serving worker can take the next request)
+          if (K > 0 && p.max_sweeps > 0 && c.decided < (p.max_sweeps - 1) / K) {
+            c.waiting = 1;
+            act = IDLE;
+          } else {
+            act = FIN;
+          }
         } else if (K > 0 && c.iter >= K && c.iter % K == 0 && c.decided < c.iter / K - 1) {
           c.waiting = 1;
           act = IDLE;
@@ -176,7 +188,19 @@ __device__ void pump(JBlock& c, const jac::chare_desc& d) {
 }
 
 template <typename T>
-__device__ void em_start_t(JBlock& c) {
+__device__ void em_start_t(JBlock& c, void* arg) {
+  if (japp::serving()) {
+    // the start of a request travels down the residual tree
+    const jac::start_msg m = *reinterpret_cast<const jac::start_msg*>(arg);
+    if (!ensure_gen<T>(c, m.gen)) return;
+    const jac::chare_desc& d = japp::chares()[c.i];
+    for (int k = 0; k < 2; k++) {
+      jac::start_msg f = m;
+      if (d.child[k] >= 0) jproxy->invoke(d.child[k], EP_START, &f, sizeof(f));
+    }
+    pump<T>(c, d);
+    return;
+  }
   const jac::chare_desc& d = japp::chares()[c.i];
   if (threadIdx.x == 0) {
     int n = 0;
@@ -190,10 +214,11 @@ __device__ void em_start_t(JBlock& c) {
 
 template <typename T>
 __device__ void em_halo_t(JBlock& c, void* arg) {
+  const jac::halo_hdr* hh = reinterpret_cast<const jac::halo_hdr*>(arg);
+  if (!ensure_gen<T>(c, hh->gen)) return;
   if (c.done) return;
   const unsigned long long t_em = charm::now_ns();
   const jac::chare_desc& d = japp::chares()[c.i];
-  const jac::halo_hdr* hh = reinterpret_cast<const jac::halo_hdr*>(arg);
   // checked build: direction, length and sweep of the halo are consistent
   if (!CHARM_VERIFY(hh->dir >= 0 && hh->dir < jac::N_DIRS && d.nbr[hh->dir] >= 0, CHARMING_ERR_APP,
                     1000 + hh->dir, c.i) ||
@@ -223,9 +248,10 @@ __device__ void em_cont_t(JBlock& c) {
 
 template <typename T>
 __device__ void em_partial_t(JBlock& c, void* arg) {
+  const jac::partial_msg* pm = reinterpret_cast<const jac::partial_msg*>(arg);
+  if (!ensure_gen<T>(c, pm->gen)) return;
   if (c.done) return;
   const jac::chare_desc& d = japp::chares()[c.i];
-  const jac::partial_msg* pm = reinterpret_cast<const jac::partial_msg*>(arg);
   int chk = pm->check;
   // Thread 0 checks and records the partial; the others learn the outcome
   // after the barrier (reading child_got themselves would race with it).
@@ -249,9 +275,10 @@ __device__ void em_partial_t(JBlock& c, void* arg) {
 
 template <typename T>
 __device__ void em_decision_t(JBlock& c, void* arg) {
+  jac::decision_msg m = *reinterpret_cast<const jac::decision_msg*>(arg);
+  if (!ensure_gen<T>(c, m.gen)) return;
   if (c.done) return;
   const jac::chare_desc& d = japp::chares()[c.i];
-  jac::decision_msg m = *reinterpret_cast<const jac::decision_msg*>(arg);
   __syncthreads();
   if (apply_decision<T>(c, d, m)) pump<T>(c, d);
 }

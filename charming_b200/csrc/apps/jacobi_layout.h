@@ -90,6 +90,7 @@ inline bool build_layout(const charming_jacobi_problem* probs, int n, int side, 
       for (int cx = 0; cx < px; cx++) {
         chare_desc d{};
         d.prob = p;
+        d.slot = p;
         d.cx = cx;
         d.cy = cy;
         d.x0 = split_start(q.nx, px, cx);
@@ -127,6 +128,7 @@ inline bool build_layout(const charming_jacobi_problem* probs, int n, int side, 
     pd.tol = q.tol;
     pd.n_chares = nc;
     pd.depth = D;
+    for (int k = 0; k < 4; k++) pd.bc[k] = q.bc[k];
     L->points += (uint64_t)q.nx * q.ny;
   }
   const int nch = (int)raw.size();

@@ -47,7 +47,8 @@ __host__ __device__ inline region edge_region(int d, int D, int w, int h) {
 
 // One chare block of one problem (host-built, read-only on the device).
 struct chare_desc {
-  int prob;            // problem index
+  int prob;            // problem index (serving: the worker's own prob_desc copy)
+  int slot;            // problem index (serving: the request's device slot)
   int cx, cy;          // chare column / row within the problem
   int x0, y0;          // first interior column / row of the block (0-based)
   int w, h;            // interior columns / rows of the block
@@ -69,6 +70,7 @@ struct prob_desc {
   int root;            // global chare index of the problem's tree root
   int n_chares;
   int depth;           // ghost depth of the problem's chares
+  double bc[4];        // boundary values: top, bottom, left, right
 };
 
 struct prob_result {
@@ -83,20 +85,53 @@ struct halo_hdr {
   int dir;             // ghost side at the receiver
   int len;             // values (the ghost region, row-major)
   int pass;            // exchange the values belong to (the sender's pass count)
-  int iter;            // sweep count of the values
+  unsigned gen;        // request generation (serving; 0 otherwise)
 };
 
 struct partial_msg {
   int check;
   int slot;            // 0 or 1: which child of the receiver sent it
+  unsigned gen;
+  int pad;
   double value;
 };
 
 struct decision_msg {
   int check;
   int stop;
+  unsigned gen;
+  int pad;
   double res0;
   double res;
+};
+
+struct start_msg {
+  unsigned gen;        // request generation (serving; 0 otherwise)
+  int slot;
+};
+
+// Serving: one admitted request, posted by the host into a ring in mapped
+// host memory that the server chare polls. seq = ticket + 1, written last.
+struct serve_req {
+  unsigned long long seq;
+  int slot;            // device problem slot (prob_desc table index)
+  int root;            // worker that holds the request's chare 0
+  unsigned gen;
+  int pad[3];
+};
+
+// Serving: completion record written by the request's last chare into a
+// ring in mapped host memory. seq = ticket + 1, written last.
+struct serve_comp {
+  unsigned long long seq;
+  int slot;
+  unsigned gen;
+  int sweeps;
+  int checks;
+  int final_buf;       // buffer (0/1) of every chare holding the result
+  int status;
+  double res0, res_last;
+  unsigned long long t_ns;   // %globaltimer at completion
 };
 
 // Even split of n cells into k parts: part i starts at split_start(n, k, i).

@@ -82,6 +82,12 @@ int ensure_init() {
   return charming_init(&cfg);
 }
 
+int set_deadline(double seconds) {
+  if (!g.inited) return CHARMING_ERR_NOT_INIT;
+  g.ds.deadline_ns = (unsigned long long)((seconds > 0 ? seconds : g.cfg.deadline_s) * 1e9);
+  return cuda_fail(cudaMemcpyToSymbol(c_rt, &g.ds, sizeof(g.ds)), "run deadline");
+}
+
 void request_stop(int value) {
   if (g.h_stop) {
     *reinterpret_cast<volatile int*>(g.h_stop) = value;

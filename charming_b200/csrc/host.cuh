@@ -31,6 +31,10 @@ int enqueue_scheduler(cudaStream_t s);
 // statistics into the last-run record; returns the run status.
 int collect_run(double kernel_ms);
 
+// Run deadline of the following launches in seconds (<= 0: the configured
+// one). Call only while no scheduler launch is running.
+int set_deadline(double seconds);
+
 // Sets the mapped host stop word read by the running scheduler
 // (1 = stop normally, 2 = stop with CHARMING_ERR_HOST_STOP).
 void request_stop(int value);

@@ -121,6 +121,7 @@ struct pe_state {
   unsigned long long red_u[4];
   unsigned long long stats[N_STATS];
   unsigned long long idle_polls_since_check;
+  unsigned long long busy_polls;       // messages found waiting (end-of-run checks every 64)
   unsigned long long arena_top;        // bytes of this PE's arena handed out this run
   // batched sends (alloc_user_msgs): per message start, ticket, bytes
   void* bm_ptr[MSG_BATCH_MAX];
@@ -170,6 +171,25 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
 __device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
   asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
 }
+// A word of shared memory that other threads of the block update with
+// atomics.
+__device__ __forceinline__ unsigned long long ld_volatile_shared_u64(const unsigned long long* p) {
+  return *reinterpret_cast<const volatile unsigned long long*>(p);
+}
+// System scope: words in mapped host memory shared with the host.
+__device__ __forceinline__ unsigned long long ld_acquire_sys_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.sys.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned long long ld_relaxed_sys_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.sys.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_sys_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.sys.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
+}
 __device__ __forceinline__ unsigned long long globaltimer() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -185,6 +205,10 @@ inline int ld_relaxed_s32(const int* p) { return __atomic_load_n(p, __ATOMIC_REL
 inline int ld_sys_s32(const volatile int* p) { return __atomic_load_n(const_cast<const int*>(p), __ATOMIC_RELAXED); }
 inline unsigned long long ld_relaxed_u64(const unsigned long long* p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
 inline void st_relaxed_u64(unsigned long long* p, unsigned long long v) { __atomic_store_n(p, v, __ATOMIC_RELAXED); }
+inline unsigned long long ld_volatile_shared_u64(const unsigned long long* p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
+inline unsigned long long ld_acquire_sys_u64(const unsigned long long* p) { return __atomic_load_n(p, __ATOMIC_ACQUIRE); }
+inline unsigned long long ld_relaxed_sys_u64(const unsigned long long* p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
+inline void st_release_sys_u64(unsigned long long* p, unsigned long long v) { __atomic_store_n(p, v, __ATOMIC_RELEASE); }
 unsigned long long globaltimer();
 #endif
 

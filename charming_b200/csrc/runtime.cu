@@ -186,7 +186,8 @@ __device__ unsigned char* reserve(int dst, unsigned long long bytes, unsigned lo
   unsigned int cells = cells_for(bytes);
   unsigned long long t = atomicAdd(&c_rt.tail[dst].v, (unsigned long long)cells);
   unsigned long long* hc = head_cache();
-  if (t + cells - hc[dst] > C) {
+  // relaxed read: other threads of the block may raise hc[dst] meanwhile
+  if (t + cells - ld_volatile_shared_u64(&hc[dst]) > C) {
     atomicAdd_block(&ps->stats[ST_SPACE_WAITS], 1ULL);
     unsigned long long start = globaltimer();
     // A receiver that frees nothing for the idle timeout is taken as stuck.
@@ -316,8 +317,9 @@ __device__ bool charm::alloc_user_msgs(message* msgs, const int* dst_pes,
     const size_t* payload_sizes, int n) {
   pe_state* ps = pes();
   if (n > MSG_BATCH_MAX) n = MSG_BATCH_MAX;
-  const int k = (int)threadIdx.x;
-  if (k < n) {  // one reservation per thread: the ring atomics overlap
+  // one reservation per thread (blocks smaller than the batch loop): the
+  // ring atomics overlap
+  for (int k = (int)threadIdx.x; k < n; k += (int)blockDim.x) {
     unsigned long long bytes = envelope::alloc_size(msgtype::user, payload_sizes[k]);
     unsigned long long t = 0;
     ps->bm_ptr[k] = reserve(dst_pes[k], bytes, &t);
@@ -343,8 +345,9 @@ __device__ void charm::send_user_msgs(int chare_id, const int* chare_idx, int ep
   pe_state* ps = pes();
   if (n > MSG_BATCH_MAX) n = MSG_BATCH_MAX;
   __syncthreads();  // payload writes of all threads are done
-  const int k = (int)threadIdx.x;
-  if (k < n && msgs[k].env) {  // one message per thread: the publishing fences overlap
+  // one message per thread: the publishing fences overlap
+  for (int k = (int)threadIdx.x; k < n; k += (int)blockDim.x) {
+    if (!msgs[k].env) continue;
     unsigned char* m = reinterpret_cast<unsigned char*>(msgs[k].env);
     envelope* env = msgs[k].env;
     env->type = msgtype::user;
@@ -537,7 +540,18 @@ __device__ int poll_inbox() {
   const unsigned long long* f = ring_flag(me, h);
   unsigned int spins = 0;
   while (true) {
-    if (ld_acquire_u64(f) == h + 1) return 1;
+    if (ld_acquire_u64(f) == h + 1) {
+      // a PE that always has a message (a chare that keeps calling itself)
+      // still sees the end of the run and its deadline
+      if ((++ps->busy_polls & 63) == 0) {
+        if (ps->term || terminated()) return 0;
+        if (globaltimer() - ps->t0 > c_rt.deadline_ns) {
+          set_error(CHARMING_ERR_DEADLINE, 1, 0);
+          return 0;
+        }
+      }
+      return 1;
+    }
     if (ps->term || terminated()) return 0;
     ++spins;
     if ((spins & 255) == 0) {
@@ -672,6 +686,7 @@ charming_scheduler_kernel(int argc, char** argv, size_t* argvs) {
     ps->n_waiting = ps->n_ready = 0;
     for (int i = 0; i < N_STATS; i++) ps->stats[i] = 0;
     ps->idle_polls_since_check = 0;
+    ps->busy_polls = 0;
     ps->arena_top = 0;
   }
   for (int i = threadIdx.x; i < c_rt.n_pes; i += blockDim.x) head_cache()[i] = c_rt.head[i].v;

@@ -6,7 +6,9 @@ stop decision applied one check period later) with messages delivered in
 per-pair FIFO order but otherwise in a random interleaving, and checks its
 invariants: a halo never arrives more than one sweep ahead, a sweep never
 starts without all halos of its sweep, every chare stops at the same sweep,
-and no tree message finds its slot occupied.
+no tree message finds its slot occupied, and once every chare has finished
+no message is left in flight and none reached a finished chare (a chare at
+max_sweeps waits for the decision of the last check first).
 """
 from __future__ import annotations
 
@@ -72,6 +74,9 @@ class Sim:
             if c.sent < c.iter:
                 K = self.K
                 if c.iter >= self.max:
+                    if K > 0 and self.max > 0 and c.decided < (self.max - 1) // K:
+                        c.waiting = True
+                        return
                     return self.finish(c)
                 if K > 0 and c.iter >= K and c.iter % K == 0 and c.decided < c.iter // K - 1:
                     c.waiting = True
@@ -133,7 +138,7 @@ class Sim:
             c.started = True
             return self.pump(c)
         if c.done:
-            return
+            raise ProtocolError(f"chare {c.idx} got {msg[0]} after it finished")
         if msg[0] == "halo":
             k = msg[1]
             if k not in (c.iter, c.iter + 1):
@@ -166,6 +171,9 @@ class Sim:
             steps += 1
             if steps > max_steps:
                 raise ProtocolError("no progress")
+        left = sum(len(q) for q in self.queues.values())
+        if left:
+            raise ProtocolError(f"{left} messages in flight after every chare finished")
         ends = set(self.finished_at.values())
         if len(ends) != 1:
             raise ProtocolError(f"chares stopped at different sweeps: {sorted(ends)}")

@@ -93,6 +93,7 @@ template <typename T> inline T __shfl_down_sync(unsigned, T v, int) { return v; 
 template <typename T> inline T __shfl_sync(unsigned, T v, int) { return v; }
 #endif
 inline void __threadfence() { std::atomic_thread_fence(std::memory_order_seq_cst); }
+inline void __threadfence_system() { std::atomic_thread_fence(std::memory_order_seq_cst); }
 inline void __nanosleep(unsigned) {}
 inline bool __isLocal(const void*) { return true; }
 inline long long clock64() { return 0; }

@@ -324,6 +324,9 @@ uint64_t now_ns() {
              std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 unsigned int smid() { return blockIdx.x; }
+namespace rt {
+unsigned long long globaltimer() { return now_ns(); }
+}  // namespace rt
 void* smem_scratch(size_t* bytes) {
   PE& pe = me_pe();
   if (bytes) *bytes = sizeof(pe.smem);

@@ -11,6 +11,12 @@
 // usage: rt_emu fanout n_pes ring_bytes n_chares msgs payload seed mode
 //        rt_emu hello n_pes ring_bytes
 //        rt_emu refnum n_pes ring_bytes reversed
+//        rt_emu serve n_pes ring_bytes n_requests seed workers_per_pe
+//               max_inflight chare_side dtype(0 f64, 1 f32)
+// serve runs the Jacobi2d solve server (apps/jacobi2d.cu in serving mode,
+// admission by apps/serve_host.h) with a host thread in the role of the
+// request loop: seeded requests of mixed sizes arrive while others run,
+// each result is compared bit for bit with the serial oracle.
 // The EMU_MT build (rt_emu_mt) runs one PE block of RT_EMU_THREADS threads
 // (barriers checked per call site, warps in lockstep) under ThreadSanitizer.
 // prints a status line; for fanout also the delivery log (8 u32 per record)
@@ -18,7 +24,11 @@
 #include "cuda_host_shim.h"
 #include "../../charming_b200/csrc/rt.cuh"
 #include "../../charming_b200/csrc/apps/suite.cuh"
+#include "../../charming_b200/csrc/apps/jacobi_types.cuh"
+#include "../../charming_b200/csrc/apps/jacobi_sweep.cuh"
+#include "../../charming_b200/csrc/apps/serve_host.h"
 
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstdlib>
@@ -116,13 +126,33 @@ void emu_shfl(void* v, unsigned bytes, int mode, int arg) {
 }
 #endif
 
+#ifdef EMU_MT
+// The bulk-copy sweep is not used by these programs (pipeline = 0); its
+// mbarrier model lives in jacobi_emu.cpp.
+namespace jac {
+[[noreturn]] static void no_tma() {
+  fprintf(stderr, "bulk-copy sweep not modelled in rt_emu\n");
+  _exit(4);
+}
+void mbar_init(unsigned long long*, unsigned) { no_tma(); }
+void mbar_inval(unsigned long long*) { no_tma(); }
+void mbar_expect_tx(unsigned long long*, unsigned) { no_tma(); }
+void mbar_arrive(unsigned long long*) { no_tma(); }
+bool mbar_test_wait(unsigned long long*, unsigned) { no_tma(); }
+bool mbar_try_wait(unsigned long long*, unsigned) { no_tma(); }
+void bulk_g2s(void*, const void*, unsigned, unsigned long long*) { no_tma(); }
+}  // namespace jac
+#endif
+
 unsigned long long charm::rt::globaltimer() {
   return (unsigned long long)std::chrono::duration_cast<std::chrono::nanoseconds>(
              std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+extern "C" int oracle_jacobi2d_f64(double* grid, int nx, int ny, int sweeps);
+extern "C" int oracle_jacobi2d_f32(float* grid, int nx, int ny, int sweeps, int threads);
+
 // programs of the library that this check does not run
-__device__ void suite::jacobi2d_main(int) { charm::end(); }
 __device__ void suite::jacobi1d_main(int) { charm::end(); }
 __device__ void suite::serve_main(int) { charm::end(); }
 
@@ -201,12 +231,195 @@ int run_scheduler(int n_pes, int threads) {
     }
   }
   for (auto& t : th) t.join();
-  return charm::rt::c_rt.ctrl[charm::rt::CTRL_STATUS];
+  const int* ctl = charm::rt::c_rt.ctrl;
+  if (ctl[charm::rt::CTRL_STATUS])
+    fprintf(stderr, "run status %d: pe %d info %d %d\n", ctl[charm::rt::CTRL_STATUS], ctl[charm::rt::CTRL_ERR_PE],
+            ctl[charm::rt::CTRL_ERR_I0], ctl[charm::rt::CTRL_ERR_I1]);
+  return ctl[charm::rt::CTRL_STATUS];
+}
+
+// ---- serving ---------------------------------------------------------------
+struct EmuServe : jserve::sink {
+  int Q = 0;
+  std::vector<jac::serve_req> req;
+  std::vector<jac::chare_desc> stage_d;
+  std::vector<jac::prob_desc> stage_p;
+  unsigned long long ticket = 0;
+  void stage_desc(int w, const jac::chare_desc& d) override { stage_d[w] = d; }
+  void stage_prob(int s, const jac::prob_desc& p) override { stage_p[s] = p; }
+  void post(int slot, int root, unsigned gen) override {
+    jac::serve_req* r = &req[ticket % Q];
+    r->slot = slot;
+    r->root = root;
+    r->gen = gen;
+    __atomic_store_n(&r->seq, ticket + 1, __ATOMIC_RELEASE);
+    ticket++;
+  }
+};
+
+double wall_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+template <typename T>
+int serve_run(int n_pes, int threads, int n_req, unsigned long long seed, int wpp, int max_inflight, int side) {
+  const int n_workers = n_pes * wpp;
+  const int OFF = jac::traits<T>::OFF, VEC = jac::traits<T>::VEC;
+  std::vector<unsigned char> slab_mem((8u << 20) + 256);
+  uintptr_t slab = (reinterpret_cast<uintptr_t>(slab_mem.data()) + 255) & ~uintptr_t(255);
+  jserve::params P;
+  P.n_pes = n_pes;
+  P.workers_per_pe = wpp;
+  P.max_inflight = max_inflight;
+  P.budget = 8u << 20;
+  P.chare_side = side;
+  P.esz = sizeof(T);
+  P.off = OFF;
+  P.vec = VEC;
+  jserve::server_state st;
+  st.init(P, slab);
+  EmuServe sk;
+  sk.Q = max_inflight;
+  sk.req.assign(max_inflight, jac::serve_req{});
+  sk.stage_d.assign(n_workers, jac::chare_desc{});
+  sk.stage_p.assign(max_inflight, jac::prob_desc{});
+  std::vector<jac::serve_comp> comp(max_inflight);
+  std::vector<jac::chare_desc> desc(n_workers);
+  std::vector<jac::prob_desc> probs(n_workers);
+  std::vector<unsigned long long> ctr(16, 0);
+  std::vector<unsigned> done(max_inflight, 0);
+  std::vector<int> bm(n_pes, wpp), sm(n_pes, 0), fin(n_workers, 0), ctl(32, 0);
+  sm[0] = 1;
+  std::vector<unsigned long long> pe_ns(4 * (size_t)n_pes, 0);
+  g_app = suite::app_params{};
+  g_app.id = suite::APP_JACOBI2D;
+  g_app.a[0] = n_workers;
+  g_app.a[2] = sizeof(T) == 8 ? CHARMING_F64 : CHARMING_F32;
+  g_app.a[6] = 1;
+  g_app.a[7] = max_inflight;
+  g_app.a[8] = max_inflight;
+  g_app.p[0] = desc.data();
+  g_app.p[1] = probs.data();
+  g_app.p[4] = fin.data();
+  g_app.p[5] = bm.data();
+  g_app.p[6] = pe_ns.data();
+  g_app.p[7] = sk.req.data();
+  g_app.p[8] = sk.stage_d.data();
+  g_app.p[9] = sk.stage_p.data();
+  g_app.p[10] = comp.data();
+  g_app.p[11] = ctr.data();
+  g_app.p[12] = done.data();
+  g_app.p[13] = ctl.data();
+  g_app.p[14] = sm.data();
+
+  // seeded requests: sizes that make 1 to ~12 chares, sweep caps, with and
+  // without residual checks and early stops
+  struct Req {
+    charming_jacobi_problem q;
+    double at;
+  };
+  std::vector<Req> reqs(std::max(n_req, 0));
+  unsigned long long z = seed;
+  auto rnd = [&]() { return suite::mix64(z++); };
+  double t = 0;
+  for (int i = 0; i < n_req; i++) {
+    charming_jacobi_problem q{};
+    q.nx = 3 + (int)(rnd() % 45);
+    q.ny = 3 + (int)(rnd() % 45);
+    q.max_sweeps = (int)(rnd() % 41);
+    int k = (int)(rnd() % 3);
+    q.check_every = k == 0 ? 0 : (k == 1 ? 5 : 3);
+    q.tol = (q.check_every && (rnd() & 1)) ? 0.3 : 0.0;
+    for (int e = 0; e < 4; e++) q.bc[e] = (double)(rnd() >> 11) * (1.0 / 9007199254740992.0);
+    reqs[i] = Req{q, t};
+    t += (double)(rnd() % 2000) * 1e-6;
+  }
+
+  if (n_req < 0) {  // a server nobody stops must still end at its deadline
+    charm::rt::c_rt.deadline_ns = 1000000000ull;
+    int st0 = run_scheduler(n_pes, threads);
+    printf("status=%d (deadline)\n", st0);
+    return st0 == CHARMING_ERR_DEADLINE ? 0 : 1;
+  }
+  int status = 0;
+  std::atomic<bool> ended{false};
+  std::thread sched([&] {
+    status = run_scheduler(n_pes, threads);
+    ended = true;
+  });
+  const double t0 = wall_s();
+  int next = 0, completed = 0, bad = 0;
+  unsigned long long comp_next = 0;
+  while (completed < n_req && wall_s() - t0 < 120.0 && !ended) {
+    const double now = wall_s() - t0;
+    while (next < n_req && reqs[next].at <= now) {
+      if (st.submit(reqs[next].q, (uint64_t)next, now) != CHARMING_OK) {
+        printf("S tag=%d refused: %s\n", next, st.err.c_str());
+        completed++;  // refused at submission (too large for this pool)
+      }
+      next++;
+    }
+    if (st.admit(sk, now) < 0) {
+      printf("admit failed: %s\n", st.err.c_str());
+      bad++;
+      break;
+    }
+    bool any = false;
+    while (true) {
+      jac::serve_comp* r = &comp[comp_next % max_inflight];
+      if (__atomic_load_n(&r->seq, __ATOMIC_ACQUIRE) != comp_next + 1) break;
+      jac::serve_comp c = *r;
+      comp_next++;
+      any = true;
+      jserve::admitted* a = st.complete(c, now);
+      if (!a) {
+        printf("completion of no request: slot %d gen %u\n", c.slot, c.gen);
+        bad++;
+        continue;
+      }
+      const charming_jacobi_problem& q = a->prob;
+      const size_t W = q.nx + 2;
+      std::vector<T> got((size_t)(q.ny + 2) * W, (T)0), ref((size_t)(q.ny + 2) * W, (T)0);
+      for (size_t y = 0; y < (size_t)q.ny + 2; y++)
+        for (size_t x = 0; x < W; x++) {
+          double v = 0.0;
+          if (y == 0) v = q.bc[0];
+          else if (y == (size_t)q.ny + 1) v = q.bc[1];
+          else if (x == 0) v = q.bc[2];
+          else if (x == W - 1) v = q.bc[3];
+          ref[y * W + x] = (T)v;
+          got[y * W + x] = (T)v;
+        }
+      for (const jac::chare_desc& d : a->chares) {
+        const T* b = reinterpret_cast<const T*>(d.buf[c.final_buf]);
+        for (int r2 = 1; r2 <= d.h; r2++)
+          for (int c2 = 1; c2 <= d.w; c2++)
+            got[(size_t)(d.y0 + r2) * W + d.x0 + c2] = b[(size_t)r2 * d.pitch + OFF - 1 + c2];
+      }
+      if (sizeof(T) == 8) oracle_jacobi2d_f64(reinterpret_cast<double*>(ref.data()), q.nx, q.ny, c.sweeps);
+      else oracle_jacobi2d_f32(reinterpret_cast<float*>(ref.data()), q.nx, q.ny, c.sweeps, 1);
+      bool same = memcmp(got.data(), ref.data(), got.size() * sizeof(T)) == 0;
+      bool sweeps_ok = q.tol > 0 ? c.sweeps <= q.max_sweeps : c.sweeps == q.max_sweeps;
+      printf("R tag=%llu nx=%d ny=%d chares=%zu max=%d K=%d tol=%g sweeps=%d checks=%d gen=%u same=%d\n",
+             (unsigned long long)a->tag, q.nx, q.ny, a->chares.size(), q.max_sweeps, q.check_every, q.tol,
+             c.sweeps, c.checks, c.gen, same ? 1 : 0);
+      if (!same || !sweeps_ok) bad++;
+      st.release(a->tag);
+      completed++;
+    }
+    if (!any) std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+  __atomic_store_n(&ctl[0], 1, __ATOMIC_RELEASE);
+  sched.join();
+  printf("status=%d completed=%d of %d bad=%d peak_inflight=%d peak_bytes=%llu\n", status, completed, n_req,
+         bad, st.peak_inflight, (unsigned long long)st.mem.peak());
+  return (status == 0 && completed == n_req && bad == 0) ? 0 : 1;
 }
 
 }  // namespace
 
 int main(int argc, char** argv) {
+  setvbuf(stdout, nullptr, _IOLBF, 0);
   if (argc < 4) {
     fprintf(stderr, "usage: %s fanout|hello|refnum n_pes ring_bytes ...\n", argv[0]);
     return 2;
@@ -260,6 +473,14 @@ int main(int argc, char** argv) {
       printf("\n");
     }
     return status;
+  }
+  if (app == "serve") {
+    if (argc < 10) return 2;
+    int n_req = atoi(argv[4]);
+    unsigned long long seed = strtoull(argv[5], nullptr, 0);
+    int wpp = atoi(argv[6]), max_inflight = atoi(argv[7]), side = atoi(argv[8]), dt = atoi(argv[9]);
+    return dt == 0 ? serve_run<double>(n_pes, threads, n_req, seed, wpp, max_inflight, side)
+                   : serve_run<float>(n_pes, threads, n_req, seed, wpp, max_inflight, side);
   }
   if (app == "hello" || app == "refnum") {
     std::vector<int> out(4 * n_pes + 16, -1);

@@ -92,3 +92,39 @@ def test_hello_chain(emus, exe, n_pes, threads):
     assert r.returncode == 0
     out = [int(x) for x in r.stdout.split("out=")[1].strip().strip(",").split(",")]
     assert out[: 2 * n_pes] == list(range(2 * n_pes))
+
+
+def serve(exe, n_pes, n_req, seed, wpp, max_inflight, side, dtype, threads=1):
+    """Solve server on the CPU: the real scheduler runs the Jacobi2d chares
+    in serving mode (apps/jacobi2d.cu) and admission runs apps/serve_host.h;
+    a host thread submits seeded requests of mixed sizes while others run
+    and compares every result bit for bit with the serial oracle."""
+    r = run(exe, ["serve", n_pes, 65536, n_req, seed, wpp, max_inflight, side, dtype], threads, timeout=900)
+    lines = r.stdout.splitlines()
+    assert r.returncode == 0 and lines and "bad=0" in lines[-1], (lines[-5:], r.stderr[-2000:])
+    results = [l for l in lines if l.startswith("R ")]
+    refused = [l for l in lines if l.startswith("S ")]
+    assert len(results) + len(refused) == n_req
+    assert all("same=1" in l for l in results)
+    # workers and slots were reused: more requests than slots completed
+    assert len(results) > max_inflight
+    return results
+
+
+@pytest.mark.parametrize("exe,n_pes,threads,n_req,dtype,seed", [
+    ("rt_emu", 6, 1, 40, 0, 7),        # ASan + UBSan, FP64
+    ("rt_emu", 6, 1, 40, 1, 8),        # FP32 sweeps, FP64 residual
+    ("rt_emu_tsan", 8, 1, 30, 1, 11),  # PE threads under ThreadSanitizer
+    ("rt_emu_mt", 1, 64, 10, 0, 5),    # one PE block of 64 threads
+])
+def test_serving_results_match_oracle(emus, exe, n_pes, threads, n_req, dtype, seed):
+    wpp = 6 if n_pes == 1 else 3
+    serve(emus[exe], n_pes, n_req, seed, wpp, 4, 16, dtype, threads)
+
+
+@pytest.mark.parametrize("exe,n_pes,threads", [("rt_emu", 4, 1), ("rt_emu_mt", 1, 32)])
+def test_server_nobody_stops_ends_at_deadline(emus, exe, n_pes, threads):
+    # the server chare calls itself forever; the busy PE must still see the
+    # run deadline (1 s here) and the run must end with DEADLINE
+    r = run(emus[exe], ["serve", n_pes, 65536, -1, 1, 2, 4, 16, 0], threads, timeout=120)
+    assert r.returncode == 0 and "status=6" in r.stdout, (r.stdout[-500:], r.stderr[-1500:])
