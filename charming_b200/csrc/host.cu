@@ -252,10 +252,30 @@ int charming_init(const charming_config* cfg_in) {
   int n_pes = cfg.n_pes > 0 ? cfg.n_pes : n_sms * cfg.pes_per_sm;
 
   // Device limits (reference: src/charming.cu:197-203).
-  e = cudaDeviceSetLimit(cudaLimitMallocHeapSize, cfg.heap_bytes);
-  if (e != cudaSuccess) return cuda_fail(e, "heap limit");
-  e = cudaDeviceSetLimit(cudaLimitStackSize, cfg.stack_bytes);
-  if (e != cudaSuccess) return cuda_fail(e, "stack limit");
+  // The heap size is fixed once a kernel of the context has run (a second
+  // charming_init in the same process): keep it when it is large enough.
+  size_t heap_now = 0;
+  e = cudaDeviceGetLimit(&heap_now, cudaLimitMallocHeapSize);
+  if (e != cudaSuccess) return cuda_fail(e, "heap limit query");
+  if (heap_now != cfg.heap_bytes) {
+    e = cudaDeviceSetLimit(cudaLimitMallocHeapSize, cfg.heap_bytes);
+    if (e != cudaSuccess && heap_now >= cfg.heap_bytes) {
+      (void)cudaGetLastError();
+      e = cudaSuccess;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "heap limit");
+  }
+  size_t stack_now = 0;
+  e = cudaDeviceGetLimit(&stack_now, cudaLimitStackSize);
+  if (e != cudaSuccess) return cuda_fail(e, "stack limit query");
+  if (stack_now != cfg.stack_bytes) {
+    e = cudaDeviceSetLimit(cudaLimitStackSize, cfg.stack_bytes);
+    if (e != cudaSuccess && stack_now >= cfg.stack_bytes) {
+      (void)cudaGetLastError();
+      e = cudaSuccess;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "stack limit");
+  }
   size_t stack_eff = 0;
   e = cudaDeviceGetLimit(&stack_eff, cudaLimitStackSize);
   if (e != cudaSuccess) return cuda_fail(e, "stack limit query");

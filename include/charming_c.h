@@ -256,6 +256,22 @@ int charming_refnum(int* out, int n_out, int* n_delivered);
 int charming_refnum_reversed(int* out, int n_out, int* n_delivered);
 
 /* ---- serving ------------------------------------------------------------ */
+/* A solve server (no counterpart in the reference; it extends the reference's
+ * model of chares in one persistent launch, src/sched/scheduler.cu:183-234,
+ * to requests that arrive while the launch runs). charming_serve_start
+ * launches the scheduler once with a pool of n_pes * workers_per_pe Jacobi2d
+ * worker chares and a server chare on PE 0, and returns at once. Requests
+ * (charming_jacobi_problem: size, boundary, sweep cap, residual period and
+ * tolerance; px/py ignored, chares of chare_side) are admitted in arrival
+ * order as a request slot, enough free workers and grid memory within the
+ * HBM budget are available; admitted requests share the PEs with those
+ * already running. A completed request's grid stays in HBM until
+ * charming_serve_release; charming_serve_fetch copies it out ((ny+2)*(nx+2)
+ * values of dtype with the boundary ring) while the server keeps running.
+ * Results equal charming_jacobi2d_run's for the same problem and chare side
+ * bit for bit. While a server runs it holds every PE: no other program of
+ * this library may run, and the caller must not synchronise the whole
+ * device. Call the serve functions from one host thread. */
 typedef struct charming_serve_config {
   uint64_t hbm_budget_bytes; /* grids admitted at once must fit in this    */
   int max_inflight;          /* device problem slots                       */
@@ -281,12 +297,21 @@ typedef struct charming_serve_stats {
 } charming_serve_stats;
 
 int charming_serve_start(const charming_serve_config* cfg, void** server);
+/* Queues a request under a caller-chosen tag (unique among requests not yet
+ * released) and admits what fits; CHARMING_ERR_CONFIG for a request that could
+ * never be admitted (larger than the budget or the worker pool). */
 int charming_serve_submit(void* server, const charming_jacobi_problem* req,
     uint64_t tag);
+/* Reads up to max_n completions (their slots and workers become free) and
+ * admits what now fits; returns the run's status if the launch ended. */
 int charming_serve_poll(void* server, charming_serve_completion* out,
     int max_n, int* n_out);
 int charming_serve_fetch(void* server, uint64_t tag, void* host_grid);
+/* Frees a completed request's grid memory. */
 int charming_serve_release(void* server, uint64_t tag);
+/* Stops admitting, waits for the requests in flight (within deadline_s),
+ * ends the launch and frees everything; never-admitted requests are
+ * dropped. */
 int charming_serve_stop(void* server, charming_serve_stats* stats);
 
 #ifdef __cplusplus

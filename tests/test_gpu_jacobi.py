@@ -212,3 +212,27 @@ def test_multi_sweep_residual_stop_rule(rt, dtype):
     ref = jac64(g0, r.sweeps) if dtype == "f64" else jac32(g0, r.sweeps)
     assert np.array_equal(bits(out), bits(ref))
     assert r.res0 == pytest.approx(r1.res0, rel=1e-12)
+
+
+def test_autotune_reinit_and_configs(rt):
+    """The autotuner re-initialises the runtime per candidate (chare side,
+    PEs per SM, ring depth); every candidate gives the same grid bit for
+    bit, and the default runtime comes back afterwards."""
+    from charming_b200.batch import Candidate, autotune, uneven_set
+    from charming_b200.runtime import Runtime
+    probs = uneven_set(seed=7, n=6, lo=32, hi=300, max_sweeps=30)
+    ref = [jac64(initial_grid(p.nx, p.ny, p.bc), 30) for p in probs]
+    cands = [Candidate(64, 1, 1 << 20), Candidate(128, 2, 4 << 20), Candidate(256, 1, 4 << 20)]
+    grids = []
+    for c in cands:
+        Runtime(**c.runtime_config())
+        with Jacobi2D(probs, chare_side=c.chare_side, use_graph=True) as j:
+            j.run()
+            grids.append([j.store(i) for i in range(len(probs))])
+    for g in grids:
+        for a, b in zip(ref, g):
+            assert np.array_equal(bits(a), bits(b))
+    tune = autotune(probs, "f64", candidates=cands)
+    assert tune.best.glups > 0 and all(c.glups > 0 for c in tune.tried)
+    Runtime()  # default configuration for the tests that follow
+    assert Runtime._active.info["n_pes"] == rt.info["n_pes"]

@@ -71,7 +71,9 @@ def test_serve_alone_equals_mix_fp32(rt):
     early on tol. Alone, in a mix, and through the batched path: the same
     sweeps, residuals and grids, equal to the FP32 oracle run for the same
     sweep count."""
-    probs = mixed(5, 12, 40, 500, 300, check_every=10, tol=1e-2)
+    probs = mixed(5, 12, 40, 500, 300, check_every=10, tol=0.05)
+    for p in probs[::2]:
+        p.tol = 1e-4  # runs to the cap
     with Server(1 << 30, max_inflight=16, workers_per_pe=8, chare_side=64, dtype="f32",
                 deadline_s=60) as s:
         alone = [serve_all(s, [p], tag0=100 + i) for i, p in enumerate(probs)]
@@ -92,7 +94,7 @@ def test_serve_alone_equals_mix_fp32(rt):
         ref = jac32(initial_grid(p.nx, p.ny, p.bc, dtype=np.float32), ca.sweeps)
         assert np.array_equal(bits(ga), bits(ref)), (i, p.nx, p.ny, ca.sweeps)
         early += ca.sweeps < p.max_sweeps
-    assert early > 0  # the stop rule fired for some
+    assert 0 < early < len(probs)  # the stop rule fired for some, not all
 
 
 def test_serve_admission_under_budget(rt):

@@ -128,3 +128,14 @@ def test_server_nobody_stops_ends_at_deadline(emus, exe, n_pes, threads):
     # run deadline (1 s here) and the run must end with DEADLINE
     r = run(emus[exe], ["serve", n_pes, 65536, -1, 1, 2, 4, 16, 0], threads, timeout=120)
     assert r.returncode == 0 and "status=6" in r.stdout, (r.stdout[-500:], r.stderr[-1500:])
+
+
+def test_serve_host_logic():
+    """Slab allocator, FIFO admission against budget / slots / workers,
+    balanced worker placement, generations and staged descriptors
+    (tests/emu/serve_host_test.cpp on apps/serve_host.h)."""
+    r = subprocess.run(["make", "-s", os.path.join("..", "..", "build", "emu", "serve_host_test")],
+                       cwd=os.path.join(ROOT, "tests", "emu"), capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    r = run(os.path.join(OUT, "serve_host_test"), [])
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr[-2000:]
