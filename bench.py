@@ -59,18 +59,50 @@ def measured_peaks() -> dict:
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """SM clock and clock-event reasons sampled during the timed region:
+    NVML read every 10 ms from a thread (read-only queries), or nvidia-smi
+    every 200 ms when NVML is unavailable."""
 
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device: int):
         self.device = device
-        self.proc = None
-        self.path = None
+        self.samples = []  # (sm_mhz, max_mhz, set of reasons)
+        self.proc = self.path = self.thread = None
+        self.stop = False
+        self.source = None
+
+    def _nvml_loop(self, nv, h):
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                rs = {name for name, attr in self.REASONS if bits & getattr(nv, attr)}
+                self.samples.append((float(sm), float(mx), rs))
+            except Exception:
+                pass
+            time.sleep(0.01)
 
     def __enter__(self):
+        try:
+            import threading
+
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self.device)
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self.thread.start()
+            self.source = "nvml 10 ms"
+            return self
+        except Exception:
+            self.thread = None
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
@@ -78,44 +110,41 @@ class ClockSampler:
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
                  "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            self.source = "nvidia-smi 200 ms"
         except OSError:
             self.proc = None
         return self
 
     def __exit__(self, *exc):
+        if self.thread:
+            self.stop = True
+            self.thread.join(timeout=5)
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
-
-    def summary(self) -> dict:
-        rows = []
-        try:
-            for line in open(self.path):
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
-                    rows.append(parts)
-        except OSError:
-            pass
-        finally:
             try:
-                os.unlink(self.path)
+                names = [n for n, _ in self.REASONS]
+                for line in open(self.path):
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                        rs = {n for n, v in zip(names, parts[5:9]) if v.lower().startswith("active")}
+                        self.samples.append((float(parts[1]), float(parts[2]), rs))
             except OSError:
                 pass
-        if not rows:
+            finally:
+                os.unlink(self.path)
+
+    def summary(self) -> dict:
+        if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows]
-        reasons = set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
-            for name, v in zip(names, r[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(name)
-        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
-        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": float(rows[0][2]),
-                "samples": len(rows), "reasons": sorted(reasons)}
+        sm = [x[0] for x in self.samples]
+        loaded = [v for v in sm if v > 0.5 * max(sm)] or sm
+        reasons = sorted(set().union(*(x[2] for x in self.samples)))
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": self.samples[0][1],
+                "samples": len(self.samples), "source": self.source, "reasons": reasons}
 
 
 def cpu_baseline(target_s: float = 12.0, threads: int | None = None) -> dict:
@@ -289,9 +318,12 @@ def precision_suite(plain_fp64_glups: float, steps: int = 2, warmup: int = 1) ->
     tune = autotune(proxy, "f32", candidates=cands)
     side = tune.best.chare_side
     with Jacobi2D(probs, dtype="f32", chare_side=side, use_graph=True) as j:
-        for _ in range(warmup):
-            j.run()
-        ts = [j.run() for _ in range(steps)]
+        ts = []
+        for k in range(warmup + steps):
+            j.init()  # every launch solves from the initial state (outside the timed launch)
+            t = j.run()
+            if k >= warmup:
+                ts.append(t)
         res = [j.result(i) for i in range(len(probs))]
         g32 = [j.store(i) for i in range(len(probs))]
     ms = statistics.mean(ts)

@@ -63,8 +63,6 @@ struct japp {
   __device__ static bool serving() { return g_app.a[6] != 0; }
   __device__ static int serve_q() { return (int)g_app.a[7]; }   // request ring entries
   __device__ static int serve_cq() { return (int)g_app.a[8]; }  // completion ring entries
-  __device__ static jac::chare_desc* chares_rw() { return reinterpret_cast<jac::chare_desc*>(g_app.p[0]); }
-  __device__ static jac::prob_desc* probs_rw() { return reinterpret_cast<jac::prob_desc*>(g_app.p[1]); }
   __device__ static jac::serve_req* serve_reqs() { return reinterpret_cast<jac::serve_req*>(g_app.p[7]); }
   __device__ static const jac::chare_desc* stage_descs() {
     return reinterpret_cast<const jac::chare_desc*>(g_app.p[8]);
@@ -100,6 +98,11 @@ struct JBlock : charm::chare {
   double res0, res_last;
   int checks;
   unsigned gen;      // request generation (serving; 0 otherwise)
+  // The chare's own copies of its block and problem descriptors: chare
+  // objects live in the PE's on-chip arena, so the entry methods read these
+  // without a trip to memory after every inbox acquire.
+  jac::chare_desc desc;
+  jac::prob_desc prob;
   __device__ JBlock() { reset(0); }
   __device__ void reset(unsigned g) {
     iter = pass = cur = 0;
@@ -186,63 +189,95 @@ __device__ double sweep_block(const jac::chare_desc& d, int cur, bool resid, int
   return resid ? suite::block_sum_f64(acc) : 0.0;
 }
 
-// Copies a rectangle between a chare grid and a packed row-major buffer
-// (to_grid: buffer -> grid). Long rows go as whole-row vector copies by all
-// threads, short ones element by element. All threads.
+// Copies up to N_DIRS rectangles between a chare grid and packed row-major
+// buffers (to_grid: buffers -> grid) in one pass over all their cells. A
+// rectangle whose rows start on 16-byte boundaries on both sides and hold
+// whole vectors moves in 16-byte vectors, the others element by element.
+// Each thread loads a batch of B units before it stores any, so the loads of
+// all rectangles are in flight together instead of one rectangle (or row)
+// after another. All threads.
 template <typename T>
-__device__ void copy_region(jac::block_view<T> g, jac::region e, T* buf, bool to_grid) {
-  if (e.nc >= 32) {
-    for (int r = 0; r < e.nr; r++) {
-      T* gp = g.at(e.r0 + r, e.c0);
-      T* bp = buf + (size_t)r * e.nc;
-      if (to_grid) charm::copy_cooperative(gp, bp, (size_t)e.nc * sizeof(T), threadIdx.x, blockDim.x);
-      else charm::copy_cooperative(bp, gp, (size_t)e.nc * sizeof(T), threadIdx.x, blockDim.x);
+__device__ void copy_rects(jac::block_view<T> g, const jac::region* e, T* const* bufs, int n, bool to_grid) {
+  using VT = typename jac::vec_of<T>::type;
+  constexpr int V = jac::traits<T>::VEC, B = 8;
+  int start[jac::N_DIRS + 1], unit[jac::N_DIRS];
+  start[0] = 0;
+  for (int k = 0; k < n; k++) {
+    const bool vec = (e[k].nc % V) == 0 &&
+                     (reinterpret_cast<uintptr_t>(g.at(e[k].r0, e[k].c0)) & 15) == 0 &&
+                     (reinterpret_cast<uintptr_t>(bufs[k]) & 15) == 0;
+    unit[k] = vec ? V : 1;
+    start[k + 1] = start[k] + e[k].nr * e[k].nc / unit[k];
+  }
+  const int total = start[n];
+  const int stride = (int)blockDim.x;
+  for (int base = (int)threadIdx.x; base < total; base += B * stride) {
+    VT v[B];
+    T* dst[B];
+    int u[B];
+#pragma unroll
+    for (int b = 0; b < B; b++) {
+      const int i = base + b * stride;
+      dst[b] = nullptr;
+      u[b] = 1;
+      if (i < total) {
+        int k = 0;
+        while (k + 1 < n && i >= start[k + 1]) k++;
+        const int nu = e[k].nc / unit[k];        // units per row
+        const int j = i - start[k];
+        const int r = j / nu, cu = j - r * nu;
+        T* gp = g.at(e[k].r0 + r, e[k].c0 + cu * unit[k]);
+        T* bp = bufs[k] + (size_t)r * e[k].nc + cu * unit[k];
+        T* src = to_grid ? bp : gp;
+        dst[b] = to_grid ? gp : bp;
+        u[b] = unit[k];
+        if (unit[k] == V) v[b] = *reinterpret_cast<const VT*>(src);
+        else reinterpret_cast<T*>(&v[b])[0] = *src;
+      }
     }
-  } else {
-    const int len = e.nr * e.nc;
-    for (int i = threadIdx.x; i < len; i += blockDim.x) {
-      const int r = i / e.nc, c = i - r * e.nc;
-      T* gp = g.at(e.r0 + r, e.c0 + c);
-      if (to_grid) *gp = buf[i];
-      else buf[i] = *gp;
+#pragma unroll
+    for (int b = 0; b < B; b++) {
+      if (!dst[b]) continue;
+      if (u[b] == V) *reinterpret_cast<VT*>(dst[b]) = v[b];
+      else *dst[b] = reinterpret_cast<const T*>(&v[b])[0];
     }
   }
 }
 
 // Packs the boundary regions of buf[cur] for every neighbour straight into
 // their inbox rings (zero-copy) and publishes them together: the ring
-// reservations and the publishing fences of the messages overlap (refnum =
-// pass in halo_mode 1). All threads.
+// reservations, the packing loads and the publishing fences of the messages
+// overlap (refnum = pass in halo_mode 1). All threads.
 template <typename T>
 __device__ void send_halos(JBlock& c, const jac::chare_desc& d) {
   unsigned long long t0 = charm::now_ns();
   int idx[jac::N_DIRS], dirs[jac::N_DIRS], refs[jac::N_DIRS];
   size_t bytes[jac::N_DIRS];
+  jac::region e[jac::N_DIRS];
   int n = 0;
+  const bool tagged = japp::halo_mode() == 1;
   for (int dir = 0; dir < jac::N_DIRS; dir++) {
     if (d.nbr[dir] < 0) continue;
-    jac::region e = jac::edge_region(dir, d.depth, d.w, d.h);
+    e[n] = jac::edge_region(dir, d.depth, d.w, d.h);
     idx[n] = d.nbr[dir];
     dirs[n] = dir;
-    refs[n] = japp::halo_mode() == 1 ? c.pass : -1;
-    bytes[n] = sizeof(jac::halo_hdr) + (size_t)e.nr * e.nc * sizeof(T);
+    refs[n] = tagged ? c.pass : -1;
+    bytes[n] = sizeof(jac::halo_hdr) + (size_t)e[n].nr * e[n].nc * sizeof(T);
     n++;
   }
   charm::message msg[jac::N_DIRS];
   if (n > 0 && jproxy->alloc_msgs(msg, idx, bytes, n)) {
-    jac::block_view<T> g = view<T>(d, c.cur);
-    for (int k = 0; k < n; k++) {
-      jac::region e = jac::edge_region(dirs[k], d.depth, d.w, d.h);
-      char* pl = reinterpret_cast<char*>(msg[k].payload());
-      if (threadIdx.x == 0) {
-        jac::halo_hdr* hh = reinterpret_cast<jac::halo_hdr*>(pl);
-        hh->dir = jac::opposite(dirs[k]);
-        hh->len = e.nr * e.nc;
-        hh->pass = c.pass;
-        hh->gen = c.gen;
-      }
-      copy_region<T>(g, e, reinterpret_cast<T*>(pl + sizeof(jac::halo_hdr)), false);
+    T* vals[jac::N_DIRS];
+    for (int k = 0; k < n; k++)
+      vals[k] = reinterpret_cast<T*>(reinterpret_cast<char*>(msg[k].payload()) + sizeof(jac::halo_hdr));
+    for (int k = (int)threadIdx.x; k < n; k += (int)blockDim.x) {  // one header per thread
+      jac::halo_hdr* hh = reinterpret_cast<jac::halo_hdr*>(msg[k].payload());
+      hh->dir = jac::opposite(dirs[k]);
+      hh->len = e[k].nr * e[k].nc;
+      hh->pass = c.pass;
+      hh->gen = c.gen;
     }
+    copy_rects<T>(view<T>(d, c.cur), e, vals, n, false);
     jproxy->invoke_msgs(idx, EP_HALO, msg, bytes, refs, n);
   }
   if (threadIdx.x == 0) japp::pe_ns()[4 * blockIdx.x + 1] += charm::now_ns() - t0;
@@ -252,9 +287,9 @@ __device__ void send_halos(JBlock& c, const jac::chare_desc& d) {
 template <typename T>
 __device__ void unpack_halo(JBlock& c, const jac::chare_desc& d, const void* arg) {
   const jac::halo_hdr* hh = reinterpret_cast<const jac::halo_hdr*>(arg);
-  const T* vals = reinterpret_cast<const T*>(reinterpret_cast<const char*>(arg) + sizeof(jac::halo_hdr));
+  T* vals = const_cast<T*>(reinterpret_cast<const T*>(reinterpret_cast<const char*>(arg) + sizeof(jac::halo_hdr)));
   jac::region gr = jac::ghost_region(hh->dir, d.depth, d.w, d.h);
-  copy_region<T>(view<T>(d, hh->pass & 1), gr, const_cast<T*>(vals), true);
+  copy_rects<T>(view<T>(d, hh->pass & 1), &gr, &vals, 1, true);
 }
 
 
@@ -287,7 +322,7 @@ __device__ void finish(JBlock& c, const jac::chare_desc& d) {
   __shared__ int s_last;
   if (threadIdx.x == 0 && japp::serving()) {
     c.done = 1;
-    const jac::prob_desc& p = japp::probs()[d.prob];
+    const jac::prob_desc& p = c.prob;
     __threadfence();
     unsigned n = atomicAdd(&japp::serve_done()[d.slot], 1u) + 1;
     if (n == (unsigned)p.n_chares) serve_complete(c, d);
@@ -295,7 +330,7 @@ __device__ void finish(JBlock& c, const jac::chare_desc& d) {
   } else if (threadIdx.x == 0) {
     c.done = 1;
     japp::final_buf()[c.i] = c.cur;
-    const jac::prob_desc& p = japp::probs()[d.prob];
+    const jac::prob_desc& p = c.prob;
     if (p.root == c.i) {
       jac::prob_result& r = japp::results()[d.prob];
       r.sweeps = c.iter;
@@ -336,18 +371,18 @@ __device__ int ensure_gen(JBlock& c, unsigned gen) {
   constexpr int WD = sizeof(jac::chare_desc) / 8, WP = sizeof(jac::prob_desc) / 8;
   {
     const unsigned long long* src = reinterpret_cast<const unsigned long long*>(japp::stage_descs() + c.i);
-    unsigned long long* dst = reinterpret_cast<unsigned long long*>(japp::chares_rw() + c.i);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&c.desc);
     for (int k = threadIdx.x; k < WD; k += blockDim.x) dst[k] = ld_relaxed_sys_u64(src + k);
   }
   __syncthreads();
-  const jac::chare_desc& d = japp::chares()[c.i];
+  const jac::chare_desc& d = c.desc;
   {
     const unsigned long long* src = reinterpret_cast<const unsigned long long*>(japp::stage_probs() + d.slot);
-    unsigned long long* dst = reinterpret_cast<unsigned long long*>(japp::probs_rw() + d.prob);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&c.prob);
     for (int k = threadIdx.x; k < WP; k += blockDim.x) dst[k] = ld_relaxed_sys_u64(src + k);
   }
   __syncthreads();
-  const jac::prob_desc& p = japp::probs()[d.prob];
+  const jac::prob_desc& p = c.prob;
   if (CHARM_VERIFY(d.w > 0 && d.h > 0 && d.depth >= 1 && d.depth <= jac::DEPTH_MAX && d.prob == c.i,
                    CHARMING_ERR_APP, 9000 + d.depth, c.i)) {
     const int D = d.depth, rows = d.h + 2 * D;
@@ -459,6 +494,16 @@ __device__ void suite::jacobi2d_main(int pe) {
     jproxy->add_entry_method<&em_partial>();
     jproxy->add_entry_method<&em_decision>();
     jproxy->create(japp::n_chares(), const_cast<int*>(japp::block_map()));
+    if (!japp::serving()) {
+      // each chare keeps its own descriptors (serving workers copy theirs
+      // per request)
+      for (int i = jproxy->start_idx; i <= jproxy->end_idx && jproxy->n_local > 0; i++) {
+        JBlock* c = jproxy->local(i);
+        if (!c) continue;
+        c->desc = japp::chares()[i];
+        c->prob = japp::probs()[c->desc.prob];
+      }
+    }
     if (japp::serving()) {
       sproxy = new charm::chare_proxy<JServer>();
       sproxy->add_entry_method<&em_poll>();

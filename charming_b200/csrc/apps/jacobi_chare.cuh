@@ -70,7 +70,7 @@ __device__ int tree_try_forward(JBlock& c, const jac::chare_desc& d, int chk) {
         s_pm.value = t;
         s_act = 1;
       } else {
-        const jac::prob_desc& p = japp::probs()[d.prob];
+        const jac::prob_desc& p = c.prob;
         double nrm = sqrt(t);
         s_dm.check = chk;
         s_dm.gen = c.gen;
@@ -99,7 +99,7 @@ __device__ int tree_try_forward(JBlock& c, const jac::chare_desc& d, int chk) {
 // tree when the pass starts at a check.
 template <typename T>
 __device__ void advance(JBlock& c, const jac::chare_desc& d) {
-  const jac::prob_desc& p = japp::probs()[d.prob];
+  const jac::prob_desc& p = c.prob;
   int K = p.check_every;
   // read before thread 0 advances the chare below
   const bool resid = K > 0 && (c.iter % K == 0);
@@ -127,7 +127,7 @@ __device__ void advance(JBlock& c, const jac::chare_desc& d) {
 // of u_iter once, and sweep whenever all halos of the current sweep are in.
 template <typename T>
 __device__ void pump(JBlock& c, const jac::chare_desc& d) {
-  const jac::prob_desc& p = japp::probs()[d.prob];
+  const jac::prob_desc& p = c.prob;
   __shared__ int s_act;
   enum { IDLE = 0, SEND = 1, FIN = 2, SWEEP = 3, SELF = 4 };
   while (true) {
@@ -193,7 +193,7 @@ __device__ void em_start_t(JBlock& c, void* arg) {
     // the start of a request travels down the residual tree
     const jac::start_msg m = *reinterpret_cast<const jac::start_msg*>(arg);
     if (!ensure_gen<T>(c, m.gen)) return;
-    const jac::chare_desc& d = japp::chares()[c.i];
+    const jac::chare_desc& d = c.desc;
     for (int k = 0; k < 2; k++) {
       jac::start_msg f = m;
       if (d.child[k] >= 0) jproxy->invoke(d.child[k], EP_START, &f, sizeof(f));
@@ -201,7 +201,7 @@ __device__ void em_start_t(JBlock& c, void* arg) {
     pump<T>(c, d);
     return;
   }
-  const jac::chare_desc& d = japp::chares()[c.i];
+  const jac::chare_desc& d = c.desc;
   if (threadIdx.x == 0) {
     int n = 0;
     for (int k = 0; k < jac::N_DIRS; k++) n += d.nbr[k] >= 0;
@@ -218,7 +218,7 @@ __device__ void em_halo_t(JBlock& c, void* arg) {
   if (!ensure_gen<T>(c, hh->gen)) return;
   if (c.done) return;
   const unsigned long long t_em = charm::now_ns();
-  const jac::chare_desc& d = japp::chares()[c.i];
+  const jac::chare_desc& d = c.desc;
   // checked build: direction, length and sweep of the halo are consistent
   if (!CHARM_VERIFY(hh->dir >= 0 && hh->dir < jac::N_DIRS && d.nbr[hh->dir] >= 0, CHARMING_ERR_APP,
                     1000 + hh->dir, c.i) ||
@@ -241,7 +241,7 @@ __device__ void em_halo_t(JBlock& c, void* arg) {
 template <typename T>
 __device__ void em_cont_t(JBlock& c) {
   if (c.done) return;
-  const jac::chare_desc& d = japp::chares()[c.i];
+  const jac::chare_desc& d = c.desc;
   advance<T>(c, d);
   pump<T>(c, d);
 }
@@ -251,7 +251,7 @@ __device__ void em_partial_t(JBlock& c, void* arg) {
   const jac::partial_msg* pm = reinterpret_cast<const jac::partial_msg*>(arg);
   if (!ensure_gen<T>(c, pm->gen)) return;
   if (c.done) return;
-  const jac::chare_desc& d = japp::chares()[c.i];
+  const jac::chare_desc& d = c.desc;
   int chk = pm->check;
   // Thread 0 checks and records the partial; the others learn the outcome
   // after the barrier (reading child_got themselves would race with it).
@@ -278,7 +278,7 @@ __device__ void em_decision_t(JBlock& c, void* arg) {
   jac::decision_msg m = *reinterpret_cast<const jac::decision_msg*>(arg);
   if (!ensure_gen<T>(c, m.gen)) return;
   if (c.done) return;
-  const jac::chare_desc& d = japp::chares()[c.i];
+  const jac::chare_desc& d = c.desc;
   __syncthreads();
   if (apply_decision<T>(c, d, m)) pump<T>(c, d);
 }

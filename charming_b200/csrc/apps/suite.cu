@@ -4,7 +4,7 @@
 #include "../host.cuh"
 #endif
 
-__device__ suite::app_params g_app;
+__constant__ suite::app_params g_app;
 
 namespace {
 __shared__ unsigned long long s_red_u64[32];

@@ -57,7 +57,9 @@ __device__ double block_sum_f64(double v);
 
 }  // namespace suite
 
-extern __device__ suite::app_params g_app;
+// Parameters of the current run (written by the host before each launch;
+// constant memory, so reads stay cached whatever the chares' loads do).
+extern __constant__ suite::app_params g_app;
 
 // Program entry points (called from charm::main on every PE, all threads).
 namespace suite {

@@ -284,12 +284,17 @@ int charming_init(const charming_config* cfg_in) {
   e = cudaFuncGetAttributes(&fa, (const void*)charming_scheduler_kernel);
   if (e != cudaSuccess) return cuda_fail(e, "scheduler attributes");
   int smem_state = (int)((sizeof(pe_state) + 8ull * n_pes + 127) / 128 * 128);
+  // on-chip object arena (chare objects, proxies, their tables); the device
+  // arena and heap take what does not fit
+  int smem_arena = cfg.pes_per_sm > 1 ? (16 << 10) : (32 << 10);
+  if (const char* ev = getenv("CHARMING_SMEM_ARENA_BYTES")) smem_arena = (int)strtol(ev, nullptr, 10) / 128 * 128;
   long per_block = (long)g.prop.sharedMemPerBlockOptin - (long)fa.sharedSizeBytes;
   long per_sm = (long)g.prop.sharedMemPerMultiprocessor / cfg.pes_per_sm -
                 (long)fa.sharedSizeBytes - (long)g.prop.reservedSharedMemPerBlock;
   long smem_total = per_block < per_sm ? per_block : per_sm;
   smem_total = smem_total / 128 * 128;
-  if (smem_total < smem_state + 1024) {
+  if (smem_arena > smem_total / 4) smem_arena = (int)(smem_total / 4) / 128 * 128;
+  if (smem_total < smem_state + smem_arena + 1024) {
     set_error_text("not enough shared memory per PE");
     return CHARMING_ERR_CONFIG;
   }
@@ -313,7 +318,7 @@ int charming_init(const charming_config* cfg_in) {
   g.inf.n_sms = n_sms;
   g.inf.threads_per_pe = cfg.threads_per_pe;
   g.inf.smem_bytes_per_pe = (int)smem_total;
-  g.inf.smem_scratch_bytes = (int)smem_total - smem_state;
+  g.inf.smem_scratch_bytes = (int)smem_total - smem_state - smem_arena;
   g.inf.regs_per_thread = fa.numRegs;
   g.inf.stack_bytes = (uint64_t)stack_eff;
   g.inf.local_bytes = (uint64_t)fa.localSizeBytes;
@@ -330,6 +335,7 @@ int charming_init(const charming_config* cfg_in) {
   ds.stash_bytes = (cfg.stash_bytes + 127) / 128 * 128;
   ds.stash_entries = cfg.stash_entries;
   ds.smem_state_bytes = smem_state;
+  ds.smem_arena_bytes = smem_arena;
   ds.smem_total = (unsigned long long)smem_total;
   ds.deadline_ns = (unsigned long long)(cfg.deadline_s * 1e9);
   ds.idle_timeout_ns = (unsigned long long)(cfg.idle_timeout_s * 1e9);

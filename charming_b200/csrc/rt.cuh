@@ -24,6 +24,8 @@ namespace rt {
 constexpr int CELL = 32;                 // ring cell, bytes
 constexpr int HDR = 32;                  // envelope (16) + regular_msg (16)
 constexpr int MAX_THREADS = 512;         // launch bound of the scheduler
+constexpr int PROXY_CACHE = 16;          // proxies per PE looked up on chip
+constexpr int SMEM_OBJ_MAX = 4096;       // larger objects skip the on-chip arena
 
 struct alignas(128) line_u64 {
   unsigned long long v;
@@ -66,6 +68,7 @@ struct device_state {
   unsigned long long stash_bytes;      // arena bytes per PE
   int stash_entries;                   // descriptors per PE
   int smem_state_bytes;                // bytes of dynamic smem the runtime keeps
+  int smem_arena_bytes;                // then this much for the on-chip object arena
   unsigned long long smem_total;       // dynamic smem bytes per PE
   unsigned long long deadline_ns;      // run limit, relative to kernel start
   unsigned long long idle_timeout_ns;  // no delivery anywhere for this long
@@ -123,6 +126,8 @@ struct pe_state {
   unsigned long long idle_polls_since_check;
   unsigned long long busy_polls;       // messages found waiting (end-of-run checks every 64)
   unsigned long long arena_top;        // bytes of this PE's arena handed out this run
+  unsigned long long sarena_top;       // bytes of the on-chip arena handed out this run
+  chare_proxy_base* pcache[PROXY_CACHE];  // proxies[0..PROXY_CACHE) of this PE's table
   // batched sends (alloc_user_msgs): per message start, ticket, bytes
   void* bm_ptr[MSG_BATCH_MAX];
   unsigned long long bm_tick[MSG_BATCH_MAX];

@@ -61,9 +61,22 @@ __device__ void charm::detail::report_error(int code, int info0, int info1) {
   set_error(code, info0, info1);
 }
 
+namespace {
+__device__ __forceinline__ unsigned char* smem_arena() {
+  return reinterpret_cast<unsigned char*>(s_mem) + c_rt.smem_state_bytes;
+}
+}  // namespace
+
 __device__ void* charm::detail::pe_alloc(size_t bytes) {
-  if (!c_rt.arena) return nullptr;
   pe_state* ps = pes();
+  if (bytes <= (size_t)SMEM_OBJ_MAX && c_rt.smem_arena_bytes > 0) {
+    unsigned long long at = (ps->sarena_top + 15) & ~15ULL;
+    if (at + bytes <= (unsigned long long)c_rt.smem_arena_bytes) {
+      ps->sarena_top = at + bytes;
+      return smem_arena() + at;
+    }
+  }
+  if (!c_rt.arena) return nullptr;
   unsigned long long at = (ps->arena_top + 15) & ~15ULL;
   if (at + bytes > c_rt.arena_bytes) return nullptr;
   ps->arena_top = at + bytes;
@@ -72,7 +85,12 @@ __device__ void* charm::detail::pe_alloc(size_t bytes) {
 
 __device__ bool charm::detail::pe_owns(const void* p) {
   const unsigned char* b = static_cast<const unsigned char*>(p);
+  if (b >= smem_arena() && b < smem_arena() + c_rt.smem_arena_bytes) return true;
   return c_rt.arena && b >= c_rt.arena && b < c_rt.arena + (unsigned long long)c_rt.n_pes * c_rt.arena_bytes;
+}
+
+__device__ void charm::detail::cache_proxy(int id, chare_proxy_base* p) {
+  if (id >= 0 && id < PROXY_CACHE) pes()->pcache[id] = p;
 }
 
 __device__ chare_proxy_table& charm::detail::my_proxy_table() {
@@ -104,7 +122,7 @@ __device__ int charm::device_atoi(const char* str, int strlen) {
 }
 
 __device__ void* charm::smem_scratch(size_t* bytes) {
-  size_t off = (size_t)c_rt.smem_state_bytes;
+  size_t off = (size_t)c_rt.smem_state_bytes + (size_t)c_rt.smem_arena_bytes;
   if (bytes) *bytes = (size_t)c_rt.smem_total - off;
   return reinterpret_cast<char*>(s_mem) + off;
 }
@@ -212,8 +230,11 @@ __device__ unsigned char* reserve(int dst, unsigned long long bytes, unsigned lo
   return ring_cell(dst, t);
 }
 
+// The release store alone orders the message before its flag: the
+// payload written by other threads of the block is ordered before it by
+// the barrier the callers pass first (release is cumulative), and a separate
+// fence would also invalidate the SM's L1.
 __device__ __forceinline__ void publish(int dst, unsigned long long ticket) {
-  __threadfence();
   st_release_u64(ring_flag(dst, ticket), ticket + 1);
 }
 
@@ -446,7 +467,7 @@ __device__ void stash_revive() {
     for (unsigned long long i = kh + threadIdx.x; i < kt; i += blockDim.x) {
       stash_key* k = keys + (i % S);
       if (k->state == KEY_WAIT) {
-        chare_proxy_base* p = tb.proxies[k->chare_id];
+        chare_proxy_base* p = k->chare_id < PROXY_CACHE ? ps->pcache[k->chare_id] : tb.proxies[k->chare_id];
         if (p->refnum_matches(k->chare_idx, k->refnum)) {
           k->state = KEY_READY;
           cnt++;
@@ -490,7 +511,8 @@ __device__ void stash_dispatch_ready() {
   }
   stash_key* k = keys + (idx % S);
   unsigned char* env = arena_of(blockIdx.x) + (k->data_off % A);
-  chare_proxy_base* p = c_rt.proxy_tables[blockIdx.x].proxies[k->chare_id];
+  chare_proxy_base* p = k->chare_id < PROXY_CACHE ? ps->pcache[k->chare_id]
+                                                   : c_rt.proxy_tables[blockIdx.x].proxies[k->chare_id];
   if (threadIdx.x == 0) ps->b_i0 = p->refnum_matches(k->chare_idx, k->refnum) ? 1 : 0;
   __syncthreads();
   int go = ps->b_i0;
@@ -499,7 +521,7 @@ __device__ void stash_dispatch_ready() {
   __syncthreads();
   if (go) {
     const regular_msg* rm = reinterpret_cast<const regular_msg*>(env + sizeof(envelope));
-    p->call(k->chare_idx, rm->ep_id, env + HDR, k->refnum);
+    p->call_fn(p, k->chare_idx, rm->ep_id, env + HDR);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -595,10 +617,14 @@ __device__ void dispatch_inbox() {
       set_error(CHARMING_ERR_BAD_MSG, env->src_pe, (int)type);
       size = CELL;
     } else if (type == (int)msgtype::regular || type == (int)msgtype::user) {
-      chare_proxy_table& tb = c_rt.proxy_tables[me];
       int cid = rm->chare_id;
-      if (cid < 0 || cid >= tb.count || (p = tb.proxies[cid]) == nullptr ||
-          !p->valid_target(rm->chare_idx, rm->ep_id)) {
+      if (cid >= 0 && cid < PROXY_CACHE) {
+        p = ps->pcache[cid];  // on chip
+      } else {
+        chare_proxy_table& tb = c_rt.proxy_tables[me];
+        p = (cid >= 0 && cid < tb.count) ? tb.proxies[cid] : nullptr;
+      }
+      if (p == nullptr || !p->valid_target(rm->chare_idx, rm->ep_id)) {
         set_error(CHARMING_ERR_BAD_TARGET, cid, rm->chare_idx);
       } else {
         action = p->refnum_matches(rm->chare_idx, rm->refnum) ? 0 : 1;
@@ -626,7 +652,7 @@ __device__ void dispatch_inbox() {
   // slots: every thread must have read them first.
   __syncthreads();
   if (action == 0) {
-    p->call(idx, ep, m + HDR, ref);
+    p->call_fn(p, idx, ep, m + HDR);
   } else if (action == 1) {
     stash_put(m, size, cid, idx, ref, src);
   }
@@ -688,6 +714,8 @@ charming_scheduler_kernel(int argc, char** argv, size_t* argvs) {
     ps->idle_polls_since_check = 0;
     ps->busy_polls = 0;
     ps->arena_top = 0;
+    ps->sarena_top = 0;
+    for (int i = 0; i < PROXY_CACHE; i++) ps->pcache[i] = nullptr;
   }
   for (int i = threadIdx.x; i < c_rt.n_pes; i += blockDim.x) head_cache()[i] = c_rt.head[i].v;
   __syncthreads();

@@ -58,6 +58,23 @@ struct mismatch_t {
   __device__ mismatch_t() : found_idx(-1) {}
 };
 
+namespace detail {
+// Per-PE bump allocator for the runtime's own objects (proxies, chare
+// objects, their tables): small objects go to a shared-memory arena of the
+// PE block, the rest to a per-PE region of device memory; reset at every
+// run, nothing freed one by one. Single-threaded. Returns nullptr when both
+// are exhausted (callers fall back to the device heap). Objects in shared
+// memory keep their cached state when a gpu-scope acquire (every inbox poll)
+// invalidates the SM's L1.
+__device__ void* pe_alloc(size_t bytes);
+// Whether p came from a PE arena (then it is not handed to free()).
+__device__ bool pe_owns(const void* p);
+}  // namespace detail
+
+struct chare_proxy_base;
+// Entry method `ep` of local chare `idx` on `arg` (all threads of the block).
+typedef bool (*proxy_call_fn)(chare_proxy_base* proxy, int idx, int ep, void* arg);
+
 struct chare_proxy_base {
   int id;        // Chare array ID (registration order on this PE)
 
@@ -75,9 +92,21 @@ struct chare_proxy_base {
   int* refnum;   // Reference numbers of local chares
   mismatch_t* mismatches;
 
+  proxy_call_fn call_fn;  // direct dispatch (no virtual call on the hot path)
+
   __device__ chare_proxy_base() : id(-1), n_local(0), n_total(0), start_idx(-1),
   end_idx(-1), loc_map(nullptr), em_count(0), async_waits(nullptr),
-  refnum(nullptr), mismatches(nullptr) {}
+  refnum(nullptr), mismatches(nullptr), call_fn(nullptr) {}
+
+  // Proxies come from the PE arena (shared memory when there is room), so
+  // the scheduler's per-message reads of them stay on chip.
+  __device__ static void* operator new(size_t bytes) {
+    void* p = detail::pe_alloc(bytes);
+    return p ? p : malloc(bytes);
+  }
+  __device__ static void operator delete(void* p) {
+    if (p && !detail::pe_owns(p)) free(p);
+  }
 
   // Runs entry method ep of local chare idx on arg (all threads of the PE
   // block). The scheduler decides the refnum match (refnum_matches, the
@@ -118,13 +147,8 @@ enum : int {
   ERR_TOO_MANY_EMS = 11,
   ERR_NO_MEMORY = 17,
 };
-// Per-PE bump allocator for the runtime's own objects (proxy tables, chare
-// objects): reset at every run, nothing freed one by one. Single-threaded.
-// Returns nullptr when the PE's arena is exhausted (callers fall back to the
-// device heap).
-__device__ void* pe_alloc(size_t bytes);
-// Whether p came from some PE's arena (then it is not handed to free()).
-__device__ bool pe_owns(const void* p);
+// Registers proxy `id` in the scheduler's on-chip lookup cache.
+__device__ void cache_proxy(int id, chare_proxy_base* p);
 template <class T>
 __device__ T* pe_array(size_t n) {  // trivially constructible T
   void* p = pe_alloc(n * sizeof(T));
@@ -151,12 +175,16 @@ __device__ int my_pe();
 
 template <typename C>
 struct chare_proxy : chare_proxy_base {
-  C** objects;                           // Local chare objects
-  entry_method_base<C>** entry_methods;  // Entry method table
+  typedef void (*em_fn_t)(C&, void*);
+  C** objects;     // Local chare objects
+  em_fn_t* em_fn;  // Entry method table: the functions themselves (the
+                   // reference keeps entry_method objects with a virtual
+                   // call operator; a function pointer saves the vtable
+                   // loads per message)
 
   // Registers this proxy in the calling PE's table (single-threaded).
   __device__ chare_proxy()
-    : chare_proxy_base(), objects(nullptr), entry_methods(nullptr) {
+    : chare_proxy_base(), objects(nullptr), em_fn(nullptr) {
     chare_proxy_table& table = detail::my_proxy_table();
     if (table.count >= CHARE_TYPE_CNT_MAX) {
       detail::report_error(detail::ERR_TOO_MANY_TYPES, table.count, 0);
@@ -164,23 +192,26 @@ struct chare_proxy : chare_proxy_base {
     }
     id = table.count++;
     table.proxies[id] = this;
-    entry_methods = detail::pe_array<entry_method_base<C>*>(EM_CNT_MAX);
-    if (entry_methods == nullptr) detail::report_error(detail::ERR_NO_MEMORY, id, 0);
+    detail::cache_proxy(id, this);
+    call_fn = &chare_proxy<C>::call_static;
+    em_fn = detail::pe_array<em_fn_t>(EM_CNT_MAX);
+    if (em_fn == nullptr) detail::report_error(detail::ERR_NO_MEMORY, id, 0);
   }
 
   // Add entry method to table (single-threaded)
   template <void Func(C&, void*)>
   __device__ void add_entry_method() {
-    if (entry_methods == nullptr || em_count >= EM_CNT_MAX) {
+    if (em_fn == nullptr || em_count >= EM_CNT_MAX) {
       detail::report_error(detail::ERR_TOO_MANY_EMS, id, em_count);
       return;
     }
-    entry_method_base<C>* em = detail::pe_make<entry_method<C, Func>>();
-    if (em == nullptr) {
-      detail::report_error(detail::ERR_NO_MEMORY, id, em_count);
-      return;
-    }
-    entry_methods[em_count++] = em;
+    em_fn[em_count++] = Func;
+  }
+
+  __device__ static bool call_static(chare_proxy_base* base, int idx, int ep, void* arg) {
+    chare_proxy<C>* self = static_cast<chare_proxy<C>*>(base);
+    self->em_fn[ep](*(self->objects[idx - self->start_idx]), arg);
+    return true;
   }
 
   // Create the chare array on every PE (single-threaded; called by each PE).
@@ -237,9 +268,7 @@ struct chare_proxy : chare_proxy_base {
 
   __device__ virtual bool call(int idx, int ep, void* arg, int ref) {
     (void)ref;
-    int local_idx = idx - start_idx;
-    (*(entry_methods[ep]))(*(objects[local_idx]), arg);
-    return true;
+    return call_static(this, idx, ep, arg);
   }
 
   __device__ virtual void release_all() {
@@ -247,14 +276,11 @@ struct chare_proxy : chare_proxy_base {
     detail::pe_free_array(objects);
     detail::pe_free_array(refnum);
     detail::pe_free_array(loc_map);
-    if (entry_methods) {
-      for (int e = 0; e < em_count; e++) detail::pe_destroy(entry_methods[e]);
-      detail::pe_free_array(entry_methods);
-    }
+    detail::pe_free_array(em_fn);
     objects = nullptr;
     refnum = nullptr;
     loc_map = nullptr;
-    entry_methods = nullptr;
+    em_fn = nullptr;
     n_local = 0;
     em_count = 0;
   }

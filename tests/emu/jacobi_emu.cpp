@@ -354,6 +354,7 @@ namespace detail {
 void* pe_alloc(size_t) { return nullptr; }  // the device heap (new) serves every object here
 bool pe_owns(const void*) { return false; }
 chare_proxy_table& my_proxy_table() { return me_pe().table; }
+void cache_proxy(int, chare_proxy_base*) {}
 void report_error(int code, int a, int b) { rt::set_error(code, a, b); }
 }  // namespace detail
 

@@ -178,6 +178,7 @@ void init_runtime(int n_pes, size_t ring_bytes) {
   ds.stash_entries = 4096;
   ds.smem_state_bytes = (int)((sizeof(pe_state) + 8ull * n_pes + 127) / 128 * 128);
   ds.smem_total = SMEM_BYTES;
+  ds.smem_arena_bytes = 8 << 10;
   ds.deadline_ns = 60ull * 1000000000ull;
   ds.idle_timeout_ns = 5ull * 1000000000ull;
   ds.tail = zalloc<line_u64>(n_pes);
