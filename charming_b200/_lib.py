@@ -15,6 +15,9 @@ LIB_DIR = os.path.join(_HERE, "lib")
 # CHARMING_CHECKED=1 selects the build with invariant checks (make CHECKS=1).
 LIB_PATH = os.path.join(LIB_DIR, "libcharming_b200_checked.so"
                         if os.environ.get("CHARMING_CHECKED") == "1" else "libcharming_b200.so")
+# CHARMING_LIB: path of another build of the same library (e.g. one compiled
+# with a different register limit).
+LIB_PATH = os.environ.get("CHARMING_LIB", LIB_PATH)
 
 u64 = C.c_uint64
 i32 = C.c_int
@@ -55,7 +58,7 @@ class Stats(C.Structure):
         ("delivered", u64), ("sent", u64), ("stashed", u64), ("revived", u64),
         ("bytes_sent", u64), ("idle_polls", u64), ("space_waits", u64),
         ("kernel_ms", f64), ("loop_ms", f64), ("main_ms", f64), ("status", i32), ("err_pe", i32),
-        ("err_info0", i32), ("err_info1", i32),
+        ("err_info0", i32), ("err_info1", i32), ("idle_ms", f64),
     ]
 
 

@@ -8,8 +8,8 @@ runs in one scheduler launch replayed from a captured CUDA graph
 (``Jacobi2D(use_graph=True)``).
 
 ``autotune`` times the set under each candidate configuration -- chare
-block side (64, 128, 256), PEs per SM (1 block of 512 threads or 2 of 256)
-and inbox ring depth -- and returns the fastest. Every candidate computes
+block side (64, 128, 256), PEs per SM (1 block of 512 threads, 2 of 256 or
+4 of 128) and inbox ring depth -- and returns the fastest. Every candidate computes
 bit-identical results (the decomposition only changes where a point is
 updated, not its arithmetic), so the choice is free to follow speed alone.
 """
@@ -90,7 +90,7 @@ class TuneResult:
 
 def default_candidates() -> list[Candidate]:
     return [Candidate(s, p, r) for s, p, r in
-            itertools.product((64, 128, 256), (1, 2), (1 << 20, 4 << 20))]
+            itertools.product((64, 128, 256), (1, 2, 4), (1 << 20, 4 << 20))]
 
 
 def time_set(problems, dtype: str, chare_side: int, runs: int = 2, warmup: int = 1,

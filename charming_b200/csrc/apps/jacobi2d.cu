@@ -126,6 +126,14 @@ struct JServer : charm::chare {
 };
 
 __shared__ charm::chare_proxy<JBlock>* jproxy;
+// This PE's phase timers (ns: sweeps, halo sending, halo entry methods),
+// kept on chip and stored through to japp::pe_ns() after every update (a
+// store only: no read of global memory on the message path).
+__shared__ unsigned long long s_pe_ns[3];
+__device__ __forceinline__ void add_pe_ns(int k, unsigned long long ns) {
+  s_pe_ns[k] += ns;
+  japp::pe_ns()[4 * blockIdx.x + k] = s_pe_ns[k];
+}
 __shared__ charm::chare_proxy<JServer>* sproxy;
 
 template <typename T>
@@ -185,7 +193,7 @@ __device__ double sweep_block(const jac::chare_desc& d, int cur, bool resid, int
                 : jac::sweep_direct<T, false>(in, out, d.w, d.h);
     __syncthreads();
   }
-  if (threadIdx.x == 0) japp::pe_ns()[4 * blockIdx.x] += charm::now_ns() - t0;
+  if (threadIdx.x == 0) add_pe_ns(0, charm::now_ns() - t0);
   return resid ? suite::block_sum_f64(acc) : 0.0;
 }
 
@@ -280,7 +288,7 @@ __device__ void send_halos(JBlock& c, const jac::chare_desc& d) {
     copy_rects<T>(view<T>(d, c.cur), e, vals, n, false);
     jproxy->invoke_msgs(idx, EP_HALO, msg, bytes, refs, n);
   }
-  if (threadIdx.x == 0) japp::pe_ns()[4 * blockIdx.x + 1] += charm::now_ns() - t0;
+  if (threadIdx.x == 0) add_pe_ns(1, charm::now_ns() - t0);
 }
 
 // Halo of pass hh->pass -> ghost zone of buf[pass & 1]. All threads.
@@ -487,6 +495,7 @@ __device__ void em_decision(JBlock& c, void* arg) {
 
 __device__ void suite::jacobi2d_main(int pe) {
   if (threadIdx.x == 0) {
+    s_pe_ns[0] = s_pe_ns[1] = s_pe_ns[2] = 0;
     jproxy = new charm::chare_proxy<JBlock>();
     jproxy->add_entry_method<&em_start>();
     jproxy->add_entry_method<&em_halo>();

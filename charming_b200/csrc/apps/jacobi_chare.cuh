@@ -234,7 +234,7 @@ __device__ void em_halo_t(JBlock& c, void* arg) {
     (void)CHARM_VERIFY(c.got[hh->pass & 1] <= jac::N_DIRS, CHARMING_ERR_APP, 4000 + c.got[hh->pass & 1], c.i);
   }
   __syncthreads();
-  if (threadIdx.x == 0) japp::pe_ns()[4 * blockIdx.x + 2] += charm::now_ns() - t_em;
+  if (threadIdx.x == 0) add_pe_ns(2, charm::now_ns() - t_em);
   if (c.started) pump<T>(c, d);  // a halo may overtake the start message
 }
 

@@ -102,7 +102,9 @@ __device__ __forceinline__ double compute_vec(const T* up, const T* mid, const T
       *reinterpret_cast<float4*>(out) = make_float4((float)o[0], (float)o[1], (float)o[2], (float)o[3]);
     }
   } else {
-    for (int k = 0; k < nvalid; k++) out[k] = o[k];
+    #pragma unroll
+    for (int k = 0; k < V; k++)  // static indices keep o[] in registers
+      if (k < nvalid) out[k] = o[k];
   }
   return acc;
 }
@@ -306,7 +308,9 @@ __device__ __forceinline__ double walk_compute(const walk_row<T, J>& U, const wa
         else ov = make_float4((float)o[0], (float)o[1], (float)o[2], (float)o[3]);
         *reinterpret_cast<VT*>(op) = ov;
       } else {
-        for (int k = 0; k < nvalid; k++) op[k] = o[k];
+        #pragma unroll
+        for (int k = 0; k < V; k++)  // static indices keep o[] in registers
+          if (k < nvalid) op[k] = o[k];
       }
     }
   }
@@ -451,7 +455,9 @@ __device__ __forceinline__ void deep_step(typename vec_of<T>::type (&W)[L][3], i
         if (nvalid >= V) {
           *reinterpret_cast<VT*>(op) = vec_from(o);
         } else {
-          for (int k = 0; k < nvalid; k++) op[k] = o[k];
+          #pragma unroll
+        for (int k = 0; k < V; k++)  // static indices keep o[] in registers
+          if (k < nvalid) op[k] = o[k];
         }
       }
     } else {

@@ -144,6 +144,9 @@ int collect_run(double kernel_ms) {
     if (t[2] > tmax) tmax = t[2];
   }
   s.loop_ms = (tmax > tmin && tmin != ~0ULL) ? (tmax - tmin) * 1e-6 : 0.0;
+  double idle = 0;
+  for (int p = 0; p < g.inf.n_pes; p++) idle += (double)st[(size_t)p * N_STATS + ST_IDLE_NS];
+  s.idle_ms = g.inf.n_pes ? idle / g.inf.n_pes * 1e-6 : 0.0;
   s.main_ms = main_max * 1e-6;
   s.kernel_ms = kernel_ms;
   s.status = ctrl_h[CTRL_STATUS];
@@ -292,6 +295,12 @@ int charming_init(const charming_config* cfg_in) {
   long per_sm = (long)g.prop.sharedMemPerMultiprocessor / cfg.pes_per_sm -
                 (long)fa.sharedSizeBytes - (long)g.prop.reservedSharedMemPerBlock;
   long smem_total = per_block < per_sm ? per_block : per_sm;
+  // A cap leaves the rest of the SM's 256 KB of L1/shared storage to the L1
+  // cache (local memory and global loads).
+  if (const char* ev = getenv("CHARMING_SMEM_PER_PE")) {
+    long cap = strtol(ev, nullptr, 10);
+    if (cap > 0 && cap < smem_total) smem_total = cap;
+  }
   smem_total = smem_total / 128 * 128;
   if (smem_arena > smem_total / 4) smem_arena = (int)(smem_total / 4) / 128 * 128;
   if (smem_total < smem_state + smem_arena + 1024) {

@@ -23,7 +23,10 @@ namespace rt {
 
 constexpr int CELL = 32;                 // ring cell, bytes
 constexpr int HDR = 32;                  // envelope (16) + regular_msg (16)
-constexpr int MAX_THREADS = 512;         // launch bound of the scheduler
+#ifndef CHARMING_MAX_THREADS
+#define CHARMING_MAX_THREADS 512
+#endif
+constexpr int MAX_THREADS = CHARMING_MAX_THREADS;  // launch bound of the scheduler
 constexpr int PROXY_CACHE = 16;          // proxies per PE looked up on chip
 constexpr int SMEM_OBJ_MAX = 4096;       // larger objects skip the on-chip arena
 
@@ -54,7 +57,8 @@ enum : int {
   ST_IDLE_POLLS,      // empty inbox polls
   ST_SPACE_WAITS,     // sends that waited for ring space
   ST_LOOP_NS,         // ns spent in the scheduler loop
-  N_STATS = 8
+  ST_IDLE_NS,         // ns spent waiting on an empty inbox
+  N_STATS = 9
 };
 
 // Device-wide runtime description, copied to __constant__ memory before each

@@ -561,8 +561,10 @@ __device__ int poll_inbox() {
   unsigned long long h = ps->head;
   const unsigned long long* f = ring_flag(me, h);
   unsigned int spins = 0;
+  unsigned long long idle_t0 = 0;
   while (true) {
     if (ld_acquire_u64(f) == h + 1) {
+      if (idle_t0) ps->stats[ST_IDLE_NS] += globaltimer() - idle_t0;
       // a PE that always has a message (a chare that keeps calling itself)
       // still sees the end of the run and its deadline
       if ((++ps->busy_polls & 63) == 0) {
@@ -575,6 +577,7 @@ __device__ int poll_inbox() {
       return 1;
     }
     if (ps->term || terminated()) return 0;
+    if (!idle_t0) idle_t0 = globaltimer();
     ++spins;
     if ((spins & 255) == 0) {
       unsigned long long now = globaltimer();

@@ -118,6 +118,8 @@ typedef struct charming_stats {
                                 (charm::main, chare creation, barriers)  */
   int status;                /* status code of the run                   */
   int err_pe, err_info0, err_info1;
+  double idle_ms;            /* mean over PEs: time waiting on an empty
+                                inbox                                    */
 } charming_stats;
 int charming_last_stats(charming_stats* out);
 

@@ -24,7 +24,7 @@ def test_uneven_set_is_seeded_and_in_range():
 def test_autotune_candidates_are_valid_configs():
     cands = default_candidates()
     assert {c.chare_side for c in cands} == {64, 128, 256}
-    assert {c.pes_per_sm for c in cands} == {1, 2}
+    assert {c.pes_per_sm for c in cands} == {1, 2, 4}
     for c in cands:
         cfg = c.runtime_config()
         assert cfg["threads_per_pe"] * cfg["pes_per_sm"] == 512
