@@ -157,10 +157,16 @@ def cpu_baseline(target_s: float = 12.0, threads: int | None = None) -> dict:
     threads = threads or os.cpu_count() or 1
     os.environ.setdefault("OMP_PROC_BIND", "close")
     g = initial_grid(NX, NY, (1.0, 0.0, 0.0, 0.0))
-    oj.jacobi2d(g, 1, threads=threads)  # thread pool and pages warm
-    t0 = time.perf_counter()
-    oj.jacobi2d(g, 4, threads=threads)
-    t1 = (time.perf_counter() - t0) / 4
+    oj.jacobi2d(g, 2, threads=threads)  # thread pool and pages warm
+    n, t1 = 8, 0.0
+    while True:  # calibrate on runs of at least ~1 s
+        t0 = time.perf_counter()
+        oj.jacobi2d(g, n, threads=threads)
+        dt0 = time.perf_counter() - t0
+        t1 = dt0 / n
+        if dt0 > 1.0 or n >= 4096:
+            break
+        n *= 4
     sweeps = int(max(4, min(20000, target_s / max(t1, 1e-6))))
     t0 = time.perf_counter()
     oj.jacobi2d(g, sweeps, threads=threads)
@@ -194,7 +200,9 @@ def set_workload(n: int, sweeps: int) -> None:
     SWEEPS = sweeps
 
 
-def dist_setup():
+def dist_setup(backend: str | None = None):
+    """Replica ranks from the torchrun environment: NCCL on GPUs, gloo
+    without one (the CPU tests of this plumbing)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -204,16 +212,24 @@ def dist_setup():
 
     import torch
     import torch.distributed as dist
-    torch.cuda.set_device(local)
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if backend is None:
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return dist, rank, local, world
 
 
+def _on_gpu(dist) -> bool:
+    return dist.get_backend() == "nccl"
+
+
 def dist_max(dist, x: float, local: int) -> float:
+    """Max over ranks (the job's time is its slowest rank's)."""
     if dist is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}" if _on_gpu(dist) else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -221,8 +237,17 @@ def dist_max(dist, x: float, local: int) -> float:
 def barrier(dist, local: int) -> None:
     if dist is not None:
         import torch
-        dist.barrier(device_ids=[local])
-        torch.cuda.synchronize(local)
+        if _on_gpu(dist):
+            dist.barrier(device_ids=[local])
+            torch.cuda.synchronize(local)
+        else:
+            dist.barrier()
+
+
+def replica_value(lups_per_rank_step: float, steps: int, world: int, max_ms: float) -> float:
+    """Whole-job GLUP/s of N replicas: all ranks' updates over the slowest
+    rank's time."""
+    return lups_per_rank_step * steps * world / (max_ms * 1e-3) / 1e9
 
 
 def traffic_from_profiles(workload: str):
@@ -500,7 +525,7 @@ def main() -> int:
     clocks = clk.summary()
     stats = rt.last_stats()
     lups = NX * NY * SWEEPS
-    value = lups * args.steps * world / (total_ms * 1e-3) / 1e9
+    value = replica_value(lups, args.steps, world, total_ms)
     info = j.info()
     msgs_per_s = info["halo_msgs_per_sweep"] * SWEEPS * args.steps / (total_ms * 1e-3)
 

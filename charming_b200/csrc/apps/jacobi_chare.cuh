@@ -130,6 +130,9 @@ __device__ void pump(JBlock& c, const jac::chare_desc& d) {
   const jac::prob_desc& p = c.prob;
   __shared__ int s_act;
   enum { IDLE = 0, SEND = 1, FIN = 2, SWEEP = 3, SELF = 4 };
+  // lattice updates a chare without neighbours may run in one entry method
+  // (a message round trip costs about as much as 20 K of them)
+  long long self_budget = 1ll << 18;
   while (true) {
     if (threadIdx.x == 0) {
       int act = IDLE;
@@ -176,8 +179,13 @@ __device__ void pump(JBlock& c, const jac::chare_desc& d) {
     if (act == SEND) {
       send_halos<T>(c, d);
     } else if (act == SELF) {
-      // no neighbours: one sweep per message, so other chares of the PE run
-      // in between
+      // no neighbours: passes back to back up to a work budget, then one
+      // message to itself, so other chares of the PE run in between
+      if (self_budget > 0) {
+        self_budget -= (long long)d.w * d.h * pass_len(d, p, c.iter);
+        advance<T>(c, d);
+        continue;
+      }
       int it = c.pass;
       jproxy->invoke(c.i, EP_CONT, &it, sizeof(int));
       return;

@@ -611,8 +611,10 @@ int run(int nx, int ny, int px, int py, int max_sweeps, int K, double tol, int n
   std::vector<std::thread> th;
   for (int p = 0; p < n_pes; p++)
     for (int t = 0; t < threads; t++) th.emplace_back(pe_thread, p, t, seed);
-  // watchdog: stop when nothing was delivered for 3 s; a block that does
-  // not leave its loop 5 s after that is stuck in a barrier
+  // watchdog: stop when nothing was delivered for 20 s (one entry method
+  // may run many passes of a chare without neighbours, slowly under the
+  // sanitizers); a block that does not leave its loop 5 s after that is
+  // stuck in a barrier
   long long last = -1;
   auto t_last = std::chrono::steady_clock::now();
   while (!g_term) {
@@ -621,7 +623,7 @@ int run(int nx, int ny, int px, int py, int max_sweeps, int K, double tol, int n
     if (now_p != last) {
       last = now_p;
       t_last = std::chrono::steady_clock::now();
-    } else if (std::chrono::steady_clock::now() - t_last > std::chrono::seconds(3)) {
+    } else if (std::chrono::steady_clock::now() - t_last > std::chrono::seconds(20)) {
       charm::rt::set_error(CHARMING_ERR_IDLE_TIMEOUT, 0, 0);
     }
   }
