@@ -447,10 +447,11 @@ def run_suites(args, headline_glups: float) -> dict:
 
 
 def exchange_depth(args) -> int:
-    """Sweeps per halo exchange the run uses (the library's choice for 0)."""
+    """Sweeps per halo exchange the run uses (the library's choice for 0:
+    6 without residual checks)."""
     if args.pipeline:
         return 1
-    return min(args.depth if args.depth > 0 else 4, 4)
+    return min(args.depth if args.depth > 0 else 6, 8)
 
 
 def workload_config(args, decomp) -> dict:
@@ -478,7 +479,7 @@ def main() -> int:
     ap.add_argument("--sweeps", type=int, default=SWEEPS)
     ap.add_argument("--tile-w", type=int, default=0)
     ap.add_argument("--depth", type=int, default=0,
-                    help="sweeps per halo exchange (ghost depth), 0: 4 (direct) / 1 (TMA)")
+                    help="sweeps per halo exchange (ghost depth), 0: 6 (direct) / 1 (TMA)")
     ap.add_argument("--small-buffers", action="store_true",
                     help="1 MiB inbox rings and stashes (smaller device footprint for ncu)")
     ap.add_argument("--headline-only", action="store_true",

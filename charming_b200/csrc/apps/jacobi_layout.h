@@ -39,9 +39,21 @@ struct layout {
   uint64_t halo_msgs = 0;               // halo messages per exchange
 };
 
-// Ghost depth of a problem whose smallest chare is wmin x hmin.
-inline int choose_depth(int requested, int pipeline, int wmin, int hmin, int off) {
-  int d = requested > 0 ? requested : (pipeline ? 1 : DEPTH_MAX);
+// Sweeps per exchange chosen when none is requested: deeper passes mean
+// fewer messages, but the wavefront's registers spill beyond this.
+constexpr int DEPTH_AUTO = 6;
+
+// Ghost depth of a problem whose smallest chare is wmin x hmin. Automatic
+// choice: DEPTH_AUTO, or with a residual period K the balanced split of K
+// into passes of at most DEPTH_AUTO (passes end at every check, so K = 10
+// runs passes of 5 + 5 instead of 6 + 4).
+inline int choose_depth(int requested, int pipeline, int wmin, int hmin, int off, int check_every = 0) {
+  int auto_d = DEPTH_AUTO;
+  if (check_every > 0) {
+    const int n = (check_every + DEPTH_AUTO - 1) / DEPTH_AUTO;
+    auto_d = (check_every + n - 1) / n;
+  }
+  int d = requested > 0 ? requested : (pipeline ? 1 : auto_d);
   if (pipeline) d = 1;  // the bulk-copy sweep runs one sweep per exchange
   d = std::min(d, DEPTH_MAX);
   d = std::min(d, std::min(wmin, hmin));
@@ -79,7 +91,7 @@ inline bool build_layout(const charming_jacobi_problem* probs, int n, int side, 
     L->px.push_back(px);
     L->py.push_back(py);
     const int wmin = q.nx / px, hmin = q.ny / py;
-    const int D = choose_depth(depth_req, pipeline, wmin, hmin, off);
+    const int D = choose_depth(depth_req, pipeline, wmin, hmin, off, q.check_every);
     int base = (int)raw.size();
     root_raw[p] = base;
     int nc = px * py;

@@ -633,6 +633,10 @@ __device__ __noinline__ double sweep_deep(block_view<T> in, block_view<T> out, i
   VT* ring = rings + (size_t)warp * P * 32;
   if (L == 2) return sweep_deep_items<T, RESID, 2>(in, out, w, h, fixed, ring, nw, warp, lane);
   if (L == 3) return sweep_deep_items<T, RESID, 3>(in, out, w, h, fixed, ring, nw, warp, lane);
+  if (L == 5) return sweep_deep_items<T, RESID, 5>(in, out, w, h, fixed, ring, nw, warp, lane);
+  if (L == 6) return sweep_deep_items<T, RESID, 6>(in, out, w, h, fixed, ring, nw, warp, lane);
+  if (L == 7) return sweep_deep_items<T, RESID, 7>(in, out, w, h, fixed, ring, nw, warp, lane);
+  if (L == 8) return sweep_deep_items<T, RESID, 8>(in, out, w, h, fixed, ring, nw, warp, lane);
   return sweep_deep_items<T, RESID, 4>(in, out, w, h, fixed, ring, nw, warp, lane);
 }
 

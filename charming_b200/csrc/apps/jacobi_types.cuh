@@ -10,7 +10,7 @@ enum dir : int {
   TOP_LEFT = 4, BOTTOM_RIGHT = 5, TOP_RIGHT = 6, BOTTOM_LEFT = 7
 };
 constexpr int N_DIRS = 8;
-constexpr int DEPTH_MAX = 4;  // sweeps per halo exchange, at most
+constexpr int DEPTH_MAX = 8;  // sweeps per halo exchange, at most
 __host__ __device__ inline int opposite(int d) { return d ^ 1; }
 __host__ __device__ inline bool dir_top(int d) { return d == TOP || d == TOP_LEFT || d == TOP_RIGHT; }
 __host__ __device__ inline bool dir_bottom(int d) {

@@ -154,10 +154,12 @@ typedef struct charming_jacobi_options {
   int halo_mode;       /* 0: halos land in the ghost ring of the sweep they
                           belong to (parity buffers); 1: halos carry refnum
                           = exchange and early ones wait in the stash       */
-  int depth;           /* sweeps per halo exchange, 1..4, with ghost zones of
+  int depth;           /* sweeps per halo exchange, 1..8, with ghost zones of
                           that depth (corners from diagonal neighbours when
-                          > 1); 0: 4 for the direct sweep, 1 for the TMA
-                          pipeline; capped by the smallest chare side.
+                          > 1); 0: 6 for the direct sweep (with a residual
+                          period K, the balanced split of K into passes of
+                          at most 6: 5 for K = 10), 1 for the TMA pipeline;
+                          capped by the smallest chare side.
                           The reference exchanges halos every sweep (1)     */
 } charming_jacobi_options;
 

@@ -75,6 +75,9 @@ def expected_stop(nx, ny, K, tol, max_sweeps, bc, dtype):
     (50, 700, 1, 9, 500, 3, 0.3, 1, 4, 1, 4, 0),
     (31, 17, 4, 2, 60, 2, 0.5, 0, 3, 0, 4, 0),
     (120, 120, 6, 6, 61, 0, 0.0, 1, 7, 1, 4, 1),
+    (96, 80, 3, 2, 3000, 10, 0.05, 1, 6, 0, 5, 1),   # depth 5: passes 5 + 5 per check
+    (200, 150, 4, 3, 43, 0, 0.0, 0, 5, 1, 5, 0),
+    (96, 80, 3, 2, 3000, 10, 0.05, 0, 6, 0, 0, 0),   # automatic depth for a period of 10
 ])
 def test_chare_code_on_cpu(emu, cfg):
     nx, ny, px, py, ms, K, tol, dt, npes, halo, depth, bal = cfg
@@ -109,6 +112,7 @@ def test_protocol_model_random_orders(px, py, K, mx, stop_at):
     (150, 90, 3, 3, 13, 4, 0.01, 1, 1, 64, 0, 0, 3),
     (300, 100, 1, 1, 17, 0, 0.0, 0, 0, 96, 0, 0, 2),
     (1100, 40, 2, 1, 9, 0, 0.0, 1, 0, 128, 0, 0, 4),
+    (48, 40, 3, 2, 300, 10, 0.2, 1, 0, 64, 0, 0, 5),
 ])
 def test_chare_code_threaded_block(emu, cfg):
     """One PE block of many threads: barriers reached from different call

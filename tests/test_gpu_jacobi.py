@@ -170,7 +170,7 @@ def test_many_chares_per_pe(rt):
     assert np.array_equal(bits(out), bits(jac64(g, 15)))
 
 
-@pytest.mark.parametrize("depth", [2, 3, 4])
+@pytest.mark.parametrize("depth", [2, 3, 4, 5, 6, 8])
 @pytest.mark.parametrize("dtype", ["f64", "f32"])
 def test_multi_sweep_passes_bit_exact(rt, depth, dtype):
     """depth sweeps per halo exchange (ghost zones of that depth, corner
