@@ -129,6 +129,7 @@ struct pe_state {
   unsigned long long stats[N_STATS];
   unsigned long long idle_polls_since_check;
   unsigned long long busy_polls;       // messages found waiting (end-of-run checks every 64)
+  unsigned long long head_pub;         // head last published to the senders
   unsigned long long arena_top;        // bytes of this PE's arena handed out this run
   unsigned long long sarena_top;       // bytes of the on-chip arena handed out this run
   chare_proxy_base* pcache[PROXY_CACHE];  // proxies[0..PROXY_CACHE) of this PE's table

@@ -207,6 +207,10 @@ __device__ unsigned char* reserve(int dst, unsigned long long bytes, unsigned lo
   // relaxed read: other threads of the block may raise hc[dst] meanwhile
   if (t + cells - ld_volatile_shared_u64(&hc[dst]) > C) {
     atomicAdd_block(&ps->stats[ST_SPACE_WAITS], 1ULL);
+    // this PE publishes its head lazily: a message to itself must not wait
+    // for space it has already consumed (ps->head is stable during an
+    // entry method; publishing it again is harmless)
+    if (dst == (int)blockIdx.x) st_release_u64(&c_rt.head[dst].v, ps->head);
     unsigned long long start = globaltimer();
     // A receiver that frees nothing for the idle timeout is taken as stuck.
     unsigned long long limit = c_rt.idle_timeout_ns ? c_rt.idle_timeout_ns : c_rt.deadline_ns;
@@ -237,6 +241,22 @@ __device__ unsigned char* reserve(int dst, unsigned long long bytes, unsigned lo
 __device__ __forceinline__ void publish(int dst, unsigned long long ticket) {
   st_release_u64(ring_flag(dst, ticket), ticket + 1);
 }
+
+// Thread 0: tell the senders how far this PE has consumed its inbox (a
+// release store: the reads of the consumed messages are done). Published
+// lazily, after an eighth of the ring or before waiting for messages.
+__device__ __forceinline__ void publish_head(pe_state* ps, int me) {
+  if (ps->head != ps->head_pub) {
+    st_release_u64(&c_rt.head[me].v, ps->head);
+    ps->head_pub = ps->head;
+  }
+}
+
+// Thread 0: the progress stamp the idle-timeout check reads.
+__device__ __forceinline__ void stamp_progress(int me) {
+  st_relaxed_u64(&c_rt.progress[me], globaltimer());
+}
+
 
 } // namespace
 
@@ -528,8 +548,7 @@ __device__ void stash_dispatch_ready() {
     ps->n_ready--;
     if (go) {
       k->state = KEY_FREE;
-      ps->stats[ST_DELIVERED]++;
-      st_relaxed_u64(&c_rt.progress[blockIdx.x], globaltimer());
+      if ((++ps->stats[ST_DELIVERED] & 15) == 0) stamp_progress(blockIdx.x);
       stash_retire();
     } else {
       k->state = KEY_WAIT;
@@ -576,8 +595,15 @@ __device__ int poll_inbox() {
       }
       return 1;
     }
-    if (ps->term || terminated()) return 0;
-    if (!idle_t0) idle_t0 = globaltimer();
+    if (ps->term || terminated()) {
+      publish_head(ps, me);
+      return 0;
+    }
+    if (!idle_t0) {  // about to wait: the senders and the idle check see where we are
+      idle_t0 = globaltimer();
+      publish_head(ps, me);
+      stamp_progress(me);
+    }
     ++spins;
     if ((spins & 255) == 0) {
       unsigned long long now = globaltimer();
@@ -662,11 +688,8 @@ __device__ void dispatch_inbox() {
   __syncthreads();
   if (threadIdx.x == 0) {
     ps->head += cells_for(size);
-    st_release_u64(&c_rt.head[me].v, ps->head);
-    if (action == 0) {
-      ps->stats[ST_DELIVERED]++;
-      st_relaxed_u64(&c_rt.progress[me], globaltimer());
-    }
+    if (ps->head - ps->head_pub >= (c_rt.ring_cells >> 3)) publish_head(ps, me);
+    if (action == 0 && (++ps->stats[ST_DELIVERED] & 15) == 0) stamp_progress(me);
   }
 }
 
@@ -709,6 +732,7 @@ charming_scheduler_kernel(int argc, char** argv, size_t* argvs) {
     ps->sent_term = 0;
     ps->revive_pending = 0;
     ps->head = c_rt.head[me].v;
+    ps->head_pub = ps->head;
     ps->t0 = globaltimer();
     ps->key_head = ps->key_tail = 0;
     ps->arena_head = ps->arena_tail = 0;
