@@ -285,7 +285,13 @@ bool mbar_test_wait(unsigned long long* b, unsigned parity) {
 }
 bool mbar_try_wait(unsigned long long* b, unsigned parity) {
   bool ok = mbar_test_wait(b, parity);
-  if (!ok) std::this_thread::yield();
+  if (!ok) {
+    // let the copy-engine thread run even when every block thread waits
+    // (the device code bounds these waits by a spin count)
+    static thread_local unsigned misses = 0;
+    if ((++misses & 63) == 0) std::this_thread::sleep_for(std::chrono::microseconds(20));
+    else std::this_thread::yield();
+  }
   return ok;
 }
 void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
