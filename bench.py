@@ -275,7 +275,7 @@ def run_reference_arm(args, rank: int) -> None:
     v = statistics.mean(s["value"] for s in samples)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": NX * NY * SWEEPS / (v * 1e9) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": workload_config(args, None),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",

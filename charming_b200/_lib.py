@@ -58,7 +58,7 @@ class Stats(C.Structure):
         ("delivered", u64), ("sent", u64), ("stashed", u64), ("revived", u64),
         ("bytes_sent", u64), ("idle_polls", u64), ("space_waits", u64),
         ("kernel_ms", f64), ("loop_ms", f64), ("main_ms", f64), ("status", i32), ("err_pe", i32),
-        ("err_info0", i32), ("err_info1", i32), ("idle_ms", f64),
+        ("err_info0", i32), ("err_info1", i32), ("idle_ms", f64), ("em_ms", f64),
     ]
 
 

@@ -58,7 +58,8 @@ enum : int {
   ST_SPACE_WAITS,     // sends that waited for ring space
   ST_LOOP_NS,         // ns spent in the scheduler loop
   ST_IDLE_NS,         // ns spent waiting on an empty inbox
-  N_STATS = 9
+  ST_EM_CYC,          // SM cycles spent inside entry methods
+  N_STATS = 10
 };
 
 // Device-wide runtime description, copied to __constant__ memory before each

@@ -541,7 +541,9 @@ __device__ void stash_dispatch_ready() {
   __syncthreads();
   if (go) {
     const regular_msg* rm = reinterpret_cast<const regular_msg*>(env + sizeof(envelope));
+    const long long c0 = clock64();
     p->call_fn(p, k->chare_idx, rm->ep_id, env + HDR);
+    if (threadIdx.x == 0) ps->stats[ST_EM_CYC] += (unsigned long long)(clock64() - c0);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -681,7 +683,9 @@ __device__ void dispatch_inbox() {
   // slots: every thread must have read them first.
   __syncthreads();
   if (action == 0) {
+    const long long c0 = clock64();
     p->call_fn(p, idx, ep, m + HDR);
+    if (threadIdx.x == 0) ps->stats[ST_EM_CYC] += (unsigned long long)(clock64() - c0);
   } else if (action == 1) {
     stash_put(m, size, cid, idx, ref, src);
   }

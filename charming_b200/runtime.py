@@ -37,6 +37,7 @@ class RunStats:
     main_ms: float
     status: int
     idle_ms: float = 0.0
+    em_ms: float = 0.0
 
 
 class Runtime:
@@ -82,7 +83,7 @@ class Runtime:
         self.lib.charming_last_stats(C.byref(st))
         return RunStats(st.delivered, st.sent, st.stashed, st.revived, st.bytes_sent,
                         st.idle_polls, st.space_waits, st.kernel_ms, st.loop_ms, st.main_ms,
-                        st.status, st.idle_ms)
+                        st.status, st.idle_ms, st.em_ms)
 
     # ---- built-in programs ---------------------------------------------------
     def hello(self) -> np.ndarray:

@@ -120,6 +120,8 @@ typedef struct charming_stats {
   int err_pe, err_info0, err_info1;
   double idle_ms;            /* mean over PEs: time waiting on an empty
                                 inbox                                    */
+  double em_ms;              /* mean over PEs: time inside entry methods
+                                (SM cycles at the nominal clock)         */
 } charming_stats;
 int charming_last_stats(charming_stats* out);
 
