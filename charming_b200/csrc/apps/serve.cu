@@ -49,8 +49,6 @@ struct Server : jserve::sink {
   int off_el = 32;
   // device
   char* d_slab = nullptr;
-  jac::chare_desc* d_desc = nullptr;
-  jac::prob_desc* d_probs = nullptr;
   unsigned long long* d_ctr = nullptr;
   unsigned int* d_done = nullptr;
   int* d_block_map = nullptr;
@@ -134,8 +132,6 @@ struct Server : jserve::sink {
 
   void free_all() {
     cudaFree(d_slab);
-    cudaFree(d_desc);
-    cudaFree(d_probs);
     cudaFree(d_ctr);
     cudaFree(d_done);
     cudaFree(d_block_map);
@@ -191,8 +187,6 @@ extern "C" int charming_serve_start(const charming_serve_config* cfg, void** ser
   P.vec = f64 ? jac::traits<double>::VEC : jac::traits<float>::VEC;
 
   cudaError_t e = cudaMalloc(&s->d_slab, cfg->hbm_budget_bytes);
-  if (e == cudaSuccess) e = cudaMalloc(&s->d_desc, sizeof(jac::chare_desc) * s->n_workers);
-  if (e == cudaSuccess) e = cudaMalloc(&s->d_probs, sizeof(jac::prob_desc) * s->n_workers);
   if (e == cudaSuccess) e = cudaMalloc(&s->d_ctr, 128);
   if (e == cudaSuccess) e = cudaMalloc(&s->d_done, sizeof(unsigned) * s->Q);
   if (e == cudaSuccess) e = cudaMalloc(&s->d_block_map, sizeof(int) * n_pes);
@@ -202,8 +196,6 @@ extern "C" int charming_serve_start(const charming_serve_config* cfg, void** ser
   if (e == cudaSuccess) e = cudaMemset(s->d_ctr, 0, 128);
   if (e == cudaSuccess) e = cudaMemset(s->d_done, 0, sizeof(unsigned) * s->Q);
   if (e == cudaSuccess) e = cudaMemset(s->d_pe_ns, 0, 32 * (size_t)n_pes);
-  if (e == cudaSuccess) e = cudaMemset(s->d_desc, 0, sizeof(jac::chare_desc) * s->n_workers);
-  if (e == cudaSuccess) e = cudaMemset(s->d_probs, 0, sizeof(jac::prob_desc) * s->n_workers);
   s->h_req = host_mapped<jac::serve_req>(s->Q, &e);
   s->h_desc = host_mapped<jac::chare_desc>(s->n_workers, &e);
   s->h_prob = host_mapped<jac::prob_desc>(s->Q, &e);
@@ -235,8 +227,8 @@ extern "C" int charming_serve_start(const charming_serve_config* cfg, void** ser
   ap.a[6] = 1;
   ap.a[7] = s->Q;
   ap.a[8] = s->CQ;
-  ap.p[0] = s->d_desc;
-  ap.p[1] = s->d_probs;
+  // p[0], p[1] (descriptor tables) stay null: each worker copies its
+  // descriptors from the staging tables into its own chare object
   ap.p[4] = s->d_final;
   ap.p[5] = s->d_block_map;
   ap.p[6] = s->d_pe_ns;
