@@ -326,6 +326,9 @@ int n_nodes() { return 1; }
 void end() { g_term = 1; }
 void abort() {}
 uint64_t now_ns() {
+  // the chare code reads the timer around every sweep and send: the
+  // watchdog counts that as progress too (one entry method may sweep long)
+  g_progress++;
   return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
              std::chrono::steady_clock::now().time_since_epoch()).count();
 }
