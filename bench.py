@@ -78,16 +78,18 @@ class ClockSampler:
         self.stop = False
         self.source = None
 
-    def _nvml_loop(self, nv, h):
-        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+    def _nvml_sample(self, nv, h, mx):
+        try:
+            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            rs = {name for name, attr in self.REASONS if bits & getattr(nv, attr)}
+            self.samples.append((float(sm), float(mx), rs))
+        except Exception:
+            pass
+
+    def _nvml_loop(self, nv, h, mx):
         while not self.stop:
-            try:
-                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
-                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
-                rs = {name for name, attr in self.REASONS if bits & getattr(nv, attr)}
-                self.samples.append((float(sm), float(mx), rs))
-            except Exception:
-                pass
+            self._nvml_sample(nv, h, mx)
             time.sleep(0.01)
 
     def __enter__(self):
@@ -97,7 +99,9 @@ class ClockSampler:
             import pynvml as nv
             nv.nvmlInit()
             h = nv.nvmlDeviceGetHandleByIndex(self.device)
-            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            self._nvml = (nv, h, mx)
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h, mx), daemon=True)
             self.thread.start()
             self.source = "nvml 10 ms"
             return self
@@ -117,6 +121,9 @@ class ClockSampler:
 
     def __exit__(self, *exc):
         if self.thread:
+            # one more reading at the end of the timed region (the sampling
+            # thread may have had little time during a short region)
+            self._nvml_sample(*self._nvml)
             self.stop = True
             self.thread.join(timeout=5)
         if self.proc:
@@ -295,6 +302,7 @@ def messaging_suite(seed: int = 0xC2) -> dict:
     log, ms = rt.fanout(4096, 16, 64, seed, 1)
     fst = rt.last_stats()
     n = 4096 * 16
+    _, ms_fifo = rt.fanout(4096, 16, 64, seed, 0)
     return {
         "pingpong": {"sm_pair": list(sm), "round_trips": 10000,
                      "oneway_ns": {str(r["size"]): round(r["oneway_us"] * 1e3, 1) for r in rows},
@@ -304,8 +312,26 @@ def messaging_suite(seed: int = 0xC2) -> dict:
         "fanout": {"chares": 4096, "msgs_per_chare": 16, "payload_bytes": 64, "refnums": "0..15",
                    "ms": ms, "msgs_per_s": n / (ms * 1e-3), "delivered": int(len(log)),
                    "stashed": fst.stashed, "status": fst.status,
+                   "fifo_msgs_per_s": n / (ms_fifo * 1e-3),
                    "checked": "counts, per-pair FIFO and checksums against the CPU model in tests"},
+        "cpu_baseline": messaging_cpu_baseline(seed),
     }
+
+
+def messaging_cpu_baseline(seed: int) -> dict:
+    """The same fan-out (FIFO mode) and pingpong on the host's cores, one
+    MPSC inbox per thread (oracle/msg_cpu.c)."""
+    from oracle import msg_cpu
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    reps = [msg_cpu.fanout(4096, 16, 64, seed, threads)[0] for _ in range(21)]
+    pp = {str(b): round(msg_cpu.pingpong_oneway_s(b, 10000 if b < (1 << 20) else 1000, seed) * 1e9, 1)
+          for b in (8, 4096, 65536, 1 << 20)}
+    return {"kind": "port", "cores": threads,
+            "fanout_fifo_msgs_per_s": 4096 * 16 / statistics.median(reps),
+            "pingpong_oneway_ns": pp,
+            "sample": "fan-out 4096 x 16 x 64 B (FIFO), median of 21; pingpong 10,000 round trips "
+                      "(1,000 for 1 MiB) between two threads"}
 
 
 def batched_suite(steps: int = 3, warmup: int = 3) -> dict:

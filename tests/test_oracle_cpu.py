@@ -216,3 +216,14 @@ def test_oracle_matches_reference_kernel_fixture(case):
 
 def test_golden_fixtures_present():
     assert _golden_cases(), "tests/golden/ref_jacobi2d.json missing (run tests/golden/gen_ref_fixtures.sh on a GPU)"
+
+
+def test_messaging_cpu_baseline_delivers_everything():
+    """The CPU baseline of the messaging benchmarks (oracle/msg_cpu.c)
+    delivers every fan-out message on any thread count, and its pingpong
+    returns a positive latency."""
+    from oracle import msg_cpu
+    for threads in (1, 3, 8):
+        s, d = msg_cpu.fanout(300, 16, 64, 0xC2, threads)
+        assert d == 300 * 16 and s > 0
+    assert msg_cpu.pingpong_oneway_s(64, 100) > 0
