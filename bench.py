@@ -416,14 +416,16 @@ def precision_suite(plain_fp64_glups: float, steps: int = 2, warmup: int = 1) ->
             "autotune": tune.as_dict()}
 
 
-def serving_suite(n_req: int, rate: float = 200.0, seed: int = 0xC5) -> dict:
+def serving_suite(n_req: int, rate: float = 200.0, seed: int = 0xC5, pes_per_sm: int = 2,
+                  chare_side: int = 512) -> dict:
     """C5: Poisson arrivals of FP32 solves into one running scheduler."""
     import torch
     from charming_b200.batch import _uniform
     from charming_b200.jacobi import Problem
     from charming_b200.runtime import Runtime
     from charming_b200.serve import Server
-    Runtime(pes_per_sm=2, threads_per_pe=256)  # two PEs per SM: messages of one overlap sweeps of the other
+    # several PEs per SM: the messages of one overlap the sweeps of another
+    Runtime(pes_per_sm=pes_per_sm, threads_per_pe=512 // pes_per_sm)
     rng = np.random.default_rng(seed)
     sides = np.exp(rng.uniform(np.log(128), np.log(4096), n_req)).round().astype(int)
     gaps = rng.exponential(1.0 / rate, n_req)
@@ -433,8 +435,8 @@ def serving_suite(n_req: int, rate: float = 200.0, seed: int = 0xC5) -> dict:
     out = torch.empty((4098 * 4098,), dtype=torch.float32, pin_memory=True).numpy()
     budget = 120 * 10**9
     lat, service, lups_done = [], [], 0
-    with Server(budget, max_inflight=64, workers_per_pe=8, chare_side=512, dtype="f32",
-                deadline_s=600) as srv:
+    with Server(budget, max_inflight=64, workers_per_pe=16 // pes_per_sm, chare_side=chare_side,
+                dtype="f32", deadline_s=600) as srv:
         t0 = time.monotonic()
         nxt = 0
         done = 0
@@ -459,8 +461,8 @@ def serving_suite(n_req: int, rate: float = 200.0, seed: int = 0xC5) -> dict:
     offered = sum(p.nx * p.ny * p.max_sweeps for p in probs) / max(arrive[-1], 1e-9)
     return {"workload": f"{n_req} FP32 solve requests, Poisson {rate:.0f} req/s, sides log-uniform "
                         "in [128, 4096], tol 1e-5 with the FP64 residual every 10 sweeps, cap 5000 "
-                        "sweeps, 120 GB HBM budget, chares of 512^2 on 2 PEs per SM, each result "
-                        "fetched to the host",
+                        f"sweeps, 120 GB HBM budget, chares of {chare_side}^2 on {pes_per_sm} PEs "
+                        "per SM, each result fetched to the host",
             "requests": n_req, "completed": done, "wall_s": wall,
             "solves_per_s": done / wall, "p50_ms": float(np.percentile(lat, 50)) * 1e3,
             "p99_ms": float(np.percentile(lat, 99)) * 1e3,
