@@ -416,9 +416,13 @@ def precision_suite(plain_fp64_glups: float, steps: int = 2, warmup: int = 1) ->
             "autotune": tune.as_dict()}
 
 
-def serving_suite(n_req: int, rate: float = 200.0, seed: int = 0xC5, pes_per_sm: int = 2,
-                  chare_side: int = 512) -> dict:
-    """C5: Poisson arrivals of FP32 solves into one running scheduler."""
+def serving_suite(n_req: int, rate: float = 200.0, seed: int = 0xC5, pes_per_sm: int = 1,
+                  chare_side: int = 2048) -> dict:
+    """C5: Poisson arrivals of FP32 solves into one running scheduler. The
+    defaults are the fastest measured (600 requests, served GLUP/s): chares
+    of 2048^2 on one 512-thread PE per SM 759; 1536^2 701; 1024^2 with 2 PEs
+    per SM 655; 512^2 with 2 PEs per SM 512; 4096^2 (one chare per request)
+    337."""
     import torch
     from charming_b200.batch import _uniform
     from charming_b200.jacobi import Problem

@@ -180,7 +180,9 @@ extern "C" int charming_serve_start(const charming_serve_config* cfg, void** ser
   P.workers_per_pe = cfg->workers_per_pe;
   P.max_inflight = cfg->max_inflight;
   P.budget = cfg->hbm_budget_bytes;
-  P.chare_side = cfg->chare_side > 0 ? cfg->chare_side : 256;
+  // default: large chares (fewer halo messages per point); requests far
+  // apart in size still spread over many PEs because many run at once
+  P.chare_side = cfg->chare_side > 0 ? cfg->chare_side : 2048;
   P.depth = 0;
   P.esz = (int)s->esz;
   P.off = s->off_el;

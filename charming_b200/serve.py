@@ -42,7 +42,7 @@ class Completion:
 
 class Server:
     def __init__(self, hbm_budget_bytes: int, max_inflight: int = 256, workers_per_pe: int = 16,
-                 chare_side: int = 256, dtype: str = "f32", deadline_s: float = 600.0):
+                 chare_side: int = 2048, dtype: str = "f32", deadline_s: float = 600.0):
         self.rt = runtime()
         self.lib = self.rt.lib
         self.dtype = np.float64 if dtype in ("f64", "float64", np.float64) else np.float32

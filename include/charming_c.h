@@ -282,7 +282,8 @@ typedef struct charming_serve_config {
   uint64_t hbm_budget_bytes; /* grids admitted at once must fit in this    */
   int max_inflight;          /* device problem slots                       */
   int workers_per_pe;        /* solver chares per PE                       */
-  int chare_side;            /* requests are cut into chares of this side  */
+  int chare_side;            /* requests are cut into chares of this side
+                                (0: 2048)                                 */
   int dtype;                 /* CHARMING_F32 (FP64 residual) or F64        */
   double deadline_s;         /* server lifetime limit                      */
 } charming_serve_config;
