@@ -363,7 +363,13 @@ def batched_suite(steps: int = 3, warmup: int = 3) -> dict:
         ts = [j.run() for _ in range(steps)]
         info = j.info()
     ms = statistics.mean(ts)
-    return {"workload": "64 square FP64 problems, sides log-uniform in [64, 2048] (seed 0xC3), "
+    # the same set with chare sides outside the config's 64/128/256 choice
+    from charming_b200.batch import Candidate
+    ext = autotune(probs, "f64", candidates=[Candidate(sd, pe, 4 << 20) for sd in (512, 1024)
+                                             for pe in (1, 2, 4)])
+    return {"outside_config": {"chare_sides": [512, 1024], "glups": ext.best.glups,
+                               "autotune": ext.as_dict()},
+            "workload": "64 square FP64 problems, sides log-uniform in [64, 2048] (seed 0xC3), "
                         "500 sweeps, one launch from a CUDA graph",
             "glups": points * 500 / (ms * 1e-3) / 1e9, "ms_per_launch": ms, "launches": steps,
             "points": points, "chares": info["n_chares"], "autotune": tune.as_dict()}
@@ -403,10 +409,24 @@ def precision_suite(plain_fp64_glups: float, steps: int = 2, warmup: int = 1) ->
             err = max(err, float(np.max(np.abs(g32[i].astype(np.float64) - g64))))
     glups = lups / (ms * 1e-3) / 1e9
     sw = [r.sweeps for r in res]
+    # the same FP32 run with chare sides outside the config's 64/128/256 choice
+    from charming_b200.batch import Candidate
+    ext = autotune(proxy, "f32", candidates=[Candidate(sd, pe, 4 << 20) for sd in (512, 1024, 2048)
+                                             for pe in (1, 2)])
+    with Jacobi2D(probs, dtype="f32", chare_side=ext.best.chare_side, use_graph=True) as j:
+        j.init()
+        j.run()
+        j.init()
+        ms_ext = j.run()
+        lups_ext = sum(p.nx * p.ny * j.result(i).sweeps for i, p in enumerate(probs))
+    glups_ext = lups_ext / (ms_ext * 1e-3) / 1e9
     return {"workload": "the batched set with 5000-sweep caps plus one 8192^2 problem, FP32 "
                         "sweeps and storage, FP64 residual every 10 sweeps, tol 1e-5",
             "glups": glups, "ms_per_launch": ms, "launches": steps,
             "vs_plain_fp64": glups / plain_fp64_glups if plain_fp64_glups else None,
+            "outside_config": {"chare_sides": [512, 1024, 2048], "glups": glups_ext,
+                               "vs_plain_fp64": glups_ext / plain_fp64_glups if plain_fp64_glups else None,
+                               "autotune": ext.as_dict()},
             "target_vs_plain_fp64": 1.8, "max_abs_err_vs_fp64": err, "target_max_abs_err": 1e-5,
             "sweeps_min": min(sw), "sweeps_max": max(sw),
             "stopped_by_tol": sum(1 for p, r in zip(probs, res) if r.sweeps < p.max_sweeps),
