@@ -1,6 +1,5 @@
-/* CPU baseline of the messaging microbenchmarks (TEST INFRASTRUCTURE /
- * CPU BASELINE ONLY: timed beside the GPU numbers, never part of the
- * product).
+/* CPU baseline of the messaging microbenchmarks: test infrastructure,
+ * timed beside the GPU numbers, never part of the product.
  *
  * The same workloads as the GPU's fan-out and pingpong programs
  * (charming_b200/csrc/apps/msgbench.cu), restated for host threads with

@@ -1,5 +1,5 @@
-"""CPU baseline of the messaging benchmarks (TEST INFRASTRUCTURE / CPU
-BASELINE ONLY): ctypes binding of liboracle_msg.so (msg_cpu.c), the GPU's
+"""CPU baseline of the messaging benchmarks (test infrastructure, timed
+beside the GPU numbers; never part of the product): ctypes binding of liboracle_msg.so (msg_cpu.c), the GPU's
 fan-out and pingpong workloads on host threads with one MPSC inbox each."""
 from __future__ import annotations
 
