@@ -29,7 +29,7 @@ STATUS = {
     0: "OK", 1: "RING_FULL", 2: "STASH_FULL", 3: "BAD_TARGET", 4: "BARRIER_TIMEOUT",
     5: "IDLE_TIMEOUT", 6: "DEADLINE", 7: "BAD_MSG", 8: "MSG_TOO_LARGE", 9: "HOST_STOP",
     10: "TOO_MANY_TYPES", 11: "TOO_MANY_EMS", 12: "PIPELINE", 13: "LAUNCH", 14: "CONFIG",
-    15: "CUDA", 16: "NOT_INIT", 17: "NO_MEMORY", 18: "APP",
+    15: "CUDA", 16: "NOT_INIT", 17: "NO_MEMORY", 18: "APP", 19: "TOO_MANY_WAITS",
 }
 F64, F32 = 0, 1
 
@@ -59,6 +59,7 @@ class Stats(C.Structure):
         ("bytes_sent", u64), ("idle_polls", u64), ("space_waits", u64),
         ("kernel_ms", f64), ("loop_ms", f64), ("main_ms", f64), ("status", i32), ("err_pe", i32),
         ("err_info0", i32), ("err_info1", i32), ("idle_ms", f64), ("em_ms", f64),
+        ("deferred", u64),
     ]
 
 
@@ -142,6 +143,8 @@ SIGNATURES = [
     ("charming_hello", i32, [C.POINTER(i32), i32, C.POINTER(i32)]),
     ("charming_refnum", i32, [C.POINTER(i32), i32, C.POINTER(i32)]),
     ("charming_refnum_reversed", i32, [C.POINTER(i32), i32, C.POINTER(i32)]),
+    ("charming_async_wait_chain", i32, [i32, i32, C.POINTER(i32), i32]),
+    ("charming_user_heap_check", i32, [i32, i32, i32, u64, C.POINTER(u64)]),
     ("charming_serve_start", i32, [C.POINTER(ServeConfig), C.POINTER(vp)]),
     ("charming_serve_submit", i32, [vp, C.POINTER(JacobiProblem), u64]),
     ("charming_serve_poll", i32, [vp, C.POINTER(ServeCompletion), i32, C.POINTER(i32)]),

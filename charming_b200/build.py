@@ -10,7 +10,10 @@ import sys
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(ROOT, "charming_b200", "csrc")
-REFERENCE = os.environ.get("CHARMING_REFERENCE", "/root/reference")
+# The reference tree (only where it is present): CHARMING_REFERENCE, else a
+# directory named "reference" beside this repository.
+REFERENCE = os.environ.get("CHARMING_REFERENCE",
+                           os.path.join(os.path.dirname(ROOT), "reference"))
 ARCH = "-gencode arch=compute_100a,code=sm_100a"
 REF_EXAMPLES = ("hello", "refnum", "pingpong")
 

@@ -35,11 +35,12 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH
 
 std::mutex g_scratch_mu;
 void* g_scratch_ptr[NOALLOC_MAX_DEVICES];  // device address of the scratch, per device
+int g_sm_count[NOALLOC_MAX_DEVICES];       // multiprocessors of each device
 
-// Resolves the scratch's device address on the current device, once per
-// device (the first call on a device does this; make that first call before
-// any stream capture).
-int scratch_on_current_device(void** out) {
+// Resolves the scratch's device address and the device's multiprocessor
+// count on the current device, once per device (the first call on a device
+// does this).
+int scratch_on_current_device(void** out, int* sms) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return charm_host::cuda_fail(e, "jacobi2d noalloc: cudaGetDevice");
@@ -52,9 +53,14 @@ int scratch_on_current_device(void** out) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return charm_host::cuda_fail(e, "jacobi2d noalloc: cudaGetSymbolAddress");
+    int n = 0;
+    e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return charm_host::cuda_fail(e, "jacobi2d noalloc: cudaDeviceGetAttribute");
+    g_sm_count[dev] = n > 0 ? n : 1;
     g_scratch_ptr[dev] = p;
   }
   *out = g_scratch_ptr[dev];
+  *sms = g_sm_count[dev];
   return CHARMING_OK;
 }
 
@@ -74,8 +80,8 @@ __global__ void __launch_bounds__(256) noalloc_sweep_kernel(const T* __restrict_
 }
 
 template <typename T>
-int run_sweeps(int nx, int ny, int sweeps, const T* in, T* out, T* scratch) {
-  const size_t bytes = (size_t)(nx + 2) * (ny + 2) * sizeof(T);
+int run_sweeps(int nx, int ny, int sweeps, const T* in, T* out, T* scratch, int sms) {
+  const size_t bytes = ((size_t)nx + 2) * ((size_t)ny + 2) * sizeof(T);
   // Both buffers start as the input (boundary ring included); the first
   // source is picked so that the last sweep writes `out`.
   cudaError_t e = cudaMemcpyAsync(out, in, bytes, cudaMemcpyDeviceToDevice, 0);
@@ -83,7 +89,7 @@ int run_sweeps(int nx, int ny, int sweeps, const T* in, T* out, T* scratch) {
   T* a = (sweeps % 2 == 0) ? out : scratch;
   T* b = (a == out) ? scratch : out;
   const long long pts = (long long)nx * ny;
-  const int blocks = (int)std::min<long long>((pts + 255) / 256, 148LL * 8);
+  const int blocks = (int)std::min<long long>((pts + 255) / 256, (long long)sms * 8);
   for (int s = 0; s < sweeps && e == cudaSuccess; s++) {
     noalloc_sweep_kernel<T><<<blocks, 256, 0, 0>>>(a, b, nx, ny);
     e = cudaGetLastError();
@@ -109,7 +115,12 @@ extern "C" int charming_jacobi2d_sweeps_noalloc(int dtype, int nx, int ny, int s
     return CHARMING_ERR_CONFIG;
   }
   const size_t esz = dtype == CHARMING_F64 ? 8 : 4;
-  const unsigned long long cells = (unsigned long long)(nx + 2) * (unsigned long long)(ny + 2);
+  // A misaligned element pointer would fault in the kernel's loads.
+  if (reinterpret_cast<uintptr_t>(dev_in) % esz || reinterpret_cast<uintptr_t>(dev_out) % esz) {
+    charm_host::set_error_text("jacobi2d noalloc: dev_in and dev_out must be aligned to the element size");
+    return CHARMING_ERR_CONFIG;
+  }
+  const unsigned long long cells = ((unsigned long long)nx + 2) * ((unsigned long long)ny + 2);
   if (cells > NOALLOC_SCRATCH_BYTES / esz) {
     charm_host::set_error_text(
         "jacobi2d noalloc: grid larger than the 16 MiB scratch ((nx+2)*(ny+2)*element size must "
@@ -124,11 +135,12 @@ extern "C" int charming_jacobi2d_sweeps_noalloc(int dtype, int nx, int ny, int s
     return CHARMING_ERR_CONFIG;
   }
   void* scratch = nullptr;
-  int rc = scratch_on_current_device(&scratch);
+  int sms = 1;
+  int rc = scratch_on_current_device(&scratch, &sms);
   if (rc) return rc;
   if (dtype == CHARMING_F64)
     return run_sweeps<double>(nx, ny, sweeps, static_cast<const double*>(dev_in),
-                              static_cast<double*>(dev_out), static_cast<double*>(scratch));
+                              static_cast<double*>(dev_out), static_cast<double*>(scratch), sms);
   return run_sweeps<float>(nx, ny, sweeps, static_cast<const float*>(dev_in),
-                           static_cast<float*>(dev_out), static_cast<float*>(scratch));
+                           static_cast<float*>(dev_out), static_cast<float*>(scratch), sms);
 }

@@ -20,6 +20,8 @@ __device__ void charm::main(int argc, char** argv, size_t* argvs, int pe) {
     case suite::APP_JACOBI2D: suite::jacobi2d_main(pe); break;
     case suite::APP_JACOBI1D: suite::jacobi1d_main(pe); break;
     case suite::APP_SERVE: suite::serve_main(pe); break;
+    case suite::APP_ASYNC_WAIT: suite::async_wait_main(pe); break;
+    case suite::APP_USER_HEAP: suite::user_heap_main(pe); break;
     default:
       if (threadIdx.x == 0 && pe == 0) charm::end();
       break;

@@ -17,6 +17,8 @@ enum app_id : int {
   APP_JACOBI2D = 5,
   APP_JACOBI1D = 6,
   APP_SERVE = 7,
+  APP_ASYNC_WAIT = 8,
+  APP_USER_HEAP = 9,
 };
 
 struct app_params {
@@ -70,6 +72,8 @@ __device__ void fanout_main(int pe);
 __device__ void jacobi2d_main(int pe);
 __device__ void jacobi1d_main(int pe);
 __device__ void serve_main(int pe);
+__device__ void async_wait_main(int pe);
+__device__ void user_heap_main(int pe);
 }  // namespace suite
 
 // Host helper: copy params to g_app and run the scheduler once.

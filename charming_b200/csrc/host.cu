@@ -140,6 +140,7 @@ int collect_run(double kernel_ms) {
     s.bytes_sent += q[ST_BYTES_SENT];
     s.idle_polls += q[ST_IDLE_POLLS];
     s.space_waits += q[ST_SPACE_WAITS];
+    s.deferred += q[ST_DEFERRED];
     if (t[1] && t[1] < tmin) tmin = t[1];
     if (t[2] > tmax) tmax = t[2];
   }
@@ -371,6 +372,27 @@ int charming_init(const charming_config* cfg_in) {
   if (const char* ev = getenv("CHARMING_ARENA_BYTES")) ds.arena_bytes = strtoull(ev, nullptr, 10);
   ds.arena = nullptr;
   if (ds.arena_bytes && (rc = dev_alloc(&ds.arena, ds.arena_bytes * n_pes, "arena"))) return rc;
+  // per-PE outbox for sends deferred while their destination ring is full:
+  // room for a few of the largest messages
+  ds.outbox_bytes = 2 * ds.max_msg + (1ull << 20);
+  if (const char* ev = getenv("CHARMING_OUTBOX_BYTES")) ds.outbox_bytes = strtoull(ev, nullptr, 10);
+  ds.outbox_bytes = (ds.outbox_bytes + 127) / 128 * 128;
+  ds.outbox_stride = ds.outbox_bytes + (ds.max_msg + OB_HDR + 127) / 128 * 128;
+  ds.outbox = nullptr;
+  if (ds.outbox_bytes && (rc = dev_alloc(&ds.outbox, ds.outbox_stride * n_pes, "outbox"))) return rc;
+  // malloc_user heap per PE
+  ds.user_heap_bytes = 1ull << 20;
+  if (const char* ev = getenv("CHARMING_USER_HEAP_BYTES")) ds.user_heap_bytes = strtoull(ev, nullptr, 10);
+  ds.user_heap_bytes = (ds.user_heap_bytes + 127) / 128 * 128;
+  ds.user_blocks_max = 1024;
+  ds.user_heap = nullptr;
+  ds.user_blocks = nullptr;
+  if (ds.user_heap_bytes) {
+    if ((rc = dev_alloc(&ds.user_heap, ds.user_heap_bytes * n_pes, "user heap"))) return rc;
+    if ((rc = dev_alloc(&ds.user_blocks, sizeof(user_block) * (size_t)ds.user_blocks_max * n_pes,
+                        "user heap blocks")))
+      return rc;
+  }
   e = cudaHostAlloc(&g.h_stop, 64, cudaHostAllocMapped);
   if (e != cudaSuccess) return cuda_fail(e, "host stop word");
   *g.h_stop = 0;
@@ -482,6 +504,7 @@ const char* charming_status_string(int code) {
     case CHARMING_ERR_NOT_INIT: return "runtime not initialised";
     case CHARMING_ERR_NO_MEMORY: return "out of memory";
     case CHARMING_ERR_APP: return "program reported a failure";
+    case CHARMING_ERR_TOO_MANY_WAITS: return "too many pending async_waits on a chare array";
     default: return "unknown status";
   }
 }

@@ -12,6 +12,11 @@
 //                           cells run past the end continues in the overhang
 //   stash_keys[pe][S]       descriptors of messages whose refnum mismatched
 //   stash_data[pe]          byte arena holding those messages
+//   outbox[pe]              sends deferred because their destination's ring
+//                           had no space: each holds its ticket and the
+//                           whole message, copied into the ring once the
+//                           receiver has consumed up to that ticket
+//   user_heap[pe]           malloc_user / free_user blocks of the PE
 // Cell and flag indices are (ticket mod C); C is a power of two.
 #pragma once
 
@@ -48,6 +53,28 @@ struct stash_key {
 
 enum : int { KEY_FREE = 0, KEY_WAIT = 1, KEY_READY = 2 };
 
+// Outbox entry header, 32 B; the message (envelope, header, payload) follows.
+struct ob_entry {
+  int dst;
+  int state;                    // OB_FILLING until the send publishes it
+  unsigned long long ticket;    // ticket taken in dst's inbox
+  unsigned long long bytes;     // message bytes
+  unsigned long long span;      // bytes of this entry in the outbox
+};
+enum : int { OB_FILLING = 0, OB_READY = 1 };
+constexpr int OB_HDR = 32;
+// A send that found no ring space for this long is moved to the outbox.
+constexpr unsigned long long DEFER_AFTER_NS = 20000;
+
+// malloc_user block record (per PE ring of records, oldest first).
+struct user_block {
+  unsigned long long off;       // virtual offset in the PE's user heap
+  unsigned long long span;      // bytes taken, wrap padding included
+  unsigned long long start;     // offset of the block's memory in the heap
+  int freed;
+  int pad;
+};
+
 enum : int {
   ST_DELIVERED = 0,   // entry methods run
   ST_SENT,            // messages sent
@@ -59,7 +86,8 @@ enum : int {
   ST_LOOP_NS,         // ns spent in the scheduler loop
   ST_IDLE_NS,         // ns spent waiting on an empty inbox
   ST_EM_CYC,          // SM cycles spent inside entry methods
-  N_STATS = 10
+  ST_DEFERRED,        // sends moved to the outbox (destination ring full)
+  N_STATS = 11
 };
 
 // Device-wide runtime description, copied to __constant__ memory before each
@@ -92,6 +120,14 @@ struct device_state {
   int free_chares_at_exit;
   unsigned char* arena;                // [n_pes][arena_bytes]: per-run bump allocator
   unsigned long long arena_bytes;      // per PE
+  unsigned char* outbox;               // [n_pes][outbox_stride]: deferred sends
+  unsigned long long outbox_bytes;     // ring part per PE (entries may run
+                                       // past it into an overhang of max_msg + OB_HDR)
+  unsigned long long outbox_stride;
+  unsigned char* user_heap;            // [n_pes][user_heap_bytes]: malloc_user
+  unsigned long long user_heap_bytes;
+  user_block* user_blocks;             // [n_pes][user_blocks_max]
+  int user_blocks_max;
 };
 
 // Words of device_state::ctrl (each on its own 128-B line).
@@ -133,6 +169,17 @@ struct pe_state {
   unsigned long long head_pub;         // head last published to the senders
   unsigned long long arena_top;        // bytes of this PE's arena handed out this run
   unsigned long long sarena_top;       // bytes of the on-chip arena handed out this run
+  // outbox (deferred sends): virtual byte offsets, entries in send order
+  unsigned long long ob_head, ob_tail;
+  int ob_count;
+  int ob_lock;                         // held by the thread allocating an entry
+  // malloc_user heap: virtual byte offsets and block records
+  unsigned long long uh_head, uh_tail;
+  unsigned long long ub_head, ub_tail;
+  int aw_count;                        // pending async_waits on this PE
+  unsigned long long stamped_delivered;  // deliveries at the last progress stamp
+  unsigned long long slow_check_ns;    // last host-stop / idle-timeout check
+  unsigned long long idle_checks;
   chare_proxy_base* pcache[PROXY_CACHE];  // proxies[0..PROXY_CACHE) of this PE's table
   // batched sends (alloc_user_msgs): per message start, ticket, bytes
   void* bm_ptr[MSG_BATCH_MAX];
@@ -201,6 +248,8 @@ __device__ __forceinline__ unsigned long long ld_relaxed_sys_u64(const unsigned 
 __device__ __forceinline__ void st_release_sys_u64(unsigned long long* p, unsigned long long v) {
   asm volatile("st.release.sys.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
 }
+// Acquire side for data published before words read with relaxed loads.
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 __device__ __forceinline__ unsigned long long globaltimer() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -220,6 +269,7 @@ inline unsigned long long ld_volatile_shared_u64(const unsigned long long* p) { 
 inline unsigned long long ld_acquire_sys_u64(const unsigned long long* p) { return __atomic_load_n(p, __ATOMIC_ACQUIRE); }
 inline unsigned long long ld_relaxed_sys_u64(const unsigned long long* p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
 inline void st_release_sys_u64(unsigned long long* p, unsigned long long v) { __atomic_store_n(p, v, __ATOMIC_RELEASE); }
+inline void fence_acq_rel_gpu() { std::atomic_thread_fence(std::memory_order_acq_rel); }
 unsigned long long globaltimer();
 #endif
 

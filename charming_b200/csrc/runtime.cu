@@ -22,6 +22,13 @@
 //     ring cells at once, so a parked message never blocks the ring.
 //   * Every wait is bounded by the run deadline (%globaltimer); a run that
 //     cannot progress ends with an error status instead of spinning forever.
+//   * A send that finds no space in its destination's ring does not block its
+//     PE for long: after a short wait the whole message goes to the PE's
+//     outbox with the ticket it already holds, the send returns, and the
+//     scheduler loop copies it into the ring once the receiver has consumed
+//     up to that ticket. Two PEs that fill each other's rings from inside
+//     entry methods therefore both finish those entry methods and free
+//     their rings (the reference spins in the sender, get.cu:241-248).
 #include "rt.cuh"
 
 // Execution-environment constants (see include/common.h).
@@ -188,8 +195,45 @@ __device__ __forceinline__ unsigned long long* ring_flag(int pe, unsigned long l
   return c_rt.flags + (unsigned long long)pe * c_rt.ring_cells + (ticket & (c_rt.ring_cells - 1));
 }
 
+__device__ __forceinline__ unsigned char* outbox_of(int pe) {
+  return c_rt.outbox + (unsigned long long)pe * c_rt.outbox_stride;
+}
+__device__ __forceinline__ bool in_outbox(const unsigned char* m) {
+  const unsigned char* b = c_rt.outbox ? outbox_of(blockIdx.x) : nullptr;
+  return b && m >= b && m < b + c_rt.outbox_stride;
+}
+
+// A new outbox entry for a message of `bytes` that holds `ticket` in dst's
+// inbox; returns where the message goes, or nullptr when the outbox is
+// full. Any thread (the threads of a batched send may call it at once; a
+// block-shared lock orders them). Entries are never allocated while the
+// scheduler loop flushes, so only reserving threads race here.
+__device__ unsigned char* outbox_put(int dst, unsigned long long ticket, unsigned long long bytes) {
+  if (!c_rt.outbox) return nullptr;
+  pe_state* ps = pes();
+  const unsigned long long span = (OB_HDR + bytes + 15) & ~15ULL;
+  while (atomicCAS_block(&ps->ob_lock, 0, 1) != 0) {
+  }
+  const unsigned long long v = ps->ob_tail;
+  const bool ok = v + span - ps->ob_head <= c_rt.outbox_bytes;
+  if (ok) ps->ob_tail = v + span;
+  __threadfence_block();
+  atomicExch_block(&ps->ob_lock, 0);
+  if (!ok) return nullptr;
+  ob_entry* e = reinterpret_cast<ob_entry*>(outbox_of(blockIdx.x) + v % c_rt.outbox_bytes);
+  e->dst = dst;
+  e->state = OB_FILLING;
+  e->ticket = ticket;
+  e->bytes = bytes;
+  e->span = span;
+  atomicAdd_block(&ps->ob_count, 1);
+  atomicAdd_block(&ps->stats[ST_DEFERRED], 1ULL);
+  return reinterpret_cast<unsigned char*>(e) + OB_HDR;
+}
+
 // Thread 0 only. Reserves `bytes` in dst's inbox; returns the message start
-// or nullptr (error recorded, or the run is ending).
+// (in the ring, or in this PE's outbox when the ring stayed full for
+// DEFER_AFTER_NS) or nullptr (error recorded, or the run is ending).
 __device__ unsigned char* reserve(int dst, unsigned long long bytes, unsigned long long* ticket) {
   pe_state* ps = pes();
   if (dst < 0 || dst >= c_rt.n_pes) {
@@ -202,15 +246,21 @@ __device__ unsigned char* reserve(int dst, unsigned long long bytes, unsigned lo
   }
   const unsigned long long C = c_rt.ring_cells;
   unsigned int cells = cells_for(bytes);
+  if (cells > C) {  // could never fit
+    set_error(CHARMING_ERR_MSG_TOO_LARGE, dst, (int)cells);
+    return nullptr;
+  }
   unsigned long long t = atomicAdd(&c_rt.tail[dst].v, (unsigned long long)cells);
   unsigned long long* hc = head_cache();
   // relaxed read: other threads of the block may raise hc[dst] meanwhile
   if (t + cells - ld_volatile_shared_u64(&hc[dst]) > C) {
     atomicAdd_block(&ps->stats[ST_SPACE_WAITS], 1ULL);
-    // this PE publishes its head lazily: a message to itself must not wait
-    // for space it has already consumed (ps->head is stable during an
-    // entry method; publishing it again is harmless)
-    if (dst == (int)blockIdx.x) st_release_u64(&c_rt.head[dst].v, ps->head);
+    // This PE publishes its head lazily. Whoever waits for space in this
+    // PE's ring meanwhile (itself included) must see all it has consumed:
+    // ps->head is stable during an entry method, and the message being
+    // processed is not yet counted as consumed, so publishing it is safe
+    // (and harmless when repeated).
+    st_release_u64(&c_rt.head[blockIdx.x].v, ps->head);
     unsigned long long start = globaltimer();
     // A receiver that frees nothing for the idle timeout is taken as stuck.
     unsigned long long limit = c_rt.idle_timeout_ns ? c_rt.idle_timeout_ns : c_rt.deadline_ns;
@@ -222,6 +272,13 @@ __device__ unsigned char* reserve(int dst, unsigned long long bytes, unsigned lo
       if ((++spins & 255) == 0) {
         if (terminated()) return nullptr;
         unsigned long long now = globaltimer();
+        if (now - start > DEFER_AFTER_NS) {
+          unsigned char* ob = outbox_put(dst, t, bytes);
+          if (ob) {
+            *ticket = t;
+            return ob;
+          }
+        }
         if (now - start > limit || now - ps->t0 > c_rt.deadline_ns) {
           set_error(CHARMING_ERR_RING_FULL, dst, (int)cells);
           return nullptr;
@@ -240,6 +297,58 @@ __device__ unsigned char* reserve(int dst, unsigned long long bytes, unsigned lo
 // fence would also invalidate the SM's L1.
 __device__ __forceinline__ void publish(int dst, unsigned long long ticket) {
   st_release_u64(ring_flag(dst, ticket), ticket + 1);
+}
+
+// Publishes the message at m (reserved by reserve() for ticket in dst's
+// inbox): in the ring, its sequence word; in the outbox, the entry is
+// marked complete for the scheduler loop to flush. Callers pass a block
+// barrier first.
+__device__ __forceinline__ void publish_msg(int dst, unsigned long long ticket, unsigned char* m) {
+  if (in_outbox(m)) {
+    reinterpret_cast<ob_entry*>(m - OB_HDR)->state = OB_READY;
+  } else {
+    publish(dst, ticket);
+  }
+}
+
+// Thread 0: whether the oldest outbox entry is complete and its receiver
+// has consumed enough for it to be copied into the ring.
+__device__ bool outbox_head_ready() {
+  pe_state* ps = pes();
+  if (ps->ob_count <= 0) return false;
+  const ob_entry* e =
+      reinterpret_cast<const ob_entry*>(outbox_of(blockIdx.x) + ps->ob_head % c_rt.outbox_bytes);
+  if (e->state != OB_READY) return false;
+  const unsigned long long h = ld_acquire_u64(&c_rt.head[e->dst].v);
+  atomicMax(&head_cache()[e->dst], h);
+  return e->ticket + cells_for(e->bytes) - h <= c_rt.ring_cells;
+}
+
+// Block-collective: copies every flushable outbox entry, oldest first, into
+// its destination ring and publishes it. An entry's receiver consumes the
+// tickets before it first, so its space always comes free in the end.
+__device__ void outbox_flush() {
+  pe_state* ps = pes();
+  while (true) {
+    if (threadIdx.x == 0) {
+      ps->b_ptr0 = outbox_head_ready() ? outbox_of(blockIdx.x) + ps->ob_head % c_rt.outbox_bytes : nullptr;
+    }
+    __syncthreads();
+    ob_entry* e = reinterpret_cast<ob_entry*>(ps->b_ptr0);
+    if (e == nullptr) {
+      __syncthreads();
+      return;
+    }
+    copy_cooperative(ring_cell(e->dst, e->ticket), reinterpret_cast<unsigned char*>(e) + OB_HDR, e->bytes,
+                     threadIdx.x, blockDim.x);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      publish(e->dst, e->ticket);
+      ps->ob_head += e->span;
+      ps->ob_count--;
+    }
+    __syncthreads();
+  }
 }
 
 // Thread 0: tell the senders how far this PE has consumed its inbox (a
@@ -305,7 +414,7 @@ __device__ void charm::send_reg_msg(int chare_id, int chare_idx, int ep_id, void
   unsigned long long t = ps->b_u1;
   int dst = ps->b_i1;
   __syncthreads();
-  if (threadIdx.x == 0) publish(dst, t);
+  if (threadIdx.x == 0) publish_msg(dst, t, m);
 }
 
 __device__ bool charm::alloc_user_msg(message& msg, int dst_pe, size_t payload_size) {
@@ -348,7 +457,7 @@ __device__ void charm::send_user_msg(int chare_id, int chare_idx, int ep_id,
     if (payload_size > msg.capacity) set_error(CHARMING_ERR_MSG_TOO_LARGE, msg.dst_pe, (int)payload_size);
     ps->stats[ST_SENT]++;
     ps->stats[ST_BYTES_SENT] += payload_size;
-    publish(msg.dst_pe, msg.offset);
+    publish_msg(msg.dst_pe, msg.offset, m);
   }
   __syncthreads();
   msg.env = nullptr;
@@ -402,15 +511,75 @@ __device__ void charm::send_user_msgs(int chare_id, const int* chare_idx, int ep
     if (payload_sizes[k] > msgs[k].capacity) set_error(CHARMING_ERR_MSG_TOO_LARGE, msgs[k].dst_pe, (int)payload_sizes[k]);
     atomicAdd_block(&ps->stats[ST_SENT], 1ULL);
     atomicAdd_block(&ps->stats[ST_BYTES_SENT], (unsigned long long)payload_sizes[k]);
-    publish(msgs[k].dst_pe, msgs[k].offset);
+    publish_msg(msgs[k].dst_pe, msgs[k].offset, m);
   }
   __syncthreads();
   for (int j = 0; j < n; j++) msgs[j].env = nullptr;
 }
 
+// ---------------------------------------------------------------------------
+// malloc_user / free_user (reference: src/comm/get/get.cu:1348-1362, where
+// they take space from the PE's message buffer and free_user returns it
+// through the release heap, so space comes back in offset order). Here each
+// PE has its own heap region in HBM, handed out as a ring: blocks are taken
+// at the tail (a block that would cross the end starts at the beginning),
+// and the head moves past the oldest blocks once they are freed, in any
+// order. Single-threaded. Blocks live until free_user or the end of the run.
+// ---------------------------------------------------------------------------
+namespace {
+__device__ __forceinline__ user_block* user_blocks_of(int pe) {
+  return c_rt.user_blocks + (unsigned long long)pe * c_rt.user_blocks_max;
+}
+}  // namespace
+
+__device__ void* charm::malloc_user(size_t size, size_t& offset) {
+  pe_state* ps = pes();
+  const unsigned long long U = c_rt.user_heap_bytes;
+  const unsigned long long B = (unsigned long long)c_rt.user_blocks_max;
+  const unsigned long long n = (size + 15) & ~15ULL;
+  if (!c_rt.user_heap || n == 0 || n > U || ps->ub_tail - ps->ub_head >= B) return nullptr;
+  unsigned long long v = ps->uh_tail;
+  const unsigned long long p = v % U;
+  if (p + n > U) v += U - p;  // does not fit before the end: start over
+  if (v + n - ps->uh_head > U) return nullptr;
+  user_block* b = user_blocks_of(blockIdx.x) + ps->ub_tail % B;
+  b->off = ps->uh_tail;        // the block's share starts where the last one ended
+  b->span = v + n - ps->uh_tail;
+  b->start = v % U;
+  b->freed = 0;
+  ps->ub_tail++;
+  ps->uh_tail = v + n;
+  offset = (size_t)(v % U);
+  return c_rt.user_heap + (unsigned long long)blockIdx.x * U + v % U;
+}
+
+__device__ void charm::free_user(size_t size, size_t offset) {
+  (void)size;  // the block is found by its offset
+  pe_state* ps = pes();
+  const unsigned long long B = (unsigned long long)c_rt.user_blocks_max;
+  user_block* blocks = user_blocks_of(blockIdx.x);
+  bool found = false;
+  for (unsigned long long i = ps->ub_head; i < ps->ub_tail; i++) {
+    user_block* b = blocks + i % B;
+    if (!b->freed && b->start == (unsigned long long)offset) {
+      b->freed = 1;
+      found = true;
+      break;
+    }
+  }
+  if (!found) {
+    set_error(CHARMING_ERR_BAD_TARGET, -2, (int)offset);
+    return;
+  }
+  while (ps->ub_head < ps->ub_tail && blocks[ps->ub_head % B].freed) ps->ub_head++;
+  ps->uh_head = ps->ub_head < ps->ub_tail ? blocks[ps->ub_head % B].off : ps->uh_tail;
+}
+
 __device__ void charm::revive_mismatches(int chare_id, int chare_idx, int refnum) {
   pes()->revive_pending = 1;
 }
+
+__device__ void charm::add_async_wait(int chare_id) { pes()->aw_count++; }
 
 // ---------------------------------------------------------------------------
 // Stash (refnum mismatches)
@@ -560,6 +729,71 @@ __device__ void stash_dispatch_ready() {
   __syncthreads();
 }
 
+// ---------------------------------------------------------------------------
+// async_wait (reference: check_async_wait, src/comm/get/get.cu:1172-1202,
+// called once per scheduler iteration in its GPU-level loop,
+// src/sched/scheduler.cu:305).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool cmp_holds(unsigned long long v, int cmp, unsigned long long x) {
+  switch (cmp) {
+    case CMP_EQ: return v == x;
+    case CMP_NE: return v != x;
+    case CMP_GT: return v > x;
+    case CMP_LE: return v <= x;
+    case CMP_LT: return v < x;
+    default: return v >= x;  // CMP_GE
+  }
+}
+
+// Block-collective: runs the entry method of the first satisfied wait (chare
+// arrays in registration order, waits in slot order), if any. The words are
+// read relaxed (no L1 invalidation per check); one acquire fence follows a
+// hit, so what their writers published before them is visible.
+__device__ void check_async_waits() {
+  pe_state* ps = pes();
+  if (threadIdx.x == 0) {
+    chare_proxy_base* hit = nullptr;
+    chare_proxy_table& tb = c_rt.proxy_tables[blockIdx.x];
+    for (int id = 0; id < tb.count && !hit; id++) {
+      chare_proxy_base* p = id < PROXY_CACHE ? ps->pcache[id] : tb.proxies[id];
+      if (p == nullptr || p->async_waits == nullptr) continue;
+      for (int i = 0; i < ASYNC_WAIT_MAX; i++) {
+        async_wait_t& aw = p->async_waits[i];
+        if (!aw.valid) continue;
+        bool ok = true;
+        for (size_t k = 0; k < aw.nelems && ok; k++)
+          ok = cmp_holds(ld_relaxed_u64(reinterpret_cast<const unsigned long long*>(aw.ivars) + k), aw.cmp,
+                         aw.cmp_value);
+        if (ok) {
+          aw.valid = false;
+          hit = p;
+          ps->b_i1 = aw.idx;
+          ps->b_i2 = aw.ep;
+          break;
+        }
+      }
+    }
+    if (hit) fence_acq_rel_gpu();
+    ps->b_ptr0 = hit;
+  }
+  __syncthreads();
+  chare_proxy_base* p = reinterpret_cast<chare_proxy_base*>(ps->b_ptr0);
+  const int idx = ps->b_i1, ep = ps->b_i2;
+  // the entry method may send at once and reuse the broadcast slots; the
+  // count changes only once every thread has read it in the loop
+  __syncthreads();
+  if (p) {
+    if (threadIdx.x == 0) ps->aw_count--;
+    const long long c0 = clock64();
+    p->call_fn(p, idx, ep, nullptr);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      ps->stats[ST_EM_CYC] += (unsigned long long)(clock64() - c0);
+      if ((++ps->stats[ST_DELIVERED] & 15) == 0) stamp_progress(blockIdx.x);
+    }
+  }
+}
+
 // Thread 0 of PE 0: stop the run when no PE has delivered anything for
 // idle_timeout_ns (e.g. a program that never calls end()).
 __device__ void check_idle_timeout(unsigned long long now) {
@@ -575,7 +809,8 @@ __device__ void check_idle_timeout(unsigned long long now) {
 }
 
 // Thread 0: wait for the message at the inbox head. Returns 1 when it has
-// arrived, 0 when this PE must leave the loop.
+// arrived, 2 when deferred sends in the outbox can be flushed or async waits
+// are pending (checked every 256 polls), 0 when this PE must leave the loop.
 __device__ int poll_inbox() {
   pe_state* ps = pes();
   const int me = blockIdx.x;
@@ -604,7 +839,12 @@ __device__ int poll_inbox() {
     if (!idle_t0) {  // about to wait: the senders and the idle check see where we are
       idle_t0 = globaltimer();
       publish_head(ps, me);
-      stamp_progress(me);
+      // deliveries since the last stamp count as progress (a return to the
+      // loop for the outbox or async waits does not)
+      if (ps->stats[ST_DELIVERED] != ps->stamped_delivered) {
+        ps->stamped_delivered = ps->stats[ST_DELIVERED];
+        stamp_progress(me);
+      }
     }
     ++spins;
     if ((spins & 255) == 0) {
@@ -613,7 +853,9 @@ __device__ int poll_inbox() {
         set_error(CHARMING_ERR_DEADLINE, 0, 0);
         return 0;
       }
-      if ((spins & 4095) == 0) {
+      // by time, not by spins: this wait may be cut short by the returns below
+      if (now - ps->slow_check_ns > 100000) {
+        ps->slow_check_ns = now;
         if (c_rt.host_stop) {
           int hs = ld_sys_s32(c_rt.host_stop);
           if (hs == 1) {
@@ -624,9 +866,13 @@ __device__ int poll_inbox() {
             return 0;
           }
         }
-        if (me == 0 && (spins & 65535) == 0) check_idle_timeout(now);
+        if (me == 0 && ++ps->idle_checks % 10 == 0) check_idle_timeout(now);
       }
       ps->stats[ST_IDLE_POLLS] += 256;
+      if ((ps->ob_count > 0 && outbox_head_ready()) || ps->aw_count > 0) {
+        ps->stats[ST_IDLE_NS] += now - idle_t0;
+        return 2;  // deferred sends can go out, or async waits to check
+      }
     }
   }
 }
@@ -700,6 +946,13 @@ __device__ void dispatch_inbox() {
 __device__ void scheduler_loop() {
   pe_state* ps = pes();
   while (true) {
+    if (ps->ob_count > 0) outbox_flush();
+    if (ps->aw_count > 0) {
+      check_async_waits();
+      if (threadIdx.x == 0 && terminated()) ps->term = 1;
+      __syncthreads();
+      if (ps->term) break;
+    }
     if (ps->revive_pending) stash_revive();
     if (ps->n_ready > 0) {
       stash_dispatch_ready();
@@ -717,6 +970,7 @@ __device__ void scheduler_loop() {
       break;
     }
     __syncthreads();
+    if (got == 2) continue;
     dispatch_inbox();
   }
 }
@@ -746,6 +1000,15 @@ charming_scheduler_kernel(int argc, char** argv, size_t* argvs) {
     ps->busy_polls = 0;
     ps->arena_top = 0;
     ps->sarena_top = 0;
+    ps->ob_head = ps->ob_tail = 0;
+    ps->ob_count = 0;
+    ps->ob_lock = 0;
+    ps->uh_head = ps->uh_tail = 0;
+    ps->ub_head = ps->ub_tail = 0;
+    ps->aw_count = 0;
+    ps->stamped_delivered = ~0ULL;
+    ps->slow_check_ns = ps->t0;
+    ps->idle_checks = 0;
     for (int i = 0; i < PROXY_CACHE; i++) ps->pcache[i] = nullptr;
   }
   for (int i = threadIdx.x; i < c_rt.n_pes; i += blockDim.x) head_cache()[i] = c_rt.head[i].v;

@@ -38,6 +38,7 @@ class RunStats:
     status: int
     idle_ms: float = 0.0
     em_ms: float = 0.0
+    deferred: int = 0
 
 
 class Runtime:
@@ -83,7 +84,7 @@ class Runtime:
         self.lib.charming_last_stats(C.byref(st))
         return RunStats(st.delivered, st.sent, st.stashed, st.revived, st.bytes_sent,
                         st.idle_polls, st.space_waits, st.kernel_ms, st.loop_ms, st.main_ms,
-                        st.status, st.idle_ms, st.em_ms)
+                        st.status, st.idle_ms, st.em_ms, st.deferred)
 
     # ---- built-in programs ---------------------------------------------------
     def hello(self) -> np.ndarray:
@@ -121,6 +122,23 @@ class Runtime:
                                        log.ctypes.data_as(C.POINTER(C.c_uint32)), cap,
                                        C.byref(n_logged), C.byref(ms)), "charming_fanout")
         return log[: min(n_logged.value, cap)], ms.value
+
+    def async_wait_chain(self, n_chares: int, broken: bool = False):
+        """Wake order of a chain of async_waits; returns (status, order).
+        A broken chain leaves the last chare waiting, so its run ends with
+        an error status, which is returned rather than raised."""
+        order = (C.c_int * n_chares)()
+        rc = self.lib.charming_async_wait_chain(n_chares, 1 if broken else 0, order, n_chares)
+        if rc and not broken:
+            check(rc, "charming_async_wait_chain")
+        return rc, [order[i] for i in range(n_chares)]
+
+    def user_heap_check(self, n_chares: int, blocks: int, rounds: int, seed: int = 5):
+        out = (C.c_uint64 * 7)()
+        check(self.lib.charming_user_heap_check(n_chares, blocks, rounds, seed, out),
+              "charming_user_heap_check")
+        keys = ("taken", "bad", "failed", "checked", "freed", "done", "bytes")
+        return {k: int(out[i]) for i, k in enumerate(keys)}
 
     def jacobi1d(self, n_chares: int, width: int, sweeps: int):
         out = np.zeros(n_chares * width + 4, dtype=np.float64)

@@ -16,7 +16,7 @@
 
 #define CHARE_TYPE_CNT_MAX 1024 // Maximum number of chare types per PE
 #define EM_CNT_MAX 128          // Maximum number of entry methods per chare type
-#define ASYNC_WAIT_MAX 16       // Kept for source compatibility
+#define ASYNC_WAIT_MAX 16       // Pending async_waits per chare array per PE
 #define MISMATCH_MAX 128        // Kept for source compatibility (stash is per PE)
 
 namespace charm {
@@ -146,6 +146,7 @@ enum : int {
   ERR_TOO_MANY_TYPES = 10,
   ERR_TOO_MANY_EMS = 11,
   ERR_NO_MEMORY = 17,
+  ERR_TOO_MANY_WAITS = 19,
 };
 // Registers proxy `id` in the scheduler's on-chip lookup cache.
 __device__ void cache_proxy(int id, chare_proxy_base* p);
@@ -277,6 +278,8 @@ struct chare_proxy : chare_proxy_base {
     detail::pe_free_array(refnum);
     detail::pe_free_array(loc_map);
     detail::pe_free_array(em_fn);
+    detail::pe_free_array(async_waits);
+    async_waits = nullptr;
     objects = nullptr;
     refnum = nullptr;
     loc_map = nullptr;
@@ -327,6 +330,17 @@ struct chare_proxy : chare_proxy_base {
   inline __device__ void invoke(int idx, int ep, message& msg, size_t size, int ref) {
     send_user_msg(id, idx, ep, msg, size, ref);
   }
+  // The reference's forms (include/chare.h:257-262) take the message by
+  // const reference: the same sends, leaving the caller's copy as it was
+  // (it must not be sent again).
+  inline __device__ void invoke(int idx, int ep, const message& msg) {
+    message m = msg;
+    send_user_msg(id, idx, ep, m, m.capacity, -1);
+  }
+  inline __device__ void invoke(int idx, int ep, const message& msg, size_t size) {
+    message m = msg;
+    send_user_msg(id, idx, ep, m, size, -1);
+  }
   inline __device__ void free_msg(message& msg) {}
 
   // Batched zero-copy messages to chares idx[0..n) (extension, see
@@ -345,6 +359,52 @@ struct chare_proxy : chare_proxy_base {
   inline __device__ void invoke_msgs(const int* idx, int ep, message* msgs, const size_t* sizes,
       const int* refnums, int n) {
     send_user_msgs(id, idx, ep, msgs, sizes, refnums, n);
+  }
+
+  // Single-threaded (reference include/chare.h:214-239, built there for its
+  // GPU-level mode only). Registers a wait: once each of the nelems 64-bit
+  // words at ivars compares true against cmp_value (cmp is one of
+  // charm::CMP_*, the NVSHMEM_CMP_* values), the scheduler runs entry method
+  // ep of local chare idx once, with a null argument, and forgets the wait.
+  // The words are read at device scope, so other PEs publish them with
+  // release stores or atomics; what they wrote before is visible to the
+  // entry method. Up to ASYNC_WAIT_MAX waits per chare array per PE. A wait
+  // that is never satisfied ends the run at the idle timeout.
+  inline __device__ void async_wait(uint64_t* ivars, size_t nelems, int cmp, uint64_t cmp_value,
+      int idx, int ep) {
+    if (idx < start_idx || idx > end_idx || ep < 0 || ep >= em_count || ivars == nullptr ||
+        cmp < CMP_EQ || cmp > CMP_GE) {
+      detail::report_error(detail::ERR_BAD_TARGET, id, idx);
+      return;
+    }
+    if (async_waits == nullptr) {
+      async_waits = detail::pe_array<async_wait_t>(ASYNC_WAIT_MAX);
+      if (async_waits == nullptr) {
+        detail::report_error(detail::ERR_NO_MEMORY, id, idx);
+        return;
+      }
+      for (int i = 0; i < ASYNC_WAIT_MAX; i++) async_waits[i].valid = false;
+    }
+    int free_idx = -1;
+    for (int i = 0; i < ASYNC_WAIT_MAX; i++) {
+      if (!async_waits[i].valid) {
+        free_idx = i;
+        break;
+      }
+    }
+    if (free_idx < 0) {
+      detail::report_error(detail::ERR_TOO_MANY_WAITS, id, idx);
+      return;
+    }
+    async_wait_t& aw = async_waits[free_idx];
+    aw.ivars = ivars;
+    aw.nelems = nelems;
+    aw.cmp = cmp;
+    aw.cmp_value = cmp_value;
+    aw.idx = idx;
+    aw.ep = ep;
+    aw.valid = true;
+    add_async_wait(id);
   }
 
   // Single-threaded (include/chare.h:243-253)

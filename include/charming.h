@@ -41,6 +41,18 @@ __device__ void barrier_local();
 
 __device__ int device_atoi(const char* str, int strlen);
 
+// Memory of the calling PE for the program's own use (reference
+// include/charming.h:33-34, GPU-level mode only there; here on every PE).
+// malloc_user returns `size` bytes (16-byte aligned) of the PE's heap region
+// in device memory, readable and writable by every PE of the GPU, and sets
+// `offset` to the block's offset in that region; nullptr when the region has
+// no room. free_user(size, offset) returns the block; space comes back in
+// allocation order once the older blocks are freed too. Single-threaded;
+// blocks live until free_user or the end of the run. The region's size per
+// PE is CHARMING_USER_HEAP_BYTES (default 1 MiB).
+__device__ void* malloc_user(size_t size, size_t& offset);
+__device__ void free_user(size_t size, size_t offset);
+
 // ---- Extensions of this runtime (not in the reference) -------------------
 // Dynamic shared memory left for entry methods after the runtime's own
 // per-PE state; 16-byte aligned. *bytes receives its size.

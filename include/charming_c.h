@@ -39,7 +39,8 @@ enum {
   CHARMING_ERR_CUDA = 15,           /* CUDA runtime error (see last_error)    */
   CHARMING_ERR_NOT_INIT = 16,       /* charming_init() not called             */
   CHARMING_ERR_NO_MEMORY = 17,      /* allocation or HBM budget exhausted     */
-  CHARMING_ERR_APP = 18             /* built-in program reported a failure    */
+  CHARMING_ERR_APP = 18,            /* built-in program reported a failure    */
+  CHARMING_ERR_TOO_MANY_WAITS = 19  /* > ASYNC_WAIT_MAX pending async_waits    */
 };
 
 /* ---- runtime ------------------------------------------------------------ */
@@ -122,6 +123,8 @@ typedef struct charming_stats {
                                 inbox                                    */
   double em_ms;              /* mean over PEs: time inside entry methods
                                 (SM cycles at the nominal clock)         */
+  uint64_t deferred;         /* sends moved to the sender's outbox because
+                                the destination ring stayed full         */
 } charming_stats;
 int charming_last_stats(charming_stats* out);
 
@@ -215,10 +218,12 @@ int charming_jacobi2d_destroy(void* handle);
  * result with max_sweeps = sweeps and check_every = 0. The second grid
  * lives in a 16 MiB scratch array inside the library (one per GPU, held
  * until exit), so (nx+2)*(ny+2)*element size must be <= 16 MiB, else
- * CHARMING_ERR_CONFIG. Works on the current device and the legacy default
- * stream and returns when done. The first call on a device looks up the
- * scratch's device address; make it before any stream capture. All calls
- * share the scratch: calls that overlap on the GPU race. */
+ * CHARMING_ERR_CONFIG; so are pointers not aligned to the element size.
+ * Works on the current device and the legacy default stream and returns
+ * when done (it synchronises that stream), so it must not be called while
+ * any stream capture is in progress. The first call on a device also looks
+ * up the scratch's device address and the device's multiprocessor count.
+ * All calls share the scratch: calls that overlap on the GPU race. */
 int charming_jacobi2d_sweeps_noalloc(int dtype, int nx, int ny, int sweeps,
     const void* dev_in, void* dev_out);
 

@@ -19,6 +19,12 @@
 #define SM_LEVEL 1
 #endif
 
+namespace charm {
+// Comparisons of chare_proxy<C>::async_wait, with the values of the
+// NVSHMEM_CMP_* constants the reference passes there.
+enum : int { CMP_EQ = 0, CMP_NE = 1, CMP_GT = 2, CMP_LE = 3, CMP_LT = 4, CMP_GE = 5 };
+}  // namespace charm
+
 // Print functions (include/common.h:7-13 of the reference)
 #define PINFO(...) printf("[INFO] " __VA_ARGS__)
 #define PERROR(...) printf("[ERROR] " __VA_ARGS__)

@@ -138,6 +138,11 @@ __device__ void send_user_msgs(int chare_id, const int* chare_idx, int ep_id, me
 // (reference: src/comm/get/get.cu:1316-1345).
 __device__ void revive_mismatches(int chare_id, int chare_idx, int refnum);
 
+// Single-threaded (called by chare_proxy<C>::async_wait): tells the
+// scheduler that a wait was registered on this PE (reference
+// include/message.h:112).
+__device__ void add_async_wait(int chare_id);
+
 } // namespace charm
 
 #endif // _MESSAGE_H_

@@ -105,6 +105,9 @@ template <typename T> inline T atomicCAS(T* p, T c, T v) {
   __atomic_compare_exchange_n(p, &c, v, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST);
   return c;
 }
+template <typename T> inline T atomicExch_block(T* p, T v) { return atomicExch(p, v); }
+template <typename T> inline T atomicCAS_block(T* p, T c, T v) { return atomicCAS(p, c, v); }
+inline void __threadfence_block() { std::atomic_thread_fence(std::memory_order_seq_cst); }
 template <typename T> inline T atomicMax(T* p, T v) {
   T old = __atomic_load_n(p, __ATOMIC_SEQ_CST);
   while (v > old && !__atomic_compare_exchange_n(p, &old, v, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST)) {

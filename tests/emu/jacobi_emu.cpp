@@ -54,32 +54,35 @@ struct Stashed {
 
 // Barrier of one PE block (or warp) that also checks that all threads
 // arrive from the same call site.
+// Arrivals are counted under a mutex (which also checks the call site);
+// waiters spin on the generation word and yield the core (much cheaper than
+// waking every thread through a condition variable at each barrier).
 struct SiteBarrier {
   std::mutex m;
-  std::condition_variable cv;
   int n = 1, count = 0;
-  unsigned long long gen = 0;
+  std::atomic<unsigned long long> gen{0};
   const char* file = nullptr;
   int line = 0;
   void sync(const char* f, int l) {
-    std::unique_lock<std::mutex> lk(m);
-    if (count == 0) {
-      file = f;
-      line = l;
-    } else if (l != line || strcmp(f, file) != 0) {
-      fprintf(stderr, "barrier divergence: thread %u at %s:%d, others at %s:%d\n", threadIdx.x, f,
-              l, file, line);
-      fflush(stderr);
-      _exit(3);
+    const unsigned long long g = gen.load(std::memory_order_acquire);
+    {
+      std::lock_guard<std::mutex> lk(m);
+      if (count == 0) {
+        file = f;
+        line = l;
+      } else if (l != line || strcmp(f, file) != 0) {
+        fprintf(stderr, "barrier divergence: thread %u at %s:%d, others at %s:%d\n", threadIdx.x, f,
+                l, file, line);
+        fflush(stderr);
+        _exit(3);
+      }
+      if (++count == n) {
+        count = 0;
+        gen.store(g + 1, std::memory_order_release);
+        return;
+      }
     }
-    if (++count == n) {
-      count = 0;
-      gen++;
-      cv.notify_all();
-    } else {
-      unsigned long long g = gen;
-      cv.wait(lk, [&] { return gen != g; });
-    }
+    while (gen.load(std::memory_order_acquire) == g) std::this_thread::yield();
   }
 };
 

@@ -54,32 +54,36 @@ void emu_sync(const char*, int) {}  // one thread per block
 // One PE block of blockDim.x threads: a barrier that checks every thread
 // arrives from the same call site, and warps of 32 in lockstep.
 namespace {
+// Arrivals are counted under a mutex (which also checks the call site);
+// waiters spin on the generation word and yield the core, which costs far
+// less than a condition-variable wake-up of every thread per barrier (a
+// PE block of 64 host threads passes several barriers per message).
 struct SiteBarrier {
   std::mutex m;
-  std::condition_variable cv;
   int n = 1, count = 0;
-  unsigned long long gen = 0;
+  std::atomic<unsigned long long> gen{0};
   const char* file = nullptr;
   int line = 0;
   void sync(const char* f, int l) {
-    std::unique_lock<std::mutex> lk(m);
-    if (count == 0) {
-      file = f;
-      line = l;
-    } else if (l != line || strcmp(f, file) != 0) {
-      fprintf(stderr, "barrier divergence: thread %u at %s:%d, others at %s:%d\n", threadIdx.x, f, l,
-              file, line);
-      fflush(stderr);
-      _exit(3);
+    const unsigned long long g = gen.load(std::memory_order_acquire);
+    {
+      std::lock_guard<std::mutex> lk(m);
+      if (count == 0) {
+        file = f;
+        line = l;
+      } else if (l != line || strcmp(f, file) != 0) {
+        fprintf(stderr, "barrier divergence: thread %u at %s:%d, others at %s:%d\n", threadIdx.x, f, l,
+                file, line);
+        fflush(stderr);
+        _exit(3);
+      }
+      if (++count == n) {
+        count = 0;
+        gen.store(g + 1, std::memory_order_release);
+        return;
+      }
     }
-    if (++count == n) {
-      count = 0;
-      gen++;
-      cv.notify_all();
-    } else {
-      unsigned long long g = gen;
-      cv.wait(lk, [&] { return gen != g; });
-    }
+    while (gen.load(std::memory_order_acquire) == g) std::this_thread::yield();
   }
 };
 SiteBarrier g_block;
@@ -179,7 +183,14 @@ void init_runtime(int n_pes, size_t ring_bytes) {
   ds.smem_state_bytes = (int)((sizeof(pe_state) + 8ull * n_pes + 127) / 128 * 128);
   ds.smem_total = SMEM_BYTES;
   ds.smem_arena_bytes = 8 << 10;
+  // The run deadline guards against a hung emulation. A PE block of many
+  // host threads is slow (every block barrier is a rendezvous of all of
+  // them), so its runs get proportionally longer.
   ds.deadline_ns = 60ull * 1000000000ull;
+  if (const char* t = getenv("RT_EMU_THREADS")) {
+    const int th = atoi(t);
+    if (th > 16) ds.deadline_ns = ds.deadline_ns / 16 * (unsigned long long)th;
+  }
   ds.idle_timeout_ns = 5ull * 1000000000ull;
   ds.tail = zalloc<line_u64>(n_pes);
   ds.head = zalloc<line_u64>(n_pes);
@@ -196,10 +207,19 @@ void init_runtime(int n_pes, size_t ring_bytes) {
   ds.free_chares_at_exit = 1;
   ds.arena_bytes = 64 << 10;
   ds.arena = zalloc<unsigned char>(ds.arena_bytes * n_pes);
+  ds.outbox_bytes = 2 * ds.max_msg + (64 << 10);
+  ds.outbox_stride = ds.outbox_bytes + (ds.max_msg + OB_HDR + 127) / 128 * 128;
+  ds.outbox = zalloc<unsigned char>(ds.outbox_stride * n_pes);
+  ds.user_heap_bytes = 64 << 10;
+  ds.user_blocks_max = 64;
+  ds.user_heap = zalloc<unsigned char>(ds.user_heap_bytes * n_pes);
+  ds.user_blocks = zalloc<user_block>((size_t)ds.user_blocks_max * n_pes);
   c_rt = ds;
   c_n_pes = c_n_pes_node = c_n_sms = n_pes;
   c_n_nodes = c_n_devs = c_n_devs_node = 1;
 }
+
+unsigned long long g_deferred = 0;  // sends moved to an outbox in the last run
 
 int run_scheduler(int n_pes, int threads) {
   blockIdx = emu_dim3{0, 0, 0};
@@ -232,6 +252,9 @@ int run_scheduler(int n_pes, int threads) {
     }
   }
   for (auto& t : th) t.join();
+  g_deferred = 0;
+  for (int p = 0; p < n_pes; p++)
+    g_deferred += charm::rt::c_rt.pe_stats[(size_t)p * charm::rt::N_STATS + charm::rt::ST_DEFERRED];
   const int* ctl = charm::rt::c_rt.ctrl;
   if (ctl[charm::rt::CTRL_STATUS])
     fprintf(stderr, "run status %d: pe %d info %d %d\n", ctl[charm::rt::CTRL_STATUS], ctl[charm::rt::CTRL_ERR_PE],
@@ -351,7 +374,8 @@ int serve_run(int n_pes, int threads, int n_req, unsigned long long seed, int wp
   const double t0 = wall_s();
   int next = 0, completed = 0, bad = 0;
   unsigned long long comp_next = 0;
-  while (completed < n_req && wall_s() - t0 < 120.0 && !ended) {
+  const double host_limit_s = 2e-9 * (double)charm::rt::c_rt.deadline_ns;
+  while (completed < n_req && wall_s() - t0 < host_limit_s && !ended) {
     const double now = wall_s() - t0;
     while (next < n_req && reqs[next].at <= now) {
       if (st.submit(reqs[next].q, (uint64_t)next, now) != CHARMING_OK) {
@@ -466,7 +490,7 @@ int main(int argc, char** argv) {
       g_app.p[2] = expected.data();
       status = run_scheduler(n_pes, threads);
     }
-    printf("status=%d delivered=%llu\n", status, (unsigned long long)ctr[1]);
+    printf("status=%d delivered=%llu deferred=%llu\n", status, (unsigned long long)ctr[1], g_deferred);
     unsigned long long nrec = std::min<unsigned long long>(ctr[0], total);
     for (unsigned long long r = 0; r < nrec; r++) {
       printf("L");
@@ -482,6 +506,39 @@ int main(int argc, char** argv) {
     int wpp = atoi(argv[6]), max_inflight = atoi(argv[7]), side = atoi(argv[8]), dt = atoi(argv[9]);
     return dt == 0 ? serve_run<double>(n_pes, threads, n_req, seed, wpp, max_inflight, side)
                    : serve_run<float>(n_pes, threads, n_req, seed, wpp, max_inflight, side);
+  }
+  if (app == "await") {  // rt_emu await n_pes ring_bytes n_chares broken
+    if (argc < 6) return 2;
+    int n = atoi(argv[4]), broken = atoi(argv[5]);
+    std::vector<unsigned long long> sig(2 * (size_t)n + 2, 0), ctr(2, 0);
+    std::vector<int> order(n, -1);
+    sig[0] = sig[1] = 1;
+    g_app.id = suite::APP_ASYNC_WAIT;
+    g_app.a[0] = n;
+    g_app.a[1] = broken;
+    g_app.p[0] = sig.data();
+    g_app.p[1] = order.data();
+    g_app.p[2] = ctr.data();
+    if (broken) charm::rt::c_rt.idle_timeout_ns = 1000000000ull;
+    int status = run_scheduler(n_pes, threads);
+    printf("status=%d order=", status);
+    for (int v : order) printf("%d,", v);
+    printf("\n");
+    return 0;
+  }
+  if (app == "userheap") {  // rt_emu userheap n_pes ring_bytes n_chares blocks rounds seed
+    if (argc < 8) return 2;
+    std::vector<unsigned long long> ctr(8, 0);
+    g_app.id = suite::APP_USER_HEAP;
+    g_app.a[0] = atoi(argv[4]);
+    g_app.a[1] = atoi(argv[5]);
+    g_app.a[2] = atoi(argv[6]);
+    g_app.a[3] = (long long)strtoull(argv[7], nullptr, 0);
+    g_app.p[0] = ctr.data();
+    int status = run_scheduler(n_pes, threads);
+    printf("status=%d taken=%llu bad=%llu failed=%llu checked=%llu freed=%llu done=%llu bytes=%llu\n", status,
+           ctr[0], ctr[1], ctr[2], ctr[3], ctr[4], ctr[5], ctr[6]);
+    return 0;
   }
   if (app == "hello" || app == "refnum") {
     std::vector<int> out(4 * n_pes + 16, -1);

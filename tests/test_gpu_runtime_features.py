@@ -1,0 +1,81 @@
+"""GPU tests of the runtime features beyond plain invoke: async_wait
+(reference include/chare.h:214-239, src/comm/get/get.cu:1172-1202),
+malloc_user / free_user (include/charming.h:33-34, get.cu:1348-1362), and
+sends that find their destination ring full (the outbox). Runs that need a
+non-default configuration (short idle timeout, small rings) go to a child
+process, so the session's runtime keeps its defaults."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+from oracle import msgmodel
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def child(code, env=None, timeout=300):
+    e = dict(os.environ, **(env or {}))
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True,
+                       timeout=timeout, env=e)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-3000:]
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def test_async_wait_chain_wakes_in_order(rt):
+    n = 3 * rt.n_pes  # several waits pending on every PE at once
+    status, order = rt.async_wait_chain(n)
+    assert status == 0
+    assert order == list(range(n))
+
+
+def test_async_wait_never_satisfied_ends_with_idle_timeout():
+    # nobody signals the last chare: its wait runs out at the (1 s) idle
+    # timeout, the run returns that status and the device stays usable
+    out = child(
+        "import json\n"
+        "from charming_b200 import runtime\n"
+        "rt = runtime()\n"
+        "st, order = rt.async_wait_chain(40, broken=True)\n"
+        "st2, order2 = rt.async_wait_chain(40)\n"
+        "print(json.dumps([st, order, st2, order2]))\n",
+        env={"CHARMING_IDLE_TIMEOUT_S": "1"})
+    st, order, st2, order2 = out
+    assert st == 5  # CHARMING_ERR_IDLE_TIMEOUT
+    assert order == list(range(39)) + [-1]
+    assert st2 == 0 and order2 == list(range(40))
+
+
+def test_user_heap_blocks_reused_and_visible_across_pes(rt):
+    n = 2 * rt.n_pes
+    out = rt.user_heap_check(n, blocks=8, rounds=300, seed=9)
+    assert out["bad"] == 0 and out["failed"] == 0
+    assert out["taken"] == out["freed"]
+    assert out["checked"] == n and out["done"] == n
+    # each PE took more than its 1 MiB heap over the run
+    assert out["bytes"] > 2 * rt.n_pes * (1 << 20)
+
+
+@pytest.mark.parametrize("n,msgs,payload,mode", [(2048, 16, 256, 1), (1024, 8, 1024, 0)])
+def test_full_rings_defer_sends(n, msgs, payload, mode):
+    # 8 KiB inbox rings: the start entry methods send far more than the
+    # rings hold, to PEs doing the same; full rings move sends to the
+    # outbox and the run completes with the model's delivery log
+    seed = 0xDEF + n
+    out = child(
+        "import json\n"
+        "from charming_b200 import runtime\n"
+        "from oracle import msgmodel\n"
+        "rt = runtime(ring_bytes=8192, max_msg_bytes=4096)\n"
+        f"log, _ = rt.fanout({n}, {msgs}, {payload}, {seed}, {mode})\n"
+        "st = rt.last_stats()\n"
+        f"chk = msgmodel.check_fanout_log(log, {n}, {msgs}, {payload}, {seed}, {mode})\n"
+        "print(json.dumps([chk.ok, chk.delivered, st.deferred, chk.errors[:5]]))\n")
+    ok, delivered, deferred, errors = out
+    assert ok, errors
+    assert delivered == n * msgs
+    assert deferred > 0

@@ -47,6 +47,7 @@ def fanout(exe, n_pes, ring, n, msgs, payload, seed, mode, threads=1):
     chk = msgmodel.check_fanout_log(log, n, msgs, payload, seed, mode)
     assert chk.ok, chk.errors
     assert chk.delivered == n * msgs
+    return int(head.split("deferred=")[1])
 
 
 @pytest.mark.parametrize("n_pes,ring,n,msgs,payload,mode", [
@@ -77,6 +78,22 @@ def test_fanout_block_collective_paths(emus, threads, n, msgs, payload, mode, ri
     fanout(emus["rt_emu_mt"], 1, ring, n, msgs, payload, 0xC0FFEE, mode, threads)
 
 
+@pytest.mark.parametrize("exe,n_pes,threads,ring,n,msgs,payload,mode", [
+    # every PE's start entry methods send far more than the receivers'
+    # rings hold, to PEs that are doing the same: each send that finds no
+    # space moves to the sender's outbox, the entry method returns, and the
+    # scheduler loop copies it into the ring later (before: RING_FULL)
+    ("rt_emu", 8, 1, 2048, 64, 16, 256, 0),
+    ("rt_emu", 4, 1, 2048, 8, 16, 1024, 1),
+    ("rt_emu_tsan", 8, 1, 2048, 64, 8, 256, 1),
+    ("rt_emu_mt", 1, 32, 2048, 16, 8, 256, 1),   # one PE sending to itself
+])
+def test_full_rings_defer_sends_instead_of_deadlock(emus, exe, n_pes, threads, ring, n, msgs, payload,
+                                                   mode):
+    deferred = fanout(emus[exe], n_pes, ring, n, msgs, payload, 0xDEF + n, mode, threads)
+    assert deferred > 0
+
+
 @pytest.mark.parametrize("reversed_order", [0, 1])
 @pytest.mark.parametrize("exe,n_pes,threads", [("rt_emu", 6, 1), ("rt_emu_mt", 1, 64)])
 def test_refnum_scenario(emus, exe, n_pes, threads, reversed_order):
@@ -94,12 +111,56 @@ def test_hello_chain(emus, exe, n_pes, threads):
     assert out[: 2 * n_pes] == list(range(2 * n_pes))
 
 
-def serve(exe, n_pes, n_req, seed, wpp, max_inflight, side, dtype, threads=1):
+@pytest.mark.parametrize("exe,n_pes,threads,n", [
+    ("rt_emu", 4, 1, 12), ("rt_emu_tsan", 6, 1, 18), ("rt_emu_mt", 1, 64, 5)])
+def test_async_wait_chain(emus, exe, n_pes, threads, n):
+    """Chare i's entry method runs once its two signal words are >= 1, which
+    chare i-1 sets when it runs: the wake order is the chain order, and
+    several waits are pending per PE at once."""
+    r = run(emus[exe], ["await", n_pes, 65536, n, 0], threads)
+    out = r.stdout.strip().split("order=")
+    assert out[0].strip() == "status=0", r.stdout + r.stderr[-2000:]
+    assert [int(x) for x in out[1].strip(",").split(",")] == list(range(n))
+
+
+@pytest.mark.parametrize("exe,n_pes,threads,n", [
+    ("rt_emu", 6, 1, 18), ("rt_emu_tsan", 3, 1, 9), ("rt_emu_mt", 1, 64, 5)])
+def test_async_wait_never_satisfied_ends_at_idle_timeout(emus, exe, n_pes, threads, n):
+    """Nobody signals the last chare: its wait runs out at the idle timeout
+    (1 s here) and the run returns that error status; the others woke in
+    order."""
+    r = run(emus[exe], ["await", n_pes, 65536, n, 1], threads, timeout=120)
+    out = r.stdout.strip().split("order=")
+    assert out[0].strip() == "status=5", r.stdout + r.stderr[-2000:]
+    assert [int(x) for x in out[1].strip(",").split(",")] == list(range(n - 1)) + [-1]
+
+
+@pytest.mark.parametrize("exe,n_pes,threads,n,blocks,rounds", [
+    ("rt_emu", 4, 1, 8, 8, 60),       # heaps of 64 KiB wrap many times
+    ("rt_emu_tsan", 4, 1, 8, 5, 60),
+    ("rt_emu_mt", 1, 64, 3, 8, 20),
+])
+def test_user_heap(emus, exe, n_pes, threads, n, blocks, rounds):
+    """malloc_user / free_user: blocks keep their contents until freed,
+    space comes back after out-of-order frees (more bytes are taken over
+    the run than the heap holds), and a block is readable from another
+    PE."""
+    r = run(emus[exe], ["userheap", n_pes, 65536, n, blocks, rounds, 5], threads)
+    f = dict(kv.split("=") for kv in r.stdout.split())
+    assert f["status"] == "0", r.stdout + r.stderr[-2000:]
+    assert int(f["bad"]) == 0
+    assert int(f["taken"]) == int(f["freed"]) and int(f["failed"]) == 0
+    assert int(f["checked"]) == n and int(f["done"]) == n
+    # the PEs took several times their 64 KiB heaps over the run
+    assert int(f["bytes"]) > 3 * n_pes * 65536
+
+
+def serve(exe, n_pes, n_req, seed, wpp, max_inflight, side, dtype, threads=1, ring=65536):
     """Solve server on the CPU: the real scheduler runs the Jacobi2d chares
     in serving mode (apps/jacobi2d.cu) and admission runs apps/serve_host.h;
     a host thread submits seeded requests of mixed sizes while others run
     and compares every result bit for bit with the serial oracle."""
-    r = run(exe, ["serve", n_pes, 65536, n_req, seed, wpp, max_inflight, side, dtype], threads, timeout=900)
+    r = run(exe, ["serve", n_pes, ring, n_req, seed, wpp, max_inflight, side, dtype], threads, timeout=900)
     lines = r.stdout.splitlines()
     assert r.returncode == 0 and lines and "bad=0" in lines[-1], (lines[-5:], r.stderr[-2000:])
     results = [l for l in lines if l.startswith("R ")]
@@ -111,15 +172,16 @@ def serve(exe, n_pes, n_req, seed, wpp, max_inflight, side, dtype, threads=1):
     return results
 
 
-@pytest.mark.parametrize("exe,n_pes,threads,n_req,dtype,seed", [
-    ("rt_emu", 6, 1, 40, 0, 7),        # ASan + UBSan, FP64
-    ("rt_emu", 6, 1, 40, 1, 8),        # FP32 sweeps, FP64 residual
-    ("rt_emu_tsan", 8, 1, 30, 1, 11),  # PE threads under ThreadSanitizer
-    ("rt_emu_mt", 1, 64, 10, 0, 5),    # one PE block of 64 threads
+@pytest.mark.parametrize("exe,n_pes,threads,n_req,dtype,seed,ring", [
+    ("rt_emu", 6, 1, 40, 0, 7, 65536),        # ASan + UBSan, FP64
+    ("rt_emu", 6, 1, 40, 1, 8, 65536),        # FP32 sweeps, FP64 residual
+    ("rt_emu_tsan", 8, 1, 30, 1, 11, 65536),  # PE threads under ThreadSanitizer
+    ("rt_emu_mt", 1, 64, 10, 0, 5, 65536),    # one PE block of 64 threads
+    ("rt_emu_mt", 1, 64, 10, 0, 5, 4096),     # and with rings that fill up
 ])
-def test_serving_results_match_oracle(emus, exe, n_pes, threads, n_req, dtype, seed):
+def test_serving_results_match_oracle(emus, exe, n_pes, threads, n_req, dtype, seed, ring):
     wpp = 6 if n_pes == 1 else 3
-    serve(emus[exe], n_pes, n_req, seed, wpp, 4, 16, dtype, threads)
+    serve(emus[exe], n_pes, n_req, seed, wpp, 4, 16, dtype, threads, ring=ring)
 
 
 @pytest.mark.parametrize("exe,n_pes,threads", [("rt_emu", 4, 1), ("rt_emu_mt", 1, 32)])

@@ -20,7 +20,7 @@ import pytest
 
 from charming_b200 import _lib
 from charming_b200.jacobi import Jacobi2D, Problem
-from oracle.jacobi import seeded_grid
+from oracle.jacobi import jacobi2d, seeded_grid
 
 
 def chare_result(grid, sweeps, dtype):
@@ -60,6 +60,8 @@ def test_noalloc_matches_chare_entry_point_twice(rt, dtype):
         ref = chare_result(g, sweeps, dtype)
         out = noalloc_result(lib, torch, g, sweeps, dtype)
         assert np.array_equal(bits(out), bits(ref)), (nx, ny, sweeps)
+        if dtype == "f64":  # and with the serial oracle itself
+            assert np.array_equal(bits(out), bits(jacobi2d(g, sweeps))), (nx, ny, sweeps)
 
 
 @pytest.mark.gpu
@@ -89,3 +91,11 @@ def test_noalloc_rejects_oversize_and_bad_arguments():
     assert fn(_lib.F64, 10, 10, -1, buf_a, buf_b) == 14
     assert fn(_lib.F64, 10, 10, 1, None, buf_b) == 14
     assert fn(_lib.F64, 10, 10, 1, buf_a, C.c_void_p((1 << 20) + 64)) == 14  # overlap
+    # element pointers not aligned to the element size
+    assert fn(_lib.F64, 10, 10, 1, C.c_void_p((1 << 20) + 4), buf_b) == 14
+    assert b"aligned" in lib.charming_last_error()
+    assert fn(_lib.F32, 10, 10, 1, buf_a, C.c_void_p((1 << 30) + 2)) == 14
+    # sizes whose +2 would overflow a 32-bit int
+    assert fn(_lib.F64, 2**31 - 1, 1, 1, buf_a, buf_b) == 14
+    assert fn(_lib.F32, 1, 2**31 - 2, 1, buf_a, buf_b) == 14
+    assert b"16 MiB" in lib.charming_last_error()
