@@ -547,6 +547,8 @@ def main() -> int:
     ap.add_argument("--tile-w", type=int, default=0)
     ap.add_argument("--depth", type=int, default=0,
                     help="sweeps per halo exchange (ghost depth), 0: 6 (direct) / 1 (TMA)")
+    ap.add_argument("--threads-per-pe", type=int, default=512)
+    ap.add_argument("--pes-per-sm", type=int, default=1)
     ap.add_argument("--small-buffers", action="store_true",
                     help="1 MiB inbox rings and stashes (smaller device footprint for ncu)")
     ap.add_argument("--headline-only", action="store_true",
@@ -566,7 +568,7 @@ def main() -> int:
 
     from charming_b200 import runtime
     from charming_b200.jacobi import Jacobi2D, Problem, initial_grid
-    cfg = dict(device=local)
+    cfg = dict(device=local, threads_per_pe=args.threads_per_pe, pes_per_sm=args.pes_per_sm)
     if args.small_buffers:
         cfg.update(ring_bytes=1 << 20, stash_bytes=2 << 20, max_msg_bytes=(256 << 10))
     rt = runtime(**cfg)

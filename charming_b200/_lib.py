@@ -144,6 +144,9 @@ SIGNATURES = [
     ("charming_refnum", i32, [C.POINTER(i32), i32, C.POINTER(i32)]),
     ("charming_refnum_reversed", i32, [C.POINTER(i32), i32, C.POINTER(i32)]),
     ("charming_async_wait_chain", i32, [i32, i32, C.POINTER(i32), i32]),
+    ("charming_sm_pingpong", i32, [i32, i32, C.POINTER(f64), C.POINTER(f64), C.POINTER(i32)]),
+    ("charming_sweep_bench", i32, [i32, i32, i32, i32, i32, i32, i32, C.POINTER(f64)]),
+    ("charming_jacobi2d_decomp1d", i32, [i32, i32, i32, i32, i32, C.POINTER(C.c_float), C.POINTER(f64)]),
     ("charming_user_heap_check", i32, [i32, i32, i32, u64, C.POINTER(u64)]),
     ("charming_serve_start", i32, [C.POINTER(ServeConfig), C.POINTER(vp)]),
     ("charming_serve_submit", i32, [vp, C.POINTER(JacobiProblem), u64]),

@@ -40,6 +40,8 @@ struct japp {
   __device__ static int pipeline() { return (int)g_app.a[3]; }
   __device__ static int tile_w() { return (int)g_app.a[4]; }
   __device__ static int halo_mode() { return (int)g_app.a[5]; }
+  // multi-sweep passes: 0 phase-split items, 1 the single-loop items
+  __device__ static bool deep_lean() { return g_app.a[9] == 0; }
   __device__ static const jac::chare_desc* chares() {
     return reinterpret_cast<const jac::chare_desc*>(g_app.p[0]);
   }
@@ -170,8 +172,8 @@ __device__ double sweep_block(const jac::chare_desc& d, int cur, bool resid, int
     int fixed = (d.nbr[jac::TOP] < 0 ? 1 : 0) | (d.nbr[jac::BOTTOM] < 0 ? 2 : 0) |
                 (d.nbr[jac::LEFT] < 0 ? 4 : 0) | (d.nbr[jac::RIGHT] < 0 ? 8 : 0);
     __syncthreads();
-    acc = resid ? jac::sweep_deep<T, true>(in, out, d.w, d.h, L, fixed)
-                : jac::sweep_deep<T, false>(in, out, d.w, d.h, L, fixed);
+    acc = resid ? jac::sweep_deep<T, true>(in, out, d.w, d.h, L, fixed, japp::deep_lean())
+                : jac::sweep_deep<T, false>(in, out, d.w, d.h, L, fixed, japp::deep_lean());
     __syncthreads();
     done = true;
   }

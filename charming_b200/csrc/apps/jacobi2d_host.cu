@@ -201,6 +201,9 @@ extern "C" int charming_jacobi2d_create(const charming_jacobi_problem* probs, in
   ap.a[3] = opt->pipeline;
   ap.a[4] = opt->tile_w;
   ap.a[5] = opt->halo_mode;
+  // CHARMING_DEEP_CHAINED=1: multi-sweep passes on the single-loop items
+  // (the phase-split ones are the default; both give the same bits)
+  ap.a[9] = getenv("CHARMING_DEEP_CHAINED") && atoi(getenv("CHARMING_DEEP_CHAINED")) ? 1 : 0;
   ap.p[0] = h->d_chares;
   ap.p[1] = h->d_probs;
   ap.p[2] = h->d_results;

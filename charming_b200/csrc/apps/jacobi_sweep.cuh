@@ -408,12 +408,36 @@ struct deep_lane {
   int fix_r0, fix_r1;              // rows kept at every level (0 / h+1), or INT_MIN
 };
 
+// The lane constants of the strip whose owned vectors are own0..own0+nown-1
+// (the lane's vector starts E = ceil(L/VEC) vectors before them).
+template <typename T, int L>
+__device__ __forceinline__ deep_lane<T> make_lane(int w, int h, int fixed, int own0, int nown, int lane) {
+  constexpr int V = traits<T>::VEC, E = (L + V - 1) / V;
+  deep_lane<T> ln;
+  ln.v = own0 - E + lane;
+  ln.col0 = 1 + ln.v * V;
+  ln.own = ln.v >= own0 && ln.v < own0 + nown;
+  ln.anyfix = false;
+#pragma unroll
+  for (int k = 0; k < V; k++) {
+    const int c = ln.col0 + k;
+    ln.fixc[k] = (c == 0 && (fixed & 4)) || (c == w + 1 && (fixed & 8));
+    ln.inw[k] = c >= 1 && c <= w;
+    ln.anyfix = ln.anyfix || ln.fixc[k];
+  }
+  ln.fix_r0 = (fixed & 1) ? 0 : INT_MIN;
+  ln.fix_r1 = (fixed & 2) ? h + 1 : INT_MIN;
+  return ln;
+}
+
 // All L levels of the wavefront at sub-step K of a three-step cycle (level-l
 // row r lives in W[l][(r - qs) mod 3], so every window index is static).
 // CHECK: a level runs only once its three input rows exist (the first 2L
 // steps of an item). Domain-boundary cells keep their value at every level:
 // a whole row by a warp-uniform branch, a column by a per-lane fix-up.
-template <typename T, bool RESID, int L, int K, bool CHECK>
+// ROWFIX / COLFIX false: the step cannot meet a domain-boundary row / the
+// strip holds no domain-boundary column, so those tests are left out.
+template <typename T, bool RESID, int L, int K, bool CHECK, bool ROWFIX = true, bool COLFIX = true>
 __device__ __forceinline__ void deep_step(typename vec_of<T>::type (&W)[L][3], int q, int qs, int w,
     const deep_lane<T>& ln, int r0, int r1, const block_view<T>& out, double& acc) {
   constexpr int V = traits<T>::VEC;
@@ -430,7 +454,7 @@ __device__ __forceinline__ void deep_step(typename vec_of<T>::type (&W)[L][3], i
     vec_to<T>(W[l - 1][sd], d);
     T left = __shfl_up_sync(FULL, m[V - 1], 1);
     T right = __shfl_down_sync(FULL, m[0], 1);
-    if (r == ln.fix_r0 || r == ln.fix_r1) {  // domain-boundary row: kept (warp-uniform)
+    if (ROWFIX && (r == ln.fix_r0 || r == ln.fix_r1)) {  // domain-boundary row: kept (warp-uniform)
 #pragma unroll
       for (int k = 0; k < V; k++) o[k] = m[k];
     } else {
@@ -442,7 +466,7 @@ __device__ __forceinline__ void deep_step(typename vec_of<T>::type (&W)[L][3], i
         if (RESID && l == 1 && ln.own && ln.inw[k] && r >= r0 && r < r1)
           acc += resid2<T>(m[k], lk, rk, u[k], d[k]);
       }
-      if (ln.anyfix) {  // the lane holding column 0 or w+1 of the domain
+      if (COLFIX && ln.anyfix) {  // the lane holding column 0 or w+1 of the domain
 #pragma unroll
         for (int k = 0; k < V; k++)
           if (ln.fixc[k]) o[k] = m[k];
@@ -528,6 +552,84 @@ __device__ __forceinline__ double deep_item(const block_view<T>& in, const block
   return acc;
 }
 
+// ---------------------------------------------------------------------------
+// The same item in three phases, so that the steady state carries no test
+// it cannot need: the fill (levels without all three input rows yet, and
+// the top boundary row, which only the first 2L steps can meet), the steady
+// state, and the tail (the last steps, where a level can meet the bottom
+// boundary row). A strip without a domain-boundary column (all but the
+// outermost strips of a chare on the domain's edge) runs a version without
+// the per-lane column fix-up. Same arithmetic and results as deep_item.
+// ---------------------------------------------------------------------------
+// Not inlined: each version gets its own register allocation (two inlined
+// bodies in one function spill).
+template <typename T, bool RESID, int L, int P, bool COLFIX>
+__device__ __noinline__ double lean_body(block_view<T> in, block_view<T> out, int w, int h, int fixed,
+    int own0, int nown, int r0, int r1, int lane, typename vec_of<T>::type* ring) {
+  constexpr int V = traits<T>::VEC;
+  const deep_lane<T> ln = make_lane<T, L>(w, h, fixed, own0, nown, lane);
+  using VT = typename vec_of<T>::type;
+  const long long e0 = (long long)traits<T>::OFF - 1 + ln.col0;  // element index in a row
+  const bool can_load = e0 >= 0 && e0 + V <= in.pitch;
+  const long long eo = can_load ? e0 : 0;
+  const unsigned nb = can_load ? 16u : 0u;
+  const int qs = r0 - L, qe = r1 - 1 + L;  // level-0 rows streamed
+  // first step at which a level may compute the bottom boundary row R
+  // (level l computes row q - l; levels 1..L-1 reach R at steps R+1..R+L-1)
+  const int q_tail = (ln.fix_r1 != INT_MIN && ln.fix_r1 + 1 <= qe) ? ln.fix_r1 + 1 : qe + 1;
+#pragma unroll
+  for (int k = 0; k < P - 1; k++) {
+    if (qs + k <= qe) cp_async16(&ring[k * 32 + lane], in.row(qs + k) + eo, nb);
+    cp_async_commit();
+  }
+  VT W[L][3];
+  double acc = 0.0;
+  int slot = 0;
+  constexpr int F = (2 * L + 2) / 3 * 3;
+  int q0 = qs;
+  for (; q0 < qs + F && q0 <= qe; q0 += 3) {  // fill
+#pragma unroll
+    for (int K = 0; K < 3; K++) {
+      const int q = q0 + K;
+      if (q > qe) break;
+      deep_fetch<T, P>(ring, lane, slot, q, qe, in, eo, nb, W[0][K]);
+      if (K == 0) deep_step<T, RESID, L, 0, true, true, COLFIX>(W, q, qs, w, ln, r0, r1, out, acc);
+      else if (K == 1) deep_step<T, RESID, L, 1, true, true, COLFIX>(W, q, qs, w, ln, r0, r1, out, acc);
+      else deep_step<T, RESID, L, 2, true, true, COLFIX>(W, q, qs, w, ln, r0, r1, out, acc);
+    }
+  }
+  for (; q0 + 2 < q_tail; q0 += 3) {  // steady: three whole steps before the tail
+    deep_fetch<T, P>(ring, lane, slot, q0, qe, in, eo, nb, W[0][0]);
+    deep_step<T, RESID, L, 0, false, false, COLFIX>(W, q0, qs, w, ln, r0, r1, out, acc);
+    deep_fetch<T, P>(ring, lane, slot, q0 + 1, qe, in, eo, nb, W[0][1]);
+    deep_step<T, RESID, L, 1, false, false, COLFIX>(W, q0 + 1, qs, w, ln, r0, r1, out, acc);
+    deep_fetch<T, P>(ring, lane, slot, q0 + 2, qe, in, eo, nb, W[0][2]);
+    deep_step<T, RESID, L, 2, false, false, COLFIX>(W, q0 + 2, qs, w, ln, r0, r1, out, acc);
+  }
+  for (; q0 <= qe; q0 += 3) {  // tail
+#pragma unroll
+    for (int K = 0; K < 3; K++) {
+      const int q = q0 + K;
+      if (q > qe) break;
+      deep_fetch<T, P>(ring, lane, slot, q, qe, in, eo, nb, W[0][K]);
+      if (K == 0) deep_step<T, RESID, L, 0, false, true, COLFIX>(W, q, qs, w, ln, r0, r1, out, acc);
+      else if (K == 1) deep_step<T, RESID, L, 1, false, true, COLFIX>(W, q, qs, w, ln, r0, r1, out, acc);
+      else deep_step<T, RESID, L, 2, false, true, COLFIX>(W, q, qs, w, ln, r0, r1, out, acc);
+    }
+  }
+  cp_async_wait<0>();
+  return acc;
+}
+
+template <typename T, bool RESID, int L, int P>
+__device__ __forceinline__ double lean_item(const block_view<T>& in, const block_view<T>& out, int w, int h,
+    int fixed, int own0, int nown, const deep_lane<T>& ln, int r0, int r1, int lane,
+    typename vec_of<T>::type* ring) {
+  if (__any_sync(0xffffffffu, ln.anyfix))
+    return lean_body<T, RESID, L, P, true>(in, out, w, h, fixed, own0, nown, r0, r1, lane, ring);
+  return lean_body<T, RESID, L, P, false>(in, out, w, h, fixed, own0, nown, r0, r1, lane, ring);
+}
+
 // The same pass, computed by thread 0 alone for blocks under one warp, with
 // levels 1..L-1 kept as three-row rings in the block's scratch.
 template <typename T, bool RESID>
@@ -571,7 +673,7 @@ __device__ double sweep_deep_simple(block_view<T> in, block_view<T> out, int w, 
 }
 
 // The items of one pass of L sweeps (one warp); one register allocation per L.
-template <typename T, bool RESID, int L>
+template <typename T, bool RESID, int L, bool LEAN>
 __device__ __noinline__ double sweep_deep_items(block_view<T> in, block_view<T> out, int w, int h,
     int fixed, typename vec_of<T>::type* ring, int nw, int warp, int lane) {
   constexpr int V = traits<T>::VEC, P = 8;
@@ -597,31 +699,21 @@ __device__ __noinline__ double sweep_deep_items(block_view<T> in, block_view<T> 
     int r0 = 1 + (int)((long long)h * g / segs), r1 = 1 + (int)((long long)h * (g + 1) / segs);
     int own0 = s * SS;
     int nown = min(SS, nv - own0);
-    deep_lane<T> ln;
-    ln.v = own0 - E + lane;
-    ln.col0 = 1 + ln.v * V;
-    ln.own = ln.v >= own0 && ln.v < own0 + nown;
-    ln.anyfix = false;
-#pragma unroll
-    for (int k = 0; k < V; k++) {
-      int c = ln.col0 + k;
-      ln.fixc[k] = (c == 0 && (fixed & 4)) || (c == w + 1 && (fixed & 8));
-      ln.inw[k] = c >= 1 && c <= w;
-      ln.anyfix = ln.anyfix || ln.fixc[k];
-    }
-    ln.fix_r0 = (fixed & 1) ? 0 : INT_MIN;
-    ln.fix_r1 = (fixed & 2) ? h + 1 : INT_MIN;
-    acc += deep_item<T, RESID, L, P>(in, out, w, ln, r0, r1, lane, ring);
+    const deep_lane<T> ln = make_lane<T, L>(w, h, fixed, own0, nown, lane);
+    if (LEAN) acc += lean_item<T, RESID, L, P>(in, out, w, h, fixed, own0, nown, ln, r0, r1, lane, ring);
+    else acc += deep_item<T, RESID, L, P>(in, out, w, ln, r0, r1, lane, ring);
   }
   return acc;
 }
 
+// lean: the phase-split items (lean_item) instead of deep_item; same
+// results bit for bit.
 template <typename T, bool RESID>
 __device__ __noinline__ double sweep_deep(block_view<T> in, block_view<T> out, int w, int h, int L,
-    int fixed) {
+    int fixed, bool lean = true) {
   if (blockDim.x < 32) return sweep_deep_simple<T, RESID>(in, out, w, h, L, fixed);
-  constexpr int P = 8;
   using VT = typename vec_of<T>::type;
+  const int P = 8;
   const int nw = (int)(blockDim.x / 32), warp = (int)(threadIdx.x / 32), lane = (int)(threadIdx.x & 31);
   if (warp >= nw) return 0.0;
   size_t sbytes = 0;
@@ -631,13 +723,19 @@ __device__ __noinline__ double sweep_deep(block_view<T> in, block_view<T> out, i
     return 0.0;
   }
   VT* ring = rings + (size_t)warp * P * 32;
-  if (L == 2) return sweep_deep_items<T, RESID, 2>(in, out, w, h, fixed, ring, nw, warp, lane);
-  if (L == 3) return sweep_deep_items<T, RESID, 3>(in, out, w, h, fixed, ring, nw, warp, lane);
-  if (L == 5) return sweep_deep_items<T, RESID, 5>(in, out, w, h, fixed, ring, nw, warp, lane);
-  if (L == 6) return sweep_deep_items<T, RESID, 6>(in, out, w, h, fixed, ring, nw, warp, lane);
-  if (L == 7) return sweep_deep_items<T, RESID, 7>(in, out, w, h, fixed, ring, nw, warp, lane);
-  if (L == 8) return sweep_deep_items<T, RESID, 8>(in, out, w, h, fixed, ring, nw, warp, lane);
-  return sweep_deep_items<T, RESID, 4>(in, out, w, h, fixed, ring, nw, warp, lane);
+#define CHARMING_DEEP_CASE(LL)                                                                 \
+  if (L == LL)                                                                                 \
+    return lean ? sweep_deep_items<T, RESID, LL, true>(in, out, w, h, fixed, ring, nw, warp, lane) \
+                : sweep_deep_items<T, RESID, LL, false>(in, out, w, h, fixed, ring, nw, warp, lane);
+  CHARMING_DEEP_CASE(2)
+  CHARMING_DEEP_CASE(3)
+  CHARMING_DEEP_CASE(5)
+  CHARMING_DEEP_CASE(6)
+  CHARMING_DEEP_CASE(7)
+  CHARMING_DEEP_CASE(8)
+#undef CHARMING_DEEP_CASE
+  return lean ? sweep_deep_items<T, RESID, 4, true>(in, out, w, h, fixed, ring, nw, warp, lane)
+              : sweep_deep_items<T, RESID, 4, false>(in, out, w, h, fixed, ring, nw, warp, lane);
 }
 
 // ---------------------------------------------------------------------------

@@ -22,6 +22,7 @@ __device__ void charm::main(int argc, char** argv, size_t* argvs, int pe) {
     case suite::APP_SERVE: suite::serve_main(pe); break;
     case suite::APP_ASYNC_WAIT: suite::async_wait_main(pe); break;
     case suite::APP_USER_HEAP: suite::user_heap_main(pe); break;
+    case suite::APP_DECOMP1D: suite::decomp1d_main(pe); break;
     default:
       if (threadIdx.x == 0 && pe == 0) charm::end();
       break;
@@ -70,6 +71,28 @@ __device__ unsigned long long suite::checksum_block(const void* data, unsigned l
     acc += checksum_word(w, i);
   }
   return block_sum_u64(acc) ^ n;
+}
+
+__device__ unsigned long long suite::checksum_warp(const void* data, unsigned long long n) {
+  const unsigned char* b = reinterpret_cast<const unsigned char*>(data);
+  const unsigned long long nw = (n + 7) / 8;
+  const bool aligned = (reinterpret_cast<uintptr_t>(b) & 7) == 0;
+  unsigned long long acc = 0;
+  const unsigned stride = blockDim.x < 32 ? blockDim.x : 32;  // blocks under a warp (host checks)
+  for (unsigned long long i = threadIdx.x & 31; i < nw; i += stride) {
+    unsigned long long w = 0;
+    if (aligned && 8 * i + 8 <= n) {
+      w = reinterpret_cast<const unsigned long long*>(b)[i];
+    } else {
+      for (int k = 0; k < 8; k++) {
+        const unsigned long long j = 8 * i + k;
+        if (j < n) w |= (unsigned long long)b[j] << (8 * k);
+      }
+    }
+    acc += checksum_word(w, i);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  return acc ^ n;
 }
 
 #ifndef CHARMING_HOST_EMULATION

@@ -19,6 +19,7 @@ enum app_id : int {
   APP_SERVE = 7,
   APP_ASYNC_WAIT = 8,
   APP_USER_HEAP = 9,
+  APP_DECOMP1D = 10,
 };
 
 struct app_params {
@@ -51,6 +52,10 @@ __host__ __device__ inline unsigned long long checksum_word(unsigned long long w
   return mix64(w ^ ((i + 1) * 0xA0761D6478BD642FULL));
 }
 
+// The same checksum computed by the 32 lanes of the calling warp alone (for
+// small payloads: no block barrier); every lane gets the result.
+__device__ unsigned long long checksum_warp(const void* data, unsigned long long n);
+
 // Block-wide sum of one u64 per thread (every thread gets the result).
 __device__ unsigned long long block_sum_u64(unsigned long long v);
 // Block-wide deterministic FP64 sum: fixed reduction tree for a given
@@ -74,6 +79,7 @@ __device__ void jacobi1d_main(int pe);
 __device__ void serve_main(int pe);
 __device__ void async_wait_main(int pe);
 __device__ void user_heap_main(int pe);
+__device__ void decomp1d_main(int pe);
 }  // namespace suite
 
 // Host helper: copy params to g_app and run the scheduler once.

@@ -34,6 +34,7 @@ constexpr int HDR = 32;                  // envelope (16) + regular_msg (16)
 constexpr int MAX_THREADS = CHARMING_MAX_THREADS;  // launch bound of the scheduler
 constexpr int PROXY_CACHE = 16;          // proxies per PE looked up on chip
 constexpr int SMEM_OBJ_MAX = 4096;       // larger objects skip the on-chip arena
+constexpr int RQ_MAX = 256;              // ready stash entries listed on chip
 
 struct alignas(128) line_u64 {
   unsigned long long v;
@@ -156,6 +157,21 @@ struct pe_state {
   unsigned long long key_head, key_tail;
   unsigned long long arena_head, arena_tail;
   int n_waiting, n_ready;
+  // the scheduler's decision for the block (written by thread 0 before the
+  // loop's first barrier; sends inside entry methods use the b_* slots)
+  int d_act;
+  int d_idx, d_ep;
+  unsigned int d_cells;     // ring cells of the message being delivered
+  void* d_p;                // proxy, outbox entry or stash arena destination
+  void* d_arg;              // entry-method argument or stash copy source
+  unsigned long long d_key; // stash key index of a stash delivery
+  unsigned long long d_bytes;
+  unsigned long long ready_cursor;  // stash keys before it are not ready
+  // ready stashed messages found by the last revive, in key order (offsets
+  // from rq_base); rq_over: more than RQ_MAX, scan from ready_cursor instead
+  unsigned long long rq_base;
+  int rq_n, rq_pos, rq_over;
+  unsigned int rq[RQ_MAX];
   // block-collective broadcast slots
   void* b_ptr0;
   const void* b_ptr1;
@@ -250,6 +266,10 @@ __device__ __forceinline__ void st_release_sys_u64(unsigned long long* p, unsign
 }
 // Acquire side for data published before words read with relaxed loads.
 __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+// A signal word polled relaxed, made an acquire by fence_acq_rel_gpu on a hit.
+__device__ __forceinline__ unsigned long long ld_signal_u64(const unsigned long long* p) {
+  return ld_relaxed_u64(p);
+}
 __device__ __forceinline__ unsigned long long globaltimer() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -270,6 +290,9 @@ inline unsigned long long ld_acquire_sys_u64(const unsigned long long* p) { retu
 inline unsigned long long ld_relaxed_sys_u64(const unsigned long long* p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
 inline void st_release_sys_u64(unsigned long long* p, unsigned long long v) { __atomic_store_n(p, v, __ATOMIC_RELEASE); }
 inline void fence_acq_rel_gpu() { std::atomic_thread_fence(std::memory_order_acq_rel); }
+// ThreadSanitizer does not model fences: the host check polls with acquire
+// loads, which give the same ordering as relaxed loads plus the fence.
+inline unsigned long long ld_signal_u64(const unsigned long long* p) { return __atomic_load_n(p, __ATOMIC_ACQUIRE); }
 unsigned long long globaltimer();
 #endif
 

@@ -324,33 +324,6 @@ __device__ bool outbox_head_ready() {
   return e->ticket + cells_for(e->bytes) - h <= c_rt.ring_cells;
 }
 
-// Block-collective: copies every flushable outbox entry, oldest first, into
-// its destination ring and publishes it. An entry's receiver consumes the
-// tickets before it first, so its space always comes free in the end.
-__device__ void outbox_flush() {
-  pe_state* ps = pes();
-  while (true) {
-    if (threadIdx.x == 0) {
-      ps->b_ptr0 = outbox_head_ready() ? outbox_of(blockIdx.x) + ps->ob_head % c_rt.outbox_bytes : nullptr;
-    }
-    __syncthreads();
-    ob_entry* e = reinterpret_cast<ob_entry*>(ps->b_ptr0);
-    if (e == nullptr) {
-      __syncthreads();
-      return;
-    }
-    copy_cooperative(ring_cell(e->dst, e->ticket), reinterpret_cast<unsigned char*>(e) + OB_HDR, e->bytes,
-                     threadIdx.x, blockDim.x);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      publish(e->dst, e->ticket);
-      ps->ob_head += e->span;
-      ps->ob_count--;
-    }
-    __syncthreads();
-  }
-}
-
 // Thread 0: tell the senders how far this PE has consumed its inbox (a
 // release store: the reads of the consumed messages are done). Published
 // lazily, after an eighth of the ring or before waiting for messages.
@@ -365,7 +338,6 @@ __device__ __forceinline__ void publish_head(pe_state* ps, int me) {
 __device__ __forceinline__ void stamp_progress(int me) {
   st_relaxed_u64(&c_rt.progress[me], globaltimer());
 }
-
 
 } // namespace
 
@@ -593,42 +565,55 @@ __device__ __forceinline__ unsigned char* arena_of(int pe) {
   return c_rt.stash_data + (unsigned long long)pe * c_rt.stash_bytes;
 }
 
-// Block-collective: copy the message at env (bytes long) into the stash.
-__device__ void stash_put(const unsigned char* env, unsigned long long bytes,
-    int chare_id, int chare_idx, int refnum, int src_pe) {
+// Scheduler actions: thread 0 decides, the block executes (one barrier
+// before, one after).
+enum : int {
+  ACT_NONE = 0,
+  ACT_EXIT,         // leave the loop
+  ACT_CALL_RING,    // entry method on the message at the inbox head
+  ACT_CALL_STASH,   // entry method on a ready stashed message
+  ACT_CALL_WAIT,    // entry method of a satisfied async_wait (null argument)
+  ACT_STASH_PUT,    // copy the message at the inbox head into the stash
+  ACT_FLUSH,        // copy the oldest outbox entry into its destination ring
+  ACT_REVIVE,       // mark waiting stashed messages whose refnum now matches
+};
+
+__device__ __forceinline__ chare_proxy_base* proxy_of(pe_state* ps, int cid) {
+  if (cid >= 0 && cid < PROXY_CACHE) return ps->pcache[cid];  // on chip
+  chare_proxy_table& tb = c_rt.proxy_tables[blockIdx.x];
+  return (cid >= 0 && cid < tb.count) ? tb.proxies[cid] : nullptr;
+}
+
+// Thread 0: a stash descriptor and arena space for a message of `bytes`;
+// the arena address, or nullptr (error recorded).
+__device__ unsigned char* stash_alloc(unsigned long long bytes, int chare_id, int chare_idx, int refnum,
+    int src_pe) {
   pe_state* ps = pes();
-  if (threadIdx.x == 0) {
-    const unsigned long long S = (unsigned long long)c_rt.stash_entries;
-    const unsigned long long A = c_rt.stash_bytes;
-    bool ok = ps->key_tail - ps->key_head < S;
-    unsigned long long v = ps->arena_tail;
-    unsigned long long p = v % A;
-    if (p + bytes > A) v += A - p;
-    if (v + bytes - ps->arena_head > A) ok = false;
-    if (!ok) {
-      set_error(CHARMING_ERR_STASH_FULL, (int)(ps->key_tail - ps->key_head), (int)bytes);
-      ps->b_ptr0 = nullptr;
-    } else {
-      stash_key* k = keys_of(blockIdx.x) + (ps->key_tail % S);
-      k->chare_id = chare_id;
-      k->chare_idx = chare_idx;
-      k->refnum = refnum;
-      k->state = KEY_WAIT;
-      k->data_off = v;
-      k->bytes = (unsigned int)bytes;
-      k->src_pe = src_pe;
-      if (ps->key_tail == ps->key_head) ps->arena_head = v;
-      ps->arena_tail = v + bytes;
-      ps->key_tail++;
-      ps->n_waiting++;
-      ps->stats[ST_STASHED]++;
-      ps->b_ptr0 = arena_of(blockIdx.x) + (v % A);
-    }
+  const unsigned long long S = (unsigned long long)c_rt.stash_entries;
+  const unsigned long long A = c_rt.stash_bytes;
+  bool ok = ps->key_tail - ps->key_head < S;
+  unsigned long long v = ps->arena_tail;
+  const unsigned long long p = v % A;
+  if (p + bytes > A) v += A - p;
+  if (v + bytes - ps->arena_head > A) ok = false;
+  if (!ok) {
+    set_error(CHARMING_ERR_STASH_FULL, (int)(ps->key_tail - ps->key_head), (int)bytes);
+    return nullptr;
   }
-  __syncthreads();
-  unsigned char* dst = reinterpret_cast<unsigned char*>(ps->b_ptr0);
-  if (dst) copy_cooperative(dst, env, bytes, threadIdx.x, blockDim.x);
-  __syncthreads();
+  stash_key* k = keys_of(blockIdx.x) + (ps->key_tail % S);
+  k->chare_id = chare_id;
+  k->chare_idx = chare_idx;
+  k->refnum = refnum;
+  k->state = KEY_WAIT;
+  k->data_off = v;
+  k->bytes = (unsigned int)bytes;
+  k->src_pe = src_pe;
+  if (ps->key_tail == ps->key_head) ps->arena_head = v;
+  ps->arena_tail = v + bytes;
+  ps->key_tail++;
+  ps->n_waiting++;
+  ps->stats[ST_STASHED]++;
+  return arena_of(blockIdx.x) + (v % A);
 }
 
 // Thread 0: drop consumed descriptors at the head and release arena bytes.
@@ -638,95 +623,91 @@ __device__ void stash_retire() {
   stash_key* keys = keys_of(blockIdx.x);
   while (ps->key_head < ps->key_tail && keys[ps->key_head % S].state == KEY_FREE) ps->key_head++;
   ps->arena_head = (ps->key_head < ps->key_tail) ? keys[ps->key_head % S].data_off : ps->arena_tail;
+  if (ps->ready_cursor < ps->key_head) ps->ready_cursor = ps->key_head;
 }
 
-// Block-collective: waiting messages whose refnum now matches become ready.
-__device__ void stash_revive() {
+// Block-collective: waiting stashed messages whose refnum now matches become
+// ready (counted into red_i[0]), and every ready one goes on the on-chip
+// ready list (thread 0 sorts it before the next decision).
+__device__ void stash_revive_scan() {
   pe_state* ps = pes();
   const unsigned long long S = (unsigned long long)c_rt.stash_entries;
   stash_key* keys = keys_of(blockIdx.x);
-  chare_proxy_table& tb = c_rt.proxy_tables[blockIdx.x];
-  unsigned long long kh = ps->key_head, kt = ps->key_tail;
-  if (threadIdx.x == 0) ps->red_i[0] = 0;
-  // revive_pending is cleared below, after this barrier: every thread has
-  // read it (scheduler_loop) before it changes
-  __syncthreads();
-  if (ps->n_waiting > 0) {
-    int cnt = 0;
-    for (unsigned long long i = kh + threadIdx.x; i < kt; i += blockDim.x) {
-      stash_key* k = keys + (i % S);
-      if (k->state == KEY_WAIT) {
-        chare_proxy_base* p = k->chare_id < PROXY_CACHE ? ps->pcache[k->chare_id] : tb.proxies[k->chare_id];
-        if (p->refnum_matches(k->chare_idx, k->refnum)) {
-          k->state = KEY_READY;
-          cnt++;
-        }
+  const unsigned long long kh = ps->key_head, kt = ps->key_tail;
+  int cnt = 0;
+  for (unsigned long long i = kh + threadIdx.x; i < kt; i += blockDim.x) {
+    stash_key* k = keys + (i % S);
+    int st = k->state;
+    if (st == KEY_WAIT) {
+      chare_proxy_base* p = proxy_of(ps, k->chare_id);
+      if (p->refnum_matches(k->chare_idx, k->refnum)) {
+        k->state = st = KEY_READY;
+        cnt++;
       }
     }
-    if (cnt) atomicAdd_block(&ps->red_i[0], cnt);
+    if (st == KEY_READY) {
+      const int pos = atomicAdd_block(&ps->rq_n, 1);
+      if (pos < RQ_MAX) ps->rq[pos] = (unsigned int)(i - kh);
+    }
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int c = ps->red_i[0];
-    ps->revive_pending = 0;
-    ps->n_ready += c;
-    ps->n_waiting -= c;
-    ps->stats[ST_REVIVED] += c;
-  }
-  __syncthreads();
+  if (cnt) atomicAdd_block(&ps->red_i[0], cnt);
 }
 
-// Block-collective: deliver the oldest ready stashed message.
-__device__ void stash_dispatch_ready() {
+// Thread 0: the ready list of the last revive in key (arrival) order.
+__device__ void ready_list_sort() {
+  pe_state* ps = pes();
+  if (ps->rq_n > RQ_MAX) {
+    ps->rq_over = 1;
+    ps->rq_n = RQ_MAX;
+  }
+  for (int a = 1; a < ps->rq_n; a++) {  // insertion sort: short lists
+    const unsigned int v = ps->rq[a];
+    int b = a - 1;
+    while (b >= 0 && ps->rq[b] > v) {
+      ps->rq[b + 1] = ps->rq[b];
+      b--;
+    }
+    ps->rq[b + 1] = v;
+  }
+  ps->rq_pos = 0;
+}
+
+// Thread 0: the oldest ready stashed message, or ~0 when none is left:
+// from the ready list, or, when that overflowed, by scanning the keys
+// from ready_cursor (keys before it are known not to be ready).
+__device__ unsigned long long stash_next_ready() {
   pe_state* ps = pes();
   const unsigned long long S = (unsigned long long)c_rt.stash_entries;
-  const unsigned long long A = c_rt.stash_bytes;
   stash_key* keys = keys_of(blockIdx.x);
-  unsigned long long kh = ps->key_head, kt = ps->key_tail;
-  if (threadIdx.x == 0) ps->red_u[0] = ~0ULL;
-  __syncthreads();
-  for (unsigned long long i = kh + threadIdx.x; i < kt; i += blockDim.x) {
+  if (!ps->rq_over) {
+    while (ps->rq_pos < ps->rq_n) {
+      const unsigned long long i = ps->rq_base + ps->rq[ps->rq_pos++];
+      if (i >= ps->key_head && i < ps->key_tail && keys[i % S].state == KEY_READY) return i;
+    }
+    return ~0ULL;
+  }
+  unsigned long long i = ps->ready_cursor < ps->key_head ? ps->key_head : ps->ready_cursor;
+  for (; i < ps->key_tail; i++)
     if (keys[i % S].state == KEY_READY) {
-      atomicMin(&ps->red_u[0], i);
-      break;
+      ps->ready_cursor = i;
+      return i;
     }
+  ps->ready_cursor = i;
+  return ~0ULL;
+}
+
+// Thread 0 of PE 0: stop the run when no PE has delivered anything for
+// idle_timeout_ns (e.g. a program that never calls end()).
+__device__ void check_idle_timeout(unsigned long long now) {
+  if (c_rt.idle_timeout_ns == 0) return;
+  unsigned long long latest = pes()->t0;
+  for (int p = 0; p < c_rt.n_pes; p++) {
+    unsigned long long v = ld_relaxed_u64(&c_rt.progress[p]);
+    if (v > latest) latest = v;
   }
-  __syncthreads();
-  unsigned long long idx = ps->red_u[0];
-  if (idx == ~0ULL) {
-    if (threadIdx.x == 0) ps->n_ready = 0;
-    __syncthreads();
-    return;
+  if (now > latest && now - latest > c_rt.idle_timeout_ns) {
+    set_error(CHARMING_ERR_IDLE_TIMEOUT, 0, 0);
   }
-  stash_key* k = keys + (idx % S);
-  unsigned char* env = arena_of(blockIdx.x) + (k->data_off % A);
-  chare_proxy_base* p = k->chare_id < PROXY_CACHE ? ps->pcache[k->chare_id]
-                                                   : c_rt.proxy_tables[blockIdx.x].proxies[k->chare_id];
-  if (threadIdx.x == 0) ps->b_i0 = p->refnum_matches(k->chare_idx, k->refnum) ? 1 : 0;
-  __syncthreads();
-  int go = ps->b_i0;
-  // The entry method may send at once, and a send reuses the broadcast
-  // slots: every thread must have read them first.
-  __syncthreads();
-  if (go) {
-    const regular_msg* rm = reinterpret_cast<const regular_msg*>(env + sizeof(envelope));
-    const long long c0 = clock64();
-    p->call_fn(p, k->chare_idx, rm->ep_id, env + HDR);
-    if (threadIdx.x == 0) ps->stats[ST_EM_CYC] += (unsigned long long)(clock64() - c0);
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    ps->n_ready--;
-    if (go) {
-      k->state = KEY_FREE;
-      if ((++ps->stats[ST_DELIVERED] & 15) == 0) stamp_progress(blockIdx.x);
-      stash_retire();
-    } else {
-      k->state = KEY_WAIT;
-      ps->n_waiting++;
-    }
-  }
-  __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
@@ -745,67 +726,34 @@ __device__ __forceinline__ bool cmp_holds(unsigned long long v, int cmp, unsigne
   }
 }
 
-// Block-collective: runs the entry method of the first satisfied wait (chare
-// arrays in registration order, waits in slot order), if any. The words are
-// read relaxed (no L1 invalidation per check); one acquire fence follows a
-// hit, so what their writers published before them is visible.
-__device__ void check_async_waits() {
+// Thread 0: the first satisfied wait (chare arrays in registration order,
+// waits in slot order), taken off the list; its proxy, or nullptr. The words
+// are read relaxed (no L1 invalidation per check); one acquire fence follows
+// a hit, so what their writers published before them is visible.
+__device__ chare_proxy_base* take_satisfied_wait(int* idx, int* ep) {
   pe_state* ps = pes();
-  if (threadIdx.x == 0) {
-    chare_proxy_base* hit = nullptr;
-    chare_proxy_table& tb = c_rt.proxy_tables[blockIdx.x];
-    for (int id = 0; id < tb.count && !hit; id++) {
-      chare_proxy_base* p = id < PROXY_CACHE ? ps->pcache[id] : tb.proxies[id];
-      if (p == nullptr || p->async_waits == nullptr) continue;
-      for (int i = 0; i < ASYNC_WAIT_MAX; i++) {
-        async_wait_t& aw = p->async_waits[i];
-        if (!aw.valid) continue;
-        bool ok = true;
-        for (size_t k = 0; k < aw.nelems && ok; k++)
-          ok = cmp_holds(ld_relaxed_u64(reinterpret_cast<const unsigned long long*>(aw.ivars) + k), aw.cmp,
-                         aw.cmp_value);
-        if (ok) {
-          aw.valid = false;
-          hit = p;
-          ps->b_i1 = aw.idx;
-          ps->b_i2 = aw.ep;
-          break;
-        }
+  chare_proxy_table& tb = c_rt.proxy_tables[blockIdx.x];
+  for (int id = 0; id < tb.count; id++) {
+    chare_proxy_base* p = proxy_of(ps, id);
+    if (p == nullptr || p->async_waits == nullptr) continue;
+    for (int i = 0; i < ASYNC_WAIT_MAX; i++) {
+      async_wait_t& aw = p->async_waits[i];
+      if (!aw.valid) continue;
+      bool ok = true;
+      for (size_t k = 0; k < aw.nelems && ok; k++)
+        ok = cmp_holds(ld_signal_u64(reinterpret_cast<const unsigned long long*>(aw.ivars) + k), aw.cmp,
+                       aw.cmp_value);
+      if (ok) {
+        aw.valid = false;
+        ps->aw_count--;
+        *idx = aw.idx;
+        *ep = aw.ep;
+        fence_acq_rel_gpu();
+        return p;
       }
     }
-    if (hit) fence_acq_rel_gpu();
-    ps->b_ptr0 = hit;
   }
-  __syncthreads();
-  chare_proxy_base* p = reinterpret_cast<chare_proxy_base*>(ps->b_ptr0);
-  const int idx = ps->b_i1, ep = ps->b_i2;
-  // the entry method may send at once and reuse the broadcast slots; the
-  // count changes only once every thread has read it in the loop
-  __syncthreads();
-  if (p) {
-    if (threadIdx.x == 0) ps->aw_count--;
-    const long long c0 = clock64();
-    p->call_fn(p, idx, ep, nullptr);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      ps->stats[ST_EM_CYC] += (unsigned long long)(clock64() - c0);
-      if ((++ps->stats[ST_DELIVERED] & 15) == 0) stamp_progress(blockIdx.x);
-    }
-  }
-}
-
-// Thread 0 of PE 0: stop the run when no PE has delivered anything for
-// idle_timeout_ns (e.g. a program that never calls end()).
-__device__ void check_idle_timeout(unsigned long long now) {
-  if (c_rt.idle_timeout_ns == 0) return;
-  unsigned long long latest = pes()->t0;
-  for (int p = 0; p < c_rt.n_pes; p++) {
-    unsigned long long v = ld_relaxed_u64(&c_rt.progress[p]);
-    if (v > latest) latest = v;
-  }
-  if (now > latest && now - latest > c_rt.idle_timeout_ns) {
-    set_error(CHARMING_ERR_IDLE_TIMEOUT, 0, 0);
-  }
+  return nullptr;
 }
 
 // Thread 0: wait for the message at the inbox head. Returns 1 when it has
@@ -877,101 +825,203 @@ __device__ int poll_inbox() {
   }
 }
 
-// Block-collective: deliver or stash the message at the inbox head, then
-// release its cells to the senders.
-__device__ void dispatch_inbox() {
+// Thread 0: the thread-0 part that closes the action the block just executed.
+__device__ void finish_action() {
   pe_state* ps = pes();
   const int me = blockIdx.x;
-  unsigned char* m = ring_cell(me, ps->head);
-  if (threadIdx.x == 0) {
+  switch (ps->d_act) {
+    case ACT_CALL_RING:
+    case ACT_STASH_PUT:
+      // the block is done with the message: release its cells
+      ps->head += ps->d_cells;
+      if (ps->head - ps->head_pub >= (c_rt.ring_cells >> 3)) publish_head(ps, me);
+      if (ps->d_act == ACT_CALL_RING && (++ps->stats[ST_DELIVERED] & 15) == 0) stamp_progress(me);
+      break;
+    case ACT_CALL_STASH: {
+      const unsigned long long S = (unsigned long long)c_rt.stash_entries;
+      keys_of(me)[ps->d_key % S].state = KEY_FREE;
+      ps->n_ready--;
+      if ((++ps->stats[ST_DELIVERED] & 15) == 0) stamp_progress(me);
+      stash_retire();
+      break;
+    }
+    case ACT_CALL_WAIT:
+      if ((++ps->stats[ST_DELIVERED] & 15) == 0) stamp_progress(me);
+      break;
+    case ACT_FLUSH: {
+      const ob_entry* e = reinterpret_cast<const ob_entry*>(ps->d_p);
+      publish(e->dst, e->ticket);
+      ps->ob_head += e->span;
+      ps->ob_count--;
+      break;
+    }
+    case ACT_REVIVE: {
+      const int c = ps->red_i[0];
+      ps->n_ready += c;
+      ps->n_waiting -= c;
+      ps->stats[ST_REVIVED] += c;
+      ready_list_sort();
+      break;
+    }
+    default:
+      break;
+  }
+  ps->d_act = ACT_NONE;
+}
+
+// Thread 0: decides what the block does next (pe_state d_* fields).
+__device__ void next_action() {
+  pe_state* ps = pes();
+  const int me = blockIdx.x;
+  const unsigned long long S = (unsigned long long)c_rt.stash_entries;
+  while (true) {
+    if (ps->term) {
+      ps->d_act = ACT_EXIT;
+      return;
+    }
+    // deferred sends whose receivers have room
+    if (ps->ob_count > 0 && outbox_head_ready()) {
+      ps->d_act = ACT_FLUSH;
+      ps->d_p = outbox_of(me) + ps->ob_head % c_rt.outbox_bytes;
+      return;
+    }
+    // satisfied async waits
+    if (ps->aw_count > 0) {
+      int idx = 0, ep = 0;
+      chare_proxy_base* p = take_satisfied_wait(&idx, &ep);
+      if (p) {
+        if (terminated()) {
+          ps->d_act = ACT_EXIT;
+          return;
+        }
+        ps->d_act = ACT_CALL_WAIT;
+        ps->d_p = p;
+        ps->d_idx = idx;
+        ps->d_ep = ep;
+        ps->d_arg = nullptr;
+        return;
+      }
+    }
+    // set_refnum since the last look: re-examine the waiting stash entries
+    if (ps->revive_pending) {
+      ps->revive_pending = 0;
+      if (ps->n_waiting > 0) {
+        ps->red_i[0] = 0;
+        ps->ready_cursor = ps->key_head;
+        ps->rq_base = ps->key_head;
+        ps->rq_n = 0;
+        ps->rq_over = 0;
+        ps->d_act = ACT_REVIVE;
+        return;
+      }
+    }
+    // ready stashed messages go before new inbox messages, oldest first
+    while (ps->n_ready > 0) {
+      const unsigned long long i = stash_next_ready();
+      if (i == ~0ULL) {
+        ps->n_ready = 0;
+        break;
+      }
+      stash_key* k = keys_of(me) + (i % S);
+      chare_proxy_base* p = proxy_of(ps, k->chare_id);
+      if (!p->refnum_matches(k->chare_idx, k->refnum)) {  // refnum moved on again
+        k->state = KEY_WAIT;
+        ps->n_ready--;
+        ps->n_waiting++;
+        continue;
+      }
+      if (terminated()) {
+        ps->d_act = ACT_EXIT;
+        return;
+      }
+      const unsigned char* env = arena_of(me) + (k->data_off % c_rt.stash_bytes);
+      const regular_msg* rm = reinterpret_cast<const regular_msg*>(env + sizeof(envelope));
+      ps->d_act = ACT_CALL_STASH;
+      ps->d_p = p;
+      ps->d_idx = k->chare_idx;
+      ps->d_ep = rm->ep_id;
+      ps->d_arg = const_cast<unsigned char*>(env) + HDR;
+      ps->d_key = i;
+      return;
+    }
+    // the inbox
+    const int got = poll_inbox();
+    if (got == 0) {
+      ps->term = 1;
+      ps->d_act = ACT_EXIT;
+      return;
+    }
+    if (got == 2) continue;
+    unsigned char* m = ring_cell(me, ps->head);
     const envelope* env = reinterpret_cast<const envelope*>(m);
     const regular_msg* rm = reinterpret_cast<const regular_msg*>(m + sizeof(envelope));
     unsigned long long size = env->size;
-    int type = (int)env->type;
-    int action = 2;  // 0 deliver, 1 stash, 2 skip
-    chare_proxy_base* p = nullptr;
+    const int type = (int)env->type;
+    ps->d_act = ACT_NONE;
     if (size < HDR || size > c_rt.max_msg || (size & (ALIGN_SIZE - 1))) {
-      set_error(CHARMING_ERR_BAD_MSG, env->src_pe, (int)type);
+      set_error(CHARMING_ERR_BAD_MSG, env->src_pe, type);
       size = CELL;
     } else if (type == (int)msgtype::regular || type == (int)msgtype::user) {
-      int cid = rm->chare_id;
-      if (cid >= 0 && cid < PROXY_CACHE) {
-        p = ps->pcache[cid];  // on chip
-      } else {
-        chare_proxy_table& tb = c_rt.proxy_tables[me];
-        p = (cid >= 0 && cid < tb.count) ? tb.proxies[cid] : nullptr;
-      }
+      const int cid = rm->chare_id;
+      chare_proxy_base* p = proxy_of(ps, cid);
       if (p == nullptr || !p->valid_target(rm->chare_idx, rm->ep_id)) {
         set_error(CHARMING_ERR_BAD_TARGET, cid, rm->chare_idx);
+      } else if (p->refnum_matches(rm->chare_idx, rm->refnum)) {
+        ps->d_act = ACT_CALL_RING;
+        ps->d_p = p;
+        ps->d_idx = rm->chare_idx;
+        ps->d_ep = rm->ep_id;
+        ps->d_arg = m + HDR;
       } else {
-        action = p->refnum_matches(rm->chare_idx, rm->refnum) ? 0 : 1;
+        unsigned char* dst = stash_alloc(size, cid, rm->chare_idx, rm->refnum, env->src_pe);
+        if (dst) {
+          ps->d_act = ACT_STASH_PUT;
+          ps->d_p = dst;
+          ps->d_arg = m;
+          ps->d_bytes = size;
+        }
       }
     } else if (type == (int)msgtype::do_terminate || type == (int)msgtype::begin_terminate) {
       atomicExch(ctrl(CTRL_TERM), 1);
     } else {
       set_error(CHARMING_ERR_BAD_MSG, env->src_pe, type);
     }
-    ps->b_ptr0 = p;
-    ps->b_i0 = action;
-    ps->b_i1 = rm->chare_idx;
-    ps->b_i2 = rm->ep_id;
-    ps->b_i3 = rm->refnum;
-    ps->b_i4 = rm->chare_id;
-    ps->b_i5 = env->src_pe;
-    ps->b_u0 = size;
-  }
-  __syncthreads();
-  const int action = ps->b_i0;
-  const unsigned long long size = ps->b_u0;
-  chare_proxy_base* p = reinterpret_cast<chare_proxy_base*>(ps->b_ptr0);
-  const int idx = ps->b_i1, ep = ps->b_i2, ref = ps->b_i3, cid = ps->b_i4, src = ps->b_i5;
-  // The entry method may send at once, and a send reuses the broadcast
-  // slots: every thread must have read them first.
-  __syncthreads();
-  if (action == 0) {
-    const long long c0 = clock64();
-    p->call_fn(p, idx, ep, m + HDR);
-    if (threadIdx.x == 0) ps->stats[ST_EM_CYC] += (unsigned long long)(clock64() - c0);
-  } else if (action == 1) {
-    stash_put(m, size, cid, idx, ref, src);
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    ps->head += cells_for(size);
+    ps->d_cells = cells_for(size);
+    if (ps->d_act != ACT_NONE) return;
+    // nothing for the block to do with it: consume it here
+    ps->head += ps->d_cells;
     if (ps->head - ps->head_pub >= (c_rt.ring_cells >> 3)) publish_head(ps, me);
-    if (action == 0 && (++ps->stats[ST_DELIVERED] & 15) == 0) stamp_progress(me);
   }
 }
 
+// The loop: thread 0 closes the last action and picks the next; the block
+// executes it. Two block barriers per message.
 __device__ void scheduler_loop() {
   pe_state* ps = pes();
+  if (threadIdx.x == 0) ps->d_act = ACT_NONE;
   while (true) {
-    if (ps->ob_count > 0) outbox_flush();
-    if (ps->aw_count > 0) {
-      check_async_waits();
-      if (threadIdx.x == 0 && terminated()) ps->term = 1;
-      __syncthreads();
-      if (ps->term) break;
-    }
-    if (ps->revive_pending) stash_revive();
-    if (ps->n_ready > 0) {
-      stash_dispatch_ready();
-      if (threadIdx.x == 0 && terminated()) ps->term = 1;
-      __syncthreads();
-      if (ps->term) break;
-      continue;
-    }
-    if (threadIdx.x == 0) ps->b_i0 = poll_inbox();
-    __syncthreads();
-    int got = ps->b_i0;
-    if (!got) {
-      if (threadIdx.x == 0) ps->term = 1;
-      __syncthreads();
-      break;
+    if (threadIdx.x == 0) {
+      finish_action();
+      next_action();
     }
     __syncthreads();
-    if (got == 2) continue;
-    dispatch_inbox();
+    const int act = ps->d_act;
+    if (act == ACT_EXIT) break;
+    chare_proxy_base* p = reinterpret_cast<chare_proxy_base*>(ps->d_p);
+    if (act == ACT_CALL_RING || act == ACT_CALL_STASH || act == ACT_CALL_WAIT) {
+      const long long c0 = clock64();
+      p->call_fn(p, ps->d_idx, ps->d_ep, ps->d_arg);
+      if (threadIdx.x == 0) ps->stats[ST_EM_CYC] += (unsigned long long)(clock64() - c0);
+    } else if (act == ACT_STASH_PUT) {
+      copy_cooperative(ps->d_p, ps->d_arg, ps->d_bytes, threadIdx.x, blockDim.x);
+    } else if (act == ACT_FLUSH) {
+      const ob_entry* e = reinterpret_cast<const ob_entry*>(ps->d_p);
+      copy_cooperative(ring_cell(e->dst, e->ticket), reinterpret_cast<const unsigned char*>(e) + OB_HDR,
+                       e->bytes, threadIdx.x, blockDim.x);
+    } else if (act == ACT_REVIVE) {
+      stash_revive_scan();
+    }
+    __syncthreads();
   }
 }
 
@@ -1006,6 +1056,11 @@ charming_scheduler_kernel(int argc, char** argv, size_t* argvs) {
     ps->uh_head = ps->uh_tail = 0;
     ps->ub_head = ps->ub_tail = 0;
     ps->aw_count = 0;
+    ps->ready_cursor = 0;
+    ps->d_act = 0;
+    ps->rq_base = 0;
+    ps->rq_n = ps->rq_pos = 0;
+    ps->rq_over = 1;  // no list yet: scan
     ps->stamped_delivered = ~0ULL;
     ps->slow_check_ns = ps->t0;
     ps->idle_checks = 0;

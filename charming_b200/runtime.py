@@ -123,6 +123,26 @@ class Runtime:
                                        C.byref(n_logged), C.byref(ms)), "charming_fanout")
         return log[: min(n_logged.value, cap)], ms.value
 
+    def sm_pingpong(self, mode: int, round_trips: int = 10000):
+        """SM-to-SM pingpong floor without the runtime (mode 0 flag, 1
+        relaxed polls, 2 with block barriers, 3 the reference's slot
+        scheme): one-way ns, cycles and the SM pair."""
+        ns, cyc = C.c_double(0.0), C.c_double(0.0)
+        sm = (C.c_int * 2)()
+        check(self.lib.charming_sm_pingpong(mode, round_trips, C.byref(ns), C.byref(cyc), sm),
+              "charming_sm_pingpong")
+        return {"oneway_ns": ns.value, "oneway_cycles": cyc.value, "sm_pair": (sm[0], sm[1])}
+
+    def sweep_bench(self, dtype: str, w: int, h: int, depth: int, passes: int, n_blocks: int = 0,
+                    variant: int = 0) -> float:
+        """Kernel ms of `passes` passes over n_blocks chare blocks of w x h
+        (sweeps only, no messages); n_blocks 0: one per PE."""
+        ms = C.c_double(0.0)
+        check(self.lib.charming_sweep_bench(_lib.F64 if dtype == "f64" else _lib.F32, w, h, depth, passes,
+                                            n_blocks or self.n_pes, variant, C.byref(ms)),
+              "charming_sweep_bench")
+        return ms.value
+
     def async_wait_chain(self, n_chares: int, broken: bool = False):
         """Wake order of a chain of async_waits; returns (status, order).
         A broken chain leaves the last chare waiting, so its run ends with
@@ -139,6 +159,17 @@ class Runtime:
               "charming_user_heap_check")
         keys = ("taken", "bad", "failed", "checked", "freed", "done", "bytes")
         return {k: int(out[i]) for i, k in enumerate(keys)}
+
+    def decomp1d(self, n_chares: int, nx: int, ny: int, iters: int, mode: int):
+        """jacobi2d-decomp1d: (ny-2) x nx float32 bands after `iters`
+        iterations (mode 0 signals waited in the entry method, 1 async_wait,
+        2 messages) and the loop's ms."""
+        out = np.zeros((ny - 2, nx), dtype=np.float32)
+        ms = C.c_double(0.0)
+        check(self.lib.charming_jacobi2d_decomp1d(n_chares, nx, ny, iters, mode,
+                                                  out.ctypes.data_as(C.POINTER(C.c_float)), C.byref(ms)),
+              "charming_jacobi2d_decomp1d")
+        return out, ms.value
 
     def jacobi1d(self, n_chares: int, width: int, sweeps: int):
         out = np.zeros(n_chares * width + 4, dtype=np.float64)

@@ -227,6 +227,59 @@ int charming_jacobi2d_destroy(void* handle);
 int charming_jacobi2d_sweeps_noalloc(int dtype, int nx, int ny, int sweeps,
     const void* dev_in, void* dev_out);
 
+/* Jacobi2d over a 1-D row decomposition (examples/jacobi2d-decomp1d/
+ * jacobi2d.cu): an ny x nx FP32 grid (nx a multiple of 4) split into bands
+ * of rows over n_chares chares as its Block::init does (:144-198), periodic
+ * top/bottom neighbours, columns 0 and nx-1 fixed to sin(2*PI*(g-1)/(ny-3))
+ * per global row g, the 4-point stencil of its jacobi_kernel (:374-383) for
+ * `iters` iterations. mode 0: boundary rows written into the neighbours'
+ * buffers and signalled, waited for inside the entry method (one chare per
+ * PE); 1: the same, resumed by async_wait; 2: boundary rows as messages
+ * tagged with the iteration as refnum. host_out receives the bands' rows
+ * ((ny-2) x nx floats); *out_ms the scheduler loop's time. */
+int charming_jacobi2d_decomp1d(int n_chares, int nx, int ny, int iters, int mode, float* host_out,
+    double* out_ms);
+
+/* SM-to-SM pingpong floor: two thread blocks on different SMs bounce a
+ * counter round_trips times, without the runtime (replaces the reference's
+ * raw baseline, examples/baseline/baseline.cu:14-160, which prints the time
+ * per iteration). mode 0: release store / acquire poll by one thread per
+ * block (the floor); 1: relaxed polls plus one acquire fence per hit; 2:
+ * mode 0 with a block barrier on each side of every hop; 3: the reference's
+ * scheme (4 slots per SM pair, block-wide slot scans, atomicCAS publish and
+ * clear). One-way time = round-trip time / 2 (block 0's clock). sm_pair
+ * (optional) receives the two blocks' SM ids. */
+int charming_sm_pingpong(int mode, int round_trips, double* oneway_ns, double* oneway_cycles,
+    int* sm_pair);
+
+/* Sweep throughput without messages (no reference counterpart; it times
+ * the chare sweep of examples/jacobi2d/jacobi2d.cu:327-334 as implemented
+ * here): n_blocks (<= n_pes) PE-shaped thread blocks each run `passes`
+ * passes of `depth` sweeps over their own w x h chare block. variant 0:
+ * multi-sweep pass with phase-split items, 1: with single-loop items
+ * (depth >= 2), 2: one
+ * direct sweep per pass (depth 1). *ms receives the kernel time. */
+int charming_sweep_bench(int dtype, int w, int h, int depth, int passes, int n_blocks, int variant,
+    double* ms);
+
+/* async_wait chain (reference include/chare.h:214-239, src/comm/get/get.cu:
+ * 1172-1202): chare i's entry method runs once its two signal words are >= 1,
+ * which chare i-1 sets from its own; the host sets chare 0's. order[i]
+ * receives chare i's wake position (-1: never woke). broken = 1: nobody
+ * signals the last chare, so the run ends at the idle timeout
+ * (CHARMING_ERR_IDLE_TIMEOUT). */
+int charming_async_wait_chain(int n_chares, int broken, int* order, int n_order);
+
+/* malloc_user / free_user check (reference include/charming.h:33-34,
+ * src/comm/get/get.cu:1348-1362): each of n_chares takes `rounds` rounds of
+ * blocks_per_round (<= 16) seeded-size blocks from its PE's heap, fills and
+ * checks them, frees them out of order, then hands one block to the next
+ * chare, which checks it on its PE. counters[0..6]: blocks taken, pattern
+ * errors, allocation failures, blocks checked by another chare, blocks
+ * freed, chares done, bytes taken. */
+int charming_user_heap_check(int n_chares, int blocks_per_round, int rounds, uint64_t seed,
+    uint64_t* counters);
+
 /* 1-D Jacobi chares (examples/jacobi1d/jacobi1d.cu:62-170): n_chares blocks
  * of `width` points, 5-point window sum/5, boundary 10 and interior 0 as in
  * that example; result is the (n_chares*width + 4)-point array. */

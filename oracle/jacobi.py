@@ -31,6 +31,7 @@ def lib():
         L.oracle_residual2_f32.argtypes = [fp, i, i]
         L.oracle_residual2_f32.restype = C.c_double
         L.oracle_jacobi1d_f64.argtypes = [dp, i, i]
+        L.oracle_decomp1d_f32.argtypes = [i, i, i, i, fp, fp]
         _lib = L
     return _lib
 
@@ -77,3 +78,23 @@ def seeded_grid(nx: int, ny: int, seed: int) -> np.ndarray:
     with np.errstate(over="ignore"):
         v = mix64((np.uint64(seed) << np.uint64(32)) + k) >> np.uint64(11)
     return (v.astype(np.float64) * (1.0 / 9007199254740992.0)).reshape(ny + 2, nx + 2)
+
+
+def decomp1d_boundary(ny: int) -> np.ndarray:
+    """Left/right column values of jacobi2d-decomp1d per global row g
+    (examples/jacobi2d-decomp1d/jacobi2d.cu:424-433: sin(2*PI*(g-1)/(ny-3))
+    with PI = 3.141592 as a float), float32[ny]."""
+    pi = float(np.float32(3.141592))
+    g = np.arange(ny, dtype=np.float64)
+    return np.sin(2.0 * pi * (g - 1.0) / float(ny - 3)).astype(np.float32)
+
+
+def decomp1d(n: int, nx: int, ny: int, iters: int) -> np.ndarray:
+    """(ny-2) x nx float32 result of the decomp1d oracle."""
+    bc = np.ascontiguousarray(decomp1d_boundary(ny))
+    out = np.zeros((ny - 2, nx), dtype=np.float32)
+    fp = C.POINTER(C.c_float)
+    rc = lib().oracle_decomp1d_f32(n, nx, ny, iters, bc.ctypes.data_as(fp), out.ctypes.data_as(fp))
+    if rc != 0:
+        raise ValueError("decomp1d: sizes the decomposition does not cover")
+    return out

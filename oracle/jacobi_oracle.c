@@ -189,3 +189,81 @@ int oracle_jacobi1d_f64(double* a0, int width, int sweeps) {
   }
   return 0;
 }
+
+/* ---- jacobi2d-decomp1d (examples/jacobi2d-decomp1d/jacobi2d.cu) ----------
+ * Row decomposition of an ny x nx FP32 grid over n chares, restating
+ * Block::init (:128-198): chunk_low = (ny-2)/n, chunk_high = chunk_low+1,
+ * num_ranks_low = n*chunk_low + n - (ny-2); chare i has chunk rows (low for
+ * i < num_ranks_low), iy_start_global as computed there, iy_end_global
+ * clamped to ny-4, local rows 1..iy_end-1 computed, and periodic neighbours
+ * top = i-1 (n-1 for chare 0), bottom = (i+1) % n. Each chare holds two
+ * buffers of (chunk_high+2) x nx floats, zero except columns 0 and nx-1 of
+ * its rows 1..chunk, which hold bc_rows[g] for the row's global index g
+ * (the reference computes sin(2*PI*(g-1)/(ny-3)) on the device, :424-433;
+ * the caller supplies the values). One iteration (jacobi_kernel, :374-383):
+ *   new[iy][ix] = 0.25 * (a[iy][ix+1] + a[iy][ix-1] + a[iy+1][ix] + a[iy-1][ix])
+ * in float, left to right, for ix in 1..nx-2; then the first computed row
+ * goes to the top neighbour's bottom ghost row (its chunk+1) and the last
+ * computed row to the bottom neighbour's row 0, columns 1..nx-2 (:386-401),
+ * into the buffer the neighbour reads next (the reference always writes its
+ * first buffer). out receives the chares' rows 1..chunk in order ((ny-2) x nx
+ * floats) from the buffer of the last iteration. Returns 0, or -1 for sizes
+ * the decomposition does not cover (chunk_low < 2, nx < 3). */
+int oracle_decomp1d_f32(int n, int nx, int ny, int iters, const float* bc_rows, float* out) {
+  if (n < 1 || nx < 3 || ny < 4 || iters < 0) return -1;
+  const int low = (ny - 2) / n, high = low + 1;
+  if (low < 2) return -1;
+  const int n_low = n * low + n - (ny - 2);
+  const size_t cnt = (size_t)nx * (high + 2);
+  float* buf = (float*)calloc((size_t)n * 2 * cnt, sizeof(float));
+  int* chunk = (int*)malloc(sizeof(int) * n);
+  int* g0 = (int*)malloc(sizeof(int) * n);
+  int* iend = (int*)malloc(sizeof(int) * n);
+  if (!buf || !chunk || !g0 || !iend) {
+    free(buf); free(chunk); free(g0); free(iend);
+    return -1;
+  }
+  for (int i = 0; i < n; i++) {
+    chunk[i] = i < n_low ? low : high;
+    g0[i] = i < n_low ? i * low + 1 : n_low * low + (i - n_low) * high + 1;
+    int gend = g0[i] + chunk[i] - 1;
+    if (gend > ny - 4) gend = ny - 4;
+    iend[i] = (gend - g0[i] + 1) + 1;
+    for (int b = 0; b < 2; b++) {
+      float* a = buf + ((size_t)i * 2 + b) * cnt;
+      for (int r = 1; r <= chunk[i]; r++) {
+        const float v = bc_rows[g0[i] + r - 1];
+        a[(size_t)r * nx] = v;
+        a[(size_t)r * nx + nx - 1] = v;
+      }
+    }
+  }
+  for (int k = 0; k < iters; k++) {
+    for (int i = 0; i < n; i++) {
+      const float* a = buf + ((size_t)i * 2 + (k & 1)) * cnt;
+      float* o = buf + ((size_t)i * 2 + ((k + 1) & 1)) * cnt;
+      for (int iy = 1; iy < iend[i]; iy++)
+        for (int ix = 1; ix < nx - 1; ix++) {
+          float s = a[(size_t)iy * nx + ix + 1] + a[(size_t)iy * nx + ix - 1];
+          s = s + a[(size_t)(iy + 1) * nx + ix];
+          s = s + a[(size_t)(iy - 1) * nx + ix];
+          o[(size_t)iy * nx + ix] = (float)(0.25 * (double)s);
+        }
+    }
+    for (int i = 0; i < n; i++) {
+      const int top = i > 0 ? i - 1 : n - 1, bot = (i + 1) % n;
+      const float* o = buf + ((size_t)i * 2 + ((k + 1) & 1)) * cnt;
+      float* t = buf + ((size_t)top * 2 + ((k + 1) & 1)) * cnt;
+      float* b = buf + ((size_t)bot * 2 + ((k + 1) & 1)) * cnt;
+      memcpy(t + (size_t)(chunk[top] + 1) * nx + 1, o + (size_t)1 * nx + 1, sizeof(float) * (nx - 2));
+      memcpy(b + 1, o + (size_t)(iend[i] - 1) * nx + 1, sizeof(float) * (nx - 2));
+    }
+  }
+  size_t row = 0;
+  for (int i = 0; i < n; i++) {
+    const float* a = buf + ((size_t)i * 2 + (iters & 1)) * cnt;
+    for (int r = 1; r <= chunk[i]; r++, row++) memcpy(out + row * nx, a + (size_t)r * nx, sizeof(float) * nx);
+  }
+  free(buf); free(chunk); free(g0); free(iend);
+  return 0;
+}

@@ -27,6 +27,7 @@
 #include "../../charming_b200/csrc/apps/jacobi_types.cuh"
 #include "../../charming_b200/csrc/apps/jacobi_sweep.cuh"
 #include "../../charming_b200/csrc/apps/serve_host.h"
+#include "../../charming_b200/csrc/apps/decomp1d.h"
 
 #include <atomic>
 #include <chrono>
@@ -154,6 +155,9 @@ unsigned long long charm::rt::globaltimer() {
 }
 
 extern "C" int oracle_jacobi2d_f64(double* grid, int nx, int ny, int sweeps);
+// apps/msgbench.cu: host plan of the fan-out (delivery counts, log offsets)
+int fanout_plan(int n, int msgs, unsigned long long seed, std::vector<int>& expected,
+    std::vector<unsigned long long>& off);
 extern "C" int oracle_jacobi2d_f32(float* grid, int nx, int ny, int sweeps, int threads);
 
 // programs of the library that this check does not run
@@ -472,12 +476,13 @@ int main(int argc, char** argv) {
     int reps = argc >= 10 ? atoi(argv[9]) : 1;
     size_t total = (size_t)n * msgs;
     std::vector<unsigned int> log(8 * total + 8);
-    std::vector<unsigned long long> ctr(8);
-    std::vector<int> expected(total);
+    std::vector<unsigned long long> ctr(8), off;
+    std::vector<int> expected;
+    const int active = fanout_plan(n, msgs, seed, expected, off);
     int status = 0;
     for (int rep = 0; rep < reps && status == 0; rep++) {  // runs in a row: rings keep their tickets
       std::fill(ctr.begin(), ctr.end(), 0ull);
-      std::fill(expected.begin(), expected.end(), 0);
+      std::fill(log.begin(), log.end(), 0u);
       g_app.id = suite::APP_FANOUT;
       g_app.a[0] = n;
       g_app.a[1] = msgs;
@@ -485,13 +490,15 @@ int main(int argc, char** argv) {
       g_app.a[3] = (long long)seed;
       g_app.a[4] = mode;
       g_app.a[5] = (long long)total;
+      g_app.a[6] = active;
       g_app.p[0] = log.data();
       g_app.p[1] = ctr.data();
       g_app.p[2] = expected.data();
+      g_app.p[3] = off.data();
       status = run_scheduler(n_pes, threads);
     }
-    printf("status=%d delivered=%llu deferred=%llu\n", status, (unsigned long long)ctr[1], g_deferred);
-    unsigned long long nrec = std::min<unsigned long long>(ctr[0], total);
+    printf("status=%d chares_done=%llu deferred=%llu\n", status, (unsigned long long)ctr[1], g_deferred);
+    unsigned long long nrec = total;
     for (unsigned long long r = 0; r < nrec; r++) {
       printf("L");
       for (int k = 0; k < 8; k++) printf(" %08x", log[8 * r + k]);
@@ -524,6 +531,49 @@ int main(int argc, char** argv) {
     printf("status=%d order=", status);
     for (int v : order) printf("%d,", v);
     printf("\n");
+    return 0;
+  }
+  if (app == "decomp1d") {  // rt_emu decomp1d n_pes ring_bytes n_chares nx ny iters mode
+    if (argc < 9) return 2;
+    const int n = atoi(argv[4]), nx = atoi(argv[5]), ny = atoi(argv[6]), iters = atoi(argv[7]),
+              mode = atoi(argv[8]);
+    std::vector<d1_desc> descs;
+    std::vector<int> g0;
+    std::vector<float> bc;
+    if (!decomp1d_plan(n, ny, descs, g0, bc)) return 2;
+    const size_t cnt = (size_t)nx * ((ny - 2) / n + 3);
+    std::vector<float> buf(cnt * 2 * n + 64, 0.f);
+    float* base = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(buf.data()) + 255) & ~uintptr_t(255));
+    for (int c = 0; c < n; c++)
+      for (int r = 1; r <= descs[c].chunk; r++)
+        for (int b = 0; b < 2; b++) {
+          base[((size_t)c * 2 + b) * cnt + (size_t)r * nx] = bc[g0[c] + r - 1];
+          base[((size_t)c * 2 + b) * cnt + (size_t)r * nx + nx - 1] = bc[g0[c] + r - 1];
+        }
+    std::vector<unsigned long long> sig(2 * (size_t)n + 8, 0);
+    g_app.id = suite::APP_DECOMP1D;
+    g_app.a[0] = n;
+    g_app.a[1] = nx;
+    g_app.a[2] = iters;
+    g_app.a[3] = mode;
+    g_app.a[4] = (long long)cnt;
+    g_app.p[0] = base;
+    g_app.p[1] = descs.data();
+    g_app.p[2] = sig.data();
+    g_app.p[3] = sig.data() + 2 * (size_t)n;
+    int status = run_scheduler(n_pes, threads);
+    printf("status=%d\n", status);
+    for (int c = 0; c < n; c++)
+      for (int r = 1; r <= descs[c].chunk; r++) {
+        printf("G");
+        for (int x = 0; x < nx; x++) {
+          const float v = base[((size_t)c * 2 + (iters & 1)) * cnt + (size_t)r * nx + x];
+          unsigned u;
+          memcpy(&u, &v, 4);
+          printf(" %08x", u);
+        }
+        printf("\n");
+      }
     return 0;
   }
   if (app == "userheap") {  // rt_emu userheap n_pes ring_bytes n_chares blocks rounds seed

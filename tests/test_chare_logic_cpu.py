@@ -113,6 +113,9 @@ def test_protocol_model_random_orders(px, py, K, mx, stop_at):
     (300, 100, 1, 1, 17, 0, 0.0, 0, 0, 96, 0, 0, 2),
     (1100, 40, 2, 1, 9, 0, 0.0, 1, 0, 128, 0, 0, 4),
     (48, 40, 3, 2, 300, 10, 0.2, 1, 0, 64, 0, 0, 5),
+    (200, 60, 2, 2, 31, 0, 0.0, 0, 0, 64, 0, 0, 6),     # deeper passes: strips and row
+    (150, 50, 1, 2, 27, 0, 0.0, 1, 1, 96, 0, 0, 7),     # runs overlap by more vectors
+    (260, 44, 2, 1, 40, 10, 0.01, 0, 0, 64, 0, 0, 8),
 ])
 def test_chare_code_threaded_block(emu, cfg):
     """One PE block of many threads: barriers reached from different call

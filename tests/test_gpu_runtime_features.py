@@ -9,6 +9,7 @@ import os
 import subprocess
 import sys
 
+import numpy as np
 import pytest
 
 from oracle import msgmodel
@@ -79,3 +80,27 @@ def test_full_rings_defer_sends(n, msgs, payload, mode):
     assert ok, errors
     assert delivered == n * msgs
     assert deferred > 0
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+def test_sm_pingpong_floor(rt, mode):
+    r = rt.sm_pingpong(mode, round_trips=2000)
+    assert r["sm_pair"][0] != r["sm_pair"][1]
+    assert 0 < r["oneway_ns"] < 100000
+
+
+@pytest.mark.parametrize("n,nx,ny,iters,mode", [
+    (148, 256, 600, 30, 0),    # signals waited inside the entry method, one chare per PE
+    (148, 256, 600, 30, 1),    # async_wait
+    (148, 256, 600, 30, 2),    # rows as refnum-tagged messages
+    (400, 64, 1203, 17, 1),    # several chares per PE, uneven bands
+    (400, 64, 1203, 17, 2),
+    (3, 1024, 40, 9, 2),       # neighbours on the same PE
+])
+def test_decomp1d_matches_oracle(rt, n, nx, ny, iters, mode):
+    from oracle import jacobi as oj
+    if mode == 0 and n > rt.n_pes:
+        pytest.skip("one chare per PE")
+    got, _ = rt.decomp1d(n, nx, ny, iters, mode)
+    ref = oj.decomp1d(n, nx, ny, iters)
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))

@@ -155,6 +155,29 @@ def test_user_heap(emus, exe, n_pes, threads, n, blocks, rounds):
     assert int(f["bytes"]) > 3 * n_pes * 65536
 
 
+@pytest.mark.parametrize("exe,n_pes,threads,n,nx,ny,iters,mode", [
+    ("rt_emu", 5, 1, 5, 16, 30, 7, 0),      # signals, one chare per PE, waits in the entry method
+    ("rt_emu", 3, 1, 7, 16, 40, 9, 1),      # signals, async_wait, several chares per PE
+    ("rt_emu", 3, 1, 7, 20, 33, 9, 2),      # rows as messages tagged with refnums
+    ("rt_emu", 1, 1, 3, 12, 20, 6, 2),      # every neighbour on the same PE
+    ("rt_emu_tsan", 4, 1, 6, 16, 30, 5, 1),
+    ("rt_emu_tsan", 4, 1, 6, 16, 30, 5, 2),
+    ("rt_emu_mt", 1, 64, 4, 136, 24, 5, 1),  # warps walking column strips
+    ("rt_emu_mt", 1, 32, 4, 64, 24, 5, 2),
+])
+def test_decomp1d_matches_oracle(emus, exe, n_pes, threads, n, nx, ny, iters, mode):
+    """jacobi2d-decomp1d on the real scheduler, bit for bit against the CPU
+    restatement (oracle/jacobi_oracle.c oracle_decomp1d_f32)."""
+    from oracle import jacobi as oj
+    r = run(emus[exe], ["decomp1d", n_pes, 65536, n, nx, ny, iters, mode], threads)
+    lines = r.stdout.splitlines()
+    assert lines and lines[0] == "status=0", (lines[:2], r.stderr[-2000:])
+    got = np.array([[int(x, 16) for x in l.split()[1:]] for l in lines if l.startswith("G ")], dtype=np.uint32)
+    ref = oj.decomp1d(n, nx, ny, iters)
+    assert got.shape == ref.shape
+    assert np.array_equal(got, ref.view(np.uint32))
+
+
 def serve(exe, n_pes, n_req, seed, wpp, max_inflight, side, dtype, threads=1, ring=65536):
     """Solve server on the CPU: the real scheduler runs the Jacobi2d chares
     in serving mode (apps/jacobi2d.cu) and admission runs apps/serve_host.h;
