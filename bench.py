@@ -309,6 +309,9 @@ def messaging_suite(seed: int = 0xC2) -> dict:
     st = rt.last_stats()
     rt = Runtime(pes_per_sm=1, threads_per_pe=128)
     small, _ = rt.pingpong([8, 64, 1024], 10000, warmup=200, seed=seed, verify=True)
+    floors = {name: rt.sm_pingpong(mode, 10000) for mode, name in
+              ((0, "flag_release_acquire"), (1, "flag_relaxed_poll_fence"), (2, "flag_with_block_barriers"),
+               (3, "reference_slot_scheme"))}
     rt = Runtime(pes_per_sm=4, threads_per_pe=128)
     log, ms = rt.fanout(4096, 16, 64, seed, 1)
     fst = rt.last_stats()
@@ -320,7 +323,11 @@ def messaging_suite(seed: int = 0xC2) -> dict:
                      "oneway_ns": {str(r["size"]): round(r["oneway_us"] * 1e3, 1) for r in rows},
                      "oneway_cycles": {str(r["size"]): round(r["oneway_cycles"], 1) for r in rows},
                      "checksum_errors": int(sum(r["checksum_errors"] for r in rows)),
-                     "status": st.status},
+                     "status": st.status,
+                     "floor": {k: {"oneway_ns": round(v["oneway_ns"], 1), "oneway_cycles": round(v["oneway_cycles"], 1)}
+                               for k, v in floors.items()},
+                     "floor_note": "two thread blocks on different SMs bouncing a counter without the runtime "
+                                   "(charming_sm_pingpong); reference_slot_scheme restates examples/baseline"},
         "fanout": {"runtime": "4 PEs of 128 threads per SM", "chares": 4096, "msgs_per_chare": 16,
                    "payload_bytes": 64, "refnums": "0..15",
                    "ms": ms, "msgs_per_s": n / (ms * 1e-3), "delivered": int(len(log)),
@@ -349,6 +356,99 @@ def messaging_cpu_baseline(seed: int) -> dict:
                       "(1,000 for 1 MiB) between two threads"}
 
 
+def _omp_threads() -> int:
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    return os.cpu_count() or 1
+
+
+def _sweep_inplace(g: np.ndarray, sweeps: int, threads: int) -> None:
+    """OpenMP oracle sweeps on the grid in place (FP64 or FP32)."""
+    import ctypes as C
+
+    from oracle import jacobi as oj
+    ny, nx = g.shape[0] - 2, g.shape[1] - 2
+    if g.dtype == np.float64:
+        oj.lib().oracle_jacobi2d_f64_omp(g.ctypes.data_as(C.POINTER(C.c_double)), nx, ny, sweeps, threads)
+    else:
+        oj.lib().oracle_jacobi2d_f32(g.ctypes.data_as(C.POINTER(C.c_float)), nx, ny, sweeps, threads)
+
+
+def cpu_set_baseline(probs, dtype: str, target_s: float = 10.0) -> dict:
+    """The batched (or precision) problem set on the host cores: every problem
+    swept by the OpenMP oracle (FP64, or FP32 with the FP64 residual every
+    10 sweeps for the precision set), for a sweep count per problem scaled so
+    the whole sample takes about target_s; GLUP/s over the sample."""
+    from charming_b200.jacobi import initial_grid
+    from oracle import jacobi as oj
+    threads = _omp_threads()
+    npdt = np.float64 if dtype == "f64" else np.float32
+    grids = [np.ascontiguousarray(initial_grid(p.nx, p.ny, p.bc, npdt)) for p in probs]
+    points = sum(p.nx * p.ny for p in probs)
+
+    def run(sweeps: int) -> float:
+        t0 = time.perf_counter()
+        for p, g in zip(probs, grids):
+            if dtype == "f64":
+                _sweep_inplace(g, sweeps, threads)
+            else:
+                done = 0
+                while done < sweeps:
+                    k = min(10, sweeps - done)
+                    _sweep_inplace(g, k, threads)
+                    oj.residual(g)
+                    done += k
+        return time.perf_counter() - t0
+    t1 = run(10) / 10
+    sweeps = int(max(10, min(5000, target_s / max(t1, 1e-9))))
+    sweeps = sweeps // 10 * 10
+    dt = run(sweeps)
+    return {"value": points * sweeps / dt / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"all {len(probs)} problems, {sweeps} sweeps each ({dtype}"
+                      f"{', FP64 residual every 10 sweeps' if dtype == 'f32' else ''}; {dt:.1f} s)"}
+
+
+def cpu_serving_baseline(probs, arrive, target_s: float = 15.0) -> dict:
+    """The serving trace on the host cores: requests in arrival order, each
+    solved with all cores (OpenMP FP32 sweeps, FP64 residual every 10 sweeps,
+    stop at the tolerance or the sweep cap, as the GPU server does), served
+    one after another from their arrival times, until about target_s of
+    solving; solves/s and latency (arrival to completion) over that prefix."""
+    from charming_b200.jacobi import initial_grid
+    from oracle import jacobi as oj
+    threads = _omp_threads()
+    t0 = time.perf_counter()
+    lat, busy_until, done, lups = [], 0.0, 0, 0
+    for p, at in zip(probs, arrive):
+        start = max(busy_until, at)
+        s0 = time.perf_counter()
+        g = np.ascontiguousarray(initial_grid(p.nx, p.ny, p.bc, np.float32))
+        r0 = None
+        sweeps = 0
+        stop_at = p.max_sweeps
+        while sweeps < stop_at:
+            if p.check_every and sweeps % p.check_every == 0:
+                r = oj.residual(g)
+                r0 = r if r0 is None else r0
+                if p.tol > 0 and (r0 == 0.0 or r <= p.tol * r0):
+                    stop_at = min(stop_at, sweeps + p.check_every)
+            k = min(p.check_every or stop_at, stop_at - sweeps)
+            _sweep_inplace(g, k, threads)
+            sweeps += k
+        solve = time.perf_counter() - s0
+        busy_until = start + solve
+        lat.append(busy_until - at)
+        lups += p.nx * p.ny * sweeps
+        done += 1
+        if time.perf_counter() - t0 > target_s:
+            break
+    span = busy_until - arrive[0]
+    return {"kind": "port", "cores": threads, "requests": done, "solves_per_s": done / span,
+            "p50_ms": float(np.percentile(lat, 50)) * 1e3, "p99_ms": float(np.percentile(lat, 99)) * 1e3,
+            "served_glups": lups / span / 1e9,
+            "sample": f"the first {done} requests of the same trace, one at a time on all cores "
+                      f"({time.perf_counter() - t0:.1f} s)"}
+
+
 def batched_suite(steps: int = 3, warmup: int = 3) -> dict:
     """C3: the 64-problem uneven FP64 set, 500 sweeps, CUDA graph, autotuned."""
     from charming_b200.batch import autotune, uneven_set
@@ -372,7 +472,8 @@ def batched_suite(steps: int = 3, warmup: int = 3) -> dict:
             "workload": "64 square FP64 problems, sides log-uniform in [64, 2048] (seed 0xC3), "
                         "500 sweeps, one launch from a CUDA graph",
             "glups": points * 500 / (ms * 1e-3) / 1e9, "ms_per_launch": ms, "launches": steps,
-            "points": points, "chares": info["n_chares"], "autotune": tune.as_dict()}
+            "points": points, "chares": info["n_chares"], "autotune": tune.as_dict(),
+            "cpu_baseline": cpu_set_baseline(probs, "f64")}
 
 
 def precision_suite(plain_fp64_glups: float, steps: int = 2, warmup: int = 1) -> dict:
@@ -433,7 +534,8 @@ def precision_suite(plain_fp64_glups: float, steps: int = 2, warmup: int = 1) ->
             "res_rel_8192": res[-1].res_last / res[-1].res0 if res[-1].res0 else None,
             "reference": "FP64 grids from the FP64 path (bit-identical to the serial oracle) "
                          "after each problem's FP32 sweep count",
-            "autotune": tune.as_dict()}
+            "autotune": tune.as_dict(),
+            "cpu_baseline": cpu_set_baseline(probs, "f32")}
 
 
 def serving_suite(n_req: int, rate: float = 200.0, seed: int = 0xC5, pes_per_sm: int = 1,
@@ -493,7 +595,8 @@ def serving_suite(n_req: int, rate: float = 200.0, seed: int = 0xC5, pes_per_sm:
             "service_p50_ms": float(np.percentile(service, 50)) * 1e3,
             "service_p99_ms": float(np.percentile(service, 99)) * 1e3,
             "offered_glups": offered / 1e9, "served_glups": lups_done / wall / 1e9,
-            "peak_inflight": stats.get("peak_inflight"), "peak_bytes": stats.get("peak_bytes")}
+            "peak_inflight": stats.get("peak_inflight"), "peak_bytes": stats.get("peak_bytes"),
+            "cpu_baseline": cpu_serving_baseline(probs, arrive)}
 
 
 def run_suites(args, headline_glups: float) -> dict:

@@ -147,6 +147,7 @@ SIGNATURES = [
     ("charming_sm_pingpong", i32, [i32, i32, C.POINTER(f64), C.POINTER(f64), C.POINTER(i32)]),
     ("charming_sweep_bench", i32, [i32, i32, i32, i32, i32, i32, i32, C.POINTER(f64)]),
     ("charming_jacobi2d_decomp1d", i32, [i32, i32, i32, i32, i32, C.POINTER(C.c_float), C.POINTER(f64)]),
+    ("charming_jacobi3d", i32, [i32, i32, i32, i32, C.POINTER(f64), C.POINTER(f64)]),
     ("charming_user_heap_check", i32, [i32, i32, i32, u64, C.POINTER(u64)]),
     ("charming_serve_start", i32, [C.POINTER(ServeConfig), C.POINTER(vp)]),
     ("charming_serve_submit", i32, [vp, C.POINTER(JacobiProblem), u64]),

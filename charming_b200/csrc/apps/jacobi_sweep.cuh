@@ -3,8 +3,12 @@
 //
 // Arithmetic (reference examples/jacobi2d/jacobi2d.cu:327-334):
 //   new = (c + l + r + u + d) * 0.2, added left to right in T, one multiply
-//   by the double 0.2 (float grids: float sum, double multiply, rounded to
-//   float). Written with _rn intrinsics so no contraction can change it.
+//   by the double 0.2 for double grids. Float grids (the reference has none)
+//   add in float and multiply by 0.2 as the float pair C_HI + C_LO
+//   (C_HI = 0.2f, C_LO = the float nearest 0.2 - C_HI) with one FMA:
+//   fma(s, C_HI, s * C_LO), within an ulp of the product with the double
+//   0.2 and without its two conversions. Written with _rn intrinsics so no
+//   contraction can change it.
 //
 // Block layout in HBM (per chare, two buffers): rows 0..h+1 (0 and h+1 are
 // ghost rows), row pitch `pitch` elements (a multiple of 128 bytes); column
@@ -42,9 +46,11 @@ template <> struct traits<float> {
 __device__ __forceinline__ double stencil(double c, double l, double r, double u, double d) {
   return __dmul_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(c, l), r), u), d), 0.2);
 }
+constexpr float STENCIL_C_HI = 0.2f;                     // 0x3e4ccccd
+constexpr float STENCIL_C_LO = -2.9802322831784522e-09f;  // 0xb14ccccd: 0.2 - C_HI, rounded
 __device__ __forceinline__ float stencil(float c, float l, float r, float u, float d) {
   float s = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(c, l), r), u), d);
-  return __double2float_rn(__dmul_rn((double)s, 0.2));
+  return __fmaf_rn(s, STENCIL_C_HI, __fmul_rn(s, STENCIL_C_LO));
 }
 // Residual term (S(u) - u)^2 with S in FP64.
 template <typename T>

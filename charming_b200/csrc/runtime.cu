@@ -231,26 +231,44 @@ __device__ unsigned char* outbox_put(int dst, unsigned long long ticket, unsigne
   return reinterpret_cast<unsigned char*>(e) + OB_HDR;
 }
 
+// Whether a message of `bytes` can go to PE dst (error recorded if not).
+__device__ bool send_allowed(int dst, unsigned long long bytes) {
+  if (dst < 0 || dst >= c_rt.n_pes) {
+    set_error(CHARMING_ERR_BAD_TARGET, -1, dst);
+    return false;
+  }
+  if (bytes > c_rt.max_msg) {
+    set_error(CHARMING_ERR_MSG_TOO_LARGE, dst, (int)(bytes > 0x7fffffffULL ? 0x7fffffff : bytes));
+    return false;
+  }
+  if (cells_for(bytes) > c_rt.ring_cells) {  // could never fit
+    set_error(CHARMING_ERR_MSG_TOO_LARGE, dst, (int)cells_for(bytes));
+    return false;
+  }
+  return true;
+}
+
+__device__ unsigned char* wait_space(int dst, unsigned long long t, unsigned long long bytes,
+    unsigned long long* ticket);
+
 // Thread 0 only. Reserves `bytes` in dst's inbox; returns the message start
 // (in the ring, or in this PE's outbox when the ring stayed full for
 // DEFER_AFTER_NS) or nullptr (error recorded, or the run is ending).
 __device__ unsigned char* reserve(int dst, unsigned long long bytes, unsigned long long* ticket) {
+  if (!send_allowed(dst, bytes)) return nullptr;
+  const unsigned long long t = atomicAdd(&c_rt.tail[dst].v, (unsigned long long)cells_for(bytes));
+  return wait_space(dst, t, bytes, ticket);
+}
+
+// The caller holds ticket t (cells_for(bytes) cells) in dst's inbox: waits
+// until the receiver has consumed enough for it, or moves the message to
+// the outbox; returns where the message goes (nullptr: error or the end of
+// the run). Any thread.
+__device__ unsigned char* wait_space(int dst, unsigned long long t, unsigned long long bytes,
+    unsigned long long* ticket) {
   pe_state* ps = pes();
-  if (dst < 0 || dst >= c_rt.n_pes) {
-    set_error(CHARMING_ERR_BAD_TARGET, -1, dst);
-    return nullptr;
-  }
-  if (bytes > c_rt.max_msg) {
-    set_error(CHARMING_ERR_MSG_TOO_LARGE, dst, (int)(bytes > 0x7fffffffULL ? 0x7fffffff : bytes));
-    return nullptr;
-  }
   const unsigned long long C = c_rt.ring_cells;
-  unsigned int cells = cells_for(bytes);
-  if (cells > C) {  // could never fit
-    set_error(CHARMING_ERR_MSG_TOO_LARGE, dst, (int)cells);
-    return nullptr;
-  }
-  unsigned long long t = atomicAdd(&c_rt.tail[dst].v, (unsigned long long)cells);
+  const unsigned int cells = cells_for(bytes);
   unsigned long long* hc = head_cache();
   // relaxed read: other threads of the block may raise hc[dst] meanwhile
   if (t + cells - ld_volatile_shared_u64(&hc[dst]) > C) {
@@ -439,14 +457,49 @@ __device__ bool charm::alloc_user_msgs(message* msgs, const int* dst_pes,
     const size_t* payload_sizes, int n) {
   pe_state* ps = pes();
   if (n > MSG_BATCH_MAX) n = MSG_BATCH_MAX;
-  // one reservation per thread (blocks smaller than the batch loop): the
-  // ring atomics overlap
-  for (int k = (int)threadIdx.x; k < n; k += (int)blockDim.x) {
-    unsigned long long bytes = envelope::alloc_size(msgtype::user, payload_sizes[k]);
-    unsigned long long t = 0;
-    ps->bm_ptr[k] = reserve(dst_pes[k], bytes, &t);
-    ps->bm_tick[k] = t;
-    ps->bm_bytes[k] = bytes;
+  if (blockDim.x >= 32) {
+    // Warp 0, one lane per message. Lanes whose messages go to the same PE
+    // form a group (__match_any_sync): its lowest lane takes the tickets of
+    // the whole group with one atomicAdd, and each lane's messages get them
+    // in batch order, so one PE's messages to another keep their order.
+    // Different PEs' reservations overlap.
+    if (threadIdx.x < 32) {
+      constexpr unsigned FULL = 0xffffffffu;
+      const int k = (int)threadIdx.x;
+      const bool act = k < n;
+      const unsigned long long bytes = act ? envelope::alloc_size(msgtype::user, payload_sizes[k]) : 0;
+      const bool ok = act && send_allowed(dst_pes[k], bytes);
+      const unsigned cells = ok ? cells_for(bytes) : 0;
+      const unsigned grp = __match_any_sync(FULL, ok ? dst_pes[k] : -1 - k);
+      const int leader = __ffs(grp) - 1;
+      unsigned pre = 0, tot = 0;
+#pragma unroll
+      for (int j = 0; j < MSG_BATCH_MAX; j++) {
+        const unsigned cj = __shfl_sync(FULL, cells, j);
+        if ((grp >> j) & 1u) {
+          if (j < k) pre += cj;
+          tot += cj;
+        }
+      }
+      unsigned long long base = 0;
+      if (ok && k == leader) base = atomicAdd(&c_rt.tail[dst_pes[k]].v, (unsigned long long)tot);
+      base = __shfl_sync(FULL, base, leader);
+      if (act) {
+        unsigned long long t = 0;
+        ps->bm_ptr[k] = ok ? wait_space(dst_pes[k], base + pre, bytes, &t) : nullptr;
+        ps->bm_tick[k] = t;
+        ps->bm_bytes[k] = bytes;
+      }
+    }
+  } else {
+    // blocks under a warp (host checks): thread by thread, in batch order
+    for (int k = (int)threadIdx.x; k < n; k += (int)blockDim.x) {
+      unsigned long long bytes = envelope::alloc_size(msgtype::user, payload_sizes[k]);
+      unsigned long long t = 0;
+      ps->bm_ptr[k] = reserve(dst_pes[k], bytes, &t);
+      ps->bm_tick[k] = t;
+      ps->bm_bytes[k] = bytes;
+    }
   }
   __syncthreads();
   bool ok = true;

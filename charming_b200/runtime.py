@@ -160,6 +160,16 @@ class Runtime:
         keys = ("taken", "bad", "failed", "checked", "freed", "done", "bytes")
         return {k: int(out[i]) for i, k in enumerate(keys)}
 
+    def jacobi3d(self, grid: np.ndarray, sweeps: int):
+        """`sweeps` 7-point FP64 sweeps of an (nz+2, ny+2, nx+2) grid; returns
+        (result, device ms of the sweeps)."""
+        g = np.ascontiguousarray(grid, dtype=np.float64).copy()
+        nz, ny, nx = (d - 2 for d in g.shape)
+        ms = C.c_double(0.0)
+        check(self.lib.charming_jacobi3d(nx, ny, nz, sweeps, g.ctypes.data_as(C.POINTER(C.c_double)),
+                                         C.byref(ms)), "charming_jacobi3d")
+        return g, ms.value
+
     def decomp1d(self, n_chares: int, nx: int, ny: int, iters: int, mode: int):
         """jacobi2d-decomp1d: (ny-2) x nx float32 bands after `iters`
         iterations (mode 0 signals waited in the entry method, 1 async_wait,

@@ -227,6 +227,13 @@ int charming_jacobi2d_destroy(void* handle);
 int charming_jacobi2d_sweeps_noalloc(int dtype, int nx, int ny, int sweeps,
     const void* dev_in, void* dev_out);
 
+/* 3-D Jacobi sweeps (the 7-point FP64 stencil of examples/jacobi-kernel/
+ * jacobi_kernel.cu:36-48, multiplied by its literal 0.142857): grid is the
+ * host's (nz+2) x (ny+2) x (nx+2) doubles, x fastest, shell fixed; it
+ * receives the result of `sweeps` sweeps. *out_ms: device time of the
+ * sweeps (copies excluded). */
+int charming_jacobi3d(int nx, int ny, int nz, int sweeps, double* grid, double* out_ms);
+
 /* Jacobi2d over a 1-D row decomposition (examples/jacobi2d-decomp1d/
  * jacobi2d.cu): an ny x nx FP32 grid (nx a multiple of 4) split into bands
  * of rows over n_chares chares as its Block::init does (:144-198), periodic

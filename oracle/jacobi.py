@@ -32,6 +32,7 @@ def lib():
         L.oracle_residual2_f32.restype = C.c_double
         L.oracle_jacobi1d_f64.argtypes = [dp, i, i]
         L.oracle_decomp1d_f32.argtypes = [i, i, i, i, fp, fp]
+        L.oracle_jacobi3d_f64.argtypes = [dp, i, i, i, i, i]
         _lib = L
     return _lib
 
@@ -98,3 +99,21 @@ def decomp1d(n: int, nx: int, ny: int, iters: int) -> np.ndarray:
     if rc != 0:
         raise ValueError("decomp1d: sizes the decomposition does not cover")
     return out
+
+
+def jacobi3d(grid: np.ndarray, sweeps: int, threads: int = 0) -> np.ndarray:
+    """`sweeps` 7-point sweeps of an (nz+2, ny+2, nx+2) FP64 grid (x fastest,
+    boundary shell fixed); serial when threads == 0."""
+    g = np.ascontiguousarray(grid, dtype=np.float64).copy()
+    nz, ny, nx = (d - 2 for d in g.shape)
+    lib().oracle_jacobi3d_f64(g.ctypes.data_as(C.POINTER(C.c_double)), nx, ny, nz, sweeps, threads)
+    return g
+
+
+def seeded_grid3d(nx: int, ny: int, nz: int, seed: int) -> np.ndarray:
+    """Every cell (shell included) = (mix64(seed * 2^32 + k) >> 11) * 2^-53,
+    k the cell's linear index (the reference-kernel harness fills the same)."""
+    k = np.arange((nx + 2) * (ny + 2) * (nz + 2), dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        v = mix64((np.uint64(seed) << np.uint64(32)) + k)
+    return ((v >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)).reshape(nz + 2, ny + 2, nx + 2)

@@ -6,8 +6,9 @@
  *   2-D: examples/jacobi2d/jacobi2d.cu:327-334
  *        new[i][j] = (t[i][j] + t[i][j-1] + t[i][j+1] + t[i-1][j] + t[i+1][j]) * 0.2
  *        evaluated left to right in the grid's type, then one multiply by the
- *        double literal 0.2 (for float grids: float sum, double multiply,
- *        rounded to float on store, as C/C++ promotion gives).
+ *        double literal 0.2. Float grids (the reference has none): float
+ *        sum s, then fmaf(s, C_HI, s * C_LO) with C_HI = 0.2f and C_LO the
+ *        float nearest 0.2 - C_HI (the GPU's FP32 sweep does the same).
  *   1-D: examples/jacobi1d/jacobi1d.cu:160-170
  *        sum = 0; for j in -2..2: sum += t[i+j]; new[i] = sum / 5
  *   Residual (project-defined, the reference has none): r = S(u) - u with S
@@ -19,6 +20,7 @@
  * jacobi_2d_kernel (examples/jacobi-kernel/jacobi_kernel.cu:26-34) by the
  * fixtures in tests/golden/.
  */
+#include <math.h>
 #include <stddef.h>
 #include <stdint.h>
 #include <string.h>
@@ -41,6 +43,9 @@ static void sweep_rows_f64(const double* t, double* n, int nx, int r0, int r1) {
   }
 }
 
+#define STENCIL_C_HI 0.2f                     /* 0x3e4ccccd */
+#define STENCIL_C_LO (-2.9802322831784522e-09f)  /* 0xb14ccccd */
+
 static void sweep_rows_f32(const float* t, float* n, int nx, int r0, int r1) {
   const size_t w = (size_t)nx + 2;
   for (int i = r0; i < r1; i++) {
@@ -53,7 +58,8 @@ static void sweep_rows_f32(const float* t, float* n, int nx, int r0, int r1) {
       s = s + c[j + 1];
       s = s + up[j];
       s = s + dn[j];
-      o[j] = (float)((double)s * 0.2);
+      const float lo = s * STENCIL_C_LO;
+      o[j] = fmaf(s, STENCIL_C_HI, lo);
     }
   }
 }
@@ -265,5 +271,44 @@ int oracle_decomp1d_f32(int n, int nx, int ny, int iters, const float* bc_rows, 
     for (int r = 1; r <= chunk[i]; r++, row++) memcpy(out + row * nx, a + (size_t)r * nx, sizeof(float) * nx);
   }
   free(buf); free(chunk); free(g0); free(iend);
+  return 0;
+}
+
+/* ---- 3-D (examples/jacobi-kernel/jacobi_kernel.cu:36-48) -----------------
+ * One sweep of the 7-point stencil over the interior of an (nz+2) x (ny+2) x
+ * (nx+2) FP64 grid, x fastest (IDX_3D, jacobi_kernel.h:7):
+ *   new = (c + x-1 + x+1 + y-1 + y+1 + z-1 + z+1) * 0.142857
+ * added left to right, one multiply by the double literal (DIVIDEBY7, :16).
+ * `sweeps` sweeps alternate between two buffers; threads > 1 splits the z
+ * planes over OpenMP threads (bit-identical to the serial order). */
+static void sweep3d_planes(const double* t, double* o, int nx, int ny, int z0, int z1) {
+  const size_t sy = (size_t)nx + 2, sz = sy * ((size_t)ny + 2);
+  for (int k = z0; k < z1; k++)
+    for (int j = 1; j <= ny; j++) {
+      const double* c = t + (size_t)k * sz + (size_t)j * sy;
+      double* w = o + (size_t)k * sz + (size_t)j * sy;
+      for (int i = 1; i <= nx; i++)
+        w[i] = (c[i] + c[i - 1] + c[i + 1] + c[i - sy] + c[i + sy] + c[i - sz] + c[i + sz]) * 0.142857;
+    }
+}
+
+int oracle_jacobi3d_f64(double* grid, int nx, int ny, int nz, int sweeps, int threads) {
+  const size_t n = ((size_t)nx + 2) * ((size_t)ny + 2) * ((size_t)nz + 2);
+  double* b = (double*)malloc(n * sizeof(double));
+  if (!b) return -1;
+  memcpy(b, grid, n * sizeof(double));
+  double *a = grid, *o = b;
+  for (int s = 0; s < sweeps; s++) {
+#ifdef _OPENMP
+    if (threads > 1) {
+#pragma omp parallel for num_threads(threads) schedule(static)
+      for (int k = 1; k <= nz; k++) sweep3d_planes(a, o, nx, ny, k, k + 1);
+    } else
+#endif
+      sweep3d_planes(a, o, nx, ny, 1, nz + 1);
+    double* t = a; a = o; o = t;
+  }
+  if (a != grid) memcpy(grid, a, n * sizeof(double));
+  free(b);
   return 0;
 }

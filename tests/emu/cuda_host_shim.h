@@ -62,6 +62,9 @@ void emu_syncwarp(const char* file, int line);
 #define __syncwarp(...) emu_syncwarp(__FILE__, __LINE__)
 bool emu_all_sync(bool p);
 bool emu_any_sync(bool p);
+unsigned emu_match_any(long long v);
+inline unsigned __match_any_sync(unsigned, long long v) { return emu_match_any(v); }
+inline unsigned __match_any_sync(unsigned, int v) { return emu_match_any(v); }
 void emu_shfl(void* v, unsigned bytes, int mode, int arg);  // mode 0 up, 1 down, 2 xor, 3 index
 inline bool __all_sync(unsigned, bool p) { return emu_all_sync(p); }
 inline bool __any_sync(unsigned, bool p) { return emu_any_sync(p); }
@@ -82,6 +85,8 @@ template <typename T> inline T __shfl_sync(unsigned, T v, int src) {
   return v;
 }
 #else
+inline unsigned __match_any_sync(unsigned, long long) { return 1u; }
+inline unsigned __match_any_sync(unsigned, int) { return 1u; }
 inline void __syncwarp(unsigned = 0xffffffffu) {}
 inline bool __all_sync(unsigned, bool p) { return p; }
 inline bool __any_sync(unsigned, bool p) { return p; }
@@ -96,6 +101,7 @@ inline void __threadfence() { std::atomic_thread_fence(std::memory_order_seq_cst
 inline void __threadfence_system() { std::atomic_thread_fence(std::memory_order_seq_cst); }
 inline void __nanosleep(unsigned) {}
 inline bool __isLocal(const void*) { return true; }
+inline int __ffs(unsigned x) { return x ? __builtin_ffs((int)x) : 0; }
 inline long long clock64() { return 0; }
 
 template <typename T> inline T atomicAdd(T* p, T v) { return __atomic_fetch_add(p, v, __ATOMIC_SEQ_CST); }

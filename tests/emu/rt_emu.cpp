@@ -107,6 +107,21 @@ bool emu_all_sync(bool p) {
   w.bar.sync("all_sync", 1);
   return r;
 }
+unsigned emu_match_any(long long v) {
+  Warp& w = my_warp();
+  const int lane = (int)(threadIdx.x & 31);
+  static_assert(sizeof(w.slot[0]) >= sizeof(long long), "slot");
+  memcpy(w.slot[lane], &v, sizeof(v));
+  w.bar.sync("match_any", 0);
+  unsigned m = 0;
+  for (int i = 0; i < 32; i++) {
+    long long o;
+    memcpy(&o, w.slot[i], sizeof(o));
+    if (o == v) m |= 1u << i;
+  }
+  w.bar.sync("match_any", 1);
+  return m;
+}
 bool emu_any_sync(bool p) {
   Warp& w = my_warp();
   w.flag[threadIdx.x & 31] = p;

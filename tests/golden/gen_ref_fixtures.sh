@@ -21,3 +21,19 @@ for c in "${cases[@]}"; do
 done
 json+="]}"
 echo "$json" > "$OUT/ref_jacobi2d.json"
+
+# the reference's 3-D kernel (jacobi_3d_kernel), same generator
+EXE3="$ROOT/oracle/_ref/ref_jacobi3d_dump"
+cases3=("6 5 4 1 1" "17 9 11 3 2" "33 7 13 5 3")
+json="{\"generator\": \"oracle/_ref/ref_jacobi3d_dump (reference jacobi_3d_kernel)\", \"cases\": ["
+first=1
+for c in "${cases3[@]}"; do
+  read -r nx ny nz sw seed <<<"$c"
+  f="ref_jacobi3d_${nx}x${ny}x${nz}_s${sw}_seed${seed}.bin"
+  "$EXE3" "$nx" "$ny" "$nz" "$sw" "$seed" "$OUT/$f"
+  [ $first -eq 1 ] || json+=", "
+  first=0
+  json+="{\"nx\": $nx, \"ny\": $ny, \"nz\": $nz, \"sweeps\": $sw, \"seed\": $seed, \"file\": \"$f\"}"
+done
+json+="]}"
+echo "$json" > "$OUT/ref_jacobi3d.json"

@@ -236,3 +236,22 @@ def test_autotune_reinit_and_configs(rt):
     assert tune.best.glups > 0 and all(c.glups > 0 for c in tune.tried)
     Runtime()  # default configuration for the tests that follow
     assert Runtime._active.info["n_pes"] == rt.info["n_pes"]
+
+
+def test_headline_configuration_bit_exact(rt):
+    """The benchmark's headline problem exactly as bench.py runs it: 8192^2
+    FP64, top 1 / others 0, the decomposition bench.py picks (4 x 37 chares
+    on a B200), 6 sweeps per halo exchange, balanced row runs, 100 sweeps,
+    compared bit for bit with the OpenMP oracle (bit-identical to the serial
+    one) on all host cores."""
+    import os
+
+    import bench
+    px, py = bench.choose_decomposition(rt.n_pes, 8192, 8192)
+    p = Problem(8192, 8192, 100, px=px, py=py, bc=(1.0, 0.0, 0.0, 0.0))
+    with Jacobi2D([p], dtype="f64", pipeline=False, balance=True, tile_w=0, depth=0) as j:
+        j.run()
+        out = j.store(0)
+        assert j.result(0).sweeps == 100
+    ref = oj.jacobi2d(initial_grid(8192, 8192, p.bc), 100, threads=os.cpu_count() or 1)
+    assert np.array_equal(bits(out), bits(ref))

@@ -104,3 +104,16 @@ def test_decomp1d_matches_oracle(rt, n, nx, ny, iters, mode):
     got, _ = rt.decomp1d(n, nx, ny, iters, mode)
     ref = oj.decomp1d(n, nx, ny, iters)
     assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+
+
+@pytest.mark.parametrize("nx,ny,nz,sweeps,seed", [
+    (6, 5, 4, 1, 1), (17, 9, 11, 3, 2), (33, 7, 13, 5, 3),   # the golden fixtures' shapes
+    (64, 48, 40, 4, 5),                                     # whole tiles
+    (97, 35, 70, 7, 6),                                     # ragged tiles, several z runs
+])
+def test_jacobi3d_matches_oracle(rt, nx, ny, nz, sweeps, seed):
+    from oracle import jacobi as oj
+    g = oj.seeded_grid3d(nx, ny, nz, seed)
+    got, _ = rt.jacobi3d(g, sweeps)
+    ref = oj.jacobi3d(g, sweeps)
+    assert np.array_equal(got.view(np.uint64), ref.view(np.uint64))

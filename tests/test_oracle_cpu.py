@@ -164,8 +164,27 @@ def test_jacobi_boundary_ring_fixed():
     assert np.array_equal(out[:, 0], g[:, 0]) and np.array_equal(out[:, -1], g[:, -1])
 
 
-def test_jacobi_f32_matches_promotion_rule():
+def _round_f32(q) -> np.float32:
+    """The float32 nearest the exact rational q (ties to even)."""
+    from fractions import Fraction
+    c = np.float32(float(q))
+    best = None
+    for v in (np.nextafter(c, np.float32(-np.inf)), c, np.nextafter(c, np.float32(np.inf))):
+        d = abs(Fraction(float(v)) - q)
+        if best is None or d < best[0] or (d == best[0] and int(v.view(np.uint32)) % 2 == 0):
+            best = (d, v)
+    return best[1]
+
+
+def test_jacobi_f32_fma_split_of_the_factor():
+    """FP32 sweeps: float sum s (left to right), then fma(s, C_HI, s * C_LO)
+    with C_HI = 0.2f and C_LO the float nearest 0.2 - C_HI; within an ulp of
+    the product with the double 0.2 rounded to float."""
+    from fractions import Fraction
     lib = oracle_lib()
+    c_hi = np.float32(0.2)
+    c_lo = np.float32(0.2 - float(c_hi))
+    assert c_hi.view(np.uint32) == 0x3E4CCCCD and c_lo.view(np.uint32) == 0xB14CCCCD
     g = seeded_grid(8, 6, 4).astype(np.float32)
     out = g.copy()
     lib.oracle_jacobi2d_f32(out.ctypes.data_as(C.POINTER(C.c_float)), 8, 6, 1, 1)
@@ -175,7 +194,11 @@ def test_jacobi_f32_matches_promotion_rule():
             s = np.float32(s + g[i, j + 1])
             s = np.float32(s + g[i - 1, j])
             s = np.float32(s + g[i + 1, j])
-            assert out[i, j] == np.float32(np.float64(s) * 0.2)
+            lo = np.float32(s * c_lo)
+            want = _round_f32(Fraction(float(s)) * Fraction(float(c_hi)) + Fraction(float(lo)))
+            assert out[i, j] == want
+            via_double = np.float32(np.float64(s) * 0.2)
+            assert abs(int(out[i, j].view(np.int32)) - int(via_double.view(np.int32))) <= 1
 
 
 def test_residual_matches_numpy():
@@ -216,6 +239,28 @@ def test_oracle_matches_reference_kernel_fixture(case):
 
 def test_golden_fixtures_present():
     assert _golden_cases(), "tests/golden/ref_jacobi2d.json missing (run tests/golden/gen_ref_fixtures.sh on a GPU)"
+    assert _golden_cases3(), "tests/golden/ref_jacobi3d.json missing (run tests/golden/gen_ref_fixtures.sh on a GPU)"
+
+
+def _golden_cases3():
+    path = os.path.join(GOLDEN, "ref_jacobi3d.json")
+    if not os.path.exists(path):
+        return []
+    with open(path) as f:
+        return json.load(f)["cases"]
+
+
+@pytest.mark.parametrize("case", _golden_cases3(), ids=lambda c: c["file"])
+def test_oracle_matches_reference_3d_kernel_fixture(case):
+    """Pin: the 3-D oracle reproduces the reference's own jacobi_3d_kernel
+    (examples/jacobi-kernel/jacobi_kernel.cu:36-48) bit for bit."""
+    from oracle.jacobi import jacobi3d, seeded_grid3d
+    nx, ny, nz, sweeps, seed = case["nx"], case["ny"], case["nz"], case["sweeps"], case["seed"]
+    ref = np.fromfile(os.path.join(GOLDEN, case["file"]), dtype="<f8").reshape(nz + 2, ny + 2, nx + 2)
+    out = jacobi3d(seeded_grid3d(nx, ny, nz, seed), sweeps)
+    assert np.array_equal(out.view(np.uint64), ref.view(np.uint64))
+    assert np.array_equal(jacobi3d(seeded_grid3d(nx, ny, nz, seed), sweeps, threads=4).view(np.uint64),
+                          ref.view(np.uint64))
 
 
 def test_messaging_cpu_baseline_delivers_everything():
