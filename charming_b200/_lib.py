@@ -148,6 +148,7 @@ SIGNATURES = [
     ("charming_sweep_bench", i32, [i32, i32, i32, i32, i32, i32, i32, C.POINTER(f64)]),
     ("charming_jacobi2d_decomp1d", i32, [i32, i32, i32, i32, i32, C.POINTER(C.c_float), C.POINTER(f64)]),
     ("charming_jacobi3d", i32, [i32, i32, i32, i32, C.POINTER(f64), C.POINTER(f64)]),
+    ("charming_jacobi2d_solve_stream", i32, [vp, i32, i32, C.POINTER(vp), C.POINTER(vp), C.POINTER(f64)]),
     ("charming_user_heap_check", i32, [i32, i32, i32, u64, C.POINTER(u64)]),
     ("charming_serve_start", i32, [C.POINTER(ServeConfig), C.POINTER(vp)]),
     ("charming_serve_submit", i32, [vp, C.POINTER(JacobiProblem), u64]),

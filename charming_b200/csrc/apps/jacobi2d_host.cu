@@ -37,6 +37,13 @@ struct JHandle {
   size_t grid_bytes = 0;
   void* d_stage = nullptr;
   size_t stage_bytes = 0;
+  // charming_jacobi2d_solve_stream: two input and two output staging
+  // buffers, copy streams and their events
+  void* d_pipe = nullptr;
+  size_t pipe_bytes = 0;
+  int* d_latch = nullptr;
+  cudaStream_t s_h2d = nullptr, s_d2h = nullptr;
+  cudaEvent_t in_ready[2] = {}, in_free[2] = {}, out_ready[2] = {}, out_free[2] = {};
   suite::app_params* h_params = nullptr;   // pinned
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
@@ -339,6 +346,113 @@ extern "C" int charming_jacobi2d_run(void* handle) {
   return charm_host::collect_run(ms);
 }
 
+// Device-side work of load (staged grid -> chare blocks) and store (chare
+// blocks -> staged grid) on stream s, without the host copies.
+static void enqueue_scatter(JHandle* h, int prob, const void* stage, cudaStream_t s) {
+  const charming_jacobi_problem& q = h->probs[prob];
+  const int nc = h->px[prob] * h->py[prob];
+  const int* co = h->d_chare_of + h->chare_of_off[prob];
+  if (h->esz == 8) scatter_kernel<double><<<nc, 256, 0, s>>>(h->d_chares, co, q.nx, q.ny, (const double*)stage);
+  else scatter_kernel<float><<<nc, 256, 0, s>>>(h->d_chares, co, q.nx, q.ny, (const float*)stage);
+}
+static void enqueue_gather(JHandle* h, int prob, void* stage, cudaStream_t s) {
+  const charming_jacobi_problem& q = h->probs[prob];
+  const size_t cells = (size_t)(q.nx + 2) * (q.ny + 2);
+  const int* co = h->d_chare_of + h->chare_of_off[prob];
+  const int blocks = (int)std::min<size_t>((cells + 255) / 256, 4096);
+  if (h->esz == 8)
+    gather_kernel<double><<<blocks, 256, 0, s>>>(h->d_chares, co, h->d_final, q.nx, q.ny, h->px[prob],
+                                                 h->py[prob], (double*)stage);
+  else
+    gather_kernel<float><<<blocks, 256, 0, s>>>(h->d_chares, co, h->d_final, q.nx, q.ny, h->px[prob],
+                                                h->py[prob], (float*)stage);
+}
+
+static int ensure_pipe(JHandle* h, size_t bytes) {
+  cudaError_t e = cudaSuccess;
+  if (h->pipe_bytes < bytes) {
+    if (h->d_pipe) cudaFree(h->d_pipe);
+    h->d_pipe = nullptr;
+    h->pipe_bytes = 0;
+    e = cudaMalloc(&h->d_pipe, 4 * bytes);
+    if (e != cudaSuccess) return check_cuda(e, "jacobi2d stream staging");
+    h->pipe_bytes = bytes;
+  }
+  if (!h->d_latch) e = cudaMalloc(&h->d_latch, 4 * sizeof(int));
+  if (e == cudaSuccess && !h->s_h2d) e = cudaStreamCreateWithFlags(&h->s_h2d, cudaStreamNonBlocking);
+  if (e == cudaSuccess && !h->s_d2h) e = cudaStreamCreateWithFlags(&h->s_d2h, cudaStreamNonBlocking);
+  for (int b = 0; b < 2 && e == cudaSuccess; b++) {
+    if (!h->in_ready[b]) e = cudaEventCreateWithFlags(&h->in_ready[b], cudaEventDisableTiming);
+    if (e == cudaSuccess && !h->in_free[b]) e = cudaEventCreateWithFlags(&h->in_free[b], cudaEventDisableTiming);
+    if (e == cudaSuccess && !h->out_ready[b]) e = cudaEventCreateWithFlags(&h->out_ready[b], cudaEventDisableTiming);
+    if (e == cudaSuccess && !h->out_free[b]) e = cudaEventCreateWithFlags(&h->out_free[b], cudaEventDisableTiming);
+  }
+  return check_cuda(e, "jacobi2d stream setup");
+}
+
+// n solves of problem prob, host_in[k] -> host_out[k], pipelined: the copy
+// of solve k+1's input (one stream) and of solve k-1's result (another)
+// overlap solve k on the runtime's stream, through two input and two
+// output staging buffers on the device. Each solve is exactly load, run,
+// store of that grid; the other problems of the handle are run too and left
+// where they end. Returns the first failing run's status.
+extern "C" int charming_jacobi2d_solve_stream(void* handle, int prob, int n, const void* const* host_in,
+    void* const* host_out, double* out_ms) {
+  JHandle* h = reinterpret_cast<JHandle*>(handle);
+  if (!h || prob < 0 || prob >= (int)h->probs.size() || n < 0 || (n > 0 && (!host_in || !host_out)))
+    return CHARMING_ERR_CONFIG;
+  const charming_jacobi_problem& q = h->probs[prob];
+  const size_t bytes = (size_t)(q.nx + 2) * (q.ny + 2) * h->esz;
+  int rc = ensure_pipe(h, bytes);
+  if (rc) return rc;
+  char* stage_in[2] = {static_cast<char*>(h->d_pipe), static_cast<char*>(h->d_pipe) + bytes};
+  char* stage_out[2] = {static_cast<char*>(h->d_pipe) + 2 * bytes, static_cast<char*>(h->d_pipe) + 3 * bytes};
+  cudaStream_t s = charm_host::stream();
+  charm_host::request_stop(0);
+  cudaError_t e = cudaMemsetAsync(h->d_latch, 0, 4 * sizeof(int), s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaEventRecord(h->ev0, h->s_h2d);
+  for (int k = 0; k < n && e == cudaSuccess; k++) {
+    const int b = k & 1;
+    // input k into stage_in[b] once solve k-2 has scattered it
+    if (k >= 2) e = cudaStreamWaitEvent(h->s_h2d, h->in_free[b], 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(stage_in[b], host_in[k], bytes, cudaMemcpyHostToDevice, h->s_h2d);
+    if (e == cudaSuccess) e = cudaEventRecord(h->in_ready[b], h->s_h2d);
+    // solve k
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, h->in_ready[b], 0);
+    if (e == cudaSuccess) {
+      enqueue_scatter(h, prob, stage_in[b], s);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(h->in_free[b], s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->d_final, 0, sizeof(int) * h->n_chares, s);
+    if (e != cudaSuccess) break;
+    if (h->opt.use_graph && h->graph_exec) e = cudaGraphLaunch(h->graph_exec, s);
+    else if ((rc = enqueue_run(h, s))) return rc;
+    if (e == cudaSuccess && (rc = charm_host::enqueue_status_latch(h->d_latch, s))) return rc;
+    // result k into stage_out[b] once the copy of result k-2 has left it
+    if (e == cudaSuccess && k >= 2) e = cudaStreamWaitEvent(s, h->out_free[b], 0);
+    if (e == cudaSuccess) {
+      enqueue_gather(h, prob, stage_out[b], s);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(h->out_ready[b], s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(h->s_d2h, h->out_ready[b], 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host_out[k], stage_out[b], bytes, cudaMemcpyDeviceToHost, h->s_d2h);
+    if (e == cudaSuccess) e = cudaEventRecord(h->out_free[b], h->s_d2h);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(h->ev1, h->s_d2h);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->s_d2h);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  float ms = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  if (out_ms) *out_ms = ms;
+  int latch[4] = {0, 0, 0, 0};
+  if (e == cudaSuccess) e = cudaMemcpy(latch, h->d_latch, sizeof(latch), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return check_cuda(e, "jacobi2d solve stream");
+  return latch[0];
+}
+
 extern "C" int charming_jacobi2d_result(void* handle, int prob, charming_jacobi_result* out) {
   JHandle* h = reinterpret_cast<JHandle*>(handle);
   if (!h || !out || prob < 0 || prob >= (int)h->probs.size()) return CHARMING_ERR_CONFIG;
@@ -397,6 +511,16 @@ extern "C" int charming_jacobi2d_destroy(void* handle) {
   cudaFree(h->d_chare_of);
   cudaFree(h->d_sweep_ns);
   cudaFree(h->d_stage);
+  cudaFree(h->d_pipe);
+  cudaFree(h->d_latch);
+  if (h->s_h2d) cudaStreamDestroy(h->s_h2d);
+  if (h->s_d2h) cudaStreamDestroy(h->s_d2h);
+  for (int b = 0; b < 2; b++) {
+    if (h->in_ready[b]) cudaEventDestroy(h->in_ready[b]);
+    if (h->in_free[b]) cudaEventDestroy(h->in_free[b]);
+    if (h->out_ready[b]) cudaEventDestroy(h->out_ready[b]);
+    if (h->out_free[b]) cudaEventDestroy(h->out_free[b]);
+  }
   if (h->h_params) cudaFreeHost(h->h_params);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);

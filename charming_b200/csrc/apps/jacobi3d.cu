@@ -10,9 +10,10 @@
 // iterations.
 //
 // Kernel: each block owns a 32 x 16 tile of (x, y) columns and a run of z
-// planes, and marches up z: the planes below and above a thread's cell stay
-// in its registers, the current plane (with a one-cell x/y rim) sits in
-// shared memory for the x and y neighbours. Each input value is read from
+// planes, and marches up z: the planes below and above a thread's cell (and
+// the next three, already loading) stay in its registers, the current plane
+// (with a one-cell x/y rim) sits in shared memory for the x and y
+// neighbours. Each input value is read from
 // DRAM once per sweep (16 B per lattice update with the store); the rim
 // cells are read by two blocks and mostly come from L2.
 #include "suite.cuh"
@@ -39,10 +40,12 @@ __global__ void __launch_bounds__(J3_TX * J3_TY) jacobi3d_kernel(const double* _
   const bool inx = x <= nx + 1, iny = y <= ny + 1;       // a cell of the grid (rim included)
   const bool own = x <= nx && y <= ny;                   // an interior column
   const long long col = (long long)(inx ? x : nx + 1) * sx + (long long)(iny ? y : ny + 1) * sy;
-  auto at = [&](int z) { return in[col + (long long)z * sz]; };
-  double prev = at(z0 - 1), cur = at(z0), next = at(z0 + 1);
+  auto at = [&](int z) { return z <= nz + 1 ? in[col + (long long)z * sz] : 0.0; };
+  // planes z-1 .. z+3 of this column in registers: three loads in flight
+  // per thread keep enough bytes moving to cover the memory latency
+  double prev = at(z0 - 1), cur = at(z0), next = at(z0 + 1), n2 = at(z0 + 2), n3 = at(z0 + 3);
   for (int z = z0; z < z1; z++) {
-    const double nn = z + 2 <= nz + 1 ? at(z + 2) : 0.0;  // one plane ahead
+    const double n4 = at(z + 4);
     plane[ty + 1][tx + 1] = cur;
     const long long zo = (long long)z * sz;
     if (tx == 0) plane[ty + 1][0] = in[col - sx + zo];
@@ -57,7 +60,9 @@ __global__ void __launch_bounds__(J3_TX * J3_TY) jacobi3d_kernel(const double* _
     __syncthreads();
     prev = cur;
     cur = next;
-    next = nn;
+    next = n2;
+    n2 = n3;
+    n3 = n4;
   }
 }
 

@@ -559,30 +559,31 @@ __device__ __forceinline__ double deep_item(const block_view<T>& in, const block
 }
 
 // ---------------------------------------------------------------------------
-// The same item in three phases, so that the steady state carries no test
-// it cannot need: the fill (levels without all three input rows yet, and
-// the top boundary row, which only the first 2L steps can meet), the steady
-// state, and the tail (the last steps, where a level can meet the bottom
-// boundary row). A strip without a domain-boundary column (all but the
-// outermost strips of a chare on the domain's edge) runs a version without
-// the per-lane column fix-up. Same arithmetic and results as deep_item.
+// The same item, with the tests taken out of the steady state: a group of
+// three steps that cannot need them (past the fill, before the steps that
+// can meet the bottom boundary row, in a strip without a domain-boundary
+// column) runs a step without the fill check, the boundary-row test and the
+// column fix-up; the other groups run the general step. One loop and two
+// step versions keep the code (and so the instruction cache footprint) as
+// small as deep_item's. Same arithmetic and results as deep_item.
 // ---------------------------------------------------------------------------
-// Not inlined: each version gets its own register allocation (two inlined
-// bodies in one function spill).
-template <typename T, bool RESID, int L, int P, bool COLFIX>
-__device__ __noinline__ double lean_body(block_view<T> in, block_view<T> out, int w, int h, int fixed,
-    int own0, int nown, int r0, int r1, int lane, typename vec_of<T>::type* ring) {
+template <typename T, bool RESID, int L, int P>
+__device__ __forceinline__ double lean_item(const block_view<T>& in, const block_view<T>& out, int w,
+    const deep_lane<T>& ln, int r0, int r1, int lane, typename vec_of<T>::type* ring) {
   constexpr int V = traits<T>::VEC;
-  const deep_lane<T> ln = make_lane<T, L>(w, h, fixed, own0, nown, lane);
   using VT = typename vec_of<T>::type;
   const long long e0 = (long long)traits<T>::OFF - 1 + ln.col0;  // element index in a row
   const bool can_load = e0 >= 0 && e0 + V <= in.pitch;
   const long long eo = can_load ? e0 : 0;
   const unsigned nb = can_load ? 16u : 0u;
   const int qs = r0 - L, qe = r1 - 1 + L;  // level-0 rows streamed
-  // first step at which a level may compute the bottom boundary row R
-  // (level l computes row q - l; levels 1..L-1 reach R at steps R+1..R+L-1)
-  const int q_tail = (ln.fix_r1 != INT_MIN && ln.fix_r1 + 1 <= qe) ? ln.fix_r1 + 1 : qe + 1;
+  constexpr int F = (2 * L + 2) / 3 * 3;   // steps of the fill (every level has its rows after)
+  // steady groups: from the end of the fill to before the first step at
+  // which a level can compute the bottom boundary row R (level l computes
+  // row q - l, so levels 1..L-1 reach R at steps R+1..R+L-1); none in a
+  // strip holding a domain-boundary column
+  int q_lean_end = (ln.fix_r1 != INT_MIN && ln.fix_r1 + 1 <= qe) ? ln.fix_r1 + 1 : qe + 1;
+  if (__any_sync(0xffffffffu, ln.anyfix)) q_lean_end = INT_MIN;
 #pragma unroll
   for (int k = 0; k < P - 1; k++) {
     if (qs + k <= qe) cp_async16(&ring[k * 32 + lane], in.row(qs + k) + eo, nb);
@@ -591,49 +592,28 @@ __device__ __noinline__ double lean_body(block_view<T> in, block_view<T> out, in
   VT W[L][3];
   double acc = 0.0;
   int slot = 0;
-  constexpr int F = (2 * L + 2) / 3 * 3;
-  int q0 = qs;
-  for (; q0 < qs + F && q0 <= qe; q0 += 3) {  // fill
+  for (int q0 = qs; q0 <= qe; q0 += 3) {
+    if (q0 >= qs + F && q0 + 2 < q_lean_end) {
+      deep_fetch<T, P>(ring, lane, slot, q0, qe, in, eo, nb, W[0][0]);
+      deep_step<T, RESID, L, 0, false, false, false>(W, q0, qs, w, ln, r0, r1, out, acc);
+      deep_fetch<T, P>(ring, lane, slot, q0 + 1, qe, in, eo, nb, W[0][1]);
+      deep_step<T, RESID, L, 1, false, false, false>(W, q0 + 1, qs, w, ln, r0, r1, out, acc);
+      deep_fetch<T, P>(ring, lane, slot, q0 + 2, qe, in, eo, nb, W[0][2]);
+      deep_step<T, RESID, L, 2, false, false, false>(W, q0 + 2, qs, w, ln, r0, r1, out, acc);
+    } else {
 #pragma unroll
-    for (int K = 0; K < 3; K++) {
-      const int q = q0 + K;
-      if (q > qe) break;
-      deep_fetch<T, P>(ring, lane, slot, q, qe, in, eo, nb, W[0][K]);
-      if (K == 0) deep_step<T, RESID, L, 0, true, true, COLFIX>(W, q, qs, w, ln, r0, r1, out, acc);
-      else if (K == 1) deep_step<T, RESID, L, 1, true, true, COLFIX>(W, q, qs, w, ln, r0, r1, out, acc);
-      else deep_step<T, RESID, L, 2, true, true, COLFIX>(W, q, qs, w, ln, r0, r1, out, acc);
-    }
-  }
-  for (; q0 + 2 < q_tail; q0 += 3) {  // steady: three whole steps before the tail
-    deep_fetch<T, P>(ring, lane, slot, q0, qe, in, eo, nb, W[0][0]);
-    deep_step<T, RESID, L, 0, false, false, COLFIX>(W, q0, qs, w, ln, r0, r1, out, acc);
-    deep_fetch<T, P>(ring, lane, slot, q0 + 1, qe, in, eo, nb, W[0][1]);
-    deep_step<T, RESID, L, 1, false, false, COLFIX>(W, q0 + 1, qs, w, ln, r0, r1, out, acc);
-    deep_fetch<T, P>(ring, lane, slot, q0 + 2, qe, in, eo, nb, W[0][2]);
-    deep_step<T, RESID, L, 2, false, false, COLFIX>(W, q0 + 2, qs, w, ln, r0, r1, out, acc);
-  }
-  for (; q0 <= qe; q0 += 3) {  // tail
-#pragma unroll
-    for (int K = 0; K < 3; K++) {
-      const int q = q0 + K;
-      if (q > qe) break;
-      deep_fetch<T, P>(ring, lane, slot, q, qe, in, eo, nb, W[0][K]);
-      if (K == 0) deep_step<T, RESID, L, 0, false, true, COLFIX>(W, q, qs, w, ln, r0, r1, out, acc);
-      else if (K == 1) deep_step<T, RESID, L, 1, false, true, COLFIX>(W, q, qs, w, ln, r0, r1, out, acc);
-      else deep_step<T, RESID, L, 2, false, true, COLFIX>(W, q, qs, w, ln, r0, r1, out, acc);
+      for (int K = 0; K < 3; K++) {
+        const int q = q0 + K;
+        if (q > qe) break;
+        deep_fetch<T, P>(ring, lane, slot, q, qe, in, eo, nb, W[0][K]);
+        if (K == 0) deep_step<T, RESID, L, 0, true>(W, q, qs, w, ln, r0, r1, out, acc);
+        else if (K == 1) deep_step<T, RESID, L, 1, true>(W, q, qs, w, ln, r0, r1, out, acc);
+        else deep_step<T, RESID, L, 2, true>(W, q, qs, w, ln, r0, r1, out, acc);
+      }
     }
   }
   cp_async_wait<0>();
   return acc;
-}
-
-template <typename T, bool RESID, int L, int P>
-__device__ __forceinline__ double lean_item(const block_view<T>& in, const block_view<T>& out, int w, int h,
-    int fixed, int own0, int nown, const deep_lane<T>& ln, int r0, int r1, int lane,
-    typename vec_of<T>::type* ring) {
-  if (__any_sync(0xffffffffu, ln.anyfix))
-    return lean_body<T, RESID, L, P, true>(in, out, w, h, fixed, own0, nown, r0, r1, lane, ring);
-  return lean_body<T, RESID, L, P, false>(in, out, w, h, fixed, own0, nown, r0, r1, lane, ring);
 }
 
 // The same pass, computed by thread 0 alone for blocks under one warp, with
@@ -706,7 +686,7 @@ __device__ __noinline__ double sweep_deep_items(block_view<T> in, block_view<T> 
     int own0 = s * SS;
     int nown = min(SS, nv - own0);
     const deep_lane<T> ln = make_lane<T, L>(w, h, fixed, own0, nown, lane);
-    if (LEAN) acc += lean_item<T, RESID, L, P>(in, out, w, h, fixed, own0, nown, ln, r0, r1, lane, ring);
+    if (LEAN) acc += lean_item<T, RESID, L, P>(in, out, w, ln, r0, r1, lane, ring);
     else acc += deep_item<T, RESID, L, P>(in, out, w, ln, r0, r1, lane, ring);
   }
   return acc;

@@ -119,6 +119,21 @@ int enqueue_scheduler(cudaStream_t s) {
   return CHARMING_OK;
 }
 
+__global__ void charming_status_latch_kernel(const int* ctrl, int* latch) {
+  if (latch[0] == 0 && ctrl[CTRL_STATUS] != 0) {
+    latch[0] = ctrl[CTRL_STATUS];
+    latch[1] = ctrl[CTRL_ERR_PE];
+    latch[2] = ctrl[CTRL_ERR_I0];
+    latch[3] = ctrl[CTRL_ERR_I1];
+  }
+}
+
+int enqueue_status_latch(int* latch, cudaStream_t s) {
+  if (!g.inited) return CHARMING_ERR_NOT_INIT;
+  charming_status_latch_kernel<<<1, 1, 0, s>>>(g.ds.ctrl, latch);
+  return cuda_fail(cudaGetLastError(), "status latch");
+}
+
 int collect_run(double kernel_ms) {
   int ctrl_h[CTRL_WORDS];
   cudaError_t e = cudaMemcpy(ctrl_h, g.ds.ctrl, sizeof(ctrl_h), cudaMemcpyDeviceToHost);

@@ -30,6 +30,10 @@ int enqueue_scheduler(cudaStream_t s);
 // After the work enqueued by enqueue_scheduler completed: read status and
 // statistics into the last-run record; returns the run status.
 int collect_run(double kernel_ms);
+// Enqueues, after a scheduler run on s, a copy of the run's status words
+// into latch[4] if latch[0] is still 0 (the first failing run of a series
+// is kept; reading the latch needs no synchronisation per run).
+int enqueue_status_latch(int* latch, cudaStream_t s);
 
 // Run deadline of the following launches in seconds (<= 0: the configured
 // one). Call only while no scheduler launch is running.

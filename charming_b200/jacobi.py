@@ -133,6 +133,23 @@ class Jacobi2D:
         check(self.lib.charming_jacobi2d_store(self.h, prob, out.ctypes.data), "charming_jacobi2d_store")
         return out
 
+    def solve_stream(self, prob: int, inputs, outputs) -> float:
+        """Solves problem prob once per input grid, results into the matching
+        output arrays, with the host copies of neighbouring solves
+        overlapping each solve (pinned arrays overlap best); returns the ms
+        from the first input copy to the last result copy."""
+        p = self.problems[prob]
+        ins = [np.ascontiguousarray(g, dtype=self.dtype) for g in inputs]
+        for g, o in zip(ins, outputs):
+            assert g.shape == o.shape == (p.ny + 2, p.nx + 2) and o.dtype == self.dtype and o.flags.c_contiguous
+        n = len(ins)
+        pin = (C.c_void_p * n)(*[g.ctypes.data for g in ins])
+        pout = (C.c_void_p * n)(*[o.ctypes.data for o in outputs])
+        ms = C.c_double(0.0)
+        check(self.lib.charming_jacobi2d_solve_stream(self.h, prob, n, pin, pout, C.byref(ms)),
+              "charming_jacobi2d_solve_stream")
+        return ms.value
+
     def result(self, prob: int) -> Result:
         r = _lib.JacobiResult()
         check(self.lib.charming_jacobi2d_result(self.h, prob, C.byref(r)), "charming_jacobi2d_result")

@@ -205,6 +205,15 @@ int charming_jacobi2d_run(void* handle);
 /* Chare blocks -> host grid (same layout as load). */
 int charming_jacobi2d_store(void* handle, int prob, void* host_grid);
 int charming_jacobi2d_result(void* handle, int prob, charming_jacobi_result* out);
+/* n solves of problem prob: host_in[k] (as load takes it) -> host_out[k] (as
+ * store gives it), each exactly load + run + store, pipelined: the copies of
+ * solve k+1's input and of solve k-1's result run on their own streams while
+ * solve k runs (two device staging buffers each way). Host buffers should be
+ * pinned for the copies to overlap. *out_ms: time from the first input copy
+ * to the last result copy. Replaces a host loop over the reference's
+ * process main (src/charming.cu:50-263) with the grid moved in and out. */
+int charming_jacobi2d_solve_stream(void* handle, int prob, int n, const void* const* host_in,
+    void* const* host_out, double* out_ms);
 int charming_jacobi2d_get_info(void* handle, charming_jacobi_info* out);
 int charming_jacobi2d_destroy(void* handle);
 

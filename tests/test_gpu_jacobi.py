@@ -255,3 +255,18 @@ def test_headline_configuration_bit_exact(rt):
         assert j.result(0).sweeps == 100
     ref = oj.jacobi2d(initial_grid(8192, 8192, p.bc), 100, threads=os.cpu_count() or 1)
     assert np.array_equal(bits(out), bits(ref))
+
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_solve_stream_matches_load_run_store(rt, use_graph):
+    """Pipelined solves (input copy of the next and result copy of the
+    previous solve overlapping each solve) give each grid's own result."""
+    p = Problem(300, 220, 23, px=3, py=2)
+    grids = [seeded_grid(300, 220, s) for s in (1, 2, 3, 4, 5)]
+    outs = [np.empty_like(g) for g in grids]
+    with Jacobi2D([p], use_graph=use_graph) as j:
+        ms = j.solve_stream(0, grids, outs)
+        assert ms > 0
+        for g, o in zip(grids, outs):
+            assert np.array_equal(bits(o), bits(jac64(g, 23)))
