@@ -40,7 +40,7 @@ class Config(C.Structure):
         ("ring_bytes", u64), ("max_msg_bytes", u64), ("stash_bytes", u64),
         ("stash_entries", i32), ("heap_bytes", u64), ("stack_bytes", u64),
         ("deadline_s", f64), ("idle_timeout_s", f64), ("free_chares_at_exit", i32),
-        ("verbose", i32),
+        ("verbose", i32), ("gpu_level", i32),
     ]
 
 
@@ -49,7 +49,7 @@ class Info(C.Structure):
         ("n_pes", i32), ("n_sms", i32), ("threads_per_pe", i32), ("smem_bytes_per_pe", i32),
         ("smem_scratch_bytes", i32), ("regs_per_thread", i32), ("ring_bytes", u64),
         ("max_msg_bytes", u64), ("device_bytes", u64), ("stack_bytes", u64),
-        ("local_bytes", u64),
+        ("local_bytes", u64), ("n_blocks", i32), ("gpu_level", i32),
     ]
 
 

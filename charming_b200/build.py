@@ -16,6 +16,7 @@ REFERENCE = os.environ.get("CHARMING_REFERENCE",
                            os.path.join(os.path.dirname(ROOT), "reference"))
 ARCH = "-gencode arch=compute_100a,code=sm_100a"
 REF_EXAMPLES = ("hello", "refnum", "pingpong")
+REF_EXAMPLES_GPU_LEVEL = ("pingpong",)
 
 
 def _run(cmd: str, cwd: str) -> None:
@@ -44,13 +45,17 @@ def build_reference_artifacts() -> bool:
     os.makedirs(out, exist_ok=True)
     lib = os.path.join(ROOT, "charming_b200", "lib", "libcharming.a")
     inc = os.path.join(ROOT, "include")
-    for ex in REF_EXAMPLES:
+    # SM-level builds of every example, and GPU-level builds (the examples'
+    # #ifndef SM_LEVEL branch, the reference's default) of those that have one
+    builds = [(ex, ex, "") for ex in REF_EXAMPLES]
+    builds += [(ex, f"{ex}_gpu_level", "-DCHARMING_GPU_LEVEL") for ex in REF_EXAMPLES_GPU_LEVEL]
+    for ex, name, flags in builds:
         src = os.path.join(REFERENCE, "examples", ex, f"{ex}.cu")
-        obj = os.path.join(out, f"{ex}.o")
-        _run(f"nvcc -std=c++17 -O2 {ARCH} -rdc=true -I{inc} -I{os.path.dirname(src)} "
+        obj = os.path.join(out, f"{name}.o")
+        _run(f"nvcc -std=c++17 -O2 {ARCH} -rdc=true {flags} -I{inc} -I{os.path.dirname(src)} "
              f"-c {src} -o {obj}", ROOT)
         _run(f"nvcc {ARCH} -rdc=true -Xnvlink -suppress-stack-size-warning "
-             f"-o {os.path.join(out, ex)} {obj} {lib} -lcudart", ROOT)
+             f"-o {os.path.join(out, name)} {obj} {lib} -lcudart", ROOT)
     _run(f"make REF={REFERENCE}", os.path.join(ROOT, "oracle", "ref"))
     return True
 

@@ -77,11 +77,19 @@ struct d1 {
 };
 
 struct D1Chare : charm::chare {
-  int k;    // iterations done
-  int got;  // halos of the next iteration received (message mode)
-  __device__ D1Chare() : k(0), got(0) {}
+  int k;     // iterations done
+  int got;   // halos of the next iteration received (message mode)
+  int next;  // the halo just received completed the iteration (message mode)
+  int ok;    // mode 0: both neighbours' signals arrived
+  __device__ D1Chare() : k(0), got(0), next(0), ok(0) {}
 };
-__shared__ charm::chare_proxy<D1Chare>* d1_proxy;
+// SM-level mode: each PE block creates its own proxy; GPU-level mode: one
+// proxy for the single PE, seen by every block.
+__shared__ charm::chare_proxy<D1Chare>* d1_proxy_block;
+__device__ charm::chare_proxy<D1Chare>* d1_proxy_gpu;
+__device__ __forceinline__ charm::chare_proxy<D1Chare>* d1_proxy() {
+  return charm::is_gpu_level() ? d1_proxy_gpu : d1_proxy_block;
+}
 
 struct d1_halo {  // message payload header; nx-2 floats follow
   int to_top_ghost;  // 1: the receiver's row 0, 0: its bottom ghost row
@@ -93,30 +101,39 @@ __device__ __forceinline__ float d1_stencil(float r, float l, float d, float u) 
   return __fmul_rn(__fadd_rn(__fadd_rn(__fadd_rn(r, l), d), u), 0.25f);
 }
 
-// All threads: rows [1, iy_end) of o from a (row pitch nx, nx % 4 == 0):
-// each warp walks column strips of 32 float4 down the rows, the three rows
-// around the output in registers, neighbours across lanes by shuffle.
+// The PE's threads (all of them, pe_thread() / pe_threads()): rows
+// [1, iy_end) of o from a (row pitch nx, nx % 4 == 0). Work items are
+// (column strip of 32 float4, run of rows); each warp walks its items'
+// rows downwards, the three rows around the output in registers,
+// neighbours across lanes by shuffle. Row runs split the strips when there
+// are more warps than strips (a GPU-level PE has thousands).
 __device__ void d1_sweep(const float* __restrict__ a, float* __restrict__ o, int nx, int iy_end) {
   constexpr unsigned FULL = 0xffffffffu;
+  const int tid = charm::pe_thread(), nthreads = charm::pe_threads();
+  if (iy_end < 2) return;
   if (blockDim.x < 32) {  // blocks under a warp (host checks): element by element
-    for (long long x = threadIdx.x; x < (long long)(iy_end - 1) * (nx - 2); x += blockDim.x) {
+    for (long long x = tid; x < (long long)(iy_end - 1) * (nx - 2); x += nthreads) {
       const int iy = 1 + (int)(x / (nx - 2)), ix = 1 + (int)(x % (nx - 2));
       const float* m = a + (size_t)iy * nx + ix;
       o[(size_t)iy * nx + ix] = d1_stencil(m[1], m[-1], m[nx], m[-nx]);
     }
     return;
   }
-  const int nv = nx / 4, warp = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31);
-  const int nw = (int)(blockDim.x >> 5);
-  if (warp >= nw || iy_end < 2) return;
-  const int strips = (nv + 31) / 32;
-  for (int s = warp; s < strips; s += nw) {
+  const int nv = nx / 4, warp = tid >> 5, lane = tid & 31, nw = nthreads >> 5;
+  const int strips = (nv + 31) / 32, rows = iy_end - 1;
+  int runs = nw / strips;
+  if (runs > rows / 8) runs = rows / 8;  // at least 8 rows per run
+  if (runs < 1) runs = 1;
+  const int run_rows = (rows + runs - 1) / runs;
+  for (int item = warp; item < strips * runs; item += nw) {
+    const int s = item % strips, r0 = 1 + (item / strips) * run_rows;
+    const int r1 = min(iy_end, r0 + run_rows);
     const int v = s * 32 + lane;
     const bool act = v < nv;
     const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
     auto ld = [&](int iy) { return act ? *reinterpret_cast<const float4*>(a + (size_t)iy * nx + 4 * v) : z; };
-    float4 U = ld(0), M = ld(1);
-    for (int iy = 1; iy < iy_end; iy++) {
+    float4 U = ld(r0 - 1), M = ld(r0);
+    for (int iy = r0; iy < r1; iy++) {
       const float4 D = ld(iy + 1);
       float left = __shfl_up_sync(FULL, M.w, 1);
       float right = __shfl_down_sync(FULL, M.x, 1);
@@ -145,10 +162,10 @@ __device__ void d1_sweep(const float* __restrict__ a, float* __restrict__ o, int
 }
 
 __device__ void d1_count_done() {
-  if (threadIdx.x == 0) {
+  if (charm::pe_thread() == 0) {
     if (atomicAdd(d1::done(), 1ULL) + 1 == (unsigned long long)d1::n()) charm::end();
   }
-  __syncthreads();
+  charm::pe_sync();
 }
 
 __device__ void d1_iterate(D1Chare& c);
@@ -159,12 +176,13 @@ __device__ void d1_put_and_signal(D1Chare& c) {
   const d1_desc& d = d1::desc(c.i);
   const int nx = d1::nx(), nb = (c.k + 1) & 1;
   const float* o = d1::buf(c.i, nb);
+  const size_t tid = (size_t)charm::pe_thread(), nt = (size_t)charm::pe_threads();
   charm::copy_cooperative(d1::buf(d.top, nb) + (size_t)d.top_ghost * nx + 1, o + nx + 1,
-                          sizeof(float) * (nx - 2), threadIdx.x, blockDim.x);
+                          sizeof(float) * (nx - 2), tid, nt);
   charm::copy_cooperative(d1::buf(d.bottom, nb) + 1, o + (size_t)(d.iy_end - 1) * nx + 1,
-                          sizeof(float) * (nx - 2), threadIdx.x, blockDim.x);
-  __syncthreads();  // the rows are written before the signals (release is cumulative)
-  if (threadIdx.x == 0) {
+                          sizeof(float) * (nx - 2), tid, nt);
+  charm::pe_sync();  // the rows are written before the signals (release is cumulative)
+  if (tid == 0) {
     st_release_u64(&d1::sig(d.top)[1], (unsigned long long)c.k + 1);
     st_release_u64(&d1::sig(d.bottom)[0], (unsigned long long)c.k + 1);
   }
@@ -177,19 +195,20 @@ __device__ void d1_send_halos(D1Chare& c) {
   const int nx = d1::nx(), nb = (c.k + 1) & 1;
   const float* o = d1::buf(c.i, nb);
   const size_t bytes = sizeof(d1_halo) + sizeof(float) * (nx - 2);
+  const int tid = charm::pe_thread();
   for (int side = 0; side < 2; side++) {
     const int to = side == 0 ? d.top : d.bottom;
     charm::message msg;
-    if (!d1_proxy->alloc_msg(msg, to, bytes)) return;
+    if (!d1_proxy()->alloc_msg(msg, to, bytes)) return;
     d1_halo* h = reinterpret_cast<d1_halo*>(msg.payload());
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
       h->to_top_ghost = side == 1;  // my last row is the bottom neighbour's row 0
       h->iter = c.k + 1;
     }
     const float* row = side == 0 ? o + nx + 1 : o + (size_t)(d.iy_end - 1) * nx + 1;
     charm::copy_cooperative(reinterpret_cast<char*>(h) + sizeof(d1_halo), row, sizeof(float) * (nx - 2),
-                            threadIdx.x, blockDim.x);
-    d1_proxy->invoke(to, EP_D_HALO, msg, bytes, c.k + 1);
+                            (size_t)tid, (size_t)charm::pe_threads());
+    d1_proxy()->invoke(to, EP_D_HALO, msg, bytes, c.k + 1);
   }
 }
 
@@ -197,29 +216,29 @@ __device__ void d1_send_halos(D1Chare& c) {
 __device__ void d1_iterate(D1Chare& c) {
   const d1_desc& d = d1::desc(c.i);
   const int mode = d1::mode(), nx = d1::nx();
+  const int tid = charm::pe_thread();
   while (true) {
     if (c.k >= d1::iters()) {
       d1_count_done();
       return;
     }
-    if (mode == D_MSG && threadIdx.x == 0) d1_proxy->set_refnum(c.i, c.k + 1);
+    if (mode == D_MSG && tid == 0) d1_proxy()->set_refnum(c.i, c.k + 1);
     d1_sweep(d1::buf(c.i, c.k & 1), d1::buf(c.i, (c.k + 1) & 1), nx, d.iy_end);
-    __syncthreads();
+    charm::pe_sync();
     if (mode == D_MSG) {
       d1_send_halos(c);
       return;  // the halos' entry method continues
     }
     d1_put_and_signal(c);
     if (mode == D_ASYNC) {
-      if (threadIdx.x == 0)
-        d1_proxy->async_wait(reinterpret_cast<uint64_t*>(d1::sig(c.i)), 2, charm::CMP_GE,
-                             (unsigned long long)c.k + 1, c.i, EP_D_RESUME);
-      __syncthreads();
+      if (tid == 0)
+        d1_proxy()->async_wait(reinterpret_cast<uint64_t*>(d1::sig(c.i)), 2, charm::CMP_GE,
+                               (unsigned long long)c.k + 1, c.i, EP_D_RESUME);
+      charm::pe_sync();
       return;
     }
     // mode 0: wait here for both neighbours (bounded by the run deadline)
-    __shared__ int s_ok;
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
       const unsigned long long want = (unsigned long long)c.k + 1;
       unsigned long long* w = d1::sig(c.i);
       unsigned spins = 0;
@@ -231,19 +250,19 @@ __device__ void d1_iterate(D1Chare& c) {
           break;
         }
       }
-      s_ok = ok;
+      c.ok = ok;
       if (ok) c.k++;
     }
-    __syncthreads();
-    if (!s_ok) return;
+    charm::pe_sync();
+    if (!c.ok) return;
   }
 }
 
 __device__ void em_iter(D1Chare& c, void* arg) { d1_iterate(c); }
 
 __device__ void em_resume(D1Chare& c, void* arg) {
-  if (threadIdx.x == 0) c.k++;
-  __syncthreads();
+  if (charm::pe_thread() == 0) c.k++;
+  charm::pe_sync();
   d1_iterate(c);
 }
 
@@ -253,33 +272,34 @@ __device__ void em_halo(D1Chare& c, void* arg) {
   const int nx = d1::nx(), nb = h->iter & 1;
   float* dst = d1::buf(c.i, nb) + (h->to_top_ghost ? 0 : (size_t)(d.chunk + 1) * nx) + 1;
   charm::copy_cooperative(dst, reinterpret_cast<const char*>(arg) + sizeof(d1_halo), sizeof(float) * (nx - 2),
-                          threadIdx.x, blockDim.x);
-  __shared__ int s_next;
-  if (threadIdx.x == 0) {
-    s_next = ++c.got == 2;
-    if (s_next) {
+                          (size_t)charm::pe_thread(), (size_t)charm::pe_threads());
+  if (charm::pe_thread() == 0) {
+    c.next = ++c.got == 2;
+    if (c.next) {
       c.got = 0;
       c.k++;
     }
   }
-  __syncthreads();
-  if (s_next) d1_iterate(c);
+  charm::pe_sync();
+  if (c.next) d1_iterate(c);
 }
 
 }  // namespace
 
 __device__ void suite::decomp1d_main(int pe) {
-  if (threadIdx.x == 0) {
-    d1_proxy = new charm::chare_proxy<D1Chare>();
-    d1_proxy->add_entry_method<&em_iter>();
-    d1_proxy->add_entry_method<&em_resume>();
-    d1_proxy->add_entry_method<&em_halo>();
-    d1_proxy->create(d1::n());
+  if (charm::pe_thread() == 0) {
+    charm::chare_proxy<D1Chare>* p = new charm::chare_proxy<D1Chare>();
+    p->add_entry_method<&em_iter>();
+    p->add_entry_method<&em_resume>();
+    p->add_entry_method<&em_halo>();
+    p->create(d1::n());
+    if (charm::is_gpu_level()) d1_proxy_gpu = p;
+    else d1_proxy_block = p;
   }
-  __syncthreads();
+  charm::pe_sync();
   charm::barrier();
-  for (int i = d1_proxy->start_idx; i <= d1_proxy->end_idx && d1_proxy->n_local > 0; i++)
-    d1_proxy->invoke(i, EP_D_ITER);
+  charm::chare_proxy<D1Chare>* p = d1_proxy();
+  for (int i = p->start_idx; i <= p->end_idx && p->n_local > 0; i++) p->invoke(i, EP_D_ITER);
 }
 
 #ifndef CHARMING_HOST_EMULATION

@@ -12,6 +12,12 @@ __shared__ double s_red_f64[32];
 }
 
 __device__ void charm::main(int argc, char** argv, size_t* argvs, int pe) {
+  // In GPU-level mode every block runs each entry method: only programs
+  // written against pe_thread()/pe_threads()/pe_sync() can run there.
+  if (charm::is_gpu_level() && g_app.id != suite::APP_DECOMP1D && g_app.id != suite::APP_NONE) {
+    if (charm::pe_thread() == 0) charm::rt::set_error(CHARMING_ERR_CONFIG, g_app.id, 1);
+    return;
+  }
   switch (g_app.id) {
     case suite::APP_HELLO: suite::hello_main(pe); break;
     case suite::APP_REFNUM: suite::refnum_main(pe); break;
@@ -24,7 +30,7 @@ __device__ void charm::main(int argc, char** argv, size_t* argvs, int pe) {
     case suite::APP_USER_HEAP: suite::user_heap_main(pe); break;
     case suite::APP_DECOMP1D: suite::decomp1d_main(pe); break;
     default:
-      if (threadIdx.x == 0 && pe == 0) charm::end();
+      if (charm::pe_thread() == 0 && pe == 0) charm::end();
       break;
   }
 }

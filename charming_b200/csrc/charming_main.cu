@@ -2,7 +2,7 @@
 // optionally charm::main_host) link against the library and get this entry
 // point, as with the reference (src/charming.cu:50-263).
 //
-// Environment overrides: CHARMING_PES_PER_SM, CHARMING_RING_BYTES,
+// Environment overrides: CHARMING_GPU_LEVEL (1: GPU-level mode), CHARMING_PES_PER_SM, CHARMING_RING_BYTES,
 // CHARMING_DEADLINE_S, CHARMING_IDLE_TIMEOUT_S, CHARMING_HEAP_BYTES,
 // CHARMING_QUIET (suppress the [INFO] lines).
 #include <cstdio>
@@ -12,6 +12,11 @@
 namespace charm {
 // Weak: programs without a host main still link (the reference requires one).
 __attribute__((weak)) void main_host(int argc, char** argv);
+}
+
+// Defined (weak) by programs compiled with -DCHARMING_GPU_LEVEL (common.h).
+extern "C" {
+extern const int charming_program_gpu_level __attribute__((weak));
 }
 
 static unsigned long long env_u64(const char* name, unsigned long long dflt) {
@@ -27,6 +32,8 @@ int main(int argc, char** argv) {
   cfg.pes_per_sm = (int)env_u64("CHARMING_PES_PER_SM", (unsigned long long)cfg.pes_per_sm);
   cfg.ring_bytes = env_u64("CHARMING_RING_BYTES", cfg.ring_bytes);
   cfg.heap_bytes = env_u64("CHARMING_HEAP_BYTES", cfg.heap_bytes);
+  cfg.gpu_level = &charming_program_gpu_level != nullptr ? charming_program_gpu_level : 0;
+  cfg.gpu_level = (int)env_u64("CHARMING_GPU_LEVEL", (unsigned long long)cfg.gpu_level);
   bool quiet = getenv("CHARMING_QUIET") != nullptr;
   cfg.verbose = quiet ? 0 : 1;
 

@@ -105,7 +105,7 @@ int enqueue_scheduler(cudaStream_t s) {
   size_t* argvs = nullptr;
   void* args[] = {&argc, &argv, &argvs};
   cudaLaunchConfig_t lc{};
-  lc.gridDim = dim3(g.inf.n_pes);
+  lc.gridDim = dim3(g.inf.n_blocks);
   lc.blockDim = dim3(g.inf.threads_per_pe);
   lc.dynamicSmemBytes = g.inf.smem_bytes_per_pe;
   lc.stream = s;
@@ -214,7 +214,7 @@ int run_scheduler(int argc, char** argv) {
   size_t* d_argvs = reinterpret_cast<size_t*>(g.d_args + (size_t)argc * sizeof(char*));
   void* args[] = {&argc, &d_argv, &d_argvs};
   cudaEventRecord(g.ev0, g.stream);
-  e = cudaLaunchCooperativeKernel((const void*)charming_scheduler_kernel, dim3(g.inf.n_pes),
+  e = cudaLaunchCooperativeKernel((const void*)charming_scheduler_kernel, dim3(g.inf.n_blocks),
       dim3(g.inf.threads_per_pe), args, (size_t)g.inf.smem_bytes_per_pe, g.stream);
   if (e != cudaSuccess) return cuda_fail(e, "scheduler launch");
   cudaEventRecord(g.ev1, g.stream);
@@ -271,7 +271,10 @@ int charming_init(const charming_config* cfg_in) {
     return CHARMING_ERR_CONFIG;
   }
   int n_sms = g.prop.multiProcessorCount;
-  int n_pes = cfg.n_pes > 0 ? cfg.n_pes : n_sms * cfg.pes_per_sm;
+  // GPU-level mode: the blocks (n_pes of them, by default one per SM slot)
+  // form one PE
+  const int n_blocks = cfg.n_pes > 0 ? cfg.n_pes : n_sms * cfg.pes_per_sm;
+  int n_pes = cfg.gpu_level ? 1 : n_blocks;
 
   // Device limits (reference: src/charming.cu:197-203).
   // The heap size is fixed once a kernel of the context has run (a second
@@ -333,16 +336,18 @@ int charming_init(const charming_config* cfg_in) {
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_blocks,
       (const void*)charming_scheduler_kernel, cfg.threads_per_pe, (size_t)smem_total);
   if (e != cudaSuccess) return cuda_fail(e, "occupancy");
-  if ((long)per_sm_blocks * n_sms < n_pes) {
+  if ((long)per_sm_blocks * n_sms < n_blocks) {
     char buf[256];
-    snprintf(buf, sizeof(buf), "%d PEs cannot be co-resident (%d blocks/SM x %d SMs)",
-        n_pes, per_sm_blocks, n_sms);
+    snprintf(buf, sizeof(buf), "%d PE blocks cannot be co-resident (%d blocks/SM x %d SMs)",
+        n_blocks, per_sm_blocks, n_sms);
     set_error_text(buf);
     return CHARMING_ERR_CONFIG;
   }
 
   g.cfg = cfg;
   g.inf.n_pes = n_pes;
+  g.inf.n_blocks = n_blocks;
+  g.inf.gpu_level = cfg.gpu_level ? 1 : 0;
   g.inf.n_sms = n_sms;
   g.inf.threads_per_pe = cfg.threads_per_pe;
   g.inf.smem_bytes_per_pe = (int)smem_total;
@@ -368,6 +373,8 @@ int charming_init(const charming_config* cfg_in) {
   ds.deadline_ns = (unsigned long long)(cfg.deadline_s * 1e9);
   ds.idle_timeout_ns = (unsigned long long)(cfg.idle_timeout_s * 1e9);
   ds.free_chares_at_exit = cfg.free_chares_at_exit;
+  ds.gpu_level = cfg.gpu_level ? 1 : 0;
+  ds.n_blocks = n_blocks;
 
   int rc;
   if ((rc = dev_alloc(&ds.tail, sizeof(line_u64) * n_pes, "inbox tails"))) return rc;
@@ -381,6 +388,7 @@ int charming_init(const charming_config* cfg_in) {
   if ((rc = dev_alloc(&ds.progress, 8ull * n_pes, "progress"))) return rc;
   if ((rc = dev_alloc(&ds.pe_stats, 8ull * N_STATS * n_pes, "stats"))) return rc;
   if ((rc = dev_alloc(&ds.pe_times, 24ull * n_pes, "times"))) return rc;
+  if (ds.gpu_level && (rc = dev_alloc(&ds.gl, sizeof(group_state), "group state"))) return rc;
   // per-PE arena for proxy tables and chare objects (reset every run; the
   // device heap takes over when a PE needs more)
   ds.arena_bytes = 256ull << 10;
@@ -435,8 +443,12 @@ int charming_init(const charming_config* cfg_in) {
   g.inited = true;
   if (cfg.verbose) {
     PINFO("Initiating CharminG (B200 runtime)\n");
-    PINFO("PEs: %d (%d per SM), SMs: %d, threads per PE: %d, regs/thread: %d\n", n_pes,
-        cfg.pes_per_sm, n_sms, cfg.threads_per_pe, fa.numRegs);
+    if (ds.gpu_level)
+      PINFO("GPU-level mode: 1 PE of %d blocks x %d threads, SMs: %d, regs/thread: %d\n", n_blocks,
+          cfg.threads_per_pe, n_sms, fa.numRegs);
+    else
+      PINFO("PEs: %d (%d per SM), SMs: %d, threads per PE: %d, regs/thread: %d\n", n_pes,
+          cfg.pes_per_sm, n_sms, cfg.threads_per_pe, fa.numRegs);
     PINFO("Dynamic smem per PE: %ld B (scratch %d B), ring %llu B per PE\n", smem_total,
         g.inf.smem_scratch_bytes, (unsigned long long)cfg.ring_bytes);
   }

@@ -129,6 +129,30 @@ struct device_state {
   unsigned long long user_heap_bytes;
   user_block* user_blocks;             // [n_pes][user_blocks_max]
   int user_blocks_max;
+  int gpu_level;                       // 1: all blocks form PE 0 (group_state below)
+  int n_blocks;                        // thread blocks of the launch (n_pes when 0)
+  struct group_state* gl;              // GPU-level mode only
+};
+
+// GPU-level mode (the reference's default build, src/sched/scheduler.cu:
+// 240-333): every thread block of the launch belongs to PE 0. Block 0 runs
+// the scheduler; all blocks run each entry method and each collective send
+// (the reference's barrier_local() = grid sync between the steps). Thread 0
+// of block 0 writes these records before a grid barrier; the other blocks
+// read them after it with L1-bypassing loads. Collective calls alternate
+// between the two slots, so a slot is rewritten only after every block has
+// passed the next call's first barrier.
+struct group_slot {
+  void* ptr[MSG_BATCH_MAX];                // message starts
+  unsigned long long u0[MSG_BATCH_MAX];    // bytes
+  unsigned long long u1[MSG_BATCH_MAX];    // tickets
+  int i0, i1;
+};
+struct group_state {
+  int act, idx, ep, pad;                   // the scheduler's decision
+  void* p;                                 // proxy
+  void* arg;                               // entry-method argument
+  group_slot slot[2];
 };
 
 // Words of device_state::ctrl (each on its own 128-B line).
@@ -193,6 +217,8 @@ struct pe_state {
   unsigned long long uh_head, uh_tail;
   unsigned long long ub_head, ub_tail;
   int aw_count;                        // pending async_waits on this PE
+  unsigned int gl_seq;                 // GPU-level mode: collective calls of this block
+  int bar_ok;                          // the last grid barrier completed
   unsigned long long stamped_delivered;  // deliveries at the last progress stamp
   unsigned long long slow_check_ns;    // last host-stop / idle-timeout check
   unsigned long long idle_checks;
@@ -308,6 +334,15 @@ __device__ __forceinline__ bool past_deadline() {
 }
 
 __device__ void grid_barrier();
+// The same; false (on every thread of the block) when it was left early
+// because the run is ending.
+__device__ bool grid_barrier_ok();
+
+__device__ __forceinline__ bool gpu_level() { return c_rt.gpu_level != 0; }
+// Loads of the group_state records written by another SM.
+__device__ __forceinline__ void* gl_ld_ptr(void* const* p) {
+  return reinterpret_cast<void*>(ld_relaxed_u64(reinterpret_cast<const unsigned long long*>(p)));
+}
 
 // Invariant checks of the checked build (-DCHARMING_CHECKS): a failed check
 // records CHARMING_ERR_APP (or the given code) with two values, and the

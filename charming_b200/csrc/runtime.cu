@@ -76,7 +76,9 @@ __device__ __forceinline__ unsigned char* smem_arena() {
 
 __device__ void* charm::detail::pe_alloc(size_t bytes) {
   pe_state* ps = pes();
-  if (bytes <= (size_t)SMEM_OBJ_MAX && c_rt.smem_arena_bytes > 0) {
+  // GPU-level mode: every block of the PE reads the objects, so none lives
+  // in one block's shared memory
+  if (bytes <= (size_t)SMEM_OBJ_MAX && c_rt.smem_arena_bytes > 0 && !gpu_level()) {
     unsigned long long at = (ps->sarena_top + 15) & ~15ULL;
     if (at + bytes <= (unsigned long long)c_rt.smem_arena_bytes) {
       ps->sarena_top = at + bytes;
@@ -87,7 +89,7 @@ __device__ void* charm::detail::pe_alloc(size_t bytes) {
   unsigned long long at = (ps->arena_top + 15) & ~15ULL;
   if (at + bytes > c_rt.arena_bytes) return nullptr;
   ps->arena_top = at + bytes;
-  return c_rt.arena + (unsigned long long)blockIdx.x * c_rt.arena_bytes + at;
+  return c_rt.arena + (unsigned long long)charm::my_pe() * c_rt.arena_bytes + at;
 }
 
 __device__ bool charm::detail::pe_owns(const void* p) {
@@ -101,7 +103,7 @@ __device__ void charm::detail::cache_proxy(int id, chare_proxy_base* p) {
 }
 
 __device__ chare_proxy_table& charm::detail::my_proxy_table() {
-  return c_rt.proxy_tables[blockIdx.x];
+  return c_rt.proxy_tables[charm::my_pe()];
 }
 
 __device__ void charm::end() {
@@ -116,9 +118,9 @@ __device__ void charm::abort() {
   __syncthreads();
 }
 
-__device__ int charm::my_pe() { return (int)blockIdx.x; }
+__device__ int charm::my_pe() { return gpu_level() ? 0 : (int)blockIdx.x; }
 __device__ int charm::n_pes() { return c_n_pes; }
-__device__ int charm::my_pe_node() { return (int)blockIdx.x; }
+__device__ int charm::my_pe_node() { return charm::my_pe(); }
 __device__ int charm::n_pes_node() { return c_n_pes_node; }
 __device__ int charm::n_nodes() { return c_n_nodes; }
 
@@ -136,6 +138,16 @@ __device__ void* charm::smem_scratch(size_t* bytes) {
 
 __device__ uint64_t charm::now_ns() { return globaltimer(); }
 
+__device__ int charm::pe_thread() {
+  return gpu_level() ? (int)(blockIdx.x * blockDim.x + threadIdx.x) : (int)threadIdx.x;
+}
+__device__ int charm::pe_threads() { return gpu_level() ? (int)(gridDim.x * blockDim.x) : (int)blockDim.x; }
+__device__ void charm::pe_sync() {
+  if (gpu_level()) grid_barrier();
+  else __syncthreads();
+}
+__device__ bool charm::is_gpu_level() { return gpu_level(); }
+
 __device__ unsigned int charm::smid() {
 #ifndef CHARMING_HOST_EMULATION
   unsigned int r;
@@ -150,7 +162,8 @@ __device__ unsigned int charm::smid() {
 // Grid barrier (sense by generation counter), bounded by the deadline.
 // All PE blocks are co-resident: the host launches cooperatively.
 // ---------------------------------------------------------------------------
-__device__ void charm::rt::grid_barrier() {
+__device__ bool charm::rt::grid_barrier_ok() {
+  pe_state* ps = pes();
   __syncthreads();
   if (threadIdx.x == 0) {
     unsigned int* count = reinterpret_cast<unsigned int*>(ctrl(CTRL_BAR_COUNT));
@@ -158,7 +171,8 @@ __device__ void charm::rt::grid_barrier() {
     unsigned int g = ld_acquire_u32(gen);
     __threadfence();
     unsigned int arrived = atomicAdd(count, 1u);
-    if (arrived == (unsigned int)c_rt.n_pes - 1) {
+    int ok = 1;
+    if (arrived == (unsigned int)c_rt.n_blocks - 1) {
       atomicExch(count, 0u);
       __threadfence();
       st_release_u32(gen, g + 1);
@@ -167,17 +181,25 @@ __device__ void charm::rt::grid_barrier() {
       unsigned int spins = 0;
       while (ld_acquire_u32(gen) == g) {
         if ((++spins & 1023) == 0) {
-          if (terminated()) break;
+          if (terminated()) {
+            ok = 0;
+            break;
+          }
           if (past_deadline()) {
             set_error(CHARMING_ERR_BARRIER_TIMEOUT, (int)arrived, 0);
+            ok = 0;
             break;
           }
         }
       }
     }
+    ps->bar_ok = ok;
   }
   __syncthreads();
+  return ps->bar_ok != 0;
 }
+
+__device__ void charm::rt::grid_barrier() { (void)grid_barrier_ok(); }
 
 __device__ void charm::barrier() { grid_barrier(); }
 __device__ void charm::barrier_local() { grid_barrier(); }
@@ -359,8 +381,135 @@ __device__ __forceinline__ void stamp_progress(int me) {
 
 } // namespace
 
+// ---------------------------------------------------------------------------
+// GPU-level mode: collective sends over all blocks of PE 0 (the reference's
+// GPU-level send_reg_msg / send_remote_msg, src/comm/get/get.cu:1224-1273:
+// GID 0 takes the space, barrier_local(), the grid copies the payload,
+// barrier_local(), GID 0 publishes). Every block calls them in the same
+// order with the same arguments.
+// ---------------------------------------------------------------------------
+namespace {
+
+__device__ __forceinline__ bool gl_lead() { return blockIdx.x == 0 && threadIdx.x == 0; }
+
+// This call's broadcast slot; the block's call count moves on before the
+// call's first grid barrier (which begins with a block barrier).
+__device__ __forceinline__ group_slot* gl_next_slot() {
+  pe_state* ps = pes();
+  const unsigned s = ps->gl_seq;
+  __syncthreads();
+  if (threadIdx.x == 0) ps->gl_seq = s + 1;
+  return &c_rt.gl->slot[s & 1];
+}
+
+__device__ void group_send_reg_msg(int chare_id, int chare_idx, int ep_id, void* buf, size_t payload_size,
+    int dst_pe, int refnum) {
+  pe_state* ps = pes();
+  group_slot* g = gl_next_slot();
+  if (gl_lead()) {
+    // taking the space does not read the payload: it overlaps the other
+    // blocks' last writes to it
+    unsigned long long bytes = envelope::alloc_size(msgtype::regular, payload_size);
+    unsigned long long t = 0;
+    unsigned char* m = reserve(dst_pe, bytes, &t);
+    if (m) {
+      envelope* env = reinterpret_cast<envelope*>(m);
+      env->type = msgtype::regular;
+      env->src_pe = 0;
+      env->size = bytes;
+      regular_msg* rm = reinterpret_cast<regular_msg*>(m + sizeof(envelope));
+      rm->chare_id = chare_id;
+      rm->chare_idx = chare_idx;
+      rm->ep_id = ep_id;
+      rm->refnum = refnum;
+      ps->stats[ST_SENT]++;
+      ps->stats[ST_BYTES_SENT] += payload_size;
+    }
+    g->ptr[0] = m;
+    g->u0[0] = (m && buf) ? payload_size : 0;
+    g->u1[0] = t;
+    g->i0 = (buf != nullptr && __isLocal(buf)) ? 1 : 0;
+    g->i1 = dst_pe;
+  }
+  grid_barrier();  // every block's payload writes are done; the space is known
+  unsigned char* m = reinterpret_cast<unsigned char*>(gl_ld_ptr(&g->ptr[0]));
+  if (m == nullptr) return;
+  const size_t n = ld_relaxed_u64(&g->u0[0]);
+  const unsigned long long t = ld_relaxed_u64(&g->u1[0]);
+  const int dst = ld_relaxed_s32(&g->i1);
+  if (n > 0) {
+    if (ld_relaxed_s32(&g->i0)) {
+      // a thread-local buffer is only addressable by the thread that owns it
+      if (gl_lead()) copy_cooperative(m + HDR, buf, n, 0, 1);
+    } else {
+      copy_cooperative(m + HDR, buf, n, (size_t)charm::pe_thread(), (size_t)charm::pe_threads());
+    }
+  }
+  grid_barrier();  // the payload is complete
+  if (gl_lead()) publish_msg(dst, t, m);
+}
+
+__device__ bool group_alloc_user_msgs(message* msgs, const int* dst_pes, const size_t* payload_sizes, int n) {
+  group_slot* g = gl_next_slot();
+  if (gl_lead()) {
+    for (int k = 0; k < n; k++) {
+      const unsigned long long bytes = envelope::alloc_size(msgtype::user, payload_sizes[k]);
+      unsigned long long t = 0;
+      g->ptr[k] = reserve(dst_pes[k], bytes, &t);
+      g->u0[k] = bytes;
+      g->u1[k] = t;
+    }
+  }
+  grid_barrier();
+  bool ok = true;
+  for (int k = 0; k < n; k++) {
+    msgs[k].env = reinterpret_cast<envelope*>(gl_ld_ptr(&g->ptr[k]));
+    msgs[k].offset = ld_relaxed_u64(&g->u1[k]);
+    msgs[k].dst_pe = dst_pes[k];
+    const unsigned long long bytes = ld_relaxed_u64(&g->u0[k]);
+    msgs[k].cells = (int)cells_for(bytes);
+    msgs[k].capacity = msgs[k].env ? (size_t)(bytes - HDR) : 0;
+    ok = ok && msgs[k].env != nullptr;
+  }
+  return ok;
+}
+
+// Block 0 publishes message k with thread k once every block is done
+// writing the payloads.
+__device__ void group_send_user_msgs(int chare_id, const int* chare_idx, int ep_id, message* msgs,
+    const size_t* payload_sizes, const int* refnums, int n) {
+  pe_state* ps = pes();
+  grid_barrier();
+  if (blockIdx.x == 0) {
+    for (int k = (int)threadIdx.x; k < n; k += (int)blockDim.x) {
+      if (!msgs[k].env) continue;
+      unsigned char* m = reinterpret_cast<unsigned char*>(msgs[k].env);
+      envelope* env = msgs[k].env;
+      env->type = msgtype::user;
+      env->src_pe = 0;
+      env->size = (size_t)msgs[k].capacity + HDR;
+      regular_msg* rm = reinterpret_cast<regular_msg*>(m + sizeof(envelope));
+      rm->chare_id = chare_id;
+      rm->chare_idx = chare_idx[k];
+      rm->ep_id = ep_id;
+      rm->refnum = refnums ? refnums[k] : -1;
+      if (payload_sizes[k] > msgs[k].capacity)
+        set_error(CHARMING_ERR_MSG_TOO_LARGE, msgs[k].dst_pe, (int)payload_sizes[k]);
+      atomicAdd_block(&ps->stats[ST_SENT], 1ULL);
+      atomicAdd_block(&ps->stats[ST_BYTES_SENT], (unsigned long long)payload_sizes[k]);
+      publish_msg(msgs[k].dst_pe, msgs[k].offset, m);
+    }
+  }
+}
+
+}  // namespace
+
 __device__ void charm::send_reg_msg(int chare_id, int chare_idx, int ep_id, void* buf,
     size_t payload_size, int dst_pe, int refnum) {
+  if (gpu_level()) {
+    group_send_reg_msg(chare_id, chare_idx, ep_id, buf, payload_size, dst_pe, refnum);
+    return;
+  }
   pe_state* ps = pes();
   if (threadIdx.x == 0) {
     unsigned long long bytes = envelope::alloc_size(msgtype::regular, payload_size);
@@ -408,6 +557,7 @@ __device__ void charm::send_reg_msg(int chare_id, int chare_idx, int ep_id, void
 }
 
 __device__ bool charm::alloc_user_msg(message& msg, int dst_pe, size_t payload_size) {
+  if (gpu_level()) return group_alloc_user_msgs(&msg, &dst_pe, &payload_size, 1);
   pe_state* ps = pes();
   if (threadIdx.x == 0) {
     unsigned long long bytes = envelope::alloc_size(msgtype::user, payload_size);
@@ -430,6 +580,11 @@ __device__ bool charm::alloc_user_msg(message& msg, int dst_pe, size_t payload_s
 __device__ void charm::send_user_msg(int chare_id, int chare_idx, int ep_id,
     message& msg, size_t payload_size, int refnum) {
   if (msg.env == nullptr) return;
+  if (gpu_level()) {
+    group_send_user_msgs(chare_id, &chare_idx, ep_id, &msg, &payload_size, &refnum, 1);
+    msg.env = nullptr;
+    return;
+  }
   pe_state* ps = pes();
   __syncthreads();  // payload writes of all threads are done
   if (threadIdx.x == 0) {
@@ -455,8 +610,9 @@ __device__ void charm::send_user_msg(int chare_id, int chare_idx, int ep_id,
 
 __device__ bool charm::alloc_user_msgs(message* msgs, const int* dst_pes,
     const size_t* payload_sizes, int n) {
-  pe_state* ps = pes();
   if (n > MSG_BATCH_MAX) n = MSG_BATCH_MAX;
+  if (gpu_level()) return group_alloc_user_msgs(msgs, dst_pes, payload_sizes, n);
+  pe_state* ps = pes();
   if (blockDim.x >= 32) {
     // Warp 0, one lane per message. Lanes whose messages go to the same PE
     // form a group (__match_any_sync): its lowest lane takes the tickets of
@@ -517,8 +673,13 @@ __device__ bool charm::alloc_user_msgs(message* msgs, const int* dst_pes,
 
 __device__ void charm::send_user_msgs(int chare_id, const int* chare_idx, int ep_id,
     message* msgs, const size_t* payload_sizes, const int* refnums, int n) {
-  pe_state* ps = pes();
   if (n > MSG_BATCH_MAX) n = MSG_BATCH_MAX;
+  if (gpu_level()) {
+    group_send_user_msgs(chare_id, chare_idx, ep_id, msgs, payload_sizes, refnums, n);
+    for (int j = 0; j < n; j++) msgs[j].env = nullptr;
+    return;
+  }
+  pe_state* ps = pes();
   __syncthreads();  // payload writes of all threads are done
   // one message per thread: the publishing fences overlap
   for (int k = (int)threadIdx.x; k < n; k += (int)blockDim.x) {
@@ -1048,9 +1209,12 @@ __device__ void next_action() {
 }
 
 // The loop: thread 0 closes the last action and picks the next; the block
-// executes it. Two block barriers per message.
+// executes it. Two block barriers per message. In GPU-level mode this is
+// block 0's loop: entry methods (and the exit) are handed to the other
+// blocks through group_state, with a grid barrier before and after.
 __device__ void scheduler_loop() {
   pe_state* ps = pes();
+  const bool group = gpu_level();
   if (threadIdx.x == 0) ps->d_act = ACT_NONE;
   while (true) {
     if (threadIdx.x == 0) {
@@ -1059,12 +1223,25 @@ __device__ void scheduler_loop() {
     }
     __syncthreads();
     const int act = ps->d_act;
+    const bool call = act == ACT_CALL_RING || act == ACT_CALL_STASH || act == ACT_CALL_WAIT;
+    if (group && (call || act == ACT_EXIT)) {
+      if (threadIdx.x == 0) {
+        group_state* gs = c_rt.gl;
+        gs->act = call ? ACT_CALL_RING : ACT_EXIT;
+        gs->p = ps->d_p;
+        gs->idx = ps->d_idx;
+        gs->ep = ps->d_ep;
+        gs->arg = ps->d_arg;
+      }
+      if (!grid_barrier_ok() || act == ACT_EXIT) break;
+    }
     if (act == ACT_EXIT) break;
     chare_proxy_base* p = reinterpret_cast<chare_proxy_base*>(ps->d_p);
-    if (act == ACT_CALL_RING || act == ACT_CALL_STASH || act == ACT_CALL_WAIT) {
+    if (call) {
       const long long c0 = clock64();
       p->call_fn(p, ps->d_idx, ps->d_ep, ps->d_arg);
       if (threadIdx.x == 0) ps->stats[ST_EM_CYC] += (unsigned long long)(clock64() - c0);
+      if (group && !grid_barrier_ok()) break;  // every block is done with the message
     } else if (act == ACT_STASH_PUT) {
       copy_cooperative(ps->d_p, ps->d_arg, ps->d_bytes, threadIdx.x, blockDim.x);
     } else if (act == ACT_FLUSH) {
@@ -1078,6 +1255,18 @@ __device__ void scheduler_loop() {
   }
 }
 
+// GPU-level mode, blocks 1..: run each entry method block 0 hands out.
+__device__ void helper_loop() {
+  const group_state* gs = c_rt.gl;
+  while (true) {
+    if (!grid_barrier_ok()) break;
+    if (ld_relaxed_s32(&gs->act) != ACT_CALL_RING) break;
+    chare_proxy_base* p = reinterpret_cast<chare_proxy_base*>(gl_ld_ptr(&gs->p));
+    p->call_fn(p, ld_relaxed_s32(&gs->idx), ld_relaxed_s32(&gs->ep), gl_ld_ptr(&gs->arg));
+    if (!grid_barrier_ok()) break;
+  }
+}
+
 } // namespace
 
 // ---------------------------------------------------------------------------
@@ -1086,7 +1275,9 @@ __device__ void scheduler_loop() {
 __global__ void __launch_bounds__(MAX_THREADS, 1)
 charming_scheduler_kernel(int argc, char** argv, size_t* argvs) {
   pe_state* ps = pes();
-  const int me = blockIdx.x;
+  const int me = charm::my_pe();
+  // the block that keeps the PE's state (every block in SM-level mode)
+  const bool keeper = !gpu_level() || blockIdx.x == 0;
   if (threadIdx.x == 0) {
     ps->my_pe = me;
     ps->term = 0;
@@ -1109,6 +1300,8 @@ charming_scheduler_kernel(int argc, char** argv, size_t* argvs) {
     ps->uh_head = ps->uh_tail = 0;
     ps->ub_head = ps->ub_tail = 0;
     ps->aw_count = 0;
+    ps->gl_seq = 0;
+    ps->bar_ok = 1;
     ps->ready_cursor = 0;
     ps->d_act = 0;
     ps->rq_base = 0;
@@ -1127,10 +1320,13 @@ charming_scheduler_kernel(int argc, char** argv, size_t* argvs) {
   grid_barrier();
 
   unsigned long long loop_t0 = globaltimer();
-  if (!terminated() && !ps->term) scheduler_loop();
+  if (!terminated() && !ps->term) {
+    if (keeper) scheduler_loop();
+    else helper_loop();
+  }
   unsigned long long loop_t1 = globaltimer();
 
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0 && keeper) {
     ps->stats[ST_LOOP_NS] = loop_t1 - loop_t0;
     for (int i = 0; i < N_STATS; i++) c_rt.pe_stats[(unsigned long long)me * N_STATS + i] = ps->stats[i];
     c_rt.pe_times[3 * me] = ps->t0;

@@ -62,6 +62,18 @@ __device__ uint64_t now_ns();
 // SM the calling thread runs on (%smid; reference src/util/util.cu:3-7).
 __device__ unsigned int smid();
 
+// The threads of the calling PE, for code that runs in both modes: in
+// SM-level mode (the default) a PE is one thread block, in GPU-level mode
+// (charming_config::gpu_level, or a program compiled with
+// -DCHARMING_GPU_LEVEL) every block of the launch. pe_thread() is the
+// reference examples' GID (threadIdx.x, or the grid-wide thread index),
+// pe_threads() their GROUP_SIZE, pe_sync() their BARRIER_LOCAL
+// (__syncthreads, or a barrier over all blocks).
+__device__ int pe_thread();
+__device__ int pe_threads();
+__device__ void pe_sync();
+__device__ bool is_gpu_level();
+
 } // namespace charm
 
 #endif // _CHARMING_H_

@@ -63,6 +63,12 @@ typedef struct charming_config {
   double idle_timeout_s;    /* stop if no message is delivered for this long */
   int free_chares_at_exit;  /* delete proxies/chares when a run ends         */
   int verbose;              /* print the configuration (PINFO) on init       */
+  int gpu_level;            /* 1: GPU-level mode, the reference's default
+                               build (src/sched/scheduler.cu:240-333): all
+                               blocks (n_pes of them, 0: one per SM slot)
+                               form a single PE that runs every entry method
+                               and collective send together; n_pes() is 1.
+                               0: SM-level mode, one PE per block          */
 } charming_config;
 
 /* Fills *cfg with defaults (148 PEs on a B200, 512 threads, 4 MiB rings). */
@@ -101,6 +107,8 @@ typedef struct charming_info {
   uint64_t device_bytes;     /* runtime buffers on the device            */
   uint64_t stack_bytes;      /* per-thread stack limit in effect         */
   uint64_t local_bytes;      /* scheduler kernel's static local memory   */
+  int n_blocks;              /* thread blocks of the scheduler launch    */
+  int gpu_level;             /* 1: GPU-level mode (n_pes is 1)           */
 } charming_info;
 int charming_get_info(charming_info* out);
 

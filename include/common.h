@@ -13,9 +13,15 @@
 #include <stddef.h>
 #include <new>  // placement new in device code
 
-// This runtime always schedules one PE per thread block (the reference's
-// -DSM_LEVEL mode). Examples that branch on SM_LEVEL pick that branch.
-#ifndef SM_LEVEL
+// Scheduling mode. By default one PE per thread block (the reference's
+// -DSM_LEVEL build), and examples that branch on SM_LEVEL pick that branch.
+// A program compiled with -DCHARMING_GPU_LEVEL takes its GPU-level branch
+// (the reference's default build: GID over the whole grid, BARRIER_LOCAL =
+// charm::barrier_local()), and the weak symbol below asks the library's
+// process main for GPU-level mode, in which all blocks form one PE.
+#ifdef CHARMING_GPU_LEVEL
+extern "C" __attribute__((weak)) const int charming_program_gpu_level = 1;
+#elif !defined(SM_LEVEL)
 #define SM_LEVEL 1
 #endif
 

@@ -8,7 +8,8 @@
 // AddressSanitizer and, separately, ThreadSanitizer; small inbox rings make
 // tickets wrap many times.
 //
-// usage: rt_emu fanout n_pes ring_bytes n_chares msgs payload seed mode
+// usage (n_pes: PE blocks; with RT_EMU_GPU_LEVEL set they form one PE):
+//        rt_emu fanout n_pes ring_bytes n_chares msgs payload seed mode
 //        rt_emu hello n_pes ring_bytes
 //        rt_emu refnum n_pes ring_bytes reversed
 //        rt_emu serve n_pes ring_bytes n_requests seed workers_per_pe
@@ -188,11 +189,16 @@ T* zalloc(size_t n) {
   return p;
 }
 
-// The parts of charming_init that build the device state.
-void init_runtime(int n_pes, size_t ring_bytes) {
+// The parts of charming_init that build the device state. GPU-level mode
+// (RT_EMU_GPU_LEVEL set): the n_blocks blocks form one PE.
+void init_runtime(int n_blocks, size_t ring_bytes, bool gpu_level) {
   using namespace charm::rt;
   device_state ds{};
+  const int n_pes = gpu_level ? 1 : n_blocks;
   ds.n_pes = n_pes;
+  ds.n_blocks = n_blocks;
+  ds.gpu_level = gpu_level ? 1 : 0;
+  ds.gl = gpu_level ? zalloc<group_state>(1) : nullptr;
   ds.threads = 1;
   ds.ring_cells = ring_bytes / CELL;
   ds.max_msg = 4096 + 64;
@@ -234,7 +240,8 @@ void init_runtime(int n_pes, size_t ring_bytes) {
   ds.user_heap = zalloc<unsigned char>(ds.user_heap_bytes * n_pes);
   ds.user_blocks = zalloc<user_block>((size_t)ds.user_blocks_max * n_pes);
   c_rt = ds;
-  c_n_pes = c_n_pes_node = c_n_sms = n_pes;
+  c_n_pes = c_n_pes_node = n_pes;
+  c_n_sms = n_blocks;
   c_n_nodes = c_n_devs = c_n_devs_node = 1;
 }
 
@@ -272,7 +279,7 @@ int run_scheduler(int n_pes, int threads) {
   }
   for (auto& t : th) t.join();
   g_deferred = 0;
-  for (int p = 0; p < n_pes; p++)
+  for (int p = 0; p < charm::rt::c_rt.n_pes; p++)
     g_deferred += charm::rt::c_rt.pe_stats[(size_t)p * charm::rt::N_STATS + charm::rt::ST_DEFERRED];
   const int* ctl = charm::rt::c_rt.ctrl;
   if (ctl[charm::rt::CTRL_STATUS])
@@ -481,7 +488,7 @@ int main(int argc, char** argv) {
   if (threads != 1) return 2;
 #endif
   size_t ring_bytes = strtoull(argv[3], nullptr, 10);
-  init_runtime(n_pes, ring_bytes);
+  init_runtime(n_pes, ring_bytes, getenv("RT_EMU_GPU_LEVEL") != nullptr);
   g_app = suite::app_params{};
   if (app == "fanout") {
     if (argc < 9) return 2;

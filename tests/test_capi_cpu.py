@@ -54,7 +54,7 @@ def test_struct_sizes_match_header():
     # the fields declared in the header instead).
     from charming_b200 import _lib
     assert C.sizeof(_lib.JacobiProblem) == 4 * 6 + 8 * 5
-    assert C.sizeof(_lib.Config) == 88
+    assert C.sizeof(_lib.Config) == 96  # gpu_level + tail padding
 
 
 def test_reference_examples_built():

@@ -94,3 +94,17 @@ def test_reference_pingpong_links_and_runs():
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     sizes = [l for l in r.stdout.splitlines() if l.startswith("Size ")]
     assert [int(l.split()[1]) for l in sizes] == [8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096]
+
+
+def test_reference_pingpong_gpu_level_links_and_runs():
+    # The example's GPU-level branch (the reference's default build: GID over
+    # the grid, BARRIER_LOCAL = charm::barrier_local()) asks for GPU-level
+    # mode: one PE of all blocks, both chares on it, every message handled
+    # by the whole grid.
+    r = _run_ref_example("pingpong_gpu_level", ["8", "4096", "20", "3"])
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "GPU-level mode: 1 PE of" in r.stdout
+    inits = sorted(l for l in r.stdout.splitlines() if l.startswith("Chare ") and "init on PE" in l)
+    assert inits == ["Chare 0 init on PE 0", "Chare 1 init on PE 0"]
+    sizes = [l for l in r.stdout.splitlines() if l.startswith("Size ")]
+    assert [int(l.split()[1]) for l in sizes] == [8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096]

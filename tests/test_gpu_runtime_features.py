@@ -106,10 +106,48 @@ def test_decomp1d_matches_oracle(rt, n, nx, ny, iters, mode):
     assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
 
 
+def test_gpu_level_decomp1d_matches_oracle():
+    # GPU-level mode (every block forms PE 0): the decomp1d chares run each
+    # entry method on the whole grid; all three ways to meet the neighbours,
+    # bit for bit against the oracle. A program that is not written for the
+    # mode is refused with a configuration error, and the runtime goes on.
+    out = child(
+        "import json\n"
+        "import numpy as np\n"
+        "from charming_b200.runtime import Runtime\n"
+        "from charming_b200._lib import CharmingError\n"
+        "from oracle import jacobi as oj\n"
+        "rt = Runtime(gpu_level=1)\n"
+        "res = [rt.n_pes, rt.info['n_blocks'], rt.info['gpu_level']]\n"
+        "for n, nx, ny, it, mode in [(1, 1024, 600, 9, 0), (1, 1024, 600, 9, 1), (1, 1024, 600, 9, 2),\n"
+        "                            (4, 512, 300, 7, 1), (4, 512, 300, 7, 2), (3, 64, 40, 5, 2),\n"
+        "                            (2, 4096, 1000, 4, 1)]:\n"
+        "    got, _ = rt.decomp1d(n, nx, ny, it, mode)\n"
+        "    ref = oj.decomp1d(n, nx, ny, it)\n"
+        "    res.append(bool(np.array_equal(got.view(np.uint32), ref.view(np.uint32))))\n"
+        "try:\n"
+        "    rt.hello()\n"
+        "    res.append('hello ran')\n"
+        "except CharmingError as e:\n"
+        "    res.append(e.code)\n"
+        "got, _ = rt.decomp1d(2, 256, 100, 3, 2)\n"
+        "res.append(bool(np.array_equal(got.view(np.uint32), oj.decomp1d(2, 256, 100, 3).view(np.uint32))))\n"
+        "print(json.dumps(res))\n")
+    n_pes, n_blocks, gl = out[:3]
+    assert n_pes == 1 and gl == 1 and n_blocks > 1
+    assert out[3:10] == [True] * 7
+    assert out[10] == 14  # CHARMING_ERR_CONFIG
+    assert out[11] is True
+
+
 @pytest.mark.parametrize("nx,ny,nz,sweeps,seed", [
     (6, 5, 4, 1, 1), (17, 9, 11, 3, 2), (33, 7, 13, 5, 3),   # the golden fixtures' shapes
     (64, 48, 40, 4, 5),                                     # whole tiles
     (97, 35, 70, 7, 6),                                     # ragged tiles, several z runs
+    # even row pitch: the TMA plane-ring kernel
+    (32, 16, 9, 4, 9),                                      # exactly one box
+    (94, 35, 70, 3, 7),                                     # ragged tiles, several z runs
+    (62, 16, 300, 2, 8),                                    # long z runs, more planes than slots
 ])
 def test_jacobi3d_matches_oracle(rt, nx, ny, nz, sweeps, seed):
     from oracle import jacobi as oj

@@ -178,6 +178,33 @@ def test_decomp1d_matches_oracle(emus, exe, n_pes, threads, n, nx, ny, iters, mo
     assert np.array_equal(got, ref.view(np.uint32))
 
 
+@pytest.mark.parametrize("exe,blocks,n,nx,ny,iters,mode", [
+    ("rt_emu", 4, 1, 64, 40, 5, 0),        # one chare, its own neighbour both ways
+    ("rt_emu", 4, 1, 64, 40, 5, 1),
+    ("rt_emu", 4, 1, 64, 40, 5, 2),
+    ("rt_emu", 3, 3, 64, 30, 4, 1),        # several chares on the one PE
+    ("rt_emu", 5, 2, 40, 50, 6, 2),
+    ("rt_emu_tsan", 4, 1, 64, 40, 5, 1),   # the blocks' hand-offs under ThreadSanitizer
+    ("rt_emu_tsan", 3, 3, 64, 30, 4, 2),
+])
+def test_gpu_level_decomp1d_matches_oracle(emus, exe, blocks, n, nx, ny, iters, mode):
+    """GPU-level mode on the real scheduler: `blocks` emulated blocks form
+    PE 0; block 0 schedules, every block runs each entry method and each
+    collective send (group_state hand-offs and grid barriers)."""
+    from oracle import jacobi as oj
+    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0", TSAN_OPTIONS="halt_on_error=1",
+               RT_EMU_THREADS="1", RT_EMU_GPU_LEVEL="1")
+    r = subprocess.run([emus[exe], "decomp1d", str(blocks), "65536", str(n), str(nx), str(ny), str(iters),
+                        str(mode)], capture_output=True, text=True, timeout=600, env=env)
+    assert "ThreadSanitizer" not in r.stderr and "runtime error" not in r.stderr, r.stderr[-3000:]
+    lines = r.stdout.splitlines()
+    assert lines and lines[0] == "status=0", (lines[:2], r.stderr[-2000:])
+    got = np.array([[int(x, 16) for x in l.split()[1:]] for l in lines if l.startswith("G ")], dtype=np.uint32)
+    ref = oj.decomp1d(n, nx, ny, iters)
+    assert got.shape == ref.shape
+    assert np.array_equal(got, ref.view(np.uint32))
+
+
 def serve(exe, n_pes, n_req, seed, wpp, max_inflight, side, dtype, threads=1, ring=65536):
     """Solve server on the CPU: the real scheduler runs the Jacobi2d chares
     in serving mode (apps/jacobi2d.cu) and admission runs apps/serve_host.h;
