@@ -59,7 +59,7 @@ class Stats(C.Structure):
         ("bytes_sent", u64), ("idle_polls", u64), ("space_waits", u64),
         ("kernel_ms", f64), ("loop_ms", f64), ("main_ms", f64), ("status", i32), ("err_pe", i32),
         ("err_info0", i32), ("err_info1", i32), ("idle_ms", f64), ("em_ms", f64),
-        ("deferred", u64),
+        ("deferred", u64), ("ticket_ms", f64), ("space_ms", f64),
     ]
 
 
@@ -86,7 +86,8 @@ class JacobiInfo(C.Structure):
         ("n_problems", i32), ("n_chares", i32), ("max_chares_per_pe", i32),
         ("interior_points", u64), ("grid_bytes", u64), ("halo_msgs_per_sweep", u64),
         ("last_run_ms", f64), ("sweep_ms_max", f64), ("sweep_ms_mean", f64),
-        ("send_ms_mean", f64), ("halo_ms_mean", f64),
+        ("send_ms_mean", f64), ("halo_ms_mean", f64), ("send_reserve_ms_mean", f64),
+        ("send_publish_ms_mean", f64),
     ]
 
 

@@ -125,9 +125,11 @@ __device__ void d1_sweep(const float* __restrict__ a, float* __restrict__ o, int
   if (runs > rows / 8) runs = rows / 8;  // at least 8 rows per run
   if (runs < 1) runs = 1;
   const int run_rows = (rows + runs - 1) / runs;
+  runs = (rows + run_rows - 1) / run_rows;  // every run starts inside the band
   for (int item = warp; item < strips * runs; item += nw) {
     const int s = item % strips, r0 = 1 + (item / strips) * run_rows;
     const int r1 = min(iy_end, r0 + run_rows);
+    if (r0 >= iy_end) continue;  // (none by construction; the loads below need it)
     const int v = s * 32 + lane;
     const bool act = v < nv;
     const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);

@@ -131,10 +131,13 @@ __shared__ charm::chare_proxy<JBlock>* jproxy;
 // This PE's phase timers (ns: sweeps, halo sending, halo entry methods),
 // kept on chip and stored through to japp::pe_ns() after every update (a
 // store only: no read of global memory on the message path).
-__shared__ unsigned long long s_pe_ns[3];
+// Slots: 0 sweeps, 1 halo sends (all of send_halos), 2 halo entry methods,
+// 3 of the sends: taking ring space, 4 of the sends: publishing.
+constexpr int PE_NS_SLOTS = 8;
+__shared__ unsigned long long s_pe_ns[5];
 __device__ __forceinline__ void add_pe_ns(int k, unsigned long long ns) {
   s_pe_ns[k] += ns;
-  japp::pe_ns()[4 * blockIdx.x + k] = s_pe_ns[k];
+  japp::pe_ns()[PE_NS_SLOTS * blockIdx.x + k] = s_pe_ns[k];
 }
 __shared__ charm::chare_proxy<JServer>* sproxy;
 
@@ -276,7 +279,9 @@ __device__ void send_halos(JBlock& c, const jac::chare_desc& d) {
     n++;
   }
   charm::message msg[jac::N_DIRS];
-  if (n > 0 && jproxy->alloc_msgs(msg, idx, bytes, n)) {
+  const bool got = n > 0 && jproxy->alloc_msgs(msg, idx, bytes, n);
+  if (threadIdx.x == 0) add_pe_ns(3, charm::now_ns() - t0);
+  if (got) {
     T* vals[jac::N_DIRS];
     for (int k = 0; k < n; k++)
       vals[k] = reinterpret_cast<T*>(reinterpret_cast<char*>(msg[k].payload()) + sizeof(jac::halo_hdr));
@@ -288,7 +293,9 @@ __device__ void send_halos(JBlock& c, const jac::chare_desc& d) {
       hh->gen = c.gen;
     }
     copy_rects<T>(view<T>(d, c.cur), e, vals, n, false);
+    const unsigned long long tp = charm::now_ns();
     jproxy->invoke_msgs(idx, EP_HALO, msg, bytes, refs, n);
+    if (threadIdx.x == 0) add_pe_ns(4, charm::now_ns() - tp);
   }
   if (threadIdx.x == 0) add_pe_ns(1, charm::now_ns() - t0);
 }
@@ -497,7 +504,7 @@ __device__ void em_decision(JBlock& c, void* arg) {
 
 __device__ void suite::jacobi2d_main(int pe) {
   if (threadIdx.x == 0) {
-    s_pe_ns[0] = s_pe_ns[1] = s_pe_ns[2] = 0;
+    for (int k = 0; k < 5; k++) s_pe_ns[k] = 0;
     jproxy = new charm::chare_proxy<JBlock>();
     jproxy->add_entry_method<&em_start>();
     jproxy->add_entry_method<&em_halo>();

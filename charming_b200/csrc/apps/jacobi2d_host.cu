@@ -184,7 +184,7 @@ extern "C" int charming_jacobi2d_create(const charming_jacobi_problem* probs, in
   if (e == cudaSuccess) e = cudaMalloc(&h->d_final, sizeof(int) * nch);
   if (e == cudaSuccess) e = cudaMalloc(&h->d_block_map, sizeof(int) * n_pes);
   if (e == cudaSuccess) e = cudaMalloc(&h->d_chare_of, sizeof(int) * h->chare_of.size());
-  if (e == cudaSuccess) e = cudaMalloc(&h->d_sweep_ns, 32 * (size_t)n_pes);
+  if (e == cudaSuccess) e = cudaMalloc(&h->d_sweep_ns, 64 * (size_t)n_pes);
   if (e == cudaSuccess) e = cudaMemcpy(h->d_chares, h->chares.data(), sizeof(jac::chare_desc) * nch, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(h->d_probs, pd.data(), sizeof(jac::prob_desc) * n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(h->d_results, 0, sizeof(jac::prob_result) * n);
@@ -302,7 +302,7 @@ extern "C" int charming_jacobi2d_store(void* handle, int prob, void* host_grid) 
 static int enqueue_run(JHandle* h, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(h->d_done, 0, 64, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->d_results, 0, sizeof(jac::prob_result) * h->probs.size(), s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(h->d_sweep_ns, 0, 32 * h->block_map.size(), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->d_sweep_ns, 0, 64 * h->block_map.size(), s);
   if (e == cudaSuccess)
     e = cudaMemcpyToSymbolAsync(g_app, h->h_params, sizeof(suite::app_params), 0,
                                 cudaMemcpyHostToDevice, s);
@@ -476,18 +476,20 @@ extern "C" int charming_jacobi2d_get_info(void* handle, charming_jacobi_info* ou
   out->grid_bytes = h->grid_bytes;
   out->halo_msgs_per_sweep = h->halo_msgs;
   out->last_run_ms = h->last_ms;
-  std::vector<unsigned long long> ns(4 * h->block_map.size());
+  std::vector<unsigned long long> ns(8 * h->block_map.size());
   cudaError_t e = cudaMemcpy(ns.data(), h->d_sweep_ns, 8 * ns.size(), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return check_cuda(e, "jacobi2d info");
-  double mx = 0, sum[3] = {0, 0, 0};
+  double mx = 0, sum[5] = {0, 0, 0, 0, 0};
   int busy = 0;
   for (size_t p = 0; p < h->block_map.size(); p++) {
-    mx = std::max(mx, (double)ns[4 * p]);
+    mx = std::max(mx, (double)ns[8 * p]);
     if (h->block_map[p] > 0) {
-      for (int k = 0; k < 3; k++) sum[k] += (double)ns[4 * p + k];
+      for (int k = 0; k < 5; k++) sum[k] += (double)ns[8 * p + k];
       busy++;
     }
   }
+  out->send_reserve_ms_mean = busy ? sum[3] / busy * 1e-6 : 0.0;
+  out->send_publish_ms_mean = busy ? sum[4] / busy * 1e-6 : 0.0;
   out->sweep_ms_max = mx * 1e-6;
   out->sweep_ms_mean = busy ? sum[0] / busy * 1e-6 : 0.0;
   out->send_ms_mean = busy ? sum[1] / busy * 1e-6 : 0.0;

@@ -194,10 +194,10 @@ extern "C" int charming_serve_start(const charming_serve_config* cfg, void** ser
   if (e == cudaSuccess) e = cudaMalloc(&s->d_block_map, sizeof(int) * n_pes);
   if (e == cudaSuccess) e = cudaMalloc(&s->d_server_map, sizeof(int) * n_pes);
   if (e == cudaSuccess) e = cudaMalloc(&s->d_final, sizeof(int) * s->n_workers);
-  if (e == cudaSuccess) e = cudaMalloc(&s->d_pe_ns, 32 * (size_t)n_pes);
+  if (e == cudaSuccess) e = cudaMalloc(&s->d_pe_ns, 64 * (size_t)n_pes);
   if (e == cudaSuccess) e = cudaMemset(s->d_ctr, 0, 128);
   if (e == cudaSuccess) e = cudaMemset(s->d_done, 0, sizeof(unsigned) * s->Q);
-  if (e == cudaSuccess) e = cudaMemset(s->d_pe_ns, 0, 32 * (size_t)n_pes);
+  if (e == cudaSuccess) e = cudaMemset(s->d_pe_ns, 0, 64 * (size_t)n_pes);
   s->h_req = host_mapped<jac::serve_req>(s->Q, &e);
   s->h_desc = host_mapped<jac::chare_desc>(s->n_workers, &e);
   s->h_prob = host_mapped<jac::prob_desc>(s->Q, &e);

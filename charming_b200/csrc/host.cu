@@ -166,6 +166,13 @@ int collect_run(double kernel_ms) {
   double em = 0;
   for (int p = 0; p < g.inf.n_pes; p++) em += (double)st[(size_t)p * N_STATS + ST_EM_CYC];
   s.em_ms = (g.inf.n_pes && g.prop.clockRate > 0) ? em / g.inf.n_pes / (double)g.prop.clockRate : 0.0;
+  double tk = 0, sp = 0;
+  for (int p = 0; p < g.inf.n_pes; p++) {
+    tk += (double)st[(size_t)p * N_STATS + ST_TICKET_NS];
+    sp += (double)st[(size_t)p * N_STATS + ST_SPACE_NS];
+  }
+  s.ticket_ms = g.inf.n_pes ? tk / g.inf.n_pes * 1e-6 : 0.0;
+  s.space_ms = g.inf.n_pes ? sp / g.inf.n_pes * 1e-6 : 0.0;
   s.main_ms = main_max * 1e-6;
   s.kernel_ms = kernel_ms;
   s.status = ctrl_h[CTRL_STATUS];

@@ -88,7 +88,9 @@ enum : int {
   ST_IDLE_NS,         // ns spent waiting on an empty inbox
   ST_EM_CYC,          // SM cycles spent inside entry methods
   ST_DEFERRED,        // sends moved to the outbox (destination ring full)
-  N_STATS = 11
+  ST_TICKET_NS,       // ns the reserving thread waited for its ticket atomics
+  ST_SPACE_NS,        // ns it then waited for ring space (head cache and waits)
+  N_STATS = 13
 };
 
 // Device-wide runtime description, copied to __constant__ memory before each

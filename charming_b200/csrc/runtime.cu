@@ -278,8 +278,14 @@ __device__ unsigned char* wait_space(int dst, unsigned long long t, unsigned lon
 // DEFER_AFTER_NS) or nullptr (error recorded, or the run is ending).
 __device__ unsigned char* reserve(int dst, unsigned long long bytes, unsigned long long* ticket) {
   if (!send_allowed(dst, bytes)) return nullptr;
+  pe_state* ps = pes();
+  const unsigned long long t0 = globaltimer();
   const unsigned long long t = atomicAdd(&c_rt.tail[dst].v, (unsigned long long)cells_for(bytes));
-  return wait_space(dst, t, bytes, ticket);
+  const unsigned long long t1 = globaltimer();
+  unsigned char* m = wait_space(dst, t, bytes, ticket);
+  atomicAdd_block(&ps->stats[ST_TICKET_NS], t1 - t0);
+  atomicAdd_block(&ps->stats[ST_SPACE_NS], globaltimer() - t1);
+  return m;
 }
 
 // The caller holds ticket t (cells_for(bytes) cells) in dst's inbox: waits
@@ -638,13 +644,21 @@ __device__ bool charm::alloc_user_msgs(message* msgs, const int* dst_pes,
         }
       }
       unsigned long long base = 0;
+      const unsigned long long ta = globaltimer();
       if (ok && k == leader) base = atomicAdd(&c_rt.tail[dst_pes[k]].v, (unsigned long long)tot);
       base = __shfl_sync(FULL, base, leader);
+      __syncwarp();
+      const unsigned long long tb = globaltimer();
       if (act) {
         unsigned long long t = 0;
         ps->bm_ptr[k] = ok ? wait_space(dst_pes[k], base + pre, bytes, &t) : nullptr;
         ps->bm_tick[k] = t;
         ps->bm_bytes[k] = bytes;
+      }
+      __syncwarp();
+      if (k == 0) {
+        ps->stats[ST_TICKET_NS] += tb - ta;
+        ps->stats[ST_SPACE_NS] += globaltimer() - tb;
       }
     }
   } else {

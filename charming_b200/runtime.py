@@ -39,6 +39,8 @@ class RunStats:
     idle_ms: float = 0.0
     em_ms: float = 0.0
     deferred: int = 0
+    ticket_ms: float = 0.0
+    space_ms: float = 0.0
 
 
 class Runtime:
@@ -84,7 +86,7 @@ class Runtime:
         self.lib.charming_last_stats(C.byref(st))
         return RunStats(st.delivered, st.sent, st.stashed, st.revived, st.bytes_sent,
                         st.idle_polls, st.space_waits, st.kernel_ms, st.loop_ms, st.main_ms,
-                        st.status, st.idle_ms, st.em_ms, st.deferred)
+                        st.status, st.idle_ms, st.em_ms, st.deferred, st.ticket_ms, st.space_ms)
 
     # ---- built-in programs ---------------------------------------------------
     def hello(self) -> np.ndarray:

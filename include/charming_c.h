@@ -133,6 +133,10 @@ typedef struct charming_stats {
                                 (SM cycles at the nominal clock)         */
   uint64_t deferred;         /* sends moved to the sender's outbox because
                                 the destination ring stayed full         */
+  double ticket_ms;          /* mean over PEs: reserving thread waiting for
+                                its inbox-ticket atomics                 */
+  double space_ms;           /* mean over PEs: then for ring space (a stale
+                                head cache refreshed, or a full ring)    */
 } charming_stats;
 int charming_last_stats(charming_stats* out);
 
@@ -195,6 +199,8 @@ typedef struct charming_jacobi_info {
   double sweep_ms_mean;       /* last run: mean over busy PEs              */
   double send_ms_mean;        /* last run: mean time packing/sending halos */
   double halo_ms_mean;        /* last run: mean time in halo entry methods */
+  double send_reserve_ms_mean;  /* of send_ms_mean: taking the ring space    */
+  double send_publish_ms_mean;  /* of send_ms_mean: publishing the messages  */
 } charming_jacobi_info;
 
 /* Decomposes the problems into chares (reference decomposition:

@@ -1,7 +1,10 @@
 // GPU-level program forms (compiled with -DCHARMING_GPU_LEVEL): the
 // reference examples' #ifndef SM_LEVEL branch (GID over the grid,
-// BARRIER_LOCAL = charm::barrier_local(), a __device__ proxy pointer) and
-// the mode-independent pe_thread() / pe_threads() / pe_sync().
+// BARRIER_LOCAL = charm::barrier_local(), __device__ proxy and data
+// pointers, `new` from GID 0) and the mode-independent pe_thread() /
+// pe_threads() / pe_sync(). Two chares on the one PE pass a counter and a
+// 1024-int array back and forth; every entry method adds 1 to each array
+// element with all threads of the grid, and GID 0 checks the sums.
 #include <charming.h>
 
 #ifdef SM_LEVEL
@@ -10,20 +13,32 @@
 #define GID (blockDim.x * blockIdx.x + threadIdx.x)
 #define BARRIER_LOCAL charm::barrier_local()
 
+constexpr int N = 1024, ROUNDS = 6;
+
 struct Cell : charm::chare {
   int hits;
   __device__ Cell() : hits(0) {}
 };
 __device__ charm::chare_proxy<Cell>* cells;
 __device__ int* data;
+__device__ int* bad;
 
 __device__ void on_msg(Cell& c, void* arg) {
+  const int round = *static_cast<const int*>(arg);
   if (GID == 0) c.hits++;
-  BARRIER_LOCAL;
-  for (int i = charm::pe_thread(); i < 1024; i += charm::pe_threads()) data[i] += 1;
+  for (int i = charm::pe_thread(); i < N; i += charm::pe_threads()) {
+    if (data[i] != round) atomicAdd(bad, 1);
+    data[i] = round + 1;
+  }
   charm::pe_sync();
-  if (c.hits < 3) cells->invoke(c.i, 0, data, 64);
-  else if (charm::pe_thread() == 0) charm::end();
+  if (round + 1 < ROUNDS) {
+    int next = round + 1;
+    cells->invoke(1 - c.i, 0, &next, sizeof(int));
+  } else if (GID == 0) {
+    printf("gpu-level forms: pe %d of %d, rounds %d, hits %d, bad %d\n", charm::my_pe(), charm::n_pes(), round + 1,
+           c.hits, *bad);
+    charm::end();
+  }
 }
 
 __device__ void charm::main(int argc, char** argv, size_t* argvs, int pe) {
@@ -31,9 +46,15 @@ __device__ void charm::main(int argc, char** argv, size_t* argvs, int pe) {
     cells = new charm::chare_proxy<Cell>();
     cells->add_entry_method<&on_msg>();
     cells->create(2);
-    data = new int[1024];
+    data = new int[N];
+    bad = new int;
+    *bad = 0;
   }
   BARRIER_LOCAL;
+  for (int i = charm::pe_thread(); i < N; i += charm::pe_threads()) data[i] = 0;
   charm::barrier();
-  if (pe == 0 && charm::is_gpu_level()) cells->invoke(0, 0);
+  if (pe == 0 && charm::is_gpu_level()) {
+    int first = 0;
+    cells->invoke(0, 0, &first, sizeof(int));
+  }
 }

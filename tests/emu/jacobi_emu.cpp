@@ -602,7 +602,7 @@ int run(int nx, int ny, int px, int py, int max_sweeps, int K, double tol, int n
   jac::prob_result res{};
   unsigned long long done = 0;
   std::vector<int> final_buf(nc, 0);
-  std::vector<unsigned long long> sweep_ns(4 * (size_t)n_pes, 0);
+  std::vector<unsigned long long> sweep_ns(8 * (size_t)n_pes, 0);
   g_app = suite::app_params{};
   g_app.id = suite::APP_JACOBI2D;
   g_app.a[0] = nc;

@@ -340,7 +340,7 @@ int serve_run(int n_pes, int threads, int n_req, unsigned long long seed, int wp
   std::vector<unsigned> done(max_inflight, 0);
   std::vector<int> bm(n_pes, wpp), sm(n_pes, 0), fin(n_workers, 0), ctl(32, 0);
   sm[0] = 1;
-  std::vector<unsigned long long> pe_ns(4 * (size_t)n_pes, 0);
+  std::vector<unsigned long long> pe_ns(8 * (size_t)n_pes, 0);
   g_app = suite::app_params{};
   g_app.id = suite::APP_JACOBI2D;
   g_app.a[0] = n_workers;

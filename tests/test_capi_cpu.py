@@ -64,3 +64,7 @@ def test_reference_examples_built():
         pytest.skip("reference tree not present")
     for ex in ("hello", "refnum", "pingpong"):
         assert os.path.exists(os.path.join(d, ex)), ex
+    # pingpong's GPU-level branch (the reference's default build) compiles and
+    # links unchanged too; it places its two chares with block_map[0] and
+    # block_map[n_pes / 2], so it needs two PEs, i.e. two GPUs, in that mode
+    assert os.path.exists(os.path.join(d, "pingpong_gpu_level"))

@@ -96,15 +96,23 @@ def test_reference_pingpong_links_and_runs():
     assert [int(l.split()[1]) for l in sizes] == [8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096]
 
 
-def test_reference_pingpong_gpu_level_links_and_runs():
-    # The example's GPU-level branch (the reference's default build: GID over
-    # the grid, BARRIER_LOCAL = charm::barrier_local()) asks for GPU-level
-    # mode: one PE of all blocks, both chares on it, every message handled
-    # by the whole grid.
-    r = _run_ref_example("pingpong_gpu_level", ["8", "4096", "20", "3"])
+
+def test_gpu_level_program_runs(tmp_path):
+    # A program in the reference's GPU-level style (tests/compile/
+    # gpu_level_forms.cu, built with -DCHARMING_GPU_LEVEL) gets GPU-level
+    # mode from the library's process main: one PE of all blocks, every
+    # entry method run by the whole grid, sends collective over the grid.
+    arch = "-gencode arch=compute_100a,code=sm_100a"
+    lib = os.path.join(ROOT, "charming_b200", "lib", "libcharming.a")
+    src = os.path.join(ROOT, "tests", "compile", "gpu_level_forms.cu")
+    obj, exe = tmp_path / "glf.o", tmp_path / "glf"
+    inc = os.path.join(ROOT, "include")
+    r = subprocess.run(f"nvcc -std=c++17 {arch} -rdc=true -DCHARMING_GPU_LEVEL -I{inc} -c {src} -o {obj} && "
+                       f"nvcc {arch} -rdc=true -Xnvlink -suppress-stack-size-warning -o {exe} {obj} {lib} -lcudart",
+                       shell=True, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    env = dict(os.environ, CHARMING_DEADLINE_S="60", CHARMING_IDLE_TIMEOUT_S="3")
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120, env=env)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     assert "GPU-level mode: 1 PE of" in r.stdout
-    inits = sorted(l for l in r.stdout.splitlines() if l.startswith("Chare ") and "init on PE" in l)
-    assert inits == ["Chare 0 init on PE 0", "Chare 1 init on PE 0"]
-    sizes = [l for l in r.stdout.splitlines() if l.startswith("Size ")]
-    assert [int(l.split()[1]) for l in sizes] == [8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096]
+    assert "gpu-level forms: pe 0 of 1, rounds 6, hits 3, bad 0" in r.stdout, r.stdout[-2000:]
