@@ -133,15 +133,18 @@ __device__ void d1_sweep(const float* __restrict__ a, float* __restrict__ o, int
     const int v = s * 32 + lane;
     const bool act = v < nv;
     const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-    auto ld = [&](int iy) { return act ? *reinterpret_cast<const float4*>(a + (size_t)iy * nx + 4 * v) : z; };
-    float4 U = ld(r0 - 1), M = ld(r0);
-    for (int iy = r0; iy < r1; iy++) {
-      const float4 D = ld(iy + 1);
+    // rows past the ghost row iy_end are never read (zeros stand in)
+    auto ld = [&](int iy) {
+      return act && iy <= iy_end ? *reinterpret_cast<const float4*>(a + (size_t)iy * nx + 4 * v) : z;
+    };
+    // output row iy from the rows above (U), at (M) and below (D)
+    auto row = [&](int iy, const float4& U, const float4& M, const float4& D) {
       float left = __shfl_up_sync(FULL, M.w, 1);
       float right = __shfl_down_sync(FULL, M.x, 1);
-      if (act && lane == 0 && v > 0) left = a[(size_t)iy * nx + 4 * v - 1];
-      if (act && lane == 31 && v + 1 < nv) right = a[(size_t)iy * nx + 4 * v + 4];
-      if (act) {
+      const bool out_row = act && iy < r1;  // the last step may run past the run
+      if (out_row && lane == 0 && v > 0) left = a[(size_t)iy * nx + 4 * v - 1];
+      if (out_row && lane == 31 && v + 1 < nv) right = a[(size_t)iy * nx + 4 * v + 4];
+      if (out_row) {
         float4 out;
         out.x = d1_stencil(M.y, left, D.x, U.x);
         out.y = d1_stencil(M.z, M.x, D.y, U.y);
@@ -157,8 +160,17 @@ __device__ void d1_sweep(const float* __restrict__ a, float* __restrict__ o, int
           if (4 * v + 3 >= 1 && 4 * v + 3 <= nx - 2) op[3] = out.w;
         }
       }
-      U = M;
-      M = D;
+    };
+    // four rows per step: their loads are in flight together
+    float4 U = ld(r0 - 1), M = ld(r0);
+    for (int iy = r0; iy < r1; iy += 4) {
+      const float4 b0 = ld(iy + 1), b1 = ld(iy + 2), b2 = ld(iy + 3), b3 = ld(iy + 4);
+      row(iy, U, M, b0);
+      row(iy + 1, M, b0, b1);
+      row(iy + 2, b0, b1, b2);
+      row(iy + 3, b1, b2, b3);
+      U = b2;
+      M = b3;
     }
   }
 }

@@ -1008,7 +1008,7 @@ __device__ int poll_inbox() {
       }
       return 1;
     }
-    if (ps->term || terminated()) {
+    if (ps->term) {
       publish_head(ps, me);
       return 0;
     }
@@ -1023,6 +1023,14 @@ __device__ int poll_inbox() {
       }
     }
     ++spins;
+    // The termination word is read every 16th poll, not on every one: every
+    // idle PE reading the same word at each poll makes its L2 slice a hot
+    // spot that slows the PEs still working (a pingpong on 2 or 4 PEs per SM
+    // took 20-70x longer).
+    if ((spins & 15) == 0 && terminated()) {
+      publish_head(ps, me);
+      return 0;
+    }
     if ((spins & 255) == 0) {
       unsigned long long now = globaltimer();
       if (now - ps->t0 > c_rt.deadline_ns) {
