@@ -87,7 +87,7 @@ class JacobiInfo(C.Structure):
         ("interior_points", u64), ("grid_bytes", u64), ("halo_msgs_per_sweep", u64),
         ("last_run_ms", f64), ("sweep_ms_max", f64), ("sweep_ms_mean", f64),
         ("send_ms_mean", f64), ("halo_ms_mean", f64), ("send_reserve_ms_mean", f64),
-        ("send_publish_ms_mean", f64),
+        ("send_publish_ms_mean", f64), ("send_setup_ms_mean", f64),
     ]
 
 

@@ -132,9 +132,10 @@ __shared__ charm::chare_proxy<JBlock>* jproxy;
 // kept on chip and stored through to japp::pe_ns() after every update (a
 // store only: no read of global memory on the message path).
 // Slots: 0 sweeps, 1 halo sends (all of send_halos), 2 halo entry methods,
-// 3 of the sends: taking ring space, 4 of the sends: publishing.
+// 3 of the sends: up to the ring space taken, 4 of the sends: publishing,
+// 5 of the sends: up to the reservation call.
 constexpr int PE_NS_SLOTS = 8;
-__shared__ unsigned long long s_pe_ns[5];
+__shared__ unsigned long long s_pe_ns[6];
 __device__ __forceinline__ void add_pe_ns(int k, unsigned long long ns) {
   s_pe_ns[k] += ns;
   japp::pe_ns()[PE_NS_SLOTS * blockIdx.x + k] = s_pe_ns[k];
@@ -170,7 +171,9 @@ __device__ double sweep_block(const jac::chare_desc& d, int cur, bool resid, int
                         L >= 1 && L <= d.depth,
                     CHARMING_ERR_APP, 8000 + cur, d.w))
     return 0.0;
-  unsigned long long t0 = charm::now_ns();
+  // phase timers: thread 0 alone reads the clock (a %globaltimer read by
+  // every thread of the block costs tens of microseconds)
+  const unsigned long long t0 = threadIdx.x == 0 ? charm::now_ns() : 0;
   if (L > 1) {
     int fixed = (d.nbr[jac::TOP] < 0 ? 1 : 0) | (d.nbr[jac::BOTTOM] < 0 ? 2 : 0) |
                 (d.nbr[jac::LEFT] < 0 ? 4 : 0) | (d.nbr[jac::RIGHT] < 0 ? 8 : 0);
@@ -263,7 +266,7 @@ __device__ void copy_rects(jac::block_view<T> g, const jac::region* e, T* const*
 // overlap (refnum = pass in halo_mode 1). All threads.
 template <typename T>
 __device__ void send_halos(JBlock& c, const jac::chare_desc& d) {
-  unsigned long long t0 = charm::now_ns();
+  const unsigned long long t0 = threadIdx.x == 0 ? charm::now_ns() : 0;
   int idx[jac::N_DIRS], dirs[jac::N_DIRS], refs[jac::N_DIRS];
   size_t bytes[jac::N_DIRS];
   jac::region e[jac::N_DIRS];
@@ -279,8 +282,9 @@ __device__ void send_halos(JBlock& c, const jac::chare_desc& d) {
     n++;
   }
   charm::message msg[jac::N_DIRS];
+  CHARM_PROF(if (threadIdx.x == 0) add_pe_ns(5, charm::now_ns() - t0);)
   const bool got = n > 0 && jproxy->alloc_msgs(msg, idx, bytes, n);
-  if (threadIdx.x == 0) add_pe_ns(3, charm::now_ns() - t0);
+  CHARM_PROF(if (threadIdx.x == 0) add_pe_ns(3, charm::now_ns() - t0);)
   if (got) {
     T* vals[jac::N_DIRS];
     for (int k = 0; k < n; k++)
@@ -293,9 +297,9 @@ __device__ void send_halos(JBlock& c, const jac::chare_desc& d) {
       hh->gen = c.gen;
     }
     copy_rects<T>(view<T>(d, c.cur), e, vals, n, false);
-    const unsigned long long tp = charm::now_ns();
+    CHARM_PROF(const unsigned long long tp = threadIdx.x == 0 ? charm::now_ns() : 0;)
     jproxy->invoke_msgs(idx, EP_HALO, msg, bytes, refs, n);
-    if (threadIdx.x == 0) add_pe_ns(4, charm::now_ns() - tp);
+    CHARM_PROF(if (threadIdx.x == 0) add_pe_ns(4, charm::now_ns() - tp);)
   }
   if (threadIdx.x == 0) add_pe_ns(1, charm::now_ns() - t0);
 }
@@ -504,7 +508,7 @@ __device__ void em_decision(JBlock& c, void* arg) {
 
 __device__ void suite::jacobi2d_main(int pe) {
   if (threadIdx.x == 0) {
-    for (int k = 0; k < 5; k++) s_pe_ns[k] = 0;
+    for (int k = 0; k < 6; k++) s_pe_ns[k] = 0;
     jproxy = new charm::chare_proxy<JBlock>();
     jproxy->add_entry_method<&em_start>();
     jproxy->add_entry_method<&em_halo>();

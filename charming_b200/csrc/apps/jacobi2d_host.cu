@@ -479,17 +479,18 @@ extern "C" int charming_jacobi2d_get_info(void* handle, charming_jacobi_info* ou
   std::vector<unsigned long long> ns(8 * h->block_map.size());
   cudaError_t e = cudaMemcpy(ns.data(), h->d_sweep_ns, 8 * ns.size(), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return check_cuda(e, "jacobi2d info");
-  double mx = 0, sum[5] = {0, 0, 0, 0, 0};
+  double mx = 0, sum[6] = {0, 0, 0, 0, 0, 0};
   int busy = 0;
   for (size_t p = 0; p < h->block_map.size(); p++) {
     mx = std::max(mx, (double)ns[8 * p]);
     if (h->block_map[p] > 0) {
-      for (int k = 0; k < 5; k++) sum[k] += (double)ns[8 * p + k];
+      for (int k = 0; k < 6; k++) sum[k] += (double)ns[8 * p + k];
       busy++;
     }
   }
   out->send_reserve_ms_mean = busy ? sum[3] / busy * 1e-6 : 0.0;
   out->send_publish_ms_mean = busy ? sum[4] / busy * 1e-6 : 0.0;
+  out->send_setup_ms_mean = busy ? sum[5] / busy * 1e-6 : 0.0;
   out->sweep_ms_max = mx * 1e-6;
   out->sweep_ms_mean = busy ? sum[0] / busy * 1e-6 : 0.0;
   out->send_ms_mean = busy ? sum[1] / busy * 1e-6 : 0.0;

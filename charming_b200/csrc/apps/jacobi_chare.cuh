@@ -225,7 +225,7 @@ __device__ void em_halo_t(JBlock& c, void* arg) {
   const jac::halo_hdr* hh = reinterpret_cast<const jac::halo_hdr*>(arg);
   if (!ensure_gen<T>(c, hh->gen)) return;
   if (c.done) return;
-  const unsigned long long t_em = charm::now_ns();
+  const unsigned long long t_em = threadIdx.x == 0 ? charm::now_ns() : 0;
   const jac::chare_desc& d = c.desc;
   // checked build: direction, length and sweep of the halo are consistent
   if (!CHARM_VERIFY(hh->dir >= 0 && hh->dir < jac::N_DIRS && d.nbr[hh->dir] >= 0, CHARMING_ERR_APP,

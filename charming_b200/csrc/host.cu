@@ -381,6 +381,10 @@ int charming_init(const charming_config* cfg_in) {
   ds.idle_timeout_ns = (unsigned long long)(cfg.idle_timeout_s * 1e9);
   ds.free_chares_at_exit = cfg.free_chares_at_exit;
   ds.gpu_level = cfg.gpu_level ? 1 : 0;
+  // pause between the inbox polls of a PE idle for 32 polls
+  // (CHARMING_IDLE_SLEEP_NS; 0 polls without pausing)
+  ds.idle_sleep_ns = 2000;
+  if (const char* ev = getenv("CHARMING_IDLE_SLEEP_NS")) ds.idle_sleep_ns = (unsigned)strtoul(ev, nullptr, 10);
   ds.n_blocks = n_blocks;
 
   int rc;

@@ -131,6 +131,7 @@ struct device_state {
   unsigned long long user_heap_bytes;
   user_block* user_blocks;             // [n_pes][user_blocks_max]
   int user_blocks_max;
+  unsigned int idle_sleep_ns;          // pause between inbox polls of a PE idle for 32 polls
   int gpu_level;                       // 1: all blocks form PE 0 (group_state below)
   int n_blocks;                        // thread blocks of the launch (n_pes when 0)
   struct group_state* gl;              // GPU-level mode only
@@ -357,6 +358,17 @@ __device__ __forceinline__ bool verify(bool ok, int code, int a, int b) {
 #define CHARM_VERIFY(cond, code, a, b) (::charm::rt::verify((cond), (code), (int)(a), (int)(b)))
 #else
 #define CHARM_VERIFY(cond, code, a, b) (true)
+#endif
+
+// Fine-grained timers of the send path (ticket atomics, ring-space waits,
+// the phases of the Jacobi halo sends): only in a build with
+// -DCHARMING_PROFILE (make VARIANT=_prof EXTRA_NVFLAGS=-DCHARMING_PROFILE,
+// selected with CHARMING_LIB); the statistics read 0 otherwise. Their timer
+// reads cost the headline launch about 7 %.
+#ifdef CHARMING_PROFILE
+#define CHARM_PROF(...) __VA_ARGS__
+#else
+#define CHARM_PROF(...)
 #endif
 
 // Message bytes -> ring cells.

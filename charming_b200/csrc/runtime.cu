@@ -278,13 +278,12 @@ __device__ unsigned char* wait_space(int dst, unsigned long long t, unsigned lon
 // DEFER_AFTER_NS) or nullptr (error recorded, or the run is ending).
 __device__ unsigned char* reserve(int dst, unsigned long long bytes, unsigned long long* ticket) {
   if (!send_allowed(dst, bytes)) return nullptr;
-  pe_state* ps = pes();
-  const unsigned long long t0 = globaltimer();
+  CHARM_PROF(pe_state* ps = pes(); const unsigned long long t0 = globaltimer();)
   const unsigned long long t = atomicAdd(&c_rt.tail[dst].v, (unsigned long long)cells_for(bytes));
-  const unsigned long long t1 = globaltimer();
+  CHARM_PROF(const unsigned long long t1 = globaltimer();)
   unsigned char* m = wait_space(dst, t, bytes, ticket);
-  atomicAdd_block(&ps->stats[ST_TICKET_NS], t1 - t0);
-  atomicAdd_block(&ps->stats[ST_SPACE_NS], globaltimer() - t1);
+  CHARM_PROF(atomicAdd_block(&ps->stats[ST_TICKET_NS], t1 - t0);
+             atomicAdd_block(&ps->stats[ST_SPACE_NS], globaltimer() - t1);)
   return m;
 }
 
@@ -644,22 +643,20 @@ __device__ bool charm::alloc_user_msgs(message* msgs, const int* dst_pes,
         }
       }
       unsigned long long base = 0;
-      const unsigned long long ta = globaltimer();
+      CHARM_PROF(const unsigned long long ta = k == 0 ? globaltimer() : 0;)
       if (ok && k == leader) base = atomicAdd(&c_rt.tail[dst_pes[k]].v, (unsigned long long)tot);
       base = __shfl_sync(FULL, base, leader);
-      __syncwarp();
-      const unsigned long long tb = globaltimer();
+      CHARM_PROF(__syncwarp(); const unsigned long long tb = k == 0 ? globaltimer() : 0;)
       if (act) {
         unsigned long long t = 0;
         ps->bm_ptr[k] = ok ? wait_space(dst_pes[k], base + pre, bytes, &t) : nullptr;
         ps->bm_tick[k] = t;
         ps->bm_bytes[k] = bytes;
       }
-      __syncwarp();
-      if (k == 0) {
+      CHARM_PROF(__syncwarp(); if (k == 0) {
         ps->stats[ST_TICKET_NS] += tb - ta;
         ps->stats[ST_SPACE_NS] += globaltimer() - tb;
-      }
+      })
     }
   } else {
     // blocks under a warp (host checks): thread by thread, in batch order
@@ -1023,11 +1020,13 @@ __device__ int poll_inbox() {
       }
     }
     ++spins;
-    // The termination word is read every 16th poll, not on every one: every
-    // idle PE reading the same word at each poll makes its L2 slice a hot
-    // spot that slows the PEs still working (a pingpong on 2 or 4 PEs per SM
-    // took 20-70x longer).
-    if ((spins & 15) == 0 && terminated()) {
+    // A PE idle for 32 polls pauses between polls: the polls of many idle
+    // PEs slowed the PEs still working (a pingpong on 2 or 4 PEs per SM took
+    // 40-100x longer, the batched set on 4 PEs per SM a third longer). The
+    // termination word is read every 16th poll, and at every paused one.
+    const bool paused = c_rt.idle_sleep_ns && spins > 32;
+    if (paused) __nanosleep(c_rt.idle_sleep_ns);
+    if ((paused || (spins & 15) == 0) && terminated()) {
       publish_head(ps, me);
       return 0;
     }

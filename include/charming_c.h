@@ -134,7 +134,8 @@ typedef struct charming_stats {
   uint64_t deferred;         /* sends moved to the sender's outbox because
                                 the destination ring stayed full         */
   double ticket_ms;          /* mean over PEs: reserving thread waiting for
-                                its inbox-ticket atomics                 */
+                                its inbox-ticket atomics (this and the
+                                next: profiling builds only, else 0)     */
   double space_ms;           /* mean over PEs: then for ring space (a stale
                                 head cache refreshed, or a full ring)    */
 } charming_stats;
@@ -199,8 +200,11 @@ typedef struct charming_jacobi_info {
   double sweep_ms_mean;       /* last run: mean over busy PEs              */
   double send_ms_mean;        /* last run: mean time packing/sending halos */
   double halo_ms_mean;        /* last run: mean time in halo entry methods */
+  /* the next three: builds with -DCHARMING_PROFILE only (else 0) */
   double send_reserve_ms_mean;  /* of send_ms_mean: taking the ring space    */
   double send_publish_ms_mean;  /* of send_ms_mean: publishing the messages  */
+  double send_setup_ms_mean;    /* of send_reserve_ms_mean: before the
+                                   reservation call                         */
 } charming_jacobi_info;
 
 /* Decomposes the problems into chares (reference decomposition:
