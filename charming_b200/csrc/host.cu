@@ -161,8 +161,8 @@ int collect_run(double kernel_ms) {
   }
   s.loop_ms = (tmax > tmin && tmin != ~0ULL) ? (tmax - tmin) * 1e-6 : 0.0;
   double idle = 0;
-  for (int p = 0; p < g.inf.n_pes; p++) idle += (double)st[(size_t)p * N_STATS + ST_IDLE_NS];
-  s.idle_ms = g.inf.n_pes ? idle / g.inf.n_pes * 1e-6 : 0.0;
+  for (int p = 0; p < g.inf.n_pes; p++) idle += (double)st[(size_t)p * N_STATS + ST_IDLE_CYC];
+  s.idle_ms = (g.inf.n_pes && g.prop.clockRate > 0) ? idle / g.inf.n_pes / (double)g.prop.clockRate : 0.0;
   double em = 0;
   for (int p = 0; p < g.inf.n_pes; p++) em += (double)st[(size_t)p * N_STATS + ST_EM_CYC];
   s.em_ms = (g.inf.n_pes && g.prop.clockRate > 0) ? em / g.inf.n_pes / (double)g.prop.clockRate : 0.0;

@@ -85,7 +85,7 @@ enum : int {
   ST_IDLE_POLLS,      // empty inbox polls
   ST_SPACE_WAITS,     // sends that waited for ring space
   ST_LOOP_NS,         // ns spent in the scheduler loop
-  ST_IDLE_NS,         // ns spent waiting on an empty inbox
+  ST_IDLE_CYC,        // SM cycles spent waiting on an empty inbox
   ST_EM_CYC,          // SM cycles spent inside entry methods
   ST_DEFERRED,        // sends moved to the outbox (destination ring full)
   ST_TICKET_NS,       // ns the reserving thread waited for its ticket atomics
@@ -223,6 +223,8 @@ struct pe_state {
   unsigned int gl_seq;                 // GPU-level mode: collective calls of this block
   int bar_ok;                          // the last grid barrier completed
   unsigned long long stamped_delivered;  // deliveries at the last progress stamp
+  unsigned long long idle_sum;         // PE 0: sum of all progress counters at the last check
+  unsigned long long idle_change_ns;   // PE 0: when that sum last changed
   unsigned long long slow_check_ns;    // last host-stop / idle-timeout check
   unsigned long long idle_checks;
   chare_proxy_base* pcache[PROXY_CACHE];  // proxies[0..PROXY_CACHE) of this PE's table

@@ -381,7 +381,7 @@ __device__ __forceinline__ void publish_head(pe_state* ps, int me) {
 
 // Thread 0: the progress stamp the idle-timeout check reads.
 __device__ __forceinline__ void stamp_progress(int me) {
-  st_relaxed_u64(&c_rt.progress[me], globaltimer());
+  st_relaxed_u64(&c_rt.progress[me], pes()->stats[ST_DELIVERED]);
 }
 
 } // namespace
@@ -925,12 +925,13 @@ __device__ unsigned long long stash_next_ready() {
 // idle_timeout_ns (e.g. a program that never calls end()).
 __device__ void check_idle_timeout(unsigned long long now) {
   if (c_rt.idle_timeout_ns == 0) return;
-  unsigned long long latest = pes()->t0;
-  for (int p = 0; p < c_rt.n_pes; p++) {
-    unsigned long long v = ld_relaxed_u64(&c_rt.progress[p]);
-    if (v > latest) latest = v;
-  }
-  if (now > latest && now - latest > c_rt.idle_timeout_ns) {
+  pe_state* ps = pes();
+  unsigned long long sum = 0;
+  for (int p = 0; p < c_rt.n_pes; p++) sum += ld_relaxed_u64(&c_rt.progress[p]);
+  if (sum != ps->idle_sum) {
+    ps->idle_sum = sum;
+    ps->idle_change_ns = now;
+  } else if (now - ps->idle_change_ns > c_rt.idle_timeout_ns) {
     set_error(CHARMING_ERR_IDLE_TIMEOUT, 0, 0);
   }
 }
@@ -993,7 +994,7 @@ __device__ int poll_inbox() {
   unsigned long long idle_t0 = 0;
   while (true) {
     if (ld_acquire_u64(f) == h + 1) {
-      if (idle_t0) ps->stats[ST_IDLE_NS] += globaltimer() - idle_t0;
+      if (idle_t0) ps->stats[ST_IDLE_CYC] += (unsigned long long)clock64() - idle_t0;
       // a PE that always has a message (a chare that keeps calling itself)
       // still sees the end of the run and its deadline
       if ((++ps->busy_polls & 63) == 0) {
@@ -1010,7 +1011,7 @@ __device__ int poll_inbox() {
       return 0;
     }
     if (!idle_t0) {  // about to wait: the senders and the idle check see where we are
-      idle_t0 = globaltimer();
+      idle_t0 = (unsigned long long)clock64() | 1;
       publish_head(ps, me);
       // deliveries since the last stamp count as progress (a return to the
       // loop for the outbox or async waits does not)
@@ -1053,7 +1054,7 @@ __device__ int poll_inbox() {
       }
       ps->stats[ST_IDLE_POLLS] += 256;
       if ((ps->ob_count > 0 && outbox_head_ready()) || ps->aw_count > 0) {
-        ps->stats[ST_IDLE_NS] += now - idle_t0;
+        ps->stats[ST_IDLE_CYC] += (unsigned long long)clock64() - idle_t0;
         return 2;  // deferred sends can go out, or async waits to check
       }
     }
@@ -1329,6 +1330,8 @@ charming_scheduler_kernel(int argc, char** argv, size_t* argvs) {
     ps->rq_n = ps->rq_pos = 0;
     ps->rq_over = 1;  // no list yet: scan
     ps->stamped_delivered = ~0ULL;
+    ps->idle_sum = ~0ULL;
+    ps->idle_change_ns = ps->t0;
     ps->slow_check_ns = ps->t0;
     ps->idle_checks = 0;
     for (int i = 0; i < PROXY_CACHE; i++) ps->pcache[i] = nullptr;

@@ -128,7 +128,7 @@ typedef struct charming_stats {
   int status;                /* status code of the run                   */
   int err_pe, err_info0, err_info1;
   double idle_ms;            /* mean over PEs: time waiting on an empty
-                                inbox                                    */
+                                inbox (SM cycles at the nominal clock)   */
   double em_ms;              /* mean over PEs: time inside entry methods
                                 (SM cycles at the nominal clock)         */
   uint64_t deferred;         /* sends moved to the sender's outbox because
