@@ -97,6 +97,8 @@ struct d1_halo {  // message payload header; nx-2 floats follow
   int pad[2];
 };
 
+constexpr int D1_STEP = 8;  // rows loaded together per warp step
+
 __device__ __forceinline__ float d1_stencil(float r, float l, float d, float u) {
   return __fmul_rn(__fadd_rn(__fadd_rn(__fadd_rn(r, l), d), u), 0.25f);
 }
@@ -105,8 +107,9 @@ __device__ __forceinline__ float d1_stencil(float r, float l, float d, float u) 
 // [1, iy_end) of o from a (row pitch nx, nx % 4 == 0). Work items are
 // (column strip of 32 float4, run of rows); each warp walks its items'
 // rows downwards, the three rows around the output in registers,
-// neighbours across lanes by shuffle. Row runs split the strips when there
-// are more warps than strips (a GPU-level PE has thousands).
+// neighbours across lanes by shuffle, D1_STEP rows loaded at once. Row runs
+// split the strips when there are more warps than strips (a GPU-level PE
+// has thousands).
 __device__ void d1_sweep(const float* __restrict__ a, float* __restrict__ o, int nx, int iy_end) {
   constexpr unsigned FULL = 0xffffffffu;
   const int tid = charm::pe_thread(), nthreads = charm::pe_threads();
@@ -161,16 +164,18 @@ __device__ void d1_sweep(const float* __restrict__ a, float* __restrict__ o, int
         }
       }
     };
-    // four rows per step: their loads are in flight together
+    // D1_STEP rows per step: their loads are in flight together
     float4 U = ld(r0 - 1), M = ld(r0);
-    for (int iy = r0; iy < r1; iy += 4) {
-      const float4 b0 = ld(iy + 1), b1 = ld(iy + 2), b2 = ld(iy + 3), b3 = ld(iy + 4);
-      row(iy, U, M, b0);
-      row(iy + 1, M, b0, b1);
-      row(iy + 2, b0, b1, b2);
-      row(iy + 3, b1, b2, b3);
-      U = b2;
-      M = b3;
+    for (int iy = r0; iy < r1; iy += D1_STEP) {
+      float4 b[D1_STEP];
+#pragma unroll
+      for (int k = 0; k < D1_STEP; k++) b[k] = ld(iy + 1 + k);
+      row(iy, U, M, b[0]);
+      row(iy + 1, M, b[0], b[1]);
+#pragma unroll
+      for (int k = 2; k < D1_STEP; k++) row(iy + k, b[k - 2], b[k - 1], b[k]);
+      U = b[D1_STEP - 2];
+      M = b[D1_STEP - 1];
     }
   }
 }

@@ -14,7 +14,8 @@
 //   jacobi3d_async_kernel (grids of at least one 34 x 18 box in x and y):
 //     the tile's planes, rim included, stream through a ring of J3_S
 //     shared-memory slots by per-thread asynchronous copies (cp.async, one
-//     commit group per plane), J3_S - 2 planes ahead of the one computed.
+//     commit group per plane), J3_S - 2 planes ahead of the one computed
+//     (J3_S = 8 by default).
 //     Each input value is read from DRAM once per sweep (16 B per lattice
 //     update with the store); the rim cells come from L2.
 //   jacobi3d_kernel (any shape): per-thread loads, the planes below and
@@ -24,12 +25,14 @@
 #ifndef CHARMING_HOST_EMULATION
 #include "jacobi_sweep.cuh"
 #include "../host.cuh"
+#include <cmath>
+#include <cstdlib>
 
 namespace {
 
 constexpr int J3_TX = 32, J3_TY = 16;
 constexpr int J3_BW = J3_TX + 2, J3_BH = J3_TY + 2;          // tensor box: tile + rim
-constexpr int J3_S = 6;                                      // plane slots
+constexpr int J3_S_DEFAULT = 8;                              // plane slots
 
 __device__ __forceinline__ double j3_stencil(double c, double xm, double xp, double ym, double yp, double zm,
     double zp) {
@@ -44,6 +47,7 @@ __device__ __forceinline__ double j3_stencil(double c, double xm, double xp, dou
 // Before output plane z is computed, planes up to z + J3_S - 2 are issued
 // and wait_group leaves J3_S - 3 of them in flight, so planes z-1, z, z+1
 // have landed.
+template <int J3_S>
 __global__ void __launch_bounds__(J3_TX * J3_TY, 3) jacobi3d_async_kernel(const double* __restrict__ in,
     double* __restrict__ out, int nx, int ny, int nz, int zrun) {
   extern __shared__ __align__(16) double j3_slots[];  // [J3_S][J3_BH][J3_BW]
@@ -132,7 +136,7 @@ __global__ void __launch_bounds__(J3_TX * J3_TY) jacobi3d_kernel(const double* _
 // with at least one full box in x and y takes it.
 bool async_shape_ok(int nx, int ny) { return nx + 2 >= J3_BW && ny + 2 >= J3_BH; }
 
-constexpr size_t J3_ASYNC_SMEM = (size_t)J3_S * J3_BW * J3_BH * 8;
+constexpr size_t j3_async_smem(int stages) { return (size_t)stages * J3_BW * J3_BH * 8; }
 
 // z planes per block for the register kernel: enough blocks to fill the GPU
 // several times over
@@ -146,14 +150,67 @@ int jacobi3d_zrun(int nx, int ny, int nz, int n_sms) {
   return zrun;
 }
 
-// z planes per block for the pipelined kernel: one wave of resident blocks
-// when the tiles leave room for it (each run adds two planes of reads).
+// z planes per block for the pipelined kernel. Blocks = tiles x runs; the
+// GPU holds `slots` of them at once, so the launch takes ceil(blocks /
+// slots) waves and the last one may run part-empty, while every run reads
+// two planes more than it writes. Picks the run count (1..32) with the best
+// product of wave fill and plane efficiency.
 int jacobi3d_async_zrun(int nx, int ny, int nz, int n_sms, int per_sm) {
   const long long tiles = (long long)((nx + J3_TX - 1) / J3_TX) * ((ny + J3_TY - 1) / J3_TY);
-  long long runs = (long long)n_sms * per_sm / tiles;
-  if (runs < 1) runs = 1;
-  if (runs > nz / 8) runs = nz / 8 > 0 ? nz / 8 : 1;
-  return (int)((nz + runs - 1) / runs);
+  const double slots = (double)n_sms * (per_sm > 0 ? per_sm : 1);
+  int best_zrun = nz;
+  double best = -1.0;
+  for (int runs = 1; runs <= 32; runs++) {
+    const int zrun = (nz + runs - 1) / runs;
+    if (zrun < 8 && runs > 1) break;
+    const long long blocks = tiles * ((nz + zrun - 1) / zrun);
+    const double waves = (double)blocks / slots;
+    const double fill = waves / std::ceil(waves);
+    const double eff = fill * zrun / (zrun + 2.0);
+    if (eff > best + 1e-9) {
+      best = eff;
+      best_zrun = zrun;
+    }
+  }
+  return best_zrun;
+}
+
+// Stage count of the pipelined kernel: CHARMING_J3_STAGES (6, 8, 10 or 12)
+// or J3_S_DEFAULT.
+int jacobi3d_stages() {
+  static int stages = 0;
+  if (!stages) {
+    stages = J3_S_DEFAULT;
+    if (const char* ev = getenv("CHARMING_J3_STAGES")) {
+      const int v = atoi(ev);
+      if (v == 6 || v == 8 || v == 10 || v == 12) stages = v;
+    }
+  }
+  return stages;
+}
+
+template <int S>
+cudaError_t jacobi3d_async_sweeps(double*& a, double*& b, int nx, int ny, int nz, int sweeps, int n_sms,
+    cudaStream_t s) {
+  int per_sm = 0;
+  cudaError_t e = cudaSuccess;
+  if (j3_async_smem(S) > 48 * 1024)
+    e = cudaFuncSetAttribute((const void*)jacobi3d_async_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)j3_async_smem(S));
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi3d_async_kernel<S>, J3_TX * J3_TY,
+                                                      j3_async_smem(S));
+  if (e != cudaSuccess) return e;
+  const int zrun = jacobi3d_async_zrun(nx, ny, nz, n_sms, per_sm);
+  const dim3 block(J3_TX, J3_TY), grid((nx + J3_TX - 1) / J3_TX, (ny + J3_TY - 1) / J3_TY, (nz + zrun - 1) / zrun);
+  for (int k = 0; k < sweeps && e == cudaSuccess; k++) {
+    jacobi3d_async_kernel<S><<<grid, block, j3_async_smem(S), s>>>(a, b, nx, ny, nz, zrun);
+    e = cudaGetLastError();
+    double* t = a;
+    a = b;
+    b = t;
+  }
+  return e;
 }
 
 // `sweeps` sweeps alternating between a and b (both hold the input,
@@ -163,18 +220,11 @@ double* jacobi3d_run(double* a, double* b, int nx, int ny, int nz, int sweeps, c
   *err = cudaSuccess;
   const dim3 block(J3_TX, J3_TY);
   if (async_shape_ok(nx, ny)) {
-    int per_sm = 0;
-    *err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi3d_async_kernel, J3_TX * J3_TY,
-                                                         J3_ASYNC_SMEM);
-    if (*err != cudaSuccess) return a;
-    const int zrun = jacobi3d_async_zrun(nx, ny, nz, n_sms, per_sm > 0 ? per_sm : 1);
-    const dim3 grid((nx + J3_TX - 1) / J3_TX, (ny + J3_TY - 1) / J3_TY, (nz + zrun - 1) / zrun);
-    for (int k = 0; k < sweeps && *err == cudaSuccess; k++) {
-      jacobi3d_async_kernel<<<grid, block, J3_ASYNC_SMEM, s>>>(a, b, nx, ny, nz, zrun);
-      *err = cudaGetLastError();
-      double* t = a;
-      a = b;
-      b = t;
+    switch (jacobi3d_stages()) {
+      case 6: *err = jacobi3d_async_sweeps<6>(a, b, nx, ny, nz, sweeps, n_sms, s); break;
+      case 10: *err = jacobi3d_async_sweeps<10>(a, b, nx, ny, nz, sweeps, n_sms, s); break;
+      case 12: *err = jacobi3d_async_sweeps<12>(a, b, nx, ny, nz, sweeps, n_sms, s); break;
+      default: *err = jacobi3d_async_sweeps<8>(a, b, nx, ny, nz, sweeps, n_sms, s); break;
     }
     return a;
   }
