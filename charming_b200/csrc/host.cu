@@ -325,11 +325,13 @@ int charming_init(const charming_config* cfg_in) {
                 (long)fa.sharedSizeBytes - (long)g.prop.reservedSharedMemPerBlock;
   long smem_total = per_block < per_sm ? per_block : per_sm;
   // A cap leaves the rest of the SM's 256 KB of L1/shared storage to the L1
-  // cache (local memory and global loads).
-  if (const char* ev = getenv("CHARMING_SMEM_PER_PE")) {
-    long cap = strtol(ev, nullptr, 10);
-    if (cap > 0 && cap < smem_total) smem_total = cap;
-  }
+  // cache (local memory and global loads). 96 KiB holds the runtime state,
+  // the object arena and the deep pass's cp.async rings of 16 warps (64 KiB),
+  // and the L1 it frees made the headline launch 4 % faster (the halo copies
+  // and the spills hit it). CHARMING_SMEM_PER_PE sets another cap (0: none).
+  long cap = 96 << 10;
+  if (const char* ev = getenv("CHARMING_SMEM_PER_PE")) cap = strtol(ev, nullptr, 10);
+  if (cap > 0 && cap < smem_total) smem_total = cap;
   smem_total = smem_total / 128 * 128;
   if (smem_arena > smem_total / 4) smem_arena = (int)(smem_total / 4) / 128 * 128;
   if (smem_total < smem_state + smem_arena + 1024) {

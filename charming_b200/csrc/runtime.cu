@@ -1025,7 +1025,8 @@ __device__ int poll_inbox() {
     // PEs slowed the PEs still working (a pingpong on 2 or 4 PEs per SM took
     // 40-100x longer, the batched set on 4 PEs per SM a third longer). The
     // termination word is read every 16th poll, and at every paused one.
-    const bool paused = c_rt.idle_sleep_ns && spins > 32;
+    // (not while async waits or deferred sends need the periodic checks below)
+    const bool paused = c_rt.idle_sleep_ns && spins > 32 && ps->aw_count == 0 && ps->ob_count == 0;
     if (paused) __nanosleep(c_rt.idle_sleep_ns);
     if ((paused || (spins & 15) == 0) && terminated()) {
       publish_head(ps, me);
