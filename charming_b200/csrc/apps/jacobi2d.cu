@@ -87,7 +87,10 @@ struct JBlock : charm::chare {
   int sent;          // last pass whose boundary went to the neighbours
   int started;       // the start message has been processed
   int got[2];        // halos received for the pass of each parity
-  int nbr_count;
+  int gotx[2];       // of which left/right halos (two-phase exchange)
+  int nbr_count;     // halos per pass
+  int nbx;           // of which left/right (two-phase exchange)
+  int sent_y;        // last pass whose top/bottom halos went out (two-phase)
   int done;
   int waiting;       // parked until the decision of check iter/K - 1 arrives
   // residual tree state for the check in progress
@@ -116,6 +119,9 @@ struct JBlock : charm::chare {
     checks = 0;
     gen = g;
     got[0] = got[1] = 0;
+    gotx[0] = gotx[1] = 0;
+    nbx = 0;
+    sent_y = -1;
     child_got[0] = child_got[1] = 0;
     child_val[0] = child_val[1] = 0.0;
   }
@@ -260,12 +266,27 @@ __device__ void copy_rects(jac::block_view<T> g, const jac::region* e, T* const*
   }
 }
 
+// Thread 0: the chare's halo counts per pass (all its neighbours; with the
+// two-phase exchange the corner directions have none).
+__device__ void count_nbrs(JBlock& c, const jac::chare_desc& d) {
+  int n = 0, nx = 0;
+  for (int k = 0; k < jac::N_DIRS; k++) {
+    if (d.nbr[k] < 0) continue;
+    n++;
+    if (d.ext > 0 && (k == jac::LEFT || k == jac::RIGHT)) nx++;
+  }
+  c.nbr_count = n;
+  c.nbx = nx;
+}
+
 // Packs the boundary regions of buf[cur] for every neighbour straight into
 // their inbox rings (zero-copy) and publishes them together: the ring
 // reservations, the packing loads and the publishing fences of the messages
-// overlap (refnum = pass in halo_mode 1). All threads.
+// overlap (refnum = pass in halo_mode 1). phase 0: every neighbour (the
+// one-phase exchange); 1: left and right; 2: top and bottom, with the ghost
+// columns the left/right halos of this pass filled. All threads.
 template <typename T>
-__device__ void send_halos(JBlock& c, const jac::chare_desc& d) {
+__device__ void send_halos(JBlock& c, const jac::chare_desc& d, int phase = 0) {
   const unsigned long long t0 = threadIdx.x == 0 ? charm::now_ns() : 0;
   int idx[jac::N_DIRS], dirs[jac::N_DIRS], refs[jac::N_DIRS];
   size_t bytes[jac::N_DIRS];
@@ -274,7 +295,9 @@ __device__ void send_halos(JBlock& c, const jac::chare_desc& d) {
   const bool tagged = japp::halo_mode() == 1;
   for (int dir = 0; dir < jac::N_DIRS; dir++) {
     if (d.nbr[dir] < 0) continue;
-    e[n] = jac::edge_region(dir, d.depth, d.w, d.h);
+    if (phase == 1 && dir != jac::LEFT && dir != jac::RIGHT) continue;
+    if (phase == 2 && dir != jac::TOP && dir != jac::BOTTOM) continue;
+    e[n] = jac::halo_edge(dir, d);
     idx[n] = d.nbr[dir];
     dirs[n] = dir;
     refs[n] = tagged ? c.pass : -1;
@@ -309,7 +332,7 @@ template <typename T>
 __device__ void unpack_halo(JBlock& c, const jac::chare_desc& d, const void* arg) {
   const jac::halo_hdr* hh = reinterpret_cast<const jac::halo_hdr*>(arg);
   T* vals = const_cast<T*>(reinterpret_cast<const T*>(reinterpret_cast<const char*>(arg) + sizeof(jac::halo_hdr)));
-  jac::region gr = jac::ghost_region(hh->dir, d.depth, d.w, d.h);
+  jac::region gr = jac::halo_ghost(hh->dir, d);
   copy_rects<T>(view<T>(d, hh->pass & 1), &gr, &vals, 1, true);
 }
 
@@ -426,9 +449,7 @@ __device__ int ensure_gen(JBlock& c, unsigned gen) {
   }
   if (threadIdx.x == 0) {
     c.reset(gen);
-    int nb = 0;
-    for (int k = 0; k < jac::N_DIRS; k++) nb += d.nbr[k] >= 0;
-    c.nbr_count = nb;
+    count_nbrs(c, d);
     c.started = 1;
   }
   __syncthreads();

@@ -108,6 +108,7 @@ __device__ void advance(JBlock& c, const jac::chare_desc& d) {
   double part = sweep_block<T>(d, c.cur, resid, L);
   if (threadIdx.x == 0) {
     c.got[c.pass & 1] = 0;
+    c.gotx[c.pass & 1] = 0;
     c.cur ^= 1;
     c.pass++;
     c.iter += L;
@@ -129,7 +130,7 @@ template <typename T>
 __device__ void pump(JBlock& c, const jac::chare_desc& d) {
   const jac::prob_desc& p = c.prob;
   __shared__ int s_act;
-  enum { IDLE = 0, SEND = 1, FIN = 2, SWEEP = 3, SELF = 4 };
+  enum { IDLE = 0, SEND = 1, FIN = 2, SWEEP = 3, SELF = 4, SEND_Y = 5 };
   // lattice updates a chare without neighbours may run in one entry method
   // (a message round trip costs about as much as 20 K of them)
   long long self_budget = 1ll << 18;
@@ -163,7 +164,12 @@ __device__ void pump(JBlock& c, const jac::chare_desc& d) {
           c.sent = c.pass;
           if (act == SEND && japp::halo_mode() == 1) jproxy->set_refnum(c.i, c.pass);
         }
-      } else if (c.nbr_count > 0 && c.got[c.pass & 1] == c.nbr_count) {
+      } else if (d.ext > 0 && c.sent_y < c.pass && c.gotx[c.pass & 1] == c.nbx) {
+        // two-phase: the left/right ghost columns of this pass are in, so
+        // the top/bottom halos can carry the corners
+        act = SEND_Y;
+        c.sent_y = c.pass;
+      } else if (c.nbr_count > 0 && c.got[c.pass & 1] == c.nbr_count && (d.ext == 0 || c.sent_y == c.pass)) {
         act = SWEEP;
       }
       s_act = act;
@@ -177,7 +183,9 @@ __device__ void pump(JBlock& c, const jac::chare_desc& d) {
       return;
     }
     if (act == SEND) {
-      send_halos<T>(c, d);
+      send_halos<T>(c, d, d.ext > 0 ? 1 : 0);
+    } else if (act == SEND_Y) {
+      send_halos<T>(c, d, 2);
     } else if (act == SELF) {
       // no neighbours: passes back to back up to a work budget, then one
       // message to itself, so other chares of the PE run in between
@@ -211,9 +219,7 @@ __device__ void em_start_t(JBlock& c, void* arg) {
   }
   const jac::chare_desc& d = c.desc;
   if (threadIdx.x == 0) {
-    int n = 0;
-    for (int k = 0; k < jac::N_DIRS; k++) n += d.nbr[k] >= 0;
-    c.nbr_count = n;
+    count_nbrs(c, d);
     c.started = 1;
   }
   __syncthreads();
@@ -230,8 +236,7 @@ __device__ void em_halo_t(JBlock& c, void* arg) {
   // checked build: direction, length and sweep of the halo are consistent
   if (!CHARM_VERIFY(hh->dir >= 0 && hh->dir < jac::N_DIRS && d.nbr[hh->dir] >= 0, CHARMING_ERR_APP,
                     1000 + hh->dir, c.i) ||
-      !CHARM_VERIFY(hh->len == jac::ghost_region(hh->dir, d.depth, d.w, d.h).nr *
-                                   jac::ghost_region(hh->dir, d.depth, d.w, d.h).nc,
+      !CHARM_VERIFY(hh->len == jac::halo_ghost(hh->dir, d).nr * jac::halo_ghost(hh->dir, d).nc,
                     CHARMING_ERR_APP, 2000 + hh->dir, hh->len) ||
       !CHARM_VERIFY(hh->pass == c.pass || hh->pass == c.pass + 1, CHARMING_ERR_APP,
                     3000 + (hh->pass - c.pass), c.i))
@@ -239,6 +244,7 @@ __device__ void em_halo_t(JBlock& c, void* arg) {
   unpack_halo<T>(c, d, arg);
   if (threadIdx.x == 0) {
     c.got[hh->pass & 1]++;
+    if (hh->dir == jac::LEFT || hh->dir == jac::RIGHT) c.gotx[hh->pass & 1]++;
     (void)CHARM_VERIFY(c.got[hh->pass & 1] <= jac::N_DIRS, CHARMING_ERR_APP, 4000 + c.got[hh->pass & 1], c.i);
   }
   __syncthreads();

@@ -13,6 +13,7 @@
 #pragma once
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstdint>
 #include <functional>
 #include <numeric>
@@ -42,6 +43,13 @@ struct layout {
 // Sweeps per exchange chosen when none is requested: deeper passes mean
 // fewer messages, but the wavefront's registers spill beyond this.
 constexpr int DEPTH_AUTO = 6;
+
+// Halos at ghost depth > 1 go in two phases without corner messages unless
+// CHARMING_HALO_CORNERS=1 asks for the one-phase exchange with them.
+inline bool halo_corner_messages() {
+  const char* ev = getenv("CHARMING_HALO_CORNERS");
+  return ev && ev[0] == '1';
+}
 
 // Ghost depth of a problem whose smallest chare is wmin x hmin. Automatic
 // choice: DEPTH_AUTO, or with a residual period K the balanced split of K
@@ -117,10 +125,15 @@ inline bool build_layout(const charming_jacobi_problem* probs, int n, int side, 
         d.nbr[BOTTOM] = id(cx, cy + 1);
         d.nbr[LEFT] = id(cx - 1, cy);
         d.nbr[RIGHT] = id(cx + 1, cy);
-        d.nbr[TOP_LEFT] = D > 1 ? id(cx - 1, cy - 1) : -1;
-        d.nbr[TOP_RIGHT] = D > 1 ? id(cx + 1, cy - 1) : -1;
-        d.nbr[BOTTOM_LEFT] = D > 1 ? id(cx - 1, cy + 1) : -1;
-        d.nbr[BOTTOM_RIGHT] = D > 1 ? id(cx + 1, cy + 1) : -1;
+        // depth > 1: the two-phase exchange carries the corners in the
+        // top/bottom halos (CHARMING_HALO_CORNERS=1: corner messages instead)
+        const bool corners = D > 1 && halo_corner_messages();
+        d.ext = (D > 1 && !corners) ? (D + vec - 1) / vec * vec : 0;
+        d.pad_ = 0;
+        d.nbr[TOP_LEFT] = corners ? id(cx - 1, cy - 1) : -1;
+        d.nbr[TOP_RIGHT] = corners ? id(cx + 1, cy - 1) : -1;
+        d.nbr[BOTTOM_LEFT] = corners ? id(cx - 1, cy + 1) : -1;
+        d.nbr[BOTTOM_RIGHT] = corners ? id(cx + 1, cy + 1) : -1;
         int r = cy * px + cx;
         d.rank = r;
         d.parent = r > 0 ? base + (r - 1) / 2 : -1;

@@ -58,9 +58,35 @@ struct chare_desc {
   int parent;          // residual tree: parent chare (-1 at the root)
   int child[2];        // residual tree: children (-1 if none)
   int rank;            // index within the problem (tree position; 0 = root)
+  int ext;             // 0: one exchange phase, corner halos from the diagonal
+                       // neighbours. > 0 (depth > 1): two phases, left/right
+                       // halos first, then top/bottom halos that also carry
+                       // ext ghost columns each side (ext >= D, whole 16-byte
+                       // vectors), so the corners arrive through the
+                       // top/bottom neighbours and no corner messages exist
+  int pad_;
   void* buf[2];        // the two pitched grids, pointing at row 0 (ghost rows
                        // 1-D..0 lie before it)
 };
+
+// The cells a halo from / to direction d covers, with the two-phase
+// exchange's wider top/bottom halos.
+__host__ __device__ inline region halo_ghost(int d, const chare_desc& c) {
+  region g = ghost_region(d, c.depth, c.w, c.h);
+  if (c.ext > 0 && (d == TOP || d == BOTTOM)) {
+    g.c0 = 1 - c.ext;
+    g.nc = c.w + 2 * c.ext;
+  }
+  return g;
+}
+__host__ __device__ inline region halo_edge(int d, const chare_desc& c) {
+  region e = edge_region(d, c.depth, c.w, c.h);
+  if (c.ext > 0 && (d == TOP || d == BOTTOM)) {
+    e.c0 = 1 - c.ext;
+    e.nc = c.w + 2 * c.ext;
+  }
+  return e;
+}
 
 struct prob_desc {
   int nx, ny, px, py;

@@ -2,7 +2,10 @@
 
 Restates the state machine of charming_b200/csrc/apps/jacobi_chare.cuh
 (halos per sweep with parity ghost buffers, the binary residual tree, the
-stop decision applied one check period later) with messages delivered in
+stop decision applied one check period later, and with two_phase the
+exchange of ghost depth > 1: left/right halos first, top/bottom halos sent
+once the left/right ones of the same pass are in, so that they carry the
+corners) with messages delivered in
 per-pair FIFO order but otherwise in a random interleaving, and checks its
 invariants: a halo never arrives more than one sweep ahead, a sweep never
 starts without all halos of its sweep, every chare stops at the same sweep,
@@ -21,6 +24,7 @@ from dataclasses import dataclass, field
 class Chare:
     idx: int
     nbrs: list
+    xn: list     # left/right neighbours (the first phase of a two-phase exchange)
     parent: int
     children: list
     rank: int
@@ -28,6 +32,8 @@ class Chare:
     sent: int = -1
     started: bool = False
     got: list = field(default_factory=lambda: [0, 0])
+    gotx: list = field(default_factory=lambda: [0, 0])
+    sent_y: int = -1
     halo_seen: dict = field(default_factory=dict)
     done: bool = False
     waiting: bool = False
@@ -45,8 +51,9 @@ class ProtocolError(AssertionError):
 
 
 class Sim:
-    def __init__(self, px, py, K, max_sweeps, stop_at_check, seed=0):
+    def __init__(self, px, py, K, max_sweeps, stop_at_check, seed=0, two_phase=False):
         self.rng = random.Random(seed)
+        self.two_phase = two_phase
         self.K, self.max = K, max_sweeps
         self.stop_at_check = stop_at_check  # residual decision that says stop
         n = px * py
@@ -56,10 +63,11 @@ class Sim:
             nb = []
             if cy > 0: nb.append(r - px)
             if cy < py - 1: nb.append(r + px)
-            if cx > 0: nb.append(r - 1)
-            if cx < px - 1: nb.append(r + 1)
+            xn = []
+            if cx > 0: xn.append(r - 1)
+            if cx < px - 1: xn.append(r + 1)
             kids = [k for k in (2 * r + 1, 2 * r + 2) if k < n]
-            self.ch.append(Chare(r, nb, (r - 1) // 2 if r > 0 else -1, kids, r))
+            self.ch.append(Chare(r, nb + xn, xn, (r - 1) // 2 if r > 0 else -1, kids, r))
         self.queues = {}  # (src, dst) -> deque of messages (per-pair FIFO)
         self.finished_at = {}
 
@@ -84,10 +92,16 @@ class Sim:
                 if K > 0 and c.iter >= K and c.iter % K == 0 and 0 <= c.stop_check <= c.iter // K - 1:
                     return self.finish(c)
                 c.sent = c.iter
-                for nb in c.nbrs:
-                    self.send(c.idx, nb, ("halo", c.iter))
+                for nb in (c.xn if self.two_phase else c.nbrs):
+                    self.send(c.idx, nb, ("halo", c.iter, "x" if self.two_phase else "all"))
                 continue
-            if c.nbrs and c.got[c.iter & 1] == len(c.nbrs):
+            if self.two_phase and c.sent_y < c.iter and c.gotx[c.iter & 1] == len(c.xn):
+                c.sent_y = c.iter
+                for nb in c.nbrs:
+                    if nb not in c.xn:
+                        self.send(c.idx, nb, ("halo", c.iter, "y"))
+                continue
+            if c.nbrs and c.got[c.iter & 1] == len(c.nbrs) and (not self.two_phase or c.sent_y == c.iter):
                 self.advance(c)
                 continue
             return
@@ -98,7 +112,10 @@ class Sim:
         K = self.K
         resid = K > 0 and c.iter % K == 0
         chk = c.iter // K if K else 0
+        if self.two_phase and c.sent_y != c.iter:
+            raise ProtocolError(f"chare {c.idx} sweeps {c.iter} before its top/bottom halos went out")
         c.got[c.iter & 1] = 0
+        c.gotx[c.iter & 1] = 0
         c.iter += 1
         if resid:
             if c.have_own:
@@ -144,7 +161,9 @@ class Sim:
             if k not in (c.iter, c.iter + 1):
                 raise ProtocolError(f"chare {c.idx} at {c.iter} got halo of sweep {k}")
             c.got[k & 1] += 1
-            if c.got[k & 1] > len(c.nbrs):
+            if msg[2] == "x":
+                c.gotx[k & 1] += 1
+            if c.got[k & 1] > len(c.nbrs) or c.gotx[k & 1] > len(c.xn):
                 raise ProtocolError(f"chare {c.idx}: too many halos of parity {k & 1}")
             if c.started:
                 self.pump(c)

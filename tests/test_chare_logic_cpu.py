@@ -90,13 +90,14 @@ def test_chare_code_on_cpu(emu, cfg):
         assert int(f["sweeps"]) == expected_stop(nx, ny, K, tol, ms, bc, dt)
 
 
+@pytest.mark.parametrize("two_phase", [False, True])
 @pytest.mark.parametrize("px,py,K,mx,stop_at", [
     (3, 2, 10, 3000, 5), (4, 4, 1, 50, 7), (5, 3, 3, 40, 100), (1, 6, 10, 55, 2), (7, 1, 0, 30, 0),
 ])
-def test_protocol_model_random_orders(px, py, K, mx, stop_at):
+def test_protocol_model_random_orders(px, py, K, mx, stop_at, two_phase):
     ends = set()
     for seed in range(25):
-        ends.add(Sim(px, py, K, mx, stop_at, seed).run())
+        ends.add(Sim(px, py, K, mx, stop_at, seed, two_phase=two_phase).run())
     assert len(ends) == 1
 
 

@@ -170,13 +170,17 @@ def test_many_chares_per_pe(rt):
     assert np.array_equal(bits(out), bits(jac64(g, 15)))
 
 
+@pytest.mark.parametrize("corner_msgs", [False, True])
 @pytest.mark.parametrize("depth", [2, 3, 4, 5, 6, 8])
 @pytest.mark.parametrize("dtype", ["f64", "f32"])
-def test_multi_sweep_passes_bit_exact(rt, depth, dtype):
-    """depth sweeps per halo exchange (ghost zones of that depth, corner
-    halos from diagonal neighbours): the same bits as one sweep per
-    exchange. Sweep counts that are not multiples of the depth end with a
-    shorter pass."""
+def test_multi_sweep_passes_bit_exact(rt, depth, dtype, corner_msgs, monkeypatch):
+    """depth sweeps per halo exchange (ghost zones of that depth): the same
+    bits as one sweep per exchange. The corners travel in the second phase
+    of a two-phase exchange (left/right halos, then top/bottom halos that
+    carry the ghost columns), or, with CHARMING_HALO_CORNERS=1, in messages
+    from the diagonal neighbours. Sweep counts that are not multiples of the
+    depth end with a shorter pass."""
+    monkeypatch.setenv("CHARMING_HALO_CORNERS", "1" if corner_msgs else "0")
     npdt = np.float64 if dtype == "f64" else np.float32
     for (nx, ny, px, py, sweeps) in [(333, 201, 5, 3, 37), (1000, 77, 7, 2, 9), (50, 700, 1, 9, 11),
                                      (2500, 40, 2, 1, 6), (300, 180, 3, 2, 40)]:
@@ -188,7 +192,7 @@ def test_multi_sweep_passes_bit_exact(rt, depth, dtype):
             info = j.info()
         ref = jac64(g, sweeps) if dtype == "f64" else jac32(g, sweeps)
         assert np.array_equal(bits(out), bits(ref)), (nx, ny, px, py, sweeps)
-        corners = 4 * (px - 1) * (py - 1)
+        corners = 4 * (px - 1) * (py - 1) if corner_msgs else 0
         edges = 2 * (px - 1) * py + 2 * px * (py - 1)
         assert info["halo_msgs_per_sweep"] == edges + corners
 
