@@ -15,7 +15,7 @@
 //     the tile's planes, rim included, stream through a ring of J3_S
 //     shared-memory slots by per-thread asynchronous copies (cp.async, one
 //     commit group per plane), J3_S - 2 planes ahead of the one computed
-//     (J3_S = 8 by default).
+//     (J3_S = 10 by default; 256 threads, two tile rows each).
 //     Each input value is read from DRAM once per sweep (16 B per lattice
 //     update with the store); the rim cells come from L2.
 //   jacobi3d_kernel (any shape): per-thread loads, the planes below and
@@ -32,7 +32,10 @@ namespace {
 
 constexpr int J3_TX = 32, J3_TY = 16;
 constexpr int J3_BW = J3_TX + 2, J3_BH = J3_TY + 2;          // tensor box: tile + rim
-constexpr int J3_S_DEFAULT = 8;                              // plane slots
+// 10 slots and 2 tile rows per thread: 293 GLUP/s at 640^3, against 265
+// with 8 slots and one row, 282 with 12 slots and two rows
+constexpr int J3_S_DEFAULT = 10;                             // plane slots
+constexpr int J3_RPT_DEFAULT = 2;                            // tile rows per thread
 
 __device__ __forceinline__ double j3_stencil(double c, double xm, double xp, double ym, double yp, double zm,
     double zp) {
@@ -42,27 +45,28 @@ __device__ __forceinline__ double j3_stencil(double c, double xm, double xp, dou
 
 // Planes z0-1 .. z1 of the tile stream through J3_S shared-memory slots:
 // plane p lives in slot (p - z0 + 1) % J3_S, one cp.async group per plane
-// (8-byte copies, each thread one or two cells of the 34 x 18 box: the tile
-// and its rim; cells outside the grid are zero-filled and never used).
-// Before output plane z is computed, planes up to z + J3_S - 2 are issued
-// and wait_group leaves J3_S - 3 of them in flight, so planes z-1, z, z+1
-// have landed.
-template <int J3_S>
-__global__ void __launch_bounds__(J3_TX * J3_TY, 3) jacobi3d_async_kernel(const double* __restrict__ in,
-    double* __restrict__ out, int nx, int ny, int nz, int zrun) {
+// (8-byte copies of the 34 x 18 box: the tile and its rim; cells outside the
+// grid are zero-filled and never used). Before output plane z is computed,
+// planes up to z + J3_S - 2 are issued and wait_group leaves J3_S - 3 of
+// them in flight, so planes z-1, z, z+1 have landed. The block has
+// 32 x (16 / RPT) threads; each computes RPT rows of the tile.
+template <int J3_S, int RPT>
+__global__ void __launch_bounds__(J3_TX * J3_TY / RPT, 3 * RPT) jacobi3d_async_kernel(
+    const double* __restrict__ in, double* __restrict__ out, int nx, int ny, int nz, int zrun) {
   extern __shared__ __align__(16) double j3_slots[];  // [J3_S][J3_BH][J3_BW]
+  constexpr int TY = J3_TY / RPT, NT = J3_TX * TY;
+  constexpr int BOX = J3_BW * J3_BH, SLOT = BOX;  // doubles per slot
+  constexpr int NC = (BOX + NT - 1) / NT;         // box cells per thread
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * J3_TX + tx;
   const int bx0 = blockIdx.x * J3_TX, by0 = blockIdx.y * J3_TY;
-  const int x = bx0 + tx + 1, y = by0 + ty + 1;
+  const int x = bx0 + tx + 1;
   const int z0 = 1 + blockIdx.z * zrun, z1 = min(nz + 1, z0 + zrun);
-  const bool own = x <= nx && y <= ny;
   const long long sy = nx + 2, sz = (long long)(nx + 2) * (ny + 2);
-  constexpr int BOX = J3_BW * J3_BH, SLOT = BOX;  // doubles per slot
-  // this thread's box cells (at most two: 612 cells, 512 threads)
-  int cell[2], goff[2];
-  bool inside[2];
-  for (int k = 0; k < 2; k++) {
-    const int e = tid + k * J3_TX * J3_TY;
+  int cell[NC], goff[NC];
+  bool inside[NC];
+#pragma unroll
+  for (int k = 0; k < NC; k++) {
+    const int e = tid + k * NT;
     cell[k] = e < BOX ? e : -1;
     const int gx = bx0 + e % J3_BW, gy = by0 + e / J3_BW;
     inside[k] = e < BOX && gx <= nx + 1 && gy <= ny + 1;
@@ -72,7 +76,8 @@ __global__ void __launch_bounds__(J3_TX * J3_TY, 3) jacobi3d_async_kernel(const 
     if (p <= z1) {
       double* slot = j3_slots + ((p - z0 + 1) % J3_S) * SLOT;
       const double* src = in + (long long)p * sz;
-      for (int k = 0; k < 2; k++) {
+#pragma unroll
+      for (int k = 0; k < NC; k++) {
         if (cell[k] < 0) continue;
         // zero-fill (source size 0) outside the grid, from a valid address
         const unsigned n = inside[k] ? 8u : 0u;
@@ -83,17 +88,21 @@ __global__ void __launch_bounds__(J3_TX * J3_TY, 3) jacobi3d_async_kernel(const 
     jac::cp_async_commit();  // one group per plane, empty past z1
   };
   for (int p = z0 - 1; p <= z0 + J3_S - 3; p++) issue(p);
-  const int c = (ty + 1) * J3_BW + tx + 1;
   for (int z = z0; z < z1; z++) {
     issue(z + J3_S - 2);              // into the slot plane z-2 used
     jac::cp_async_wait<J3_S - 3>();  // planes up to z+1 have landed (this thread's copies)
     __syncthreads();                 // ... and every other thread's
-    if (own) {
-      const double* m = j3_slots + ((z - z0 + 1) % J3_S) * SLOT;
-      const double* lo = j3_slots + ((z - z0) % J3_S) * SLOT;
-      const double* hi = j3_slots + ((z - z0 + 2) % J3_S) * SLOT;
-      out[(long long)y * sy + x + (long long)z * sz] =
-          j3_stencil(m[c], m[c - 1], m[c + 1], m[c - J3_BW], m[c + J3_BW], lo[c], hi[c]);
+    const double* m = j3_slots + ((z - z0 + 1) % J3_S) * SLOT;
+    const double* lo = j3_slots + ((z - z0) % J3_S) * SLOT;
+    const double* hi = j3_slots + ((z - z0 + 2) % J3_S) * SLOT;
+#pragma unroll
+    for (int r = 0; r < RPT; r++) {
+      const int yy = ty + r * TY, y = by0 + yy + 1;
+      if (x <= nx && y <= ny) {
+        const int c = (yy + 1) * J3_BW + tx + 1;
+        out[(long long)y * sy + x + (long long)z * sz] =
+            j3_stencil(m[c], m[c - 1], m[c + 1], m[c - J3_BW], m[c + J3_BW], lo[c], hi[c]);
+      }
     }
     __syncthreads();  // plane z-1's slot takes plane z+J3_S-1 next
   }
@@ -175,36 +184,49 @@ int jacobi3d_async_zrun(int nx, int ny, int nz, int n_sms, int per_sm) {
   return best_zrun;
 }
 
-// Stage count of the pipelined kernel: CHARMING_J3_STAGES (6, 8, 10 or 12)
-// or J3_S_DEFAULT.
+// Rows per thread of the pipelined kernel: CHARMING_J3_RPT (1 or 2) with
+// CHARMING_J3_STAGES (8 with 1 row, 10 or 12 with 2), else the defaults.
+int jacobi3d_rpt() {
+  static int rpt = 0;
+  if (!rpt) {
+    rpt = J3_RPT_DEFAULT;
+    if (const char* ev = getenv("CHARMING_J3_RPT")) {
+      const int v = atoi(ev);
+      if (v == 1 || v == 2) rpt = v;
+    }
+  }
+  return rpt;
+}
+
+// Stage count of the pipelined kernel (see jacobi3d_rpt).
 int jacobi3d_stages() {
   static int stages = 0;
   if (!stages) {
     stages = J3_S_DEFAULT;
     if (const char* ev = getenv("CHARMING_J3_STAGES")) {
       const int v = atoi(ev);
-      if (v == 6 || v == 8 || v == 10 || v == 12) stages = v;
+      if (v == 8 || v == 10 || v == 12) stages = v;
     }
   }
   return stages;
 }
 
-template <int S>
+template <int S, int RPT>
 cudaError_t jacobi3d_async_sweeps(double*& a, double*& b, int nx, int ny, int nz, int sweeps, int n_sms,
     cudaStream_t s) {
   int per_sm = 0;
   cudaError_t e = cudaSuccess;
+  const void* fn = (const void*)jacobi3d_async_kernel<S, RPT>;
   if (j3_async_smem(S) > 48 * 1024)
-    e = cudaFuncSetAttribute((const void*)jacobi3d_async_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)j3_async_smem(S));
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)j3_async_smem(S));
   if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi3d_async_kernel<S>, J3_TX * J3_TY,
-                                                      j3_async_smem(S));
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jacobi3d_async_kernel<S, RPT>,
+                                                      J3_TX * J3_TY / RPT, j3_async_smem(S));
   if (e != cudaSuccess) return e;
   const int zrun = jacobi3d_async_zrun(nx, ny, nz, n_sms, per_sm);
-  const dim3 block(J3_TX, J3_TY), grid((nx + J3_TX - 1) / J3_TX, (ny + J3_TY - 1) / J3_TY, (nz + zrun - 1) / zrun);
+  const dim3 block(J3_TX, J3_TY / RPT), grid((nx + J3_TX - 1) / J3_TX, (ny + J3_TY - 1) / J3_TY, (nz + zrun - 1) / zrun);
   for (int k = 0; k < sweeps && e == cudaSuccess; k++) {
-    jacobi3d_async_kernel<S><<<grid, block, j3_async_smem(S), s>>>(a, b, nx, ny, nz, zrun);
+    jacobi3d_async_kernel<S, RPT><<<grid, block, j3_async_smem(S), s>>>(a, b, nx, ny, nz, zrun);
     e = cudaGetLastError();
     double* t = a;
     a = b;
@@ -220,12 +242,10 @@ double* jacobi3d_run(double* a, double* b, int nx, int ny, int nz, int sweeps, c
   *err = cudaSuccess;
   const dim3 block(J3_TX, J3_TY);
   if (async_shape_ok(nx, ny)) {
-    switch (jacobi3d_stages()) {
-      case 6: *err = jacobi3d_async_sweeps<6>(a, b, nx, ny, nz, sweeps, n_sms, s); break;
-      case 10: *err = jacobi3d_async_sweeps<10>(a, b, nx, ny, nz, sweeps, n_sms, s); break;
-      case 12: *err = jacobi3d_async_sweeps<12>(a, b, nx, ny, nz, sweeps, n_sms, s); break;
-      default: *err = jacobi3d_async_sweeps<8>(a, b, nx, ny, nz, sweeps, n_sms, s); break;
-    }
+    const int st = jacobi3d_stages(), rpt = jacobi3d_rpt();
+    if (st == 8 && rpt == 1) *err = jacobi3d_async_sweeps<8, 1>(a, b, nx, ny, nz, sweeps, n_sms, s);
+    else if (st == 12 && rpt == 2) *err = jacobi3d_async_sweeps<12, 2>(a, b, nx, ny, nz, sweeps, n_sms, s);
+    else *err = jacobi3d_async_sweeps<10, 2>(a, b, nx, ny, nz, sweeps, n_sms, s);
     return a;
   }
   const int zrun = jacobi3d_zrun(nx, ny, nz, n_sms);
