@@ -552,7 +552,7 @@ def precision_suite(plain_fp64_glups: float, steps: int = 2, warmup: int = 1) ->
 
 
 def serving_suite(n_req: int, rate: float = 200.0, seed: int = 0xC5, pes_per_sm: int = 1,
-                  chare_side: int = 2048) -> dict:
+                  chare_side: int = 2048, max_inflight: int = 64, with_cpu: bool = True) -> dict:
     """C5: Poisson arrivals of FP32 solves into one running scheduler. The
     defaults are the fastest measured (600 requests, served GLUP/s): chares
     of 2048^2 on one 512-thread PE per SM 759; 1536^2 701; 1024^2 with 2 PEs
@@ -575,7 +575,7 @@ def serving_suite(n_req: int, rate: float = 200.0, seed: int = 0xC5, pes_per_sm:
     budget = 120 * 10**9
     lat, service, lups_done = [], [], 0
     sweeps_of = [0] * n_req
-    with Server(budget, max_inflight=64, workers_per_pe=16 // pes_per_sm, chare_side=chare_side,
+    with Server(budget, max_inflight=max_inflight, workers_per_pe=16 // pes_per_sm, chare_side=chare_side,
                 dtype="f32", deadline_s=600) as srv:
         t0 = time.monotonic()
         nxt = 0
@@ -611,7 +611,7 @@ def serving_suite(n_req: int, rate: float = 200.0, seed: int = 0xC5, pes_per_sm:
             "service_p99_ms": float(np.percentile(service, 99)) * 1e3,
             "offered_glups": offered / 1e9, "served_glups": lups_done / wall / 1e9,
             "peak_inflight": stats.get("peak_inflight"), "peak_bytes": stats.get("peak_bytes"),
-            "cpu_baseline": cpu_serving_baseline(probs, arrive, sweeps_of)}
+            "cpu_baseline": cpu_serving_baseline(probs, arrive, sweeps_of) if with_cpu else None}
 
 
 def run_suites(args, headline_glups: float) -> dict:
