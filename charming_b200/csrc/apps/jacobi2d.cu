@@ -142,8 +142,12 @@ __shared__ charm::chare_proxy<JBlock>* jproxy;
 // 5 of the sends: up to the reservation call.
 constexpr int PE_NS_SLOTS = 8;
 __shared__ unsigned long long s_pe_ns[6];
-__device__ __forceinline__ void add_pe_ns(int k, unsigned long long ns) {
-  s_pe_ns[k] += ns;
+// The phase timers count SM cycles (clock64, a register read, instead of
+// the %globaltimer reads of the run-level checks); the host converts them
+// with the SM clock rate.
+__device__ __forceinline__ unsigned long long pe_clock() { return (unsigned long long)clock64(); }
+__device__ __forceinline__ void add_pe_cyc(int k, unsigned long long cyc) {
+  s_pe_ns[k] += cyc;
   japp::pe_ns()[PE_NS_SLOTS * blockIdx.x + k] = s_pe_ns[k];
 }
 __shared__ charm::chare_proxy<JServer>* sproxy;
@@ -177,9 +181,8 @@ __device__ double sweep_block(const jac::chare_desc& d, int cur, bool resid, int
                         L >= 1 && L <= d.depth,
                     CHARMING_ERR_APP, 8000 + cur, d.w))
     return 0.0;
-  // phase timers: thread 0 alone reads the clock (a %globaltimer read by
-  // every thread of the block costs tens of microseconds)
-  const unsigned long long t0 = threadIdx.x == 0 ? charm::now_ns() : 0;
+  // phase timers: thread 0 alone reads the clock
+  const unsigned long long t0 = threadIdx.x == 0 ? pe_clock() : 0;
   if (L > 1) {
     int fixed = (d.nbr[jac::TOP] < 0 ? 1 : 0) | (d.nbr[jac::BOTTOM] < 0 ? 2 : 0) |
                 (d.nbr[jac::LEFT] < 0 ? 4 : 0) | (d.nbr[jac::RIGHT] < 0 ? 8 : 0);
@@ -207,7 +210,7 @@ __device__ double sweep_block(const jac::chare_desc& d, int cur, bool resid, int
                 : jac::sweep_direct<T, false>(in, out, d.w, d.h);
     __syncthreads();
   }
-  if (threadIdx.x == 0) add_pe_ns(0, charm::now_ns() - t0);
+  if (threadIdx.x == 0) add_pe_cyc(0, pe_clock() - t0);
   return resid ? suite::block_sum_f64(acc) : 0.0;
 }
 
@@ -287,7 +290,7 @@ __device__ void count_nbrs(JBlock& c, const jac::chare_desc& d) {
 // columns the left/right halos of this pass filled. All threads.
 template <typename T>
 __device__ void send_halos(JBlock& c, const jac::chare_desc& d, int phase = 0) {
-  const unsigned long long t0 = threadIdx.x == 0 ? charm::now_ns() : 0;
+  const unsigned long long t0 = threadIdx.x == 0 ? pe_clock() : 0;
   int idx[jac::N_DIRS], dirs[jac::N_DIRS], refs[jac::N_DIRS];
   size_t bytes[jac::N_DIRS];
   jac::region e[jac::N_DIRS];
@@ -305,9 +308,9 @@ __device__ void send_halos(JBlock& c, const jac::chare_desc& d, int phase = 0) {
     n++;
   }
   charm::message msg[jac::N_DIRS];
-  CHARM_PROF(if (threadIdx.x == 0) add_pe_ns(5, charm::now_ns() - t0);)
+  CHARM_PROF(if (threadIdx.x == 0) add_pe_cyc(5, pe_clock() - t0);)
   const bool got = n > 0 && jproxy->alloc_msgs(msg, idx, bytes, n);
-  CHARM_PROF(if (threadIdx.x == 0) add_pe_ns(3, charm::now_ns() - t0);)
+  CHARM_PROF(if (threadIdx.x == 0) add_pe_cyc(3, pe_clock() - t0);)
   if (got) {
     T* vals[jac::N_DIRS];
     for (int k = 0; k < n; k++)
@@ -320,11 +323,11 @@ __device__ void send_halos(JBlock& c, const jac::chare_desc& d, int phase = 0) {
       hh->gen = c.gen;
     }
     copy_rects<T>(view<T>(d, c.cur), e, vals, n, false);
-    CHARM_PROF(const unsigned long long tp = threadIdx.x == 0 ? charm::now_ns() : 0;)
+    CHARM_PROF(const unsigned long long tp = threadIdx.x == 0 ? pe_clock() : 0;)
     jproxy->invoke_msgs(idx, EP_HALO, msg, bytes, refs, n);
-    CHARM_PROF(if (threadIdx.x == 0) add_pe_ns(4, charm::now_ns() - tp);)
+    CHARM_PROF(if (threadIdx.x == 0) add_pe_cyc(4, pe_clock() - tp);)
   }
-  if (threadIdx.x == 0) add_pe_ns(1, charm::now_ns() - t0);
+  if (threadIdx.x == 0) add_pe_cyc(1, pe_clock() - t0);
 }
 
 // Halo of pass hh->pass -> ghost zone of buf[pass & 1]. All threads.

@@ -476,9 +476,14 @@ extern "C" int charming_jacobi2d_get_info(void* handle, charming_jacobi_info* ou
   out->grid_bytes = h->grid_bytes;
   out->halo_msgs_per_sweep = h->halo_msgs;
   out->last_run_ms = h->last_ms;
+  // the per-PE phase timers count SM cycles
   std::vector<unsigned long long> ns(8 * h->block_map.size());
   cudaError_t e = cudaMemcpy(ns.data(), h->d_sweep_ns, 8 * ns.size(), cudaMemcpyDeviceToHost);
+  int dev = 0, khz = 0;
+  if (e == cudaSuccess) e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, dev);
   if (e != cudaSuccess) return check_cuda(e, "jacobi2d info");
+  const double ms_per = khz > 0 ? 1.0 / khz : 0.0;
   double mx = 0, sum[6] = {0, 0, 0, 0, 0, 0};
   int busy = 0;
   for (size_t p = 0; p < h->block_map.size(); p++) {
@@ -488,13 +493,13 @@ extern "C" int charming_jacobi2d_get_info(void* handle, charming_jacobi_info* ou
       busy++;
     }
   }
-  out->send_reserve_ms_mean = busy ? sum[3] / busy * 1e-6 : 0.0;
-  out->send_publish_ms_mean = busy ? sum[4] / busy * 1e-6 : 0.0;
-  out->send_setup_ms_mean = busy ? sum[5] / busy * 1e-6 : 0.0;
-  out->sweep_ms_max = mx * 1e-6;
-  out->sweep_ms_mean = busy ? sum[0] / busy * 1e-6 : 0.0;
-  out->send_ms_mean = busy ? sum[1] / busy * 1e-6 : 0.0;
-  out->halo_ms_mean = busy ? sum[2] / busy * 1e-6 : 0.0;
+  out->send_reserve_ms_mean = busy ? sum[3] / busy * ms_per : 0.0;
+  out->send_publish_ms_mean = busy ? sum[4] / busy * ms_per : 0.0;
+  out->send_setup_ms_mean = busy ? sum[5] / busy * ms_per : 0.0;
+  out->sweep_ms_max = mx * ms_per;
+  out->sweep_ms_mean = busy ? sum[0] / busy * ms_per : 0.0;
+  out->send_ms_mean = busy ? sum[1] / busy * ms_per : 0.0;
+  out->halo_ms_mean = busy ? sum[2] / busy * ms_per : 0.0;
   return CHARMING_OK;
 }
 

@@ -231,7 +231,7 @@ __device__ void em_halo_t(JBlock& c, void* arg) {
   const jac::halo_hdr* hh = reinterpret_cast<const jac::halo_hdr*>(arg);
   if (!ensure_gen<T>(c, hh->gen)) return;
   if (c.done) return;
-  const unsigned long long t_em = threadIdx.x == 0 ? charm::now_ns() : 0;
+  const unsigned long long t_em = threadIdx.x == 0 ? pe_clock() : 0;
   const jac::chare_desc& d = c.desc;
   // checked build: direction, length and sweep of the halo are consistent
   if (!CHARM_VERIFY(hh->dir >= 0 && hh->dir < jac::N_DIRS && d.nbr[hh->dir] >= 0, CHARMING_ERR_APP,
@@ -248,7 +248,7 @@ __device__ void em_halo_t(JBlock& c, void* arg) {
     (void)CHARM_VERIFY(c.got[hh->pass & 1] <= jac::N_DIRS, CHARMING_ERR_APP, 4000 + c.got[hh->pass & 1], c.i);
   }
   __syncthreads();
-  if (threadIdx.x == 0) add_pe_ns(2, charm::now_ns() - t_em);
+  if (threadIdx.x == 0) add_pe_cyc(2, pe_clock() - t_em);
   if (c.started) pump<T>(c, d);  // a halo may overtake the start message
 }
 

@@ -1344,12 +1344,12 @@ charming_scheduler_kernel(int argc, char** argv, size_t* argvs) {
   charm::main(argc, argv, argvs, me);
   grid_barrier();
 
-  unsigned long long loop_t0 = globaltimer();
+  const unsigned long long loop_t0 = threadIdx.x == 0 ? globaltimer() : 0;
   if (!terminated() && !ps->term) {
     if (keeper) scheduler_loop();
     else helper_loop();
   }
-  unsigned long long loop_t1 = globaltimer();
+  const unsigned long long loop_t1 = threadIdx.x == 0 ? globaltimer() : 0;
 
   if (threadIdx.x == 0 && keeper) {
     ps->stats[ST_LOOP_NS] = loop_t1 - loop_t0;

@@ -196,6 +196,7 @@ typedef struct charming_jacobi_info {
   uint64_t grid_bytes;        /* device bytes of all chare grids           */
   uint64_t halo_msgs_per_sweep; /* halo messages per exchange (every `depth` sweeps) */
   double last_run_ms;         /* CUDA-event time of the last run           */
+  /* the phase times below: SM cycles at the nominal clock */
   double sweep_ms_max;        /* last run: max over PEs of time in sweeps  */
   double sweep_ms_mean;       /* last run: mean over busy PEs              */
   double send_ms_mean;        /* last run: mean time packing/sending halos */
