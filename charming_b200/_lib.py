@@ -49,7 +49,7 @@ class Info(C.Structure):
         ("n_pes", i32), ("n_sms", i32), ("threads_per_pe", i32), ("smem_bytes_per_pe", i32),
         ("smem_scratch_bytes", i32), ("regs_per_thread", i32), ("ring_bytes", u64),
         ("max_msg_bytes", u64), ("device_bytes", u64), ("stack_bytes", u64),
-        ("local_bytes", u64), ("n_blocks", i32), ("gpu_level", i32),
+        ("local_bytes", u64), ("n_blocks", i32), ("gpu_level", i32), ("n_devs", i32), ("my_dev", i32),
     ]
 
 
@@ -117,10 +117,23 @@ class ServeStats(C.Structure):
     ]
 
 
+# Several GPUs (charming_devices): the host's allgather and barrier.
+ALLGATHER_FN = C.CFUNCTYPE(i32, vp, vp, vp, C.c_size_t)
+BARRIER_FN = C.CFUNCTYPE(i32, vp)
+
+
+class Devices(C.Structure):
+    _fields_ = [
+        ("rank", i32), ("world", i32), ("virtual_devs", i32), ("reserved", i32),
+        ("allgather", ALLGATHER_FN), ("barrier", BARRIER_FN), ("ctx", vp),
+    ]
+
+
 # (name, restype, argtypes) for every entry point of charming_c.h
 SIGNATURES = [
     ("charming_default_config", None, [C.POINTER(Config)]),
     ("charming_init", i32, [C.POINTER(Config)]),
+    ("charming_init_devices", i32, [C.POINTER(Config), C.POINTER(Devices)]),
     ("charming_run", i32, [i32, C.POINTER(C.c_char_p)]),
     ("charming_fini", i32, []),
     ("charming_timer_start", i32, []),

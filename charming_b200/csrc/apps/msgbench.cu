@@ -154,9 +154,12 @@ __device__ void ping_recv(PingChare& c, void* arg) {
 // Fan-out. g_app: a[0] n_chares, a[1] msgs per chare, a[2] payload bytes,
 // a[3] seed, a[4] mode (0: refnum -1, 1: message k carries refnum k),
 // a[5] log capacity (records), a[6] chares that receive anything;
-// p[0] log (u32[cap][8]), p[1] counters (u64[2]: 0, chares done),
-// p[2] expected counts (int[n][msgs]), p[3] log offsets (u64[n+1]: chare
-// d's deliveries go to records off[d]..off[d+1]-1, in delivery order).
+// a[7] 1: the run spans several GPUs, chares report done to chare 0 in a
+// message (its counter is the only one); p[0] log (u32[cap][8]), p[1]
+// counters (u64[2]: 0, chares done), p[2] expected counts (int[n][msgs]),
+// p[3] log offsets (u64[n+1]: chare d's deliveries go to records
+// off[d]..off[d+1]-1, in delivery order; over several processes each logs
+// the deliveries to its own chares, the others' records stay zero).
 // The host computes the counts and offsets (fanout_plan), so a delivery
 // needs no atomic: only a chare's last one counts it done.
 // Destination of message k of chare s: mix64(seed ^ ((s*msgs+k+1)*G)) % n.
@@ -206,10 +209,25 @@ __device__ void fan_start(FanChare& c, void* arg) {
   }
 }
 
+__device__ void fan_record(FanChare& c, void* arg, bool relay, int* s_last);
+
 // Warp 0 handles a delivery (the other warps have nothing to do and return
 // at once): checksum by its lanes, the record and the refnum ladder by lane 0.
+// Over several GPUs a chare's last delivery is reported to chare 0 in a
+// message, which the whole block sends.
 __device__ void fan_recv(FanChare& c, void* arg) {
-  if (threadIdx.x >= 32) return;
+  const bool relay = g_app.a[7] != 0;
+  __shared__ int s_last;
+  if (threadIdx.x >= 32 && !relay) return;
+  if (threadIdx.x < 32) fan_record(c, arg, relay, &s_last);
+  if (relay) {
+    __syncthreads();
+    if (s_last) fan_proxy->invoke(0, 2);
+  }
+}
+
+// Warp 0 of fan_recv.
+__device__ void fan_record(FanChare& c, void* arg, bool relay, int* s_last) {
   int msgs = (int)g_app.a[1], payload = (int)g_app.a[2];
   int mode = (int)g_app.a[4];
   unsigned long long cs = suite::checksum_warp(arg, (unsigned long long)payload);
@@ -238,10 +256,21 @@ __device__ void fan_recv(FanChare& c, void* arg) {
         fan_proxy->set_refnum(c.i, c.cur_ref);
       }
     }
-    if ((unsigned long long)c.seq == off[c.i + 1] - off[c.i]) {  // this chare's last delivery
+    const bool last = (unsigned long long)c.seq == off[c.i + 1] - off[c.i];  // this chare's last delivery
+    if (relay) {
+      *s_last = last ? 1 : 0;
+    } else if (last) {
       unsigned long long done = atomicAdd(&ctr[1], 1ULL) + 1;
       if (done == (unsigned long long)g_app.a[6]) charm::end();
     }
+  }
+}
+
+// Chare 0 (several GPUs): one more chare has all its deliveries.
+__device__ void fan_done(FanChare& c, void* arg) {
+  if (threadIdx.x == 0) {
+    unsigned long long* ctr = reinterpret_cast<unsigned long long*>(g_app.p[1]);
+    if (++ctr[1] == (unsigned long long)g_app.a[6]) charm::end();
   }
 }
 
@@ -274,6 +303,7 @@ __device__ void suite::fanout_main(int pe) {
     fan_proxy = new charm::chare_proxy<FanChare>();
     fan_proxy->add_entry_method<&fan_start>();
     fan_proxy->add_entry_method<&fan_recv>();
+    fan_proxy->add_entry_method<&fan_done>();
     fan_proxy->create(n);
   }
   __syncthreads();
@@ -396,6 +426,7 @@ extern "C" int charming_fanout(int n_chares, int msgs_per_chare, int payload_byt
   p.a[4] = mode;
   p.a[5] = (long long)log_capacity;
   p.a[6] = active;
+  p.a[7] = charm_host::info().n_devs > 1 ? 1 : 0;
   p.p[0] = d_log;
   p.p[1] = d_ctr;
   p.p[2] = d_exp;

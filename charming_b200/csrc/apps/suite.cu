@@ -18,6 +18,13 @@ __device__ void charm::main(int argc, char** argv, size_t* argvs, int pe) {
     if (charm::pe_thread() == 0) charm::rt::set_error(CHARMING_ERR_CONFIG, g_app.id, 1);
     return;
   }
+  // Over several processes only the message programs run: the others keep
+  // their grids and logs in one process's memory.
+  if (charm::rt::c_rt.n_procs > 1 && g_app.id != suite::APP_HELLO && g_app.id != suite::APP_REFNUM &&
+      g_app.id != suite::APP_PINGPONG && g_app.id != suite::APP_FANOUT && g_app.id != suite::APP_NONE) {
+    if (threadIdx.x == 0) charm::rt::set_error(CHARMING_ERR_CONFIG, g_app.id, 2);
+    return;
+  }
   switch (g_app.id) {
     case suite::APP_HELLO: suite::hello_main(pe); break;
     case suite::APP_REFNUM: suite::refnum_main(pe); break;

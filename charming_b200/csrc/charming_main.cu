@@ -5,9 +5,16 @@
 // Environment overrides: CHARMING_GPU_LEVEL (1: GPU-level mode), CHARMING_PES_PER_SM, CHARMING_RING_BYTES,
 // CHARMING_DEADLINE_S, CHARMING_IDLE_TIMEOUT_S, CHARMING_HEAP_BYTES,
 // CHARMING_QUIET (suppress the [INFO] lines).
+// Several GPUs, one process each (the reference's multi-GPU launch through
+// MPI or NVSHMEM's launcher): WORLD_SIZE > 1, RANK, LOCAL_RANK (the GPU;
+// default RANK), as torchrun sets them, and CHARMING_RDV_DIR, an empty
+// directory all ranks see, for the bootstrap. CHARMING_VIRTUAL_DEVS=n (one
+// process): this GPU's PEs form n GPUs in one launch.
 #include <cstdio>
 #include <cstdlib>
+#include <memory>
 #include "../../include/charming_c.h"
+#include "rendezvous.h"
 
 namespace charm {
 // Weak: programs without a host main still link (the reference requires one).
@@ -35,9 +42,27 @@ int main(int argc, char** argv) {
   cfg.gpu_level = &charming_program_gpu_level != nullptr ? charming_program_gpu_level : 0;
   cfg.gpu_level = (int)env_u64("CHARMING_GPU_LEVEL", (unsigned long long)cfg.gpu_level);
   bool quiet = getenv("CHARMING_QUIET") != nullptr;
-  cfg.verbose = quiet ? 0 : 1;
 
-  int rc = charming_init(&cfg);
+  charming_devices devs{};
+  devs.world = (int)env_u64("WORLD_SIZE", 1);
+  devs.rank = (int)env_u64("RANK", 0);
+  devs.virtual_devs = (int)env_u64("CHARMING_VIRTUAL_DEVS", 1);
+  std::unique_ptr<charm_host::file_rendezvous> rdv;
+  if (devs.world > 1) {
+    const char* dir = getenv("CHARMING_RDV_DIR");
+    if (!dir) {
+      fprintf(stderr, "[ERROR] WORLD_SIZE > 1 needs CHARMING_RDV_DIR (an empty directory all ranks see)\n");
+      return CHARMING_ERR_CONFIG;
+    }
+    rdv.reset(new charm_host::file_rendezvous(dir, devs.rank, devs.world));
+    devs.allgather = &charm_host::file_rendezvous::allgather_cb;
+    devs.barrier = &charm_host::file_rendezvous::barrier_cb;
+    devs.ctx = rdv.get();
+    cfg.device = (int)env_u64("LOCAL_RANK", (unsigned long long)devs.rank);
+  }
+  cfg.verbose = (quiet || devs.rank != 0) ? 0 : 1;
+
+  int rc = charming_init_devices(&cfg, &devs);
   if (rc != CHARMING_OK) {
     fprintf(stderr, "[ERROR] charming_init: %s (%s)\n", charming_status_string(rc),
         charming_last_error());
@@ -50,7 +75,7 @@ int main(int argc, char** argv) {
     fprintf(stderr, "[ERROR] run ended with status %d: %s (pe %d, info %d %d) %s\n", rc,
         charming_status_string(rc), st.err_pe, st.err_info0, st.err_info1, charming_last_error());
   }
-  if (!quiet) {
+  if (!quiet && devs.rank == 0) {
     printf("[INFO] Exiting CharminG: %llu messages delivered, %.3f ms\n",
         (unsigned long long)st.delivered, st.kernel_ms);
   }

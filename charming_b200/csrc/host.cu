@@ -2,9 +2,12 @@
 // core C ABI (charming_init / run / fini / stats).
 //
 // Replaces the reference's process main (src/charming.cu:50-263) and
-// comm_init_host / comm_fini_host (src/comm/get/get.cu:69-169) for one GPU:
-// no NVSHMEM or MPI bootstrap, plain cudaMalloc'd HBM for the inbox rings,
-// and a cooperative launch so that every PE block is resident.
+// comm_init_host / comm_fini_host (src/comm/get/get.cu:69-169): no NVSHMEM or
+// MPI bootstrap, plain cudaMalloc'd HBM for the inbox rings, and a
+// cooperative launch so that every PE block is resident. Over several GPUs
+// (one process each), every GPU's inbox side is one allocation exported with
+// CUDA IPC and mapped by the others; the host's allgather and barrier
+// (charming_devices) exchange the handles and order the runs.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -33,6 +36,11 @@ struct HostRuntime {
   charming_stats last{};
   char* d_args = nullptr;
   size_t d_args_cap = 0;
+  int n_local = 0;                  // PE slots of this launch (1 in GPU-level mode)
+  int rank = 0, world = 1, vdevs = 1;
+  charming_devices devs{};          // the host collectives (world > 1)
+  std::vector<void*> ipc_opened;    // peers' inbox regions mapped here
+  std::vector<int*> launch_ctrl;    // control words of this launch's GPUs
 };
 
 HostRuntime g;
@@ -55,6 +63,58 @@ int dev_alloc(T** p, size_t bytes, const char* what) {
 }
 
 bool is_pow2(uint64_t v) { return v && !(v & (v - 1)); }
+
+// One GPU's inbox side in one allocation (what another GPU maps): tails,
+// heads, control words, progress stamps, then flags and rings on 2 MiB
+// boundaries.
+struct inbox_layout {
+  size_t tail, head, ctrl, progress, flags, ring, bytes;
+};
+inbox_layout inbox_layout_for(int pes, const device_state& ds) {
+  auto up = [](size_t v, size_t a) { return (v + a - 1) / a * a; };
+  inbox_layout L{};
+  size_t o = 0;
+  L.tail = o;
+  o = up(o + sizeof(line_u64) * (size_t)pes, 4096);
+  L.head = o;
+  o = up(o + sizeof(line_u64) * (size_t)pes, 4096);
+  L.ctrl = o;
+  o = up(o + sizeof(int) * CTRL_WORDS, 4096);
+  L.progress = o;
+  o = up(o + 8ull * (size_t)pes, 2u << 20);
+  L.flags = o;
+  o = up(o + 8ull * ds.ring_cells * (size_t)pes, 2u << 20);
+  L.ring = o;
+  o = up(o + ds.ring_stride * (size_t)pes, 2u << 20);
+  L.bytes = o;
+  return L;
+}
+dev_inbox carve_inbox(unsigned char* base, const inbox_layout& L) {
+  dev_inbox d{};
+  d.tail = reinterpret_cast<line_u64*>(base + L.tail);
+  d.head = reinterpret_cast<line_u64*>(base + L.head);
+  d.ctrl = reinterpret_cast<int*>(base + L.ctrl);
+  d.progress = reinterpret_cast<unsigned long long*>(base + L.progress);
+  d.flags = reinterpret_cast<unsigned long long*>(base + L.flags);
+  d.ring = base + L.ring;
+  return d;
+}
+
+// What each rank tells the others at init.
+struct peer_record {
+  cudaIpcMemHandle_t handle;
+  uint64_t region_bytes, ring_bytes, max_msg;
+  int32_t pes, rank;
+};
+
+int host_barrier() {
+  if (g.world <= 1) return CHARMING_OK;
+  if (g.devs.barrier(g.devs.ctx) != 0) {
+    g_err = "host barrier failed";
+    return CHARMING_ERR_CONFIG;
+  }
+  return CHARMING_OK;
+}
 
 double env_double(const char* name, double dflt) {
   const char* s = getenv(name);
@@ -96,7 +156,11 @@ void request_stop(int value) {
 
 int enqueue_scheduler(cudaStream_t s) {
   if (!g.inited) return CHARMING_ERR_NOT_INIT;
-  int nb = (g.inf.n_pes + 255) / 256;
+  if (g.world > 1) {  // runs over several processes need the host barriers of run_scheduler
+    g_err = "stream-ordered runs are single-process";
+    return CHARMING_ERR_CONFIG;
+  }
+  int nb = (g.n_local + 255) / 256;
   charming_reset_kernel<<<nb, 256, 0, s>>>();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "reset kernel launch");
@@ -135,16 +199,22 @@ int enqueue_status_latch(int* latch, cudaStream_t s) {
 }
 
 int collect_run(double kernel_ms) {
+  // the first error any of this launch's GPUs recorded
   int ctrl_h[CTRL_WORDS];
-  cudaError_t e = cudaMemcpy(ctrl_h, g.ds.ctrl, sizeof(ctrl_h), cudaMemcpyDeviceToHost);
-  if (e != cudaSuccess) return cuda_fail(e, "read status");
-  std::vector<unsigned long long> st((size_t)g.inf.n_pes * N_STATS), tm((size_t)g.inf.n_pes * 3);
+  cudaError_t e = cudaSuccess;
+  for (size_t d = 0; d < g.launch_ctrl.size(); d++) {
+    e = cudaMemcpy(ctrl_h, g.launch_ctrl[d], sizeof(ctrl_h), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "read status");
+    if (ctrl_h[CTRL_STATUS] != 0) break;
+  }
+  const int n_local = g.n_local;
+  std::vector<unsigned long long> st((size_t)n_local * N_STATS), tm((size_t)n_local * 3);
   e = cudaMemcpy(st.data(), g.ds.pe_stats, st.size() * 8, cudaMemcpyDeviceToHost);
   if (e == cudaSuccess) e = cudaMemcpy(tm.data(), g.ds.pe_times, tm.size() * 8, cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_fail(e, "read stats");
   charming_stats s{};
   unsigned long long tmin = ~0ULL, tmax = 0, main_max = 0;
-  for (int p = 0; p < g.inf.n_pes; p++) {
+  for (int p = 0; p < n_local; p++) {
     const unsigned long long* t = &tm[3 * (size_t)p];
     if (t[1] > t[0] && t[1] - t[0] > main_max) main_max = t[1] - t[0];
     const unsigned long long* q = &st[(size_t)p * N_STATS];
@@ -161,18 +231,18 @@ int collect_run(double kernel_ms) {
   }
   s.loop_ms = (tmax > tmin && tmin != ~0ULL) ? (tmax - tmin) * 1e-6 : 0.0;
   double idle = 0;
-  for (int p = 0; p < g.inf.n_pes; p++) idle += (double)st[(size_t)p * N_STATS + ST_IDLE_CYC];
-  s.idle_ms = (g.inf.n_pes && g.prop.clockRate > 0) ? idle / g.inf.n_pes / (double)g.prop.clockRate : 0.0;
+  for (int p = 0; p < n_local; p++) idle += (double)st[(size_t)p * N_STATS + ST_IDLE_CYC];
+  s.idle_ms = (n_local && g.prop.clockRate > 0) ? idle / n_local / (double)g.prop.clockRate : 0.0;
   double em = 0;
-  for (int p = 0; p < g.inf.n_pes; p++) em += (double)st[(size_t)p * N_STATS + ST_EM_CYC];
-  s.em_ms = (g.inf.n_pes && g.prop.clockRate > 0) ? em / g.inf.n_pes / (double)g.prop.clockRate : 0.0;
+  for (int p = 0; p < n_local; p++) em += (double)st[(size_t)p * N_STATS + ST_EM_CYC];
+  s.em_ms = (n_local && g.prop.clockRate > 0) ? em / n_local / (double)g.prop.clockRate : 0.0;
   double tk = 0, sp = 0;
-  for (int p = 0; p < g.inf.n_pes; p++) {
+  for (int p = 0; p < n_local; p++) {
     tk += (double)st[(size_t)p * N_STATS + ST_TICKET_NS];
     sp += (double)st[(size_t)p * N_STATS + ST_SPACE_NS];
   }
-  s.ticket_ms = g.inf.n_pes ? tk / g.inf.n_pes * 1e-6 : 0.0;
-  s.space_ms = g.inf.n_pes ? sp / g.inf.n_pes * 1e-6 : 0.0;
+  s.ticket_ms = n_local ? tk / n_local * 1e-6 : 0.0;
+  s.space_ms = n_local ? sp / n_local * 1e-6 : 0.0;
   s.main_ms = main_max * 1e-6;
   s.kernel_ms = kernel_ms;
   s.status = ctrl_h[CTRL_STATUS];
@@ -212,10 +282,17 @@ int run_scheduler(int argc, char** argv) {
   if (e != cudaSuccess) return cuda_fail(e, "argv copy");
   *reinterpret_cast<volatile int*>(g.h_stop) = 0;
 
-  int nb = (g.inf.n_pes + 255) / 256;
+  // Several processes: the previous run has ended on every GPU (the barrier
+  // at the end of run_scheduler); every GPU resets before any launches.
+  int nb = (g.n_local + 255) / 256;
   charming_reset_kernel<<<nb, 256, 0, g.stream>>>();
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "reset kernel launch");
+  if (g.world > 1) {
+    e = cudaStreamSynchronize(g.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "reset");
+    if (int rc = host_barrier()) return rc;
+  }
 
   char** d_argv = reinterpret_cast<char**>(g.d_args);
   size_t* d_argvs = reinterpret_cast<size_t*>(g.d_args + (size_t)argc * sizeof(char*));
@@ -227,6 +304,8 @@ int run_scheduler(int argc, char** argv) {
   cudaEventRecord(g.ev1, g.stream);
   e = cudaStreamSynchronize(g.stream);
   if (e != cudaSuccess) return cuda_fail(e, "scheduler run");
+  // every launch has ended: nothing writes this GPU's control words any more
+  if (int rc = host_barrier()) return rc;
   float ms = 0.f;
   cudaEventElapsedTime(&ms, g.ev0, g.ev1);
   return collect_run(ms);
@@ -256,9 +335,23 @@ void charming_default_config(charming_config* cfg) {
   cfg->verbose = 0;
 }
 
-int charming_init(const charming_config* cfg_in) {
+int charming_init(const charming_config* cfg_in) { return charming_init_devices(cfg_in, nullptr); }
+
+int charming_init_devices(const charming_config* cfg_in, const charming_devices* devs) {
   if (g.inited) return CHARMING_OK;
   charming_config cfg = *cfg_in;
+  charming_devices dv{};
+  dv.world = 1;
+  dv.virtual_devs = 1;
+  if (devs) dv = *devs;
+  if (dv.world < 1) dv.world = 1;
+  if (dv.virtual_devs < 1) dv.virtual_devs = 1;
+  const int n_devs = dv.world > 1 ? dv.world : dv.virtual_devs;
+  if (n_devs > MAX_DEVS || dv.rank < 0 || dv.rank >= dv.world || (dv.world > 1 && dv.virtual_devs > 1) ||
+      (dv.world > 1 && (!dv.allgather || !dv.barrier)) || (n_devs > 1 && cfg.gpu_level)) {
+    set_error_text("invalid charming_devices (at most 8 GPUs, SM-level mode, collectives for world > 1)");
+    return CHARMING_ERR_CONFIG;
+  }
   g.inf = charming_info{};
   cudaError_t e = cudaSetDevice(cfg.device);
   if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
@@ -281,7 +374,16 @@ int charming_init(const charming_config* cfg_in) {
   // GPU-level mode: the blocks (n_pes of them, by default one per SM slot)
   // form one PE
   const int n_blocks = cfg.n_pes > 0 ? cfg.n_pes : n_sms * cfg.pes_per_sm;
-  int n_pes = cfg.gpu_level ? 1 : n_blocks;
+  if (n_blocks % dv.virtual_devs) {
+    set_error_text("PE blocks must split evenly into the virtual GPUs");
+    return CHARMING_ERR_CONFIG;
+  }
+  // Several GPUs: P PEs per GPU (all of this launch's blocks per process, or
+  // an equal share of them per virtual GPU), numbered globally.
+  const int pes_per_dev = dv.world > 1 ? n_blocks : n_blocks / dv.virtual_devs;
+  const int n_pes = cfg.gpu_level ? 1 : pes_per_dev * n_devs;
+  const int n_local = cfg.gpu_level ? 1 : n_blocks;  // this launch's PE slots
+  const int dev0 = dv.world > 1 ? dv.rank : 0;        // its first GPU
 
   // Device limits (reference: src/charming.cu:197-203).
   // The heap size is fixed once a kernel of the context has run (a second
@@ -354,7 +456,16 @@ int charming_init(const charming_config* cfg_in) {
   }
 
   g.cfg = cfg;
+  g.n_local = n_local;
+  g.rank = dv.rank;
+  g.world = dv.world;
+  g.vdevs = dv.virtual_devs;
+  g.devs = dv;
+  g.launch_ctrl.clear();
+  g.ipc_opened.clear();
   g.inf.n_pes = n_pes;
+  g.inf.n_devs = n_devs;
+  g.inf.my_dev = dev0;
   g.inf.n_blocks = n_blocks;
   g.inf.gpu_level = cfg.gpu_level ? 1 : 0;
   g.inf.n_sms = n_sms;
@@ -388,26 +499,71 @@ int charming_init(const charming_config* cfg_in) {
   ds.idle_sleep_ns = 2000;
   if (const char* ev = getenv("CHARMING_IDLE_SLEEP_NS")) ds.idle_sleep_ns = (unsigned)strtoul(ev, nullptr, 10);
   ds.n_blocks = n_blocks;
+  ds.n_devs = n_devs;
+  ds.pes_per_dev = cfg.gpu_level ? 1 : pes_per_dev;
+  ds.pe0 = dev0 * ds.pes_per_dev;
+  ds.n_procs = dv.world;
 
   int rc;
-  if ((rc = dev_alloc(&ds.tail, sizeof(line_u64) * n_pes, "inbox tails"))) return rc;
-  if ((rc = dev_alloc(&ds.head, sizeof(line_u64) * n_pes, "inbox heads"))) return rc;
-  if ((rc = dev_alloc(&ds.flags, 8ull * ds.ring_cells * n_pes, "inbox flags"))) return rc;
-  if ((rc = dev_alloc(&ds.ring, ds.ring_stride * n_pes, "inbox rings"))) return rc;
-  if ((rc = dev_alloc(&ds.stash_keys, sizeof(stash_key) * (size_t)ds.stash_entries * n_pes, "stash keys"))) return rc;
-  if ((rc = dev_alloc(&ds.stash_data, ds.stash_bytes * n_pes, "stash arena"))) return rc;
-  if ((rc = dev_alloc(&ds.proxy_tables, sizeof(charm::chare_proxy_table) * n_pes, "proxy tables"))) return rc;
-  if ((rc = dev_alloc(&ds.ctrl, sizeof(int) * CTRL_WORDS, "control words"))) return rc;
-  if ((rc = dev_alloc(&ds.progress, 8ull * n_pes, "progress"))) return rc;
-  if ((rc = dev_alloc(&ds.pe_stats, 8ull * N_STATS * n_pes, "stats"))) return rc;
-  if ((rc = dev_alloc(&ds.pe_times, 24ull * n_pes, "times"))) return rc;
+  // The inbox side: one region per GPU of this launch (one, or one per
+  // virtual GPU); with several processes, the others' regions mapped here.
+  const inbox_layout L = inbox_layout_for(cfg.gpu_level ? 1 : pes_per_dev, ds);
+  const int launch_devs = dv.world > 1 ? 1 : dv.virtual_devs;
+  unsigned char* own_region = nullptr;
+  for (int k = 0; k < launch_devs; k++) {
+    unsigned char* base = nullptr;
+    if ((rc = dev_alloc(&base, L.bytes, "inbox region"))) return rc;
+    if (k == 0) own_region = base;
+    ds.dev[dev0 + k] = carve_inbox(base, L);
+    g.launch_ctrl.push_back(ds.dev[dev0 + k].ctrl);
+  }
+  ds.tail = ds.dev[dev0].tail;
+  ds.head = ds.dev[dev0].head;
+  ds.flags = ds.dev[dev0].flags;
+  ds.ring = ds.dev[dev0].ring;
+  ds.ctrl = ds.dev[dev0].ctrl;
+  ds.progress = ds.dev[dev0].progress;
+  if (dv.world > 1) {
+    peer_record mine{};
+    e = cudaIpcGetMemHandle(&mine.handle, own_region);
+    if (e != cudaSuccess) return cuda_fail(e, "export the inbox region");
+    mine.region_bytes = L.bytes;
+    mine.ring_bytes = cfg.ring_bytes;
+    mine.max_msg = ds.max_msg;
+    mine.pes = pes_per_dev;
+    mine.rank = dv.rank;
+    std::vector<peer_record> all((size_t)dv.world);
+    if (dv.allgather(dv.ctx, &mine, all.data(), sizeof(peer_record)) != 0) {
+      set_error_text("host allgather failed");
+      return CHARMING_ERR_CONFIG;
+    }
+    for (int r = 0; r < dv.world; r++) {
+      const peer_record& q = all[(size_t)r];
+      if (q.rank != r || q.pes != mine.pes || q.region_bytes != mine.region_bytes ||
+          q.ring_bytes != mine.ring_bytes || q.max_msg != mine.max_msg) {
+        set_error_text("ranks disagree on PEs per GPU, ring or message sizes");
+        return CHARMING_ERR_CONFIG;
+      }
+      if (r == dv.rank) continue;
+      void* peer = nullptr;
+      e = cudaIpcOpenMemHandle(&peer, q.handle, cudaIpcMemLazyEnablePeerAccess);
+      if (e != cudaSuccess) return cuda_fail(e, "map a peer GPU's inbox region");
+      g.ipc_opened.push_back(peer);
+      ds.dev[r] = carve_inbox(static_cast<unsigned char*>(peer), L);
+    }
+  }
+  if ((rc = dev_alloc(&ds.stash_keys, sizeof(stash_key) * (size_t)ds.stash_entries * n_local, "stash keys"))) return rc;
+  if ((rc = dev_alloc(&ds.stash_data, ds.stash_bytes * n_local, "stash arena"))) return rc;
+  if ((rc = dev_alloc(&ds.proxy_tables, sizeof(charm::chare_proxy_table) * n_local, "proxy tables"))) return rc;
+  if ((rc = dev_alloc(&ds.pe_stats, 8ull * N_STATS * n_local, "stats"))) return rc;
+  if ((rc = dev_alloc(&ds.pe_times, 24ull * n_local, "times"))) return rc;
   if (ds.gpu_level && (rc = dev_alloc(&ds.gl, sizeof(group_state), "group state"))) return rc;
   // per-PE arena for proxy tables and chare objects (reset every run; the
   // device heap takes over when a PE needs more)
   ds.arena_bytes = 256ull << 10;
   if (const char* ev = getenv("CHARMING_ARENA_BYTES")) ds.arena_bytes = strtoull(ev, nullptr, 10);
   ds.arena = nullptr;
-  if (ds.arena_bytes && (rc = dev_alloc(&ds.arena, ds.arena_bytes * n_pes, "arena"))) return rc;
+  if (ds.arena_bytes && (rc = dev_alloc(&ds.arena, ds.arena_bytes * n_local, "arena"))) return rc;
   // per-PE outbox for sends deferred while their destination ring is full:
   // room for a few of the largest messages
   ds.outbox_bytes = 2 * ds.max_msg + (1ull << 20);
@@ -415,7 +571,7 @@ int charming_init(const charming_config* cfg_in) {
   ds.outbox_bytes = (ds.outbox_bytes + 127) / 128 * 128;
   ds.outbox_stride = ds.outbox_bytes + (ds.max_msg + OB_HDR + 127) / 128 * 128;
   ds.outbox = nullptr;
-  if (ds.outbox_bytes && (rc = dev_alloc(&ds.outbox, ds.outbox_stride * n_pes, "outbox"))) return rc;
+  if (ds.outbox_bytes && (rc = dev_alloc(&ds.outbox, ds.outbox_stride * n_local, "outbox"))) return rc;
   // malloc_user heap per PE
   ds.user_heap_bytes = 1ull << 20;
   if (const char* ev = getenv("CHARMING_USER_HEAP_BYTES")) ds.user_heap_bytes = strtoull(ev, nullptr, 10);
@@ -424,8 +580,8 @@ int charming_init(const charming_config* cfg_in) {
   ds.user_heap = nullptr;
   ds.user_blocks = nullptr;
   if (ds.user_heap_bytes) {
-    if ((rc = dev_alloc(&ds.user_heap, ds.user_heap_bytes * n_pes, "user heap"))) return rc;
-    if ((rc = dev_alloc(&ds.user_blocks, sizeof(user_block) * (size_t)ds.user_blocks_max * n_pes,
+    if ((rc = dev_alloc(&ds.user_heap, ds.user_heap_bytes * n_local, "user heap"))) return rc;
+    if ((rc = dev_alloc(&ds.user_blocks, sizeof(user_block) * (size_t)ds.user_blocks_max * n_local,
                         "user heap blocks")))
       return rc;
   }
@@ -436,12 +592,13 @@ int charming_init(const charming_config* cfg_in) {
   if (e != cudaSuccess) return cuda_fail(e, "host stop pointer");
   ds.host_stop = g.d_stop;
 
-  int one = 1, zero = 0;
+  // one NVSwitch domain: every GPU of the run is on this node
+  int one = 1;
   e = cudaMemcpyToSymbol(c_n_sms, &n_sms, sizeof(int));
-  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_my_dev, &zero, sizeof(int));
-  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_my_dev_node, &zero, sizeof(int));
-  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_n_devs, &one, sizeof(int));
-  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_n_devs_node, &one, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_my_dev, &dev0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_my_dev_node, &dev0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_n_devs, &n_devs, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_n_devs_node, &n_devs, sizeof(int));
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_n_nodes, &one, sizeof(int));
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_n_pes, &n_pes, sizeof(int));
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_n_pes_node, &n_pes, sizeof(int));
@@ -459,6 +616,10 @@ int charming_init(const charming_config* cfg_in) {
     if (ds.gpu_level)
       PINFO("GPU-level mode: 1 PE of %d blocks x %d threads, SMs: %d, regs/thread: %d\n", n_blocks,
           cfg.threads_per_pe, n_sms, fa.numRegs);
+    else if (n_devs > 1)
+      PINFO("PEs: %d on %d GPUs (%d per GPU, %s; this process: GPU %d), threads per PE: %d, regs/thread: %d\n",
+          n_pes, n_devs, pes_per_dev, dv.world > 1 ? "one process each" : "virtual, one launch", dev0,
+          cfg.threads_per_pe, fa.numRegs);
     else
       PINFO("PEs: %d (%d per SM), SMs: %d, threads per PE: %d, regs/thread: %d\n", n_pes,
           cfg.pes_per_sm, n_sms, cfg.threads_per_pe, fa.numRegs);
@@ -496,6 +657,16 @@ int charming_timer_stop(double* ms) {
 int charming_fini(void) {
   if (!g.inited) return CHARMING_OK;
   cudaDeviceSynchronize();
+  if (g.world > 1) {
+    // unmap the peers' regions once no GPU runs; free this one once every
+    // peer has unmapped it
+    (void)host_barrier();
+    for (void* p : g.ipc_opened) cudaIpcCloseMemHandle(p);
+    (void)host_barrier();
+  }
+  g.ipc_opened.clear();
+  g.launch_ctrl.clear();
+  g.world = 1;
   for (void* p : g.dev_allocs) cudaFree(p);
   g.dev_allocs.clear();
   if (g.d_args) cudaFree(g.d_args);

@@ -18,6 +18,14 @@
 //                           receiver has consumed up to that ticket
 //   user_heap[pe]           malloc_user / free_user blocks of the PE
 // Cell and flag indices are (ticket mod C); C is a power of two.
+//
+// A run over several GPUs (one process per GPU, one NVSwitch domain): global
+// PE p is local PE p % pes_per_dev of GPU p / pes_per_dev. Each GPU's inbox
+// side (tail, head, flags, ring, control words, progress stamps) is one
+// allocation; the others reach it through device_state::dev[], mapped with
+// CUDA IPC. A sender writes straight into the receiver's ring over NVLink:
+// no relay PE between GPUs. The ticket atomics, sequence words, heads and
+// control words then use system scope.
 #pragma once
 
 #include <charming.h>
@@ -93,6 +101,19 @@ enum : int {
   N_STATS = 13
 };
 
+constexpr int MAX_DEVS = 8;  // GPUs of one NVSwitch domain
+
+// The inbox side of one GPU's PEs as this process addresses it: its own
+// memory, or a peer GPU's mapped over NVLink.
+struct dev_inbox {
+  line_u64* tail;                      // [pes_per_dev]
+  line_u64* head;                      // [pes_per_dev]
+  unsigned long long* flags;           // [pes_per_dev][C]
+  unsigned char* ring;                 // [pes_per_dev][ring_stride]
+  int* ctrl;                           // [CTRL_WORDS]
+  unsigned long long* progress;        // [pes_per_dev]
+};
+
 // Device-wide runtime description, copied to __constant__ memory before each
 // launch.
 struct device_state {
@@ -135,6 +156,12 @@ struct device_state {
   int gpu_level;                       // 1: all blocks form PE 0 (group_state below)
   int n_blocks;                        // thread blocks of the launch (n_pes when 0)
   struct group_state* gl;              // GPU-level mode only
+  // several GPUs (n_devs > 1); with one GPU, dev[0] holds the fields above
+  int n_devs;                          // GPUs of the run
+  int pes_per_dev;                     // PEs on each GPU
+  int pe0;                             // global PE of this launch's block 0
+  int n_procs;                         // processes (1: GPUs emulated in one launch)
+  dev_inbox dev[MAX_DEVS];
 };
 
 // GPU-level mode (the reference's default build, src/sched/scheduler.cu:
@@ -167,7 +194,8 @@ enum : int {
   CTRL_ERR_I1 = 35,
   CTRL_BAR_COUNT = 64,
   CTRL_BAR_GEN = 96,
-  CTRL_WORDS = 128
+  CTRL_XBAR = 128,      // GPU 0 only: arrivals at cross-process barriers
+  CTRL_WORDS = 160
 };
 
 extern __constant__ device_state c_rt;
@@ -295,6 +323,14 @@ __device__ __forceinline__ unsigned long long ld_relaxed_sys_u64(const unsigned 
 __device__ __forceinline__ void st_release_sys_u64(unsigned long long* p, unsigned long long v) {
   asm volatile("st.release.sys.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
 }
+__device__ __forceinline__ void st_relaxed_sys_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.sys.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned int ld_acquire_sys_u32(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
 // Acquire side for data published before words read with relaxed loads.
 __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 // A signal word polled relaxed, made an acquire by fence_acq_rel_gpu on a hit.
@@ -320,6 +356,8 @@ inline unsigned long long ld_volatile_shared_u64(const unsigned long long* p) { 
 inline unsigned long long ld_acquire_sys_u64(const unsigned long long* p) { return __atomic_load_n(p, __ATOMIC_ACQUIRE); }
 inline unsigned long long ld_relaxed_sys_u64(const unsigned long long* p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
 inline void st_release_sys_u64(unsigned long long* p, unsigned long long v) { __atomic_store_n(p, v, __ATOMIC_RELEASE); }
+inline void st_relaxed_sys_u64(unsigned long long* p, unsigned long long v) { __atomic_store_n(p, v, __ATOMIC_RELAXED); }
+inline unsigned int ld_acquire_sys_u32(const unsigned int* p) { return __atomic_load_n(p, __ATOMIC_ACQUIRE); }
 inline void fence_acq_rel_gpu() { std::atomic_thread_fence(std::memory_order_acq_rel); }
 // ThreadSanitizer does not model fences: the host check polls with acquire
 // loads, which give the same ordering as relaxed loads plus the fence.
@@ -327,11 +365,39 @@ inline unsigned long long ld_signal_u64(const unsigned long long* p) { return __
 unsigned long long globaltimer();
 #endif
 
+// Control words of this launch (grid barrier; with one GPU, all of them).
 __device__ __forceinline__ int* ctrl(int w) { return c_rt.ctrl + w; }
 
-// Error path: first error wins; every PE stops.
+// ---- several GPUs ----------------------------------------------------------
+__device__ __forceinline__ bool multi_dev() { return c_rt.n_devs > 1; }
+__device__ __forceinline__ int dev_of(int pe) { return multi_dev() ? pe / c_rt.pes_per_dev : 0; }
+__device__ __forceinline__ int local_of(int pe) { return multi_dev() ? pe % c_rt.pes_per_dev : pe; }
+// The GPU the calling block belongs to.
+__device__ __forceinline__ int my_dev() {
+  return multi_dev() ? (c_rt.pe0 + (int)blockIdx.x) / c_rt.pes_per_dev : 0;
+}
+__device__ __forceinline__ int* dev_ctrl(int d, int w) { return c_rt.dev[d].ctrl + w; }
+// Inbox words other GPUs read or write: system scope when the run has more
+// than one GPU.
+__device__ __forceinline__ unsigned long long ld_acquire_x(const unsigned long long* p) {
+  return multi_dev() ? ld_acquire_sys_u64(p) : ld_acquire_u64(p);
+}
+__device__ __forceinline__ void st_release_x(unsigned long long* p, unsigned long long v) {
+  if (multi_dev()) st_release_sys_u64(p, v);
+  else st_release_u64(p, v);
+}
+__device__ __forceinline__ unsigned long long atomic_add_x(unsigned long long* p, unsigned long long v) {
+  return multi_dev() ? atomicAdd_system(p, v) : atomicAdd(p, v);
+}
+
+// Error path: first error wins; every PE (of every GPU) stops.
 __device__ void set_error(int code, int info0, int info1);
-__device__ __forceinline__ bool terminated() { return ld_relaxed_s32(ctrl(CTRL_TERM)) != 0; }
+// Every PE of every GPU leaves its loop (end(), a terminate message, the
+// host's stop word).
+__device__ void raise_term();
+__device__ __forceinline__ bool terminated() {
+  return multi_dev() ? ld_sys_s32(dev_ctrl(my_dev(), CTRL_TERM)) != 0 : ld_relaxed_s32(ctrl(CTRL_TERM)) != 0;
+}
 
 // Deadline check for bounded waits (thread-local view).
 __device__ __forceinline__ bool past_deadline() {
@@ -344,6 +410,10 @@ __device__ void grid_barrier();
 __device__ bool grid_barrier_ok();
 
 __device__ __forceinline__ bool gpu_level() { return c_rt.gpu_level != 0; }
+// The calling PE's index in this process's per-PE arrays (stash, outbox,
+// user heap, proxy tables, arena, statistics), and their length.
+__device__ __forceinline__ int local_slot() { return gpu_level() ? 0 : (int)blockIdx.x; }
+__device__ __forceinline__ int local_slots() { return gpu_level() ? 1 : c_rt.n_blocks; }
 // Loads of the group_state records written by another SM.
 __device__ __forceinline__ void* gl_ld_ptr(void* const* p) {
   return reinterpret_cast<void*>(ld_relaxed_u64(reinterpret_cast<const unsigned long long*>(p)));

@@ -54,14 +54,36 @@ using namespace charm::rt;
 // Errors and termination
 // ---------------------------------------------------------------------------
 __device__ void charm::rt::set_error(int code, int info0, int info1) {
-  int prev = atomicCAS(ctrl(CTRL_STATUS), 0, code);
-  if (prev == 0) {
-    atomicExch(ctrl(CTRL_ERR_PE), (int)blockIdx.x);
-    atomicExch(ctrl(CTRL_ERR_I0), info0);
-    atomicExch(ctrl(CTRL_ERR_I1), info1);
+  const int pe = c_rt.pe0 + (int)blockIdx.x;
+  if (!multi_dev()) {
+    int prev = atomicCAS(ctrl(CTRL_STATUS), 0, code);
+    if (prev == 0) {
+      atomicExch(ctrl(CTRL_ERR_PE), pe);
+      atomicExch(ctrl(CTRL_ERR_I0), info0);
+      atomicExch(ctrl(CTRL_ERR_I1), info1);
+    }
+    __threadfence();
+    atomicExch(ctrl(CTRL_TERM), 1);
+    return;
   }
-  __threadfence();
-  atomicExch(ctrl(CTRL_TERM), 1);
+  // Several GPUs: each records the first error it hears of, then all stop.
+  for (int d = 0; d < c_rt.n_devs; d++) {
+    if (atomicCAS_system(dev_ctrl(d, CTRL_STATUS), 0, code) == 0) {
+      atomicExch_system(dev_ctrl(d, CTRL_ERR_PE), pe);
+      atomicExch_system(dev_ctrl(d, CTRL_ERR_I0), info0);
+      atomicExch_system(dev_ctrl(d, CTRL_ERR_I1), info1);
+    }
+  }
+  __threadfence_system();
+  for (int d = 0; d < c_rt.n_devs; d++) atomicExch_system(dev_ctrl(d, CTRL_TERM), 1);
+}
+
+__device__ void charm::rt::raise_term() {
+  if (!multi_dev()) {
+    atomicExch(ctrl(CTRL_TERM), 1);
+    return;
+  }
+  for (int d = 0; d < c_rt.n_devs; d++) atomicExch_system(dev_ctrl(d, CTRL_TERM), 1);
 }
 
 __device__ void charm::detail::report_error(int code, int info0, int info1) {
@@ -89,13 +111,13 @@ __device__ void* charm::detail::pe_alloc(size_t bytes) {
   unsigned long long at = (ps->arena_top + 15) & ~15ULL;
   if (at + bytes > c_rt.arena_bytes) return nullptr;
   ps->arena_top = at + bytes;
-  return c_rt.arena + (unsigned long long)charm::my_pe() * c_rt.arena_bytes + at;
+  return c_rt.arena + (unsigned long long)local_slot() * c_rt.arena_bytes + at;
 }
 
 __device__ bool charm::detail::pe_owns(const void* p) {
   const unsigned char* b = static_cast<const unsigned char*>(p);
   if (b >= smem_arena() && b < smem_arena() + c_rt.smem_arena_bytes) return true;
-  return c_rt.arena && b >= c_rt.arena && b < c_rt.arena + (unsigned long long)c_rt.n_pes * c_rt.arena_bytes;
+  return c_rt.arena && b >= c_rt.arena && b < c_rt.arena + (unsigned long long)local_slots() * c_rt.arena_bytes;
 }
 
 __device__ void charm::detail::cache_proxy(int id, chare_proxy_base* p) {
@@ -103,11 +125,11 @@ __device__ void charm::detail::cache_proxy(int id, chare_proxy_base* p) {
 }
 
 __device__ chare_proxy_table& charm::detail::my_proxy_table() {
-  return c_rt.proxy_tables[charm::my_pe()];
+  return c_rt.proxy_tables[local_slot()];
 }
 
 __device__ void charm::end() {
-  if (!terminated()) atomicExch(ctrl(CTRL_TERM), 1);
+  if (!terminated()) raise_term();
 }
 
 __device__ void charm::send_begin_term_msg() { charm::end(); }
@@ -118,7 +140,7 @@ __device__ void charm::abort() {
   __syncthreads();
 }
 
-__device__ int charm::my_pe() { return gpu_level() ? 0 : (int)blockIdx.x; }
+__device__ int charm::my_pe() { return gpu_level() ? 0 : c_rt.pe0 + (int)blockIdx.x; }
 __device__ int charm::n_pes() { return c_n_pes; }
 __device__ int charm::my_pe_node() { return charm::my_pe(); }
 __device__ int charm::n_pes_node() { return c_n_pes_node; }
@@ -201,7 +223,36 @@ __device__ bool charm::rt::grid_barrier_ok() {
 
 __device__ void charm::rt::grid_barrier() { (void)grid_barrier_ok(); }
 
-__device__ void charm::barrier() { grid_barrier(); }
+// Thread 0 of block 0 of each process: all processes of the run. Arrivals
+// take tickets on one counter in GPU 0's control words (never reset within
+// a run); the k-th barrier is complete when it reaches (k + 1) * n_procs.
+__device__ bool xproc_barrier_ok() {
+  unsigned int* cnt = reinterpret_cast<unsigned int*>(dev_ctrl(0, CTRL_XBAR));
+  const unsigned int n = (unsigned int)c_rt.n_procs;
+  const unsigned int goal = (atomicAdd_system(cnt, 1u) / n + 1) * n;
+  unsigned int spins = 0;
+  while ((int)(ld_acquire_sys_u32(cnt) - goal) < 0) {
+    if ((++spins & 255) == 0) {
+      if (terminated()) return false;
+      if (past_deadline()) {
+        set_error(CHARMING_ERR_BARRIER_TIMEOUT, -1, (int)goal);
+        return false;
+      }
+    }
+    __nanosleep(200);
+  }
+  return true;
+}
+
+// All PEs of the run (reference: nvshmem_barrier_all and a grid sync,
+// src/sched/scheduler.cu:336-344); barrier_local(): this GPU's launch.
+__device__ void charm::barrier() {
+  grid_barrier();
+  if (c_rt.n_procs > 1) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) (void)xproc_barrier_ok();
+    grid_barrier();
+  }
+}
 __device__ void charm::barrier_local() { grid_barrier(); }
 
 // ---------------------------------------------------------------------------
@@ -209,12 +260,24 @@ __device__ void charm::barrier_local() { grid_barrier(); }
 // ---------------------------------------------------------------------------
 namespace {
 
+// PE pe's inbox words and cells (global PE number; with several GPUs, in
+// the memory of the GPU it lives on).
 __device__ __forceinline__ unsigned char* ring_cell(int pe, unsigned long long ticket) {
-  return c_rt.ring + (unsigned long long)pe * c_rt.ring_stride +
-         (ticket & (c_rt.ring_cells - 1)) * CELL;
+  unsigned char* base = multi_dev() ? c_rt.dev[dev_of(pe)].ring : c_rt.ring;
+  return base + (unsigned long long)local_of(pe) * c_rt.ring_stride + (ticket & (c_rt.ring_cells - 1)) * CELL;
 }
 __device__ __forceinline__ unsigned long long* ring_flag(int pe, unsigned long long ticket) {
-  return c_rt.flags + (unsigned long long)pe * c_rt.ring_cells + (ticket & (c_rt.ring_cells - 1));
+  unsigned long long* base = multi_dev() ? c_rt.dev[dev_of(pe)].flags : c_rt.flags;
+  return base + (unsigned long long)local_of(pe) * c_rt.ring_cells + (ticket & (c_rt.ring_cells - 1));
+}
+__device__ __forceinline__ unsigned long long* tail_of(int pe) {
+  return multi_dev() ? &c_rt.dev[dev_of(pe)].tail[local_of(pe)].v : &c_rt.tail[pe].v;
+}
+__device__ __forceinline__ unsigned long long* head_of(int pe) {
+  return multi_dev() ? &c_rt.dev[dev_of(pe)].head[local_of(pe)].v : &c_rt.head[pe].v;
+}
+__device__ __forceinline__ unsigned long long* progress_of(int pe) {
+  return multi_dev() ? &c_rt.dev[dev_of(pe)].progress[local_of(pe)] : &c_rt.progress[pe];
 }
 
 __device__ __forceinline__ unsigned char* outbox_of(int pe) {
@@ -279,7 +342,7 @@ __device__ unsigned char* wait_space(int dst, unsigned long long t, unsigned lon
 __device__ unsigned char* reserve(int dst, unsigned long long bytes, unsigned long long* ticket) {
   if (!send_allowed(dst, bytes)) return nullptr;
   CHARM_PROF(pe_state* ps = pes(); const unsigned long long t0 = globaltimer();)
-  const unsigned long long t = atomicAdd(&c_rt.tail[dst].v, (unsigned long long)cells_for(bytes));
+  const unsigned long long t = atomic_add_x(tail_of(dst), (unsigned long long)cells_for(bytes));
   CHARM_PROF(const unsigned long long t1 = globaltimer();)
   unsigned char* m = wait_space(dst, t, bytes, ticket);
   CHARM_PROF(atomicAdd_block(&ps->stats[ST_TICKET_NS], t1 - t0);
@@ -305,13 +368,13 @@ __device__ unsigned char* wait_space(int dst, unsigned long long t, unsigned lon
     // ps->head is stable during an entry method, and the message being
     // processed is not yet counted as consumed, so publishing it is safe
     // (and harmless when repeated).
-    st_release_u64(&c_rt.head[blockIdx.x].v, ps->head);
+    st_release_x(head_of(ps->my_pe), ps->head);
     unsigned long long start = globaltimer();
     // A receiver that frees nothing for the idle timeout is taken as stuck.
     unsigned long long limit = c_rt.idle_timeout_ns ? c_rt.idle_timeout_ns : c_rt.deadline_ns;
     unsigned int spins = 0;
     while (true) {
-      unsigned long long h = ld_acquire_u64(&c_rt.head[dst].v);
+      unsigned long long h = ld_acquire_x(head_of(dst));
       atomicMax(&hc[dst], h);  // monotonic; several threads may reserve at once
       if (t + cells - h <= C) break;
       if ((++spins & 255) == 0) {
@@ -341,7 +404,7 @@ __device__ unsigned char* wait_space(int dst, unsigned long long t, unsigned lon
 // the barrier the callers pass first (release is cumulative), and a separate
 // fence would also invalidate the SM's L1.
 __device__ __forceinline__ void publish(int dst, unsigned long long ticket) {
-  st_release_u64(ring_flag(dst, ticket), ticket + 1);
+  st_release_x(ring_flag(dst, ticket), ticket + 1);
 }
 
 // Publishes the message at m (reserved by reserve() for ticket in dst's
@@ -364,7 +427,7 @@ __device__ bool outbox_head_ready() {
   const ob_entry* e =
       reinterpret_cast<const ob_entry*>(outbox_of(blockIdx.x) + ps->ob_head % c_rt.outbox_bytes);
   if (e->state != OB_READY) return false;
-  const unsigned long long h = ld_acquire_u64(&c_rt.head[e->dst].v);
+  const unsigned long long h = ld_acquire_x(head_of(e->dst));
   atomicMax(&head_cache()[e->dst], h);
   return e->ticket + cells_for(e->bytes) - h <= c_rt.ring_cells;
 }
@@ -374,14 +437,15 @@ __device__ bool outbox_head_ready() {
 // lazily, after an eighth of the ring or before waiting for messages.
 __device__ __forceinline__ void publish_head(pe_state* ps, int me) {
   if (ps->head != ps->head_pub) {
-    st_release_u64(&c_rt.head[me].v, ps->head);
+    st_release_x(head_of(me), ps->head);
     ps->head_pub = ps->head;
   }
 }
 
 // Thread 0: the progress stamp the idle-timeout check reads.
 __device__ __forceinline__ void stamp_progress(int me) {
-  st_relaxed_u64(&c_rt.progress[me], pes()->stats[ST_DELIVERED]);
+  if (multi_dev()) st_relaxed_sys_u64(progress_of(me), pes()->stats[ST_DELIVERED]);
+  else st_relaxed_u64(progress_of(me), pes()->stats[ST_DELIVERED]);
 }
 
 } // namespace
@@ -523,7 +587,7 @@ __device__ void charm::send_reg_msg(int chare_id, int chare_idx, int ep_id, void
     if (m) {
       envelope* env = reinterpret_cast<envelope*>(m);
       env->type = msgtype::regular;
-      env->src_pe = (int)blockIdx.x;
+      env->src_pe = c_rt.pe0 + (int)blockIdx.x;
       env->size = bytes;
       regular_msg* rm = reinterpret_cast<regular_msg*>(m + sizeof(envelope));
       rm->chare_id = chare_id;
@@ -596,7 +660,7 @@ __device__ void charm::send_user_msg(int chare_id, int chare_idx, int ep_id,
     unsigned char* m = reinterpret_cast<unsigned char*>(msg.env);
     envelope* env = msg.env;
     env->type = msgtype::user;
-    env->src_pe = (int)blockIdx.x;
+    env->src_pe = c_rt.pe0 + (int)blockIdx.x;
     // The ring advances by the reserved size, whatever part was filled.
     env->size = (size_t)msg.capacity + HDR;
     regular_msg* rm = reinterpret_cast<regular_msg*>(m + sizeof(envelope));
@@ -644,7 +708,7 @@ __device__ bool charm::alloc_user_msgs(message* msgs, const int* dst_pes,
       }
       unsigned long long base = 0;
       CHARM_PROF(const unsigned long long ta = k == 0 ? globaltimer() : 0;)
-      if (ok && k == leader) base = atomicAdd(&c_rt.tail[dst_pes[k]].v, (unsigned long long)tot);
+      if (ok && k == leader) base = atomic_add_x(tail_of(dst_pes[k]), (unsigned long long)tot);
       base = __shfl_sync(FULL, base, leader);
       CHARM_PROF(__syncwarp(); const unsigned long long tb = k == 0 ? globaltimer() : 0;)
       if (act) {
@@ -698,7 +762,7 @@ __device__ void charm::send_user_msgs(int chare_id, const int* chare_idx, int ep
     unsigned char* m = reinterpret_cast<unsigned char*>(msgs[k].env);
     envelope* env = msgs[k].env;
     env->type = msgtype::user;
-    env->src_pe = (int)blockIdx.x;
+    env->src_pe = c_rt.pe0 + (int)blockIdx.x;
     env->size = (size_t)msgs[k].capacity + HDR;
     regular_msg* rm = reinterpret_cast<regular_msg*>(m + sizeof(envelope));
     rm->chare_id = chare_id;
@@ -927,7 +991,11 @@ __device__ void check_idle_timeout(unsigned long long now) {
   if (c_rt.idle_timeout_ns == 0) return;
   pe_state* ps = pes();
   unsigned long long sum = 0;
-  for (int p = 0; p < c_rt.n_pes; p++) sum += ld_relaxed_u64(&c_rt.progress[p]);
+  if (multi_dev()) {
+    for (int p = 0; p < c_rt.n_pes; p++) sum += ld_relaxed_sys_u64(progress_of(p));
+  } else {
+    for (int p = 0; p < c_rt.n_pes; p++) sum += ld_relaxed_u64(&c_rt.progress[p]);
+  }
   if (sum != ps->idle_sum) {
     ps->idle_sum = sum;
     ps->idle_change_ns = now;
@@ -987,13 +1055,13 @@ __device__ chare_proxy_base* take_satisfied_wait(int* idx, int* ep) {
 // are pending (checked every 256 polls), 0 when this PE must leave the loop.
 __device__ int poll_inbox() {
   pe_state* ps = pes();
-  const int me = blockIdx.x;
+  const int me = ps->my_pe;
   unsigned long long h = ps->head;
   const unsigned long long* f = ring_flag(me, h);
   unsigned int spins = 0;
   unsigned long long idle_t0 = 0;
   while (true) {
-    if (ld_acquire_u64(f) == h + 1) {
+    if (ld_acquire_x(f) == h + 1) {
       if (idle_t0) ps->stats[ST_IDLE_CYC] += (unsigned long long)clock64() - idle_t0;
       // a PE that always has a message (a chare that keeps calling itself)
       // still sees the end of the run and its deadline
@@ -1044,7 +1112,7 @@ __device__ int poll_inbox() {
         if (c_rt.host_stop) {
           int hs = ld_sys_s32(c_rt.host_stop);
           if (hs == 1) {
-            atomicExch(ctrl(CTRL_TERM), 1);
+            raise_term();
             return 0;
           } else if (hs > 1) {
             set_error(CHARMING_ERR_HOST_STOP, hs, 0);
@@ -1065,7 +1133,7 @@ __device__ int poll_inbox() {
 // Thread 0: the thread-0 part that closes the action the block just executed.
 __device__ void finish_action() {
   pe_state* ps = pes();
-  const int me = blockIdx.x;
+  const int me = ps->my_pe;
   switch (ps->d_act) {
     case ACT_CALL_RING:
     case ACT_STASH_PUT:
@@ -1076,7 +1144,7 @@ __device__ void finish_action() {
       break;
     case ACT_CALL_STASH: {
       const unsigned long long S = (unsigned long long)c_rt.stash_entries;
-      keys_of(me)[ps->d_key % S].state = KEY_FREE;
+      keys_of(blockIdx.x)[ps->d_key % S].state = KEY_FREE;
       ps->n_ready--;
       if ((++ps->stats[ST_DELIVERED] & 15) == 0) stamp_progress(me);
       stash_retire();
@@ -1109,7 +1177,8 @@ __device__ void finish_action() {
 // Thread 0: decides what the block does next (pe_state d_* fields).
 __device__ void next_action() {
   pe_state* ps = pes();
-  const int me = blockIdx.x;
+  const int me = ps->my_pe;
+  const int slot = blockIdx.x;
   const unsigned long long S = (unsigned long long)c_rt.stash_entries;
   while (true) {
     if (ps->term) {
@@ -1119,7 +1188,7 @@ __device__ void next_action() {
     // deferred sends whose receivers have room
     if (ps->ob_count > 0 && outbox_head_ready()) {
       ps->d_act = ACT_FLUSH;
-      ps->d_p = outbox_of(me) + ps->ob_head % c_rt.outbox_bytes;
+      ps->d_p = outbox_of(slot) + ps->ob_head % c_rt.outbox_bytes;
       return;
     }
     // satisfied async waits
@@ -1159,7 +1228,7 @@ __device__ void next_action() {
         ps->n_ready = 0;
         break;
       }
-      stash_key* k = keys_of(me) + (i % S);
+      stash_key* k = keys_of(slot) + (i % S);
       chare_proxy_base* p = proxy_of(ps, k->chare_id);
       if (!p->refnum_matches(k->chare_idx, k->refnum)) {  // refnum moved on again
         k->state = KEY_WAIT;
@@ -1171,7 +1240,7 @@ __device__ void next_action() {
         ps->d_act = ACT_EXIT;
         return;
       }
-      const unsigned char* env = arena_of(me) + (k->data_off % c_rt.stash_bytes);
+      const unsigned char* env = arena_of(slot) + (k->data_off % c_rt.stash_bytes);
       const regular_msg* rm = reinterpret_cast<const regular_msg*>(env + sizeof(envelope));
       ps->d_act = ACT_CALL_STASH;
       ps->d_p = p;
@@ -1219,7 +1288,7 @@ __device__ void next_action() {
         }
       }
     } else if (type == (int)msgtype::do_terminate || type == (int)msgtype::begin_terminate) {
-      atomicExch(ctrl(CTRL_TERM), 1);
+      raise_term();
     } else {
       set_error(CHARMING_ERR_BAD_MSG, env->src_pe, type);
     }
@@ -1299,6 +1368,7 @@ __global__ void __launch_bounds__(MAX_THREADS, 1)
 charming_scheduler_kernel(int argc, char** argv, size_t* argvs) {
   pe_state* ps = pes();
   const int me = charm::my_pe();
+  const int slot = local_slot();
   // the block that keeps the PE's state (every block in SM-level mode)
   const bool keeper = !gpu_level() || blockIdx.x == 0;
   if (threadIdx.x == 0) {
@@ -1306,7 +1376,7 @@ charming_scheduler_kernel(int argc, char** argv, size_t* argvs) {
     ps->term = 0;
     ps->sent_term = 0;
     ps->revive_pending = 0;
-    ps->head = c_rt.head[me].v;
+    ps->head = *head_of(me);
     ps->head_pub = ps->head;
     ps->t0 = globaltimer();
     ps->key_head = ps->key_tail = 0;
@@ -1337,7 +1407,8 @@ charming_scheduler_kernel(int argc, char** argv, size_t* argvs) {
     ps->idle_checks = 0;
     for (int i = 0; i < PROXY_CACHE; i++) ps->pcache[i] = nullptr;
   }
-  for (int i = threadIdx.x; i < c_rt.n_pes; i += blockDim.x) head_cache()[i] = c_rt.head[i].v;
+  for (int i = threadIdx.x; i < c_rt.n_pes; i += blockDim.x)
+    head_cache()[i] = multi_dev() ? ld_relaxed_sys_u64(head_of(i)) : c_rt.head[i].v;
   __syncthreads();
 
   grid_barrier();
@@ -1353,12 +1424,12 @@ charming_scheduler_kernel(int argc, char** argv, size_t* argvs) {
 
   if (threadIdx.x == 0 && keeper) {
     ps->stats[ST_LOOP_NS] = loop_t1 - loop_t0;
-    for (int i = 0; i < N_STATS; i++) c_rt.pe_stats[(unsigned long long)me * N_STATS + i] = ps->stats[i];
-    c_rt.pe_times[3 * me] = ps->t0;
-    c_rt.pe_times[3 * me + 1] = loop_t0;
-    c_rt.pe_times[3 * me + 2] = loop_t1;
+    for (int i = 0; i < N_STATS; i++) c_rt.pe_stats[(unsigned long long)slot * N_STATS + i] = ps->stats[i];
+    c_rt.pe_times[3 * slot] = ps->t0;
+    c_rt.pe_times[3 * slot + 1] = loop_t0;
+    c_rt.pe_times[3 * slot + 2] = loop_t1;
     if (c_rt.free_chares_at_exit) {
-      chare_proxy_table& tb = c_rt.proxy_tables[me];
+      chare_proxy_table& tb = c_rt.proxy_tables[slot];
       for (int i = tb.count - 1; i >= 0; i--) {
         chare_proxy_base* p = tb.proxies[i];
         if (p) {
@@ -1372,22 +1443,30 @@ charming_scheduler_kernel(int argc, char** argv, size_t* argvs) {
   }
 }
 
-// Resets per-run control words: every inbox restarts at its current tail
-// (messages left over from an earlier run are dropped), proxy tables empty.
+// Resets per-run control words of this launch's GPUs: every inbox restarts
+// at its current tail (messages left over from an earlier run are dropped),
+// proxy tables empty. With several GPUs, the host runs it on every GPU
+// between two host barriers: after every launch of the last run has ended,
+// before any of the next starts.
 __global__ void charming_reset_kernel() {
-  int n = c_rt.n_pes;
+  const int n = c_rt.gpu_level ? c_rt.n_pes : c_rt.n_blocks;  // PEs of this launch
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    unsigned long long t = c_rt.tail[i].v;
-    c_rt.head[i].v = t;
-    c_rt.progress[i] = 0;
+    const int pe = c_rt.pe0 + i;
+    *head_of(pe) = *tail_of(pe);
+    *progress_of(pe) = 0;
     c_rt.proxy_tables[i].count = 0;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    c_rt.ctrl[CTRL_TERM] = 0;
-    c_rt.ctrl[CTRL_STATUS] = 0;
-    c_rt.ctrl[CTRL_ERR_PE] = -1;
-    c_rt.ctrl[CTRL_ERR_I0] = 0;
-    c_rt.ctrl[CTRL_ERR_I1] = 0;
+    const int d0 = dev_of(c_rt.pe0), d1 = dev_of(c_rt.pe0 + n - 1);
+    for (int d = d0; d <= d1; d++) {
+      int* w = c_rt.dev[d].ctrl;
+      w[CTRL_TERM] = 0;
+      w[CTRL_STATUS] = 0;
+      w[CTRL_ERR_PE] = -1;
+      w[CTRL_ERR_I0] = 0;
+      w[CTRL_ERR_I1] = 0;
+      w[CTRL_XBAR] = 0;
+    }
     c_rt.ctrl[CTRL_BAR_COUNT] = 0;
   }
 }

@@ -43,12 +43,46 @@ class RunStats:
     space_ms: float = 0.0
 
 
+def host_collectives(group=None):
+    """The allgather and barrier a run over several GPUs needs from its host
+    (charming_devices), over a torch.distributed process group (a CPU
+    backend such as gloo: they exchange host bytes).  Returns the two ctypes
+    callbacks; keep them alive as long as the runtime."""
+    import torch
+    import torch.distributed as dist
+
+    def allgather(_ctx, mine, out, nbytes):
+        try:
+            t = torch.frombuffer(bytearray(C.string_at(mine, nbytes)), dtype=torch.uint8)
+            parts = [torch.empty_like(t) for _ in range(dist.get_world_size(group))]
+            dist.all_gather(parts, t, group=group)
+            buf = b"".join(bytes(p.numpy()) for p in parts)
+            C.memmove(out, buf, len(buf))
+            return 0
+        except Exception:  # the C side reports the failure
+            return -1
+
+    def barrier(_ctx):
+        try:
+            dist.barrier(group=group)
+            return 0
+        except Exception:
+            return -1
+
+    return _lib.ALLGATHER_FN(allgather), _lib.BARRIER_FN(barrier)
+
+
 class Runtime:
-    """One initialised runtime on one GPU (process-wide, like the reference)."""
+    """One initialised runtime on one GPU (process-wide, like the reference).
+
+    Several GPUs: ``group`` (a torch.distributed process group, one rank per
+    GPU, a CPU backend) makes a run over all its ranks, collective like the
+    reference's NVSHMEM runs; ``virtual_devs=n`` splits this GPU's PEs into n
+    GPUs in one launch (the same transport on one GPU)."""
 
     _active: "Runtime | None" = None
 
-    def __init__(self, **overrides):
+    def __init__(self, group=None, virtual_devs: int = 1, **overrides):
         self.lib = _lib.load()
         cfg = _lib.Config()
         self.lib.charming_default_config(C.byref(cfg))
@@ -58,7 +92,15 @@ class Runtime:
             setattr(cfg, k, v)
         if Runtime._active is not None:
             Runtime._active.fini()
-        check(self.lib.charming_init(C.byref(cfg)), "charming_init")
+        devs = _lib.Devices()
+        devs.rank, devs.world, devs.virtual_devs = 0, 1, virtual_devs
+        self._callbacks = None
+        if group is not None:
+            import torch.distributed as dist
+            devs.rank, devs.world = dist.get_rank(group), dist.get_world_size(group)
+            self._callbacks = host_collectives(group)
+            devs.allgather, devs.barrier = self._callbacks
+        check(self.lib.charming_init_devices(C.byref(cfg), C.byref(devs)), "charming_init_devices")
         Runtime._active = self
         self.config = cfg
         inf = _lib.Info()

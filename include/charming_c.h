@@ -78,6 +78,45 @@ void charming_default_config(charming_config* cfg);
  * (NVSHMEM/MPI init, proxy tables, limits, comm_init_host). */
 int charming_init(const charming_config* cfg);
 
+/* ---- several GPUs ----------------------------------------------------------
+ * One process per GPU of one NVSwitch domain. Replaces the reference's
+ * multi-GPU transport: NVSHMEM PEs, with a communication element (CE) per
+ * GPU that relays messages to and from other GPUs as request/forward
+ * messages (src/comm/get/get.cu:518-690, :783-862; src/sched/scheduler.cu:
+ * 78-163). Here every GPU's inbox side is exported with CUDA IPC and mapped
+ * by the others, and a PE sends to a PE on another GPU exactly as to one on
+ * its own GPU: its ticket atomic and payload stores cross NVLink. There is
+ * no CE. PEs are numbered globally: GPU g holds PEs g*P .. g*P + P - 1, P
+ * (PEs per GPU) equal on all GPUs; charm::n_pes() counts all of them.
+ *
+ * The host supplies two collectives over the processes (torch.distributed
+ * in the Python package, files in a shared directory in the process main):
+ * allgather of `bytes` from each rank into all[world * bytes] in rank order,
+ * and a barrier. Each returns 0 on success. */
+typedef int (*charming_allgather_fn)(void* ctx, const void* mine, void* all, size_t bytes);
+typedef int (*charming_barrier_fn)(void* ctx);
+
+typedef struct charming_devices {
+  int rank;                  /* this process's GPU in the run, 0..world-1    */
+  int world;                 /* processes (GPUs) of the run; 1: this GPU only */
+  int virtual_devs;          /* > 1, with world == 1: this GPU's PEs form that
+                                many GPUs, each with its own inbox memory and
+                                control words, in one launch (the multi-GPU
+                                transport's code path, run on one GPU)      */
+  int reserved;
+  charming_allgather_fn allgather;
+  charming_barrier_fn barrier;
+  void* ctx;                 /* passed to both                              */
+} charming_devices;
+
+/* charming_init over several GPUs (devs == NULL, or world == 1 and
+ * virtual_devs <= 1: charming_init). With world > 1 it is collective: every
+ * rank calls it with equal PEs per GPU, ring and message sizes, and
+ * charming_run and charming_fini are collective too. SM-level mode only;
+ * the message programs (hello, refnum, pingpong, fan-out) and programs
+ * linked against the process main run over several processes. */
+int charming_init_devices(const charming_config* cfg, const charming_devices* devs);
+
 /* Runs charm::main on every PE and then the scheduler until charm::end(),
  * an error, or a limit. One cooperative launch of the persistent scheduler
  * kernel. Replaces src/charming.cu:146-169 (argv to device) and :234-244
@@ -109,6 +148,8 @@ typedef struct charming_info {
   uint64_t local_bytes;      /* scheduler kernel's static local memory   */
   int n_blocks;              /* thread blocks of the scheduler launch    */
   int gpu_level;             /* 1: GPU-level mode (n_pes is 1)           */
+  int n_devs;                /* GPUs of the run (virtual ones included)  */
+  int my_dev;                /* this process's (first) GPU               */
 } charming_info;
 int charming_get_info(charming_info* out);
 

@@ -112,6 +112,11 @@ template <typename T> inline T atomicCAS(T* p, T c, T v) {
   return c;
 }
 template <typename T> inline T atomicExch_block(T* p, T v) { return atomicExch(p, v); }
+// system scope (other GPUs): the same C++ atomics; in the two-process check
+// they act on memory both processes map
+template <typename T> inline T atomicAdd_system(T* p, T v) { return atomicAdd(p, v); }
+template <typename T> inline T atomicExch_system(T* p, T v) { return atomicExch(p, v); }
+template <typename T> inline T atomicCAS_system(T* p, T c, T v) { return atomicCAS(p, c, v); }
 template <typename T> inline T atomicCAS_block(T* p, T c, T v) { return atomicCAS(p, c, v); }
 inline void __threadfence_block() { std::atomic_thread_fence(std::memory_order_seq_cst); }
 template <typename T> inline T atomicMax(T* p, T v) {

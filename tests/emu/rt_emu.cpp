@@ -8,6 +8,11 @@
 // AddressSanitizer and, separately, ThreadSanitizer; small inbox rings make
 // tickets wrap many times.
 //
+// Several GPUs: RT_EMU_VDEVS=n splits the PE blocks into n GPUs in one
+// process (each GPU's inbox side its own allocation); RT_EMU_WORLD=w,
+// RT_EMU_RANK=r and RT_EMU_DIR=<empty directory> run w processes, one GPU
+// each, whose inbox sides are files every process maps shared (in the role
+// of CUDA IPC), bootstrapped by the process main's file rendezvous.
 // usage (n_pes: PE blocks; with RT_EMU_GPU_LEVEL set they form one PE):
 //        rt_emu fanout n_pes ring_bytes n_chares msgs payload seed mode
 //        rt_emu hello n_pes ring_bytes
@@ -29,6 +34,11 @@
 #include "../../charming_b200/csrc/apps/jacobi_sweep.cuh"
 #include "../../charming_b200/csrc/apps/serve_host.h"
 #include "../../charming_b200/csrc/apps/decomp1d.h"
+#include "../../charming_b200/csrc/rendezvous.h"
+
+#include <fcntl.h>
+#include <memory>
+#include <sys/mman.h>
 
 #include <atomic>
 #include <chrono>
@@ -189,12 +199,67 @@ T* zalloc(size_t n) {
   return p;
 }
 
+int env_int(const char* name, int dflt) {
+  const char* v = getenv(name);
+  return v ? atoi(v) : dflt;
+}
+
+// Several processes: this one's rank and the rendezvous.
+int g_rank = 0, g_world = 1;
+std::unique_ptr<charm_host::file_rendezvous> g_rdv;
+
+// One GPU's inbox side for pes PEs, carved from base (bytes: inbox_bytes).
+size_t inbox_bytes(int pes, const charm::rt::device_state& ds) {
+  using namespace charm::rt;
+  return 2 * sizeof(line_u64) * pes + 4 * CTRL_WORDS + 8ull * pes + 8ull * ds.ring_cells * pes +
+         ds.ring_stride * pes + 4096;
+}
+charm::rt::dev_inbox carve(unsigned char* base, int pes, const charm::rt::device_state& ds) {
+  using namespace charm::rt;
+  dev_inbox d{};
+  size_t o = 0;
+  auto take = [&](size_t n) {
+    unsigned char* p = base + o;
+    o = (o + n + 255) / 256 * 256;
+    return p;
+  };
+  d.tail = reinterpret_cast<line_u64*>(take(sizeof(line_u64) * pes));
+  d.head = reinterpret_cast<line_u64*>(take(sizeof(line_u64) * pes));
+  d.ctrl = reinterpret_cast<int*>(take(4 * CTRL_WORDS));
+  d.progress = reinterpret_cast<unsigned long long*>(take(8ull * pes));
+  d.flags = reinterpret_cast<unsigned long long*>(take(8ull * ds.ring_cells * pes));
+  d.ring = take(ds.ring_stride * pes);
+  return d;
+}
+
+// A file of `bytes` in the shared directory, mapped shared.
+unsigned char* map_file(const std::string& path, size_t bytes, bool create) {
+  const int fd = open(path.c_str(), create ? (O_RDWR | O_CREAT | O_EXCL) : O_RDWR, 0600);
+  if (fd < 0 || (create && ftruncate(fd, (off_t)bytes) != 0)) {
+    fprintf(stderr, "cannot %s %s\n", create ? "create" : "open", path.c_str());
+    _exit(5);
+  }
+  void* p = mmap(nullptr, bytes, PROT_READ | PROT_WRITE, MAP_SHARED, fd, 0);
+  close(fd);
+  if (p == MAP_FAILED) {
+    fprintf(stderr, "cannot map %s\n", path.c_str());
+    _exit(5);
+  }
+  return static_cast<unsigned char*>(p);
+}
+
 // The parts of charming_init that build the device state. GPU-level mode
 // (RT_EMU_GPU_LEVEL set): the n_blocks blocks form one PE.
 void init_runtime(int n_blocks, size_t ring_bytes, bool gpu_level) {
   using namespace charm::rt;
   device_state ds{};
-  const int n_pes = gpu_level ? 1 : n_blocks;
+  const int vdevs = env_int("RT_EMU_VDEVS", 1);
+  g_world = env_int("RT_EMU_WORLD", 1);
+  g_rank = env_int("RT_EMU_RANK", 0);
+  const int n_devs = g_world > 1 ? g_world : vdevs;
+  const int pes_per_dev = g_world > 1 ? n_blocks : n_blocks / vdevs;
+  const int n_pes = gpu_level ? 1 : pes_per_dev * n_devs;
+  const int n_local = gpu_level ? 1 : n_blocks;
   ds.n_pes = n_pes;
   ds.n_blocks = n_blocks;
   ds.gpu_level = gpu_level ? 1 : 0;
@@ -217,32 +282,56 @@ void init_runtime(int n_blocks, size_t ring_bytes, bool gpu_level) {
     if (th > 16) ds.deadline_ns = ds.deadline_ns / 16 * (unsigned long long)th;
   }
   ds.idle_timeout_ns = 5ull * 1000000000ull;
-  ds.tail = zalloc<line_u64>(n_pes);
-  ds.head = zalloc<line_u64>(n_pes);
-  ds.flags = zalloc<unsigned long long>(ds.ring_cells * n_pes);
-  ds.ring = zalloc<unsigned char>(ds.ring_stride * n_pes);
-  ds.stash_keys = zalloc<stash_key>((size_t)ds.stash_entries * n_pes);
-  ds.stash_data = zalloc<unsigned char>(ds.stash_bytes * n_pes);
-  ds.proxy_tables = zalloc<charm::chare_proxy_table>(n_pes);
-  ds.ctrl = zalloc<int>(CTRL_WORDS);
-  ds.progress = zalloc<unsigned long long>(n_pes);
-  ds.pe_stats = zalloc<unsigned long long>((size_t)N_STATS * n_pes);
-  ds.pe_times = zalloc<unsigned long long>(3 * (size_t)n_pes);
+  // the inbox side of each GPU (virtual ones: one allocation each; several
+  // processes: this one's own file, then the others' files mapped)
+  ds.n_devs = n_devs;
+  ds.pes_per_dev = gpu_level ? 1 : pes_per_dev;
+  ds.n_procs = g_world;
+  ds.pe0 = g_world > 1 ? g_rank * pes_per_dev : 0;
+  const int P = gpu_level ? 1 : pes_per_dev;
+  const size_t ib = inbox_bytes(P, ds);
+  if (g_world > 1) {
+    const char* dir = getenv("RT_EMU_DIR");
+    if (!dir) _exit(5);
+    g_rdv.reset(new charm_host::file_rendezvous(dir, g_rank, g_world, 60.0));
+    const std::string own = std::string(dir) + "/inbox." + std::to_string(g_rank);
+    ds.dev[g_rank] = carve(map_file(own, ib, true), P, ds);
+    if (g_rdv->barrier() != 0) _exit(6);  // every file exists at its size
+    for (int r = 0; r < g_world; r++)
+      if (r != g_rank)
+        ds.dev[r] = carve(map_file(std::string(dir) + "/inbox." + std::to_string(r), ib, false), P, ds);
+  } else {
+    for (int d = 0; d < vdevs; d++) ds.dev[d] = carve(zalloc<unsigned char>(ib), P, ds);
+  }
+  const int dev0 = g_world > 1 ? g_rank : 0;
+  ds.tail = ds.dev[dev0].tail;
+  ds.head = ds.dev[dev0].head;
+  ds.flags = ds.dev[dev0].flags;
+  ds.ring = ds.dev[dev0].ring;
+  ds.ctrl = ds.dev[dev0].ctrl;
+  ds.progress = ds.dev[dev0].progress;
+  ds.stash_keys = zalloc<stash_key>((size_t)ds.stash_entries * n_local);
+  ds.stash_data = zalloc<unsigned char>(ds.stash_bytes * n_local);
+  ds.proxy_tables = zalloc<charm::chare_proxy_table>(n_local);
+  ds.pe_stats = zalloc<unsigned long long>((size_t)N_STATS * n_local);
+  ds.pe_times = zalloc<unsigned long long>(3 * (size_t)n_local);
   ds.host_stop = nullptr;
   ds.free_chares_at_exit = 1;
   ds.arena_bytes = 64 << 10;
-  ds.arena = zalloc<unsigned char>(ds.arena_bytes * n_pes);
+  ds.arena = zalloc<unsigned char>(ds.arena_bytes * n_local);
   ds.outbox_bytes = 2 * ds.max_msg + (64 << 10);
   ds.outbox_stride = ds.outbox_bytes + (ds.max_msg + OB_HDR + 127) / 128 * 128;
-  ds.outbox = zalloc<unsigned char>(ds.outbox_stride * n_pes);
+  ds.outbox = zalloc<unsigned char>(ds.outbox_stride * n_local);
   ds.user_heap_bytes = 64 << 10;
   ds.user_blocks_max = 64;
-  ds.user_heap = zalloc<unsigned char>(ds.user_heap_bytes * n_pes);
-  ds.user_blocks = zalloc<user_block>((size_t)ds.user_blocks_max * n_pes);
+  ds.user_heap = zalloc<unsigned char>(ds.user_heap_bytes * n_local);
+  ds.user_blocks = zalloc<user_block>((size_t)ds.user_blocks_max * n_local);
   c_rt = ds;
   c_n_pes = c_n_pes_node = n_pes;
   c_n_sms = n_blocks;
-  c_n_nodes = c_n_devs = c_n_devs_node = 1;
+  c_n_nodes = 1;
+  c_n_devs = c_n_devs_node = n_devs;
+  c_my_dev = c_my_dev_node = dev0;
 }
 
 unsigned long long g_deferred = 0;  // sends moved to an outbox in the last run
@@ -252,6 +341,8 @@ int run_scheduler(int n_pes, int threads) {
   gridDim = emu_dim3{1, 1, 1};
   blockDim = emu_dim3{1, 1, 1};
   charming_reset_kernel();
+  // several processes: every GPU resets before any runs
+  if (g_rdv && g_rdv->barrier() != 0) _exit(6);
   gridDim = emu_dim3{(unsigned)n_pes, 1, 1};
   blockDim = emu_dim3{(unsigned)threads, 1, 1};
 #ifdef EMU_MT
@@ -278,10 +369,17 @@ int run_scheduler(int n_pes, int threads) {
     }
   }
   for (auto& t : th) t.join();
+  // every process's run has ended: nothing writes this one's words any more
+  if (g_rdv && g_rdv->barrier() != 0) _exit(6);
   g_deferred = 0;
-  for (int p = 0; p < charm::rt::c_rt.n_pes; p++)
+  const int n_local = charm::rt::c_rt.gpu_level ? 1 : n_pes;
+  for (int p = 0; p < n_local; p++)
     g_deferred += charm::rt::c_rt.pe_stats[(size_t)p * charm::rt::N_STATS + charm::rt::ST_DEFERRED];
+  // the first error any of this process's GPUs recorded
   const int* ctl = charm::rt::c_rt.ctrl;
+  const int launch_devs = g_world > 1 ? 1 : charm::rt::c_rt.n_devs;
+  for (int d = 0; d < launch_devs && ctl[charm::rt::CTRL_STATUS] == 0; d++)
+    ctl = charm::rt::c_rt.dev[(g_world > 1 ? g_rank : 0) + d].ctrl;
   if (ctl[charm::rt::CTRL_STATUS])
     fprintf(stderr, "run status %d: pe %d info %d %d\n", ctl[charm::rt::CTRL_STATUS], ctl[charm::rt::CTRL_ERR_PE],
             ctl[charm::rt::CTRL_ERR_I0], ctl[charm::rt::CTRL_ERR_I1]);
@@ -496,6 +594,9 @@ int main(int argc, char** argv) {
     unsigned long long seed = strtoull(argv[7], nullptr, 0);
     int mode = atoi(argv[8]);
     int reps = argc >= 10 ? atoi(argv[9]) : 1;
+    // argv[10] = 1: a program that never ends (one chare more counted as
+    // receiving than receive anything): the idle timeout stops every GPU
+    const int never_ends = argc >= 11 ? atoi(argv[10]) : 0;
     size_t total = (size_t)n * msgs;
     std::vector<unsigned int> log(8 * total + 8);
     std::vector<unsigned long long> ctr(8), off;
@@ -512,21 +613,24 @@ int main(int argc, char** argv) {
       g_app.a[3] = (long long)seed;
       g_app.a[4] = mode;
       g_app.a[5] = (long long)total;
-      g_app.a[6] = active;
+      g_app.a[6] = active + never_ends;
+      g_app.a[7] = charm::rt::c_rt.n_devs > 1 ? 1 : 0;
       g_app.p[0] = log.data();
       g_app.p[1] = ctr.data();
       g_app.p[2] = expected.data();
       g_app.p[3] = off.data();
       status = run_scheduler(n_pes, threads);
     }
-    printf("status=%d chares_done=%llu deferred=%llu\n", status, (unsigned long long)ctr[1], g_deferred);
+    const int* ectl = charm::rt::c_rt.ctrl;
+    printf("status=%d chares_done=%llu deferred=%llu err_pe=%d\n", status, (unsigned long long)ctr[1], g_deferred,
+           status ? ectl[charm::rt::CTRL_ERR_PE] : -1);
     unsigned long long nrec = total;
     for (unsigned long long r = 0; r < nrec; r++) {
       printf("L");
       for (int k = 0; k < 8; k++) printf(" %08x", log[8 * r + k]);
       printf("\n");
     }
-    return status;
+    return never_ends ? 0 : status;
   }
   if (app == "serve") {
     if (argc < 10) return 2;

@@ -47,7 +47,7 @@ def fanout(exe, n_pes, ring, n, msgs, payload, seed, mode, threads=1):
     chk = msgmodel.check_fanout_log(log, n, msgs, payload, seed, mode)
     assert chk.ok, chk.errors
     assert chk.delivered == n * msgs
-    return int(head.split("deferred=")[1])
+    return int(head.split("deferred=")[1].split()[0])
 
 
 @pytest.mark.parametrize("n_pes,ring,n,msgs,payload,mode", [
