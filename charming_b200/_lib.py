@@ -15,9 +15,14 @@ LIB_DIR = os.path.join(_HERE, "lib")
 # CHARMING_CHECKED=1 selects the build with invariant checks (make CHECKS=1).
 LIB_PATH = os.path.join(LIB_DIR, "libcharming_b200_checked.so"
                         if os.environ.get("CHARMING_CHECKED") == "1" else "libcharming_b200.so")
+# The multi-GPU build (runs over several GPUs, or virtual GPUs on one):
+# loaded instead when the first runtime of the process asks for several
+# GPUs, or with CHARMING_MULTI_GPU=1.
+MULTI_LIB_PATH = os.path.join(LIB_DIR, "libcharming_b200_multi.so")
 # CHARMING_LIB: path of another build of the same library (e.g. one compiled
-# with a different register limit).
-LIB_PATH = os.environ.get("CHARMING_LIB", LIB_PATH)
+# with a different register limit); it is used whatever the runtime asks for.
+LIB_OVERRIDE = os.environ.get("CHARMING_LIB")
+LIB_PATH = LIB_OVERRIDE or LIB_PATH
 
 u64 = C.c_uint64
 i32 = C.c_int
@@ -146,6 +151,7 @@ SIGNATURES = [
     ("charming_jacobi2d_init", i32, [vp]),
     ("charming_jacobi2d_load", i32, [vp, i32, vp]),
     ("charming_jacobi2d_run", i32, [vp]),
+    ("charming_jacobi2d_run_n", i32, [vp, i32, C.POINTER(f64)]),
     ("charming_jacobi2d_store", i32, [vp, i32, vp]),
     ("charming_jacobi2d_result", i32, [vp, i32, C.POINTER(JacobiResult)]),
     ("charming_jacobi2d_get_info", i32, [vp, C.POINTER(JacobiInfo)]),
@@ -176,17 +182,26 @@ _lib = None
 _lock = threading.Lock()
 
 
-def load() -> C.CDLL:
-    """Loads libcharming_b200.so; raises if it has not been built."""
+def load(multi: bool = False) -> C.CDLL:
+    """Loads libcharming_b200.so (multi: the multi-GPU build); raises if it
+    has not been built. One build per process: asking for several GPUs
+    after the single-GPU build was loaded raises."""
     global _lib
+    multi = multi or os.environ.get("CHARMING_MULTI_GPU") == "1"
     with _lock:
         if _lib is not None:
+            if multi and not _lib.multi_gpu:
+                raise RuntimeError("this process loaded the single-GPU build of the library; several "
+                                   "GPUs need the multi-GPU build (set CHARMING_MULTI_GPU=1, or create "
+                                   "the multi-GPU runtime first)")
             return _lib
-        if not os.path.exists(LIB_PATH):
+        path = MULTI_LIB_PATH if (multi and not LIB_OVERRIDE) else LIB_PATH
+        if not os.path.exists(path):
             raise RuntimeError(
-                f"{LIB_PATH} is missing: build it with charming_b200.build.build_all() "
+                f"{path} is missing: build it with charming_b200.build.build_all() "
                 "(there is no CPU fallback)")
-        lib = C.CDLL(LIB_PATH, mode=C.RTLD_GLOBAL)
+        lib = C.CDLL(path, mode=C.RTLD_GLOBAL)
+        lib.multi_gpu = multi or path == MULTI_LIB_PATH
         missing = []
         for name, res, args in SIGNATURES:
             fn = getattr(lib, name, None)

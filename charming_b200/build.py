@@ -17,6 +17,8 @@ REFERENCE = os.environ.get("CHARMING_REFERENCE",
 ARCH = "-gencode arch=compute_100a,code=sm_100a"
 REF_EXAMPLES = ("hello", "refnum", "pingpong")
 REF_EXAMPLES_GPU_LEVEL = ("pingpong",)
+# the multi-GPU build of the library (several GPUs, or virtual GPUs on one)
+MULTI = "VARIANT=_multi EXTRA_NVFLAGS=-DCHARMING_MULTI_GPU"
 
 
 def _run(cmd: str, cwd: str) -> None:
@@ -30,6 +32,7 @@ def build_runtime(jobs: int = 8) -> None:
     _run(f"make -j{jobs}", CSRC)
     # the same runtime with invariant checks (CHARMING_CHECKED=1 selects it)
     _run(f"make -j{jobs} CHECKS=1", CSRC)
+    _run(f"make -j{jobs} {MULTI}", CSRC)
 
 
 def build_oracle() -> None:
@@ -47,9 +50,12 @@ def build_reference_artifacts() -> bool:
     inc = os.path.join(ROOT, "include")
     # SM-level builds of every example, and GPU-level builds (the examples'
     # #ifndef SM_LEVEL branch, the reference's default) of those that have one
-    builds = [(ex, ex, "") for ex in REF_EXAMPLES]
-    builds += [(ex, f"{ex}_gpu_level", "-DCHARMING_GPU_LEVEL") for ex in REF_EXAMPLES_GPU_LEVEL]
-    for ex, name, flags in builds:
+    lib_multi = os.path.join(ROOT, "charming_b200", "lib", "libcharming_multi.a")
+    builds = [(ex, ex, "", lib) for ex in REF_EXAMPLES]
+    builds += [(ex, f"{ex}_gpu_level", "-DCHARMING_GPU_LEVEL", lib) for ex in REF_EXAMPLES_GPU_LEVEL]
+    # against the multi-GPU build: several GPUs (WORLD_SIZE, or CHARMING_VIRTUAL_DEVS)
+    builds += [(ex, f"{ex}_multi", "", lib_multi) for ex in REF_EXAMPLES]
+    for ex, name, flags, lib in builds:
         src = os.path.join(REFERENCE, "examples", ex, f"{ex}.cu")
         obj = os.path.join(out, f"{name}.o")
         _run(f"nvcc -std=c++17 -O2 {ARCH} -rdc=true {flags} -I{inc} -I{os.path.dirname(src)} "

@@ -347,6 +347,13 @@ int charming_init_devices(const charming_config* cfg_in, const charming_devices*
   if (dv.world < 1) dv.world = 1;
   if (dv.virtual_devs < 1) dv.virtual_devs = 1;
   const int n_devs = dv.world > 1 ? dv.world : dv.virtual_devs;
+#ifndef CHARMING_MULTI_GPU
+  if (n_devs > 1) {
+    set_error_text("this build is single-GPU: several GPUs need the multi-GPU build "
+                   "(libcharming_b200_multi.so, libcharming_multi.a)");
+    return CHARMING_ERR_CONFIG;
+  }
+#endif
   if (n_devs > MAX_DEVS || dv.rank < 0 || dv.rank >= dv.world || (dv.world > 1 && dv.virtual_devs > 1) ||
       (dv.world > 1 && (!dv.allgather || !dv.barrier)) || (n_devs > 1 && cfg.gpu_level)) {
     set_error_text("invalid charming_devices (at most 8 GPUs, SM-level mode, collectives for world > 1)");

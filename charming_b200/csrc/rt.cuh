@@ -19,7 +19,8 @@
 //   user_heap[pe]           malloc_user / free_user blocks of the PE
 // Cell and flag indices are (ticket mod C); C is a power of two.
 //
-// A run over several GPUs (one process per GPU, one NVSwitch domain): global
+// A run over several GPUs (one process per GPU, one NVSwitch domain; the
+// multi-GPU build of the library, see multi_dev() below): global
 // PE p is local PE p % pes_per_dev of GPU p / pes_per_dev. Each GPU's inbox
 // side (tail, head, flags, ring, control words, progress stamps) is one
 // allocation; the others reach it through device_state::dev[], mapped with
@@ -369,7 +370,16 @@ unsigned long long globaltimer();
 __device__ __forceinline__ int* ctrl(int w) { return c_rt.ctrl + w; }
 
 // ---- several GPUs ----------------------------------------------------------
+// Several GPUs need the multi-GPU build of the library (-DCHARMING_MULTI_GPU:
+// libcharming_b200_multi.so, libcharming_multi.a). In the default build
+// multi_dev() is a compile-time false and the message path carries no test
+// of the GPU count: the test cost a one-way pingpong message on one GPU
+// about 6 % (4.55 against 4.30 us).
+#ifdef CHARMING_MULTI_GPU
 __device__ __forceinline__ bool multi_dev() { return c_rt.n_devs > 1; }
+#else
+__device__ __forceinline__ constexpr bool multi_dev() { return false; }
+#endif
 __device__ __forceinline__ int dev_of(int pe) { return multi_dev() ? pe / c_rt.pes_per_dev : 0; }
 __device__ __forceinline__ int local_of(int pe) { return multi_dev() ? pe % c_rt.pes_per_dev : pe; }
 // The GPU the calling block belongs to.
@@ -395,8 +405,10 @@ __device__ void set_error(int code, int info0, int info1);
 // Every PE of every GPU leaves its loop (end(), a terminate message, the
 // host's stop word).
 __device__ void raise_term();
+__device__ bool terminated_multi();  // out of line, like the other several-GPU lookups
 __device__ __forceinline__ bool terminated() {
-  return multi_dev() ? ld_sys_s32(dev_ctrl(my_dev(), CTRL_TERM)) != 0 : ld_relaxed_s32(ctrl(CTRL_TERM)) != 0;
+  if (multi_dev()) return terminated_multi();
+  return ld_relaxed_s32(ctrl(CTRL_TERM)) != 0;
 }
 
 // Deadline check for bounded waits (thread-local view).

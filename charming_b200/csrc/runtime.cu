@@ -78,6 +78,10 @@ __device__ void charm::rt::set_error(int code, int info0, int info1) {
   for (int d = 0; d < c_rt.n_devs; d++) atomicExch_system(dev_ctrl(d, CTRL_TERM), 1);
 }
 
+__device__ __noinline__ bool charm::rt::terminated_multi() {
+  return ld_sys_s32(dev_ctrl(my_dev(), CTRL_TERM)) != 0;
+}
+
 __device__ void charm::rt::raise_term() {
   if (!multi_dev()) {
     atomicExch(ctrl(CTRL_TERM), 1);
@@ -261,23 +265,41 @@ __device__ void charm::barrier_local() { grid_barrier(); }
 namespace {
 
 // PE pe's inbox words and cells (global PE number; with several GPUs, in
-// the memory of the GPU it lives on).
+// the memory of the GPU it lives on). The several-GPU lookups (a division
+// and an indexed table) are out of line, so that the compiler cannot
+// evaluate them ahead of the branch on the single-GPU path.
+enum : int { W_TAIL = 0, W_HEAD, W_PROGRESS, W_RING, W_FLAGS };
+__device__ __noinline__ void* inbox_of_dev(int pe, int what, unsigned long long ticket) {
+  const dev_inbox& d = c_rt.dev[pe / c_rt.pes_per_dev];
+  const unsigned long long l = (unsigned long long)(pe % c_rt.pes_per_dev);
+  const unsigned long long cell = ticket & (c_rt.ring_cells - 1);
+  switch (what) {
+    case W_TAIL: return &d.tail[l].v;
+    case W_HEAD: return &d.head[l].v;
+    case W_PROGRESS: return &d.progress[l];
+    case W_RING: return d.ring + l * c_rt.ring_stride + cell * CELL;
+    default: return d.flags + l * c_rt.ring_cells + cell;
+  }
+}
 __device__ __forceinline__ unsigned char* ring_cell(int pe, unsigned long long ticket) {
-  unsigned char* base = multi_dev() ? c_rt.dev[dev_of(pe)].ring : c_rt.ring;
-  return base + (unsigned long long)local_of(pe) * c_rt.ring_stride + (ticket & (c_rt.ring_cells - 1)) * CELL;
+  if (multi_dev()) return static_cast<unsigned char*>(inbox_of_dev(pe, W_RING, ticket));
+  return c_rt.ring + (unsigned long long)pe * c_rt.ring_stride + (ticket & (c_rt.ring_cells - 1)) * CELL;
 }
 __device__ __forceinline__ unsigned long long* ring_flag(int pe, unsigned long long ticket) {
-  unsigned long long* base = multi_dev() ? c_rt.dev[dev_of(pe)].flags : c_rt.flags;
-  return base + (unsigned long long)local_of(pe) * c_rt.ring_cells + (ticket & (c_rt.ring_cells - 1));
+  if (multi_dev()) return static_cast<unsigned long long*>(inbox_of_dev(pe, W_FLAGS, ticket));
+  return c_rt.flags + (unsigned long long)pe * c_rt.ring_cells + (ticket & (c_rt.ring_cells - 1));
 }
 __device__ __forceinline__ unsigned long long* tail_of(int pe) {
-  return multi_dev() ? &c_rt.dev[dev_of(pe)].tail[local_of(pe)].v : &c_rt.tail[pe].v;
+  if (multi_dev()) return static_cast<unsigned long long*>(inbox_of_dev(pe, W_TAIL, 0));
+  return &c_rt.tail[pe].v;
 }
 __device__ __forceinline__ unsigned long long* head_of(int pe) {
-  return multi_dev() ? &c_rt.dev[dev_of(pe)].head[local_of(pe)].v : &c_rt.head[pe].v;
+  if (multi_dev()) return static_cast<unsigned long long*>(inbox_of_dev(pe, W_HEAD, 0));
+  return &c_rt.head[pe].v;
 }
 __device__ __forceinline__ unsigned long long* progress_of(int pe) {
-  return multi_dev() ? &c_rt.dev[dev_of(pe)].progress[local_of(pe)] : &c_rt.progress[pe];
+  if (multi_dev()) return static_cast<unsigned long long*>(inbox_of_dev(pe, W_PROGRESS, 0));
+  return &c_rt.progress[pe];
 }
 
 __device__ __forceinline__ unsigned char* outbox_of(int pe) {

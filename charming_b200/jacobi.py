@@ -126,6 +126,13 @@ class Jacobi2D:
         check(self.lib.charming_jacobi2d_run(self.h), "charming_jacobi2d_run")
         return self.info()["last_run_ms"]
 
+    def run_n(self, n_runs: int) -> float:
+        """n_runs runs enqueued back to back and synchronised once (no host
+        work between them); returns the CUDA-event ms of all of them."""
+        ms = C.c_double(0.0)
+        check(self.lib.charming_jacobi2d_run_n(self.h, n_runs, C.byref(ms)), "charming_jacobi2d_run_n")
+        return ms.value
+
     def store(self, prob: int, out: np.ndarray | None = None) -> np.ndarray:
         p = self.problems[prob]
         if out is None:

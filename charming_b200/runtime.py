@@ -78,12 +78,13 @@ class Runtime:
     Several GPUs: ``group`` (a torch.distributed process group, one rank per
     GPU, a CPU backend) makes a run over all its ranks, collective like the
     reference's NVSHMEM runs; ``virtual_devs=n`` splits this GPU's PEs into n
-    GPUs in one launch (the same transport on one GPU)."""
+    GPUs in one launch (the same transport on one GPU). Both load the
+    multi-GPU build of the library (one build per process)."""
 
     _active: "Runtime | None" = None
 
     def __init__(self, group=None, virtual_devs: int = 1, **overrides):
-        self.lib = _lib.load()
+        self.lib = _lib.load(multi=group is not None or virtual_devs > 1)
         cfg = _lib.Config()
         self.lib.charming_default_config(C.byref(cfg))
         for k, v in overrides.items():

@@ -262,6 +262,12 @@ int charming_jacobi2d_load(void* handle, int prob, const void* host_grid);
  * chare logic follows examples/jacobi2d/jacobi2d.cu:93-279 with halos tagged
  * refnum = sweep. */
 int charming_jacobi2d_run(void* handle);
+/* n_runs runs of charming_jacobi2d_run enqueued back to back on the
+ * runtime's stream and synchronised once: no host work between them (a
+ * status latch after each keeps the first failure, which is returned).
+ * *total_ms: CUDA-event time of all of them; the statistics are the last
+ * run's, last_run_ms their mean. */
+int charming_jacobi2d_run_n(void* handle, int n_runs, double* total_ms);
 /* Chare blocks -> host grid (same layout as load). */
 int charming_jacobi2d_store(void* handle, int prob, void* host_grid);
 int charming_jacobi2d_result(void* handle, int prob, charming_jacobi_result* out);

@@ -31,6 +31,21 @@ def test_library_exports_every_declared_symbol():
     assert not lib.missing_symbols
 
 
+def test_multi_gpu_build_exports_every_declared_symbol():
+    # the multi-GPU build (several GPUs, one process each, or virtual GPUs)
+    # is the same C ABI; a fresh process, since one process holds one build
+    # (a second copy's CUDA registrations clash with the first's)
+    import json
+    import subprocess
+    import sys
+    code = ("import ctypes, json, sys; sys.path.insert(0, %r); from tests.test_capi_cpu import declared_functions; "
+            "lib = ctypes.CDLL(%r); print(json.dumps([n for n in declared_functions() if not hasattr(lib, n)]))"
+            % (ROOT, os.path.join(ROOT, "charming_b200", "lib", "libcharming_b200_multi.so")))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=ROOT, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert json.loads(r.stdout.strip().splitlines()[-1]) == []
+
+
 def test_bindings_cover_every_declared_symbol():
     from charming_b200 import _lib
     bound = {n for n, _, _ in _lib.SIGNATURES}
@@ -64,6 +79,7 @@ def test_reference_examples_built():
         pytest.skip("reference tree not present")
     for ex in ("hello", "refnum", "pingpong"):
         assert os.path.exists(os.path.join(d, ex)), ex
+        assert os.path.exists(os.path.join(d, f"{ex}_multi")), ex  # against libcharming_multi.a
     # pingpong's GPU-level branch (the reference's default build) compiles and
     # links unchanged too; it places its two chares with block_map[0] and
     # block_map[n_pes / 2], so it needs two PEs, i.e. two GPUs, in that mode

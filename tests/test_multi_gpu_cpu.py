@@ -190,3 +190,43 @@ def test_processes_idle_timeout_reaches_every_gpu(emus):
         head, _ = parse_fanout(r)
         assert head["status"] == "5", (r.stdout[:200], r.stderr[-1000:])  # CHARMING_ERR_IDLE_TIMEOUT
         assert head["err_pe"] == "0"
+
+
+# ---- the Python host's collectives (torch.distributed, gloo) -------------------
+
+def _collectives_rank(rank, world, port, q):
+    import ctypes as C
+    import torch.distributed as dist
+    dist.init_process_group("gloo", rank=rank, world_size=world, init_method=f"tcp://127.0.0.1:{port}")
+    from charming_b200.runtime import host_collectives
+    ag, bar = host_collectives()
+    mine = (C.c_ubyte * 72)(*[(rank * 31 + i) & 255 for i in range(72)])
+    out = (C.c_ubyte * (72 * world))()
+    rc = ag(None, C.cast(mine, C.c_void_p), C.cast(out, C.c_void_p), 72)
+    rc2 = bar(None)
+    q.put((rank, rc, rc2, bytes(out)))
+    dist.destroy_process_group()
+
+
+def test_python_host_collectives_over_gloo():
+    """The allgather and barrier that charming_init_devices calls back into
+    (here called through their ctypes function pointers, as the library
+    does): every rank gets every rank's record in rank order."""
+    import multiprocessing as mp
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    world = 2
+    ps = [ctx.Process(target=_collectives_rank, args=(r, world, port, q)) for r in range(world)]
+    for p in ps:
+        p.start()
+    got = [q.get(timeout=120) for _ in range(world)]
+    for p in ps:
+        p.join(timeout=60)
+    want = b"".join(bytes((r * 31 + i) & 255 for i in range(72)) for r in range(world))
+    for rank, rc, rc2, out in got:
+        assert rc == 0 and rc2 == 0
+        assert out == want
