@@ -614,9 +614,50 @@ def serving_suite(n_req: int, rate: float = 200.0, seed: int = 0xC5, pes_per_sm:
             "cpu_baseline": cpu_serving_baseline(probs, arrive, sweeps_of) if with_cpu else None}
 
 
+MULTI_GPU_CHILD = """
+import json
+from charming_b200.runtime import Runtime
+out = {}
+for v in (2, 1):
+    rt = Runtime(virtual_devs=v)
+    rows, _ = rt.pingpong([8, 64, 4096], round_trips=10000, warmup=100, seed=1, verify=False)
+    seed = 0xC0FFEE + 4096 + 1
+    rt.fanout(4096, 16, 64, seed, 1)
+    log, ms = rt.fanout(4096, 16, 64, seed, 1)
+    out[v] = {"pingpong_oneway_ns": {str(r["size"]): round(r["oneway_us"] * 1e3, 1) for r in rows},
+              "fanout_msgs_per_s": 4096 * 16 / (ms * 1e-3), "n_pes": rt.n_pes}
+    rt.fini()
+print(json.dumps(out))
+"""
+
+
+def multi_gpu_suite() -> dict:
+    """The multi-GPU transport (its own build of the library, so in a child
+    process) on one B200: the 148 PEs form 2 virtual GPUs, each with its own
+    inbox memory; PE 0 and PE 74 (pingpong) sit on different ones, and the
+    fan-out's messages cross between them with system-scope tickets and
+    flags. Beside it, the same build with one GPU."""
+    r = subprocess.run([sys.executable, "-c", MULTI_GPU_CHILD], cwd=ROOT, capture_output=True, text=True,
+                       timeout=600)
+    if r.returncode != 0:
+        return {"error": r.stderr[-500:]}
+    res = json.loads(r.stdout.strip().splitlines()[-1])
+    two, one = res["2"], res["1"]
+    return {"build": "libcharming_b200_multi.so", "virtual_gpus": 2,
+            "pingpong_oneway_ns_cross_gpu": two["pingpong_oneway_ns"],
+            "fanout_msgs_per_s_2_gpus": two["fanout_msgs_per_s"],
+            "one_gpu_same_build": {"pingpong_oneway_ns": one["pingpong_oneway_ns"],
+                                   "fanout_msgs_per_s": one["fanout_msgs_per_s"]},
+            "workload": "pingpong 8/64/4096 B, 10000 round trips; fan-out 4096 chares x 16 msgs of 64 B, "
+                        "refnums 0..15, 1 PE of 512 threads per SM",
+            "note": "virtual GPUs: a peer's rings are this GPU's memory, so NVLink's latency is not in "
+                    "these numbers; the difference to one GPU is the system-scope protocol"}
+
+
 def run_suites(args, headline_glups: float) -> dict:
     out = {}
     for name, fn in (("messaging", lambda: messaging_suite()),
+                     ("multi_gpu", lambda: multi_gpu_suite()),
                      ("batched", lambda: batched_suite()),
                      ("precision", lambda: precision_suite(headline_glups)),
                      ("serving", lambda: serving_suite(args.serve_requests))):

@@ -154,8 +154,9 @@ __device__ void ping_recv(PingChare& c, void* arg) {
 // Fan-out. g_app: a[0] n_chares, a[1] msgs per chare, a[2] payload bytes,
 // a[3] seed, a[4] mode (0: refnum -1, 1: message k carries refnum k),
 // a[5] log capacity (records), a[6] chares that receive anything;
-// a[7] 1: the run spans several GPUs, chares report done to chare 0 in a
-// message (its counter is the only one); p[0] log (u32[cap][8]), p[1]
+// a[7] 1: the run spans several processes, chares report done to chare 0
+// in a message (its process's counter is the only one); p[0] log
+// (u32[cap][8]), p[1]
 // counters (u64[2]: 0, chares done), p[2] expected counts (int[n][msgs]),
 // p[3] log offsets (u64[n+1]: chare d's deliveries go to records
 // off[d]..off[d+1]-1, in delivery order; over several processes each logs
@@ -213,8 +214,8 @@ __device__ void fan_record(FanChare& c, void* arg, bool relay, int* s_last);
 
 // Warp 0 handles a delivery (the other warps have nothing to do and return
 // at once): checksum by its lanes, the record and the refnum ladder by lane 0.
-// Over several GPUs a chare's last delivery is reported to chare 0 in a
-// message, which the whole block sends.
+// Over several processes a chare's last delivery is reported to chare 0 in
+// a message, which the whole block sends.
 __device__ void fan_recv(FanChare& c, void* arg) {
   const bool relay = g_app.a[7] != 0;
   __shared__ int s_last;
@@ -266,7 +267,7 @@ __device__ void fan_record(FanChare& c, void* arg, bool relay, int* s_last) {
   }
 }
 
-// Chare 0 (several GPUs): one more chare has all its deliveries.
+// Chare 0 (several processes): one more chare has all its deliveries.
 __device__ void fan_done(FanChare& c, void* arg) {
   if (threadIdx.x == 0) {
     unsigned long long* ctr = reinterpret_cast<unsigned long long*>(g_app.p[1]);
@@ -426,7 +427,7 @@ extern "C" int charming_fanout(int n_chares, int msgs_per_chare, int payload_byt
   p.a[4] = mode;
   p.a[5] = (long long)log_capacity;
   p.a[6] = active;
-  p.a[7] = charm_host::info().n_devs > 1 ? 1 : 0;
+  p.a[7] = charm_host::n_procs() > 1 ? 1 : 0;
   p.p[0] = d_log;
   p.p[1] = d_ctr;
   p.p[2] = d_exp;

@@ -134,6 +134,7 @@ void set_error_text(const std::string& s) { g_err = s; }
 bool initialised() { return g.inited; }
 cudaStream_t stream() { return g.stream; }
 const charming_info& info() { return g.inf; }
+int n_procs() { return g.world; }
 
 int ensure_init() {
   if (g.inited) return CHARMING_OK;

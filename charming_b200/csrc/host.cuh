@@ -18,6 +18,8 @@ bool initialised();
 
 cudaStream_t stream();
 const charming_info& info();
+// Processes of the run (1 unless charming_init_devices was given world > 1).
+int n_procs();
 
 // One scheduler run: reset kernel + cooperative launch on stream(), then
 // synchronise and collect status and statistics.

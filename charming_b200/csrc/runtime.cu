@@ -425,8 +425,16 @@ __device__ unsigned char* wait_space(int dst, unsigned long long t, unsigned lon
 // payload written by other threads of the block is ordered before it by
 // the barrier the callers pass first (release is cumulative), and a separate
 // fence would also invalidate the SM's L1.
+//
+// Several GPUs: a message to a PE on another GPU is released at system
+// scope, one to a PE of the sender's own GPU at GPU scope (the receiver
+// acquires at system scope, which pairs with either): a system-scope
+// release waits until the sender's writes are visible to every GPU and the
+// host, which a message that stays on its GPU does not need.
 __device__ __forceinline__ void publish(int dst, unsigned long long ticket) {
-  st_release_x(ring_flag(dst, ticket), ticket + 1);
+  unsigned long long* f = ring_flag(dst, ticket);
+  if (multi_dev() && dev_of(dst) != my_dev()) st_release_sys_u64(f, ticket + 1);
+  else st_release_u64(f, ticket + 1);
 }
 
 // Publishes the message at m (reserved by reserve() for ticket in dst's

@@ -614,7 +614,7 @@ int main(int argc, char** argv) {
       g_app.a[4] = mode;
       g_app.a[5] = (long long)total;
       g_app.a[6] = active + never_ends;
-      g_app.a[7] = charm::rt::c_rt.n_devs > 1 ? 1 : 0;
+      g_app.a[7] = charm::rt::c_rt.n_procs > 1 ? 1 : 0;
       g_app.p[0] = log.data();
       g_app.p[1] = ctr.data();
       g_app.p[2] = expected.data();

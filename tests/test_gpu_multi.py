@@ -150,3 +150,41 @@ def test_reference_examples_over_virtual_gpus():
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     sizes = [l for l in r.stdout.splitlines() if l.startswith("Size ")]
     assert [int(l.split()[1]) for l in sizes] == [8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096]
+
+
+IPC_RANK = """
+import json, sys
+import torch.distributed as dist
+rank, port = int(sys.argv[1]), sys.argv[2]
+dist.init_process_group("gloo", rank=rank, world_size=2, init_method="tcp://127.0.0.1:" + port)
+from charming_b200.runtime import Runtime
+rt = Runtime(group=dist.group.WORLD, n_pes=16, ring_bytes=1 << 16, max_msg_bytes=4096,
+             stash_bytes=1 << 20, heap_bytes=64 << 20)
+info = dict(rt.info)
+rt.fini()
+dist.destroy_process_group()
+print(json.dumps({k: info[k] for k in ("n_pes", "n_blocks", "n_devs", "my_dev")}))
+"""
+
+
+def test_two_processes_export_and_map_inbox_regions():
+    """The host side of a run over two processes, on the one GPU this test
+    run has: each exports its inbox region with CUDA IPC, the handles go
+    through the Python host's allgather (torch.distributed, gloo), each maps
+    the other's region, and fini unmaps and frees them between barriers.
+    No run is launched: scheduler kernels of two processes that wait on one
+    another must not share one GPU (the transport itself is run on one GPU
+    by the virtual-GPU tests above, and across processes on the CPU)."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    procs = [subprocess.Popen([sys.executable, "-c", IPC_RANK, str(r), str(port)], cwd=ROOT,
+                              stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True) for r in range(2)]
+    outs = []
+    for p in procs:
+        o, e = p.communicate(timeout=300)
+        assert p.returncode == 0, o[-2000:] + e[-3000:]
+        outs.append(json.loads(o.strip().splitlines()[-1]))
+    for rank, info in enumerate(outs):
+        assert info == {"n_pes": 32, "n_blocks": 16, "n_devs": 2, "my_dev": rank}
