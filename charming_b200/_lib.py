@@ -64,7 +64,7 @@ class Stats(C.Structure):
         ("bytes_sent", u64), ("idle_polls", u64), ("space_waits", u64),
         ("kernel_ms", f64), ("loop_ms", f64), ("main_ms", f64), ("status", i32), ("err_pe", i32),
         ("err_info0", i32), ("err_info1", i32), ("idle_ms", f64), ("em_ms", f64),
-        ("deferred", u64), ("ticket_ms", f64), ("space_ms", f64),
+        ("deferred", u64), ("ticket_ms", f64), ("space_ms", f64), ("batched", u64),
     ]
 
 

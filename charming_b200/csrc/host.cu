@@ -227,6 +227,7 @@ int collect_run(double kernel_ms) {
     s.idle_polls += q[ST_IDLE_POLLS];
     s.space_waits += q[ST_SPACE_WAITS];
     s.deferred += q[ST_DEFERRED];
+    s.batched += q[ST_BATCHED];
     if (t[1] && t[1] < tmin) tmin = t[1];
     if (t[2] > tmax) tmax = t[2];
   }

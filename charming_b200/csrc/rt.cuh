@@ -99,7 +99,8 @@ enum : int {
   ST_DEFERRED,        // sends moved to the outbox (destination ring full)
   ST_TICKET_NS,       // ns the reserving thread waited for its ticket atomics
   ST_SPACE_NS,        // ns it then waited for ring space (head cache and waits)
-  N_STATS = 13
+  ST_BATCHED,         // deliveries run beside others in a batch of warp-level entry methods
+  N_STATS = 14
 };
 
 constexpr int MAX_DEVS = 8;  // GPUs of one NVSwitch domain
@@ -257,6 +258,17 @@ struct pe_state {
   unsigned long long slow_check_ns;    // last host-stop / idle-timeout check
   unsigned long long idle_checks;
   chare_proxy_base* pcache[PROXY_CACHE];  // proxies[0..PROXY_CACHE) of this PE's table
+  // a batch of warp-level deliveries (consecutive inbox messages to
+  // different chares, one per warp): thread 0 picks the first, warp 0's
+  // scan adds the rest
+  int nb;                              // deliveries in the batch
+  unsigned int nb_cells;               // ring cells they take from the head
+  unsigned long long bkey0;            // chare of the first (array << 32 | index)
+  chare_proxy_base* bp[MAX_THREADS / 32];
+  void* barg[MAX_THREADS / 32];
+  int bidx[MAX_THREADS / 32], bep[MAX_THREADS / 32];
+  unsigned long long bstash[MAX_THREADS / 32];  // stash keys of a stash batch
+  unsigned long long bkeys[MAX_THREADS / 32];   // its chares
   // batched sends (alloc_user_msgs): per message start, ticket, bytes
   void* bm_ptr[MSG_BATCH_MAX];
   unsigned long long bm_tick[MSG_BATCH_MAX];

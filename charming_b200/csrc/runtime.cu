@@ -741,11 +741,22 @@ __device__ bool charm::alloc_user_msgs(message* msgs, const int* dst_pes,
       if (ok && k == leader) base = atomic_add_x(tail_of(dst_pes[k]), (unsigned long long)tot);
       base = __shfl_sync(FULL, base, leader);
       CHARM_PROF(__syncwarp(); const unsigned long long tb = k == 0 ? globaltimer() : 0;)
-      if (act) {
-        unsigned long long t = 0;
-        ps->bm_ptr[k] = ok ? wait_space(dst_pes[k], base + pre, bytes, &t) : nullptr;
-        ps->bm_tick[k] = t;
-        ps->bm_bytes[k] = bytes;
+      // A group's lanes wait for ring space in ticket order, one round per
+      // message of the group: a message that finds the ring full moves to
+      // the outbox, which flushes strictly in entry order, so a group's
+      // later ticket must never enter it before an earlier one. Lanes of
+      // different groups wait together.
+      const int rank = __popc(grp & ((1u << k) - 1));
+      int rounds = __popc(grp);
+      for (int o = 16; o > 0; o >>= 1) rounds = max(rounds, __shfl_xor_sync(FULL, rounds, o));
+      for (int r = 0; r < rounds; r++) {
+        if (act && rank == r) {
+          unsigned long long t = 0;
+          ps->bm_ptr[k] = ok ? wait_space(dst_pes[k], base + pre, bytes, &t) : nullptr;
+          ps->bm_tick[k] = t;
+          ps->bm_bytes[k] = bytes;
+        }
+        __syncwarp();
       }
       CHARM_PROF(__syncwarp(); if (k == 0) {
         ps->stats[ST_TICKET_NS] += tb - ta;
@@ -867,7 +878,8 @@ __device__ void charm::free_user(size_t size, size_t offset) {
 }
 
 __device__ void charm::revive_mismatches(int chare_id, int chare_idx, int refnum) {
-  pes()->revive_pending = 1;
+  // the warps of a batch of warp-level entry methods may set it together
+  atomicExch_block(&pes()->revive_pending, 1);
 }
 
 __device__ void charm::add_async_wait(int chare_id) { pes()->aw_count++; }
@@ -895,7 +907,12 @@ enum : int {
   ACT_STASH_PUT,    // copy the message at the inbox head into the stash
   ACT_FLUSH,        // copy the oldest outbox entry into its destination ring
   ACT_REVIVE,       // mark waiting stashed messages whose refnum now matches
+  ACT_CALL_BATCH,   // warp-level entry methods on consecutive inbox messages, one per warp
+  ACT_STASH_BATCH,  // warp-level entry methods on ready stashed messages, one per warp
 };
+
+// Batches of warp-level deliveries need whole warps and at least two of them.
+__device__ __forceinline__ bool batching() { return !gpu_level() && blockDim.x >= 64 && (blockDim.x & 31) == 0; }
 
 __device__ __forceinline__ chare_proxy_base* proxy_of(pe_state* ps, int cid) {
   if (cid >= 0 && cid < PROXY_CACHE) return ps->pcache[cid];  // on chip
@@ -1183,6 +1200,26 @@ __device__ void finish_action() {
     case ACT_CALL_WAIT:
       if ((++ps->stats[ST_DELIVERED] & 15) == 0) stamp_progress(me);
       break;
+    case ACT_STASH_BATCH: {
+      const unsigned long long S = (unsigned long long)c_rt.stash_entries;
+      for (int b = 0; b < ps->nb; b++) keys_of(blockIdx.x)[ps->bstash[b] % S].state = KEY_FREE;
+      ps->n_ready -= ps->nb;
+      const unsigned long long d0 = ps->stats[ST_DELIVERED];
+      ps->stats[ST_DELIVERED] = d0 + (unsigned long long)ps->nb;
+      if (ps->nb > 1) ps->stats[ST_BATCHED] += (unsigned long long)ps->nb;
+      if ((d0 >> 4) != (ps->stats[ST_DELIVERED] >> 4)) stamp_progress(me);
+      stash_retire();
+      break;
+    }
+    case ACT_CALL_BATCH: {
+      ps->head += ps->nb_cells;
+      if (ps->head - ps->head_pub >= (c_rt.ring_cells >> 3)) publish_head(ps, me);
+      const unsigned long long d0 = ps->stats[ST_DELIVERED];
+      ps->stats[ST_DELIVERED] = d0 + (unsigned long long)ps->nb;
+      if (ps->nb > 1) ps->stats[ST_BATCHED] += (unsigned long long)ps->nb;
+      if ((d0 >> 4) != (ps->stats[ST_DELIVERED] >> 4)) stamp_progress(me);
+      break;
+    }
     case ACT_FLUSH: {
       const ob_entry* e = reinterpret_cast<const ob_entry*>(ps->d_p);
       publish(e->dst, e->ticket);
@@ -1202,6 +1239,53 @@ __device__ void finish_action() {
       break;
   }
   ps->d_act = ACT_NONE;
+}
+
+// Thread 0: a batch of warp-level deliveries from the ready stashed messages,
+// the first (key i) already chosen: the next ready ones in arrival order
+// while each is for a warp-level entry method of a chare not yet in the
+// batch and its refnum matches (the first that is not is left for the
+// next decision, as for inbox batches).
+__device__ void stash_batch(chare_proxy_base* p, const stash_key* k, int ep, void* arg, unsigned long long i) {
+  pe_state* ps = pes();
+  const unsigned long long S = (unsigned long long)c_rt.stash_entries;
+  stash_key* keys = keys_of(blockIdx.x);
+  const int maxb = (int)(blockDim.x >> 5);
+  ps->d_act = ACT_STASH_BATCH;
+  ps->nb = 1;
+  ps->bp[0] = p;
+  ps->bidx[0] = k->chare_idx;
+  ps->bep[0] = ep;
+  ps->barg[0] = arg;
+  ps->bstash[0] = i;
+  ps->bkeys[0] = ((unsigned long long)(unsigned)k->chare_id << 32) | (unsigned)k->chare_idx;
+  while (ps->nb < maxb && ps->n_ready > ps->nb) {
+    const int pos = ps->rq_pos;
+    const unsigned long long cur = ps->ready_cursor;
+    const unsigned long long j = stash_next_ready();
+    bool take = j != ~0ULL;
+    const stash_key* kj = take ? keys + (j % S) : nullptr;
+    chare_proxy_base* pj = take ? proxy_of(ps, kj->chare_id) : nullptr;
+    const unsigned char* env = take ? arena_of(blockIdx.x) + (kj->data_off % c_rt.stash_bytes) : nullptr;
+    const int epj = take ? reinterpret_cast<const regular_msg*>(env + sizeof(envelope))->ep_id : 0;
+    const unsigned long long key =
+        take ? ((unsigned long long)(unsigned)kj->chare_id << 32) | (unsigned)kj->chare_idx : 0;
+    take = take && pj->warp_em(epj) && pj->refnum_matches(kj->chare_idx, kj->refnum);
+    for (int b = 0; take && b < ps->nb; b++) take = ps->bkeys[b] != key;
+    if (!take) {  // leave it for the next decision
+      ps->rq_pos = pos;
+      ps->ready_cursor = cur;
+      break;
+    }
+    const int n = ps->nb;
+    ps->bp[n] = pj;
+    ps->bidx[n] = kj->chare_idx;
+    ps->bep[n] = epj;
+    ps->barg[n] = const_cast<unsigned char*>(env) + HDR;
+    ps->bstash[n] = j;
+    ps->bkeys[n] = key;
+    ps->nb = n + 1;
+  }
 }
 
 // Thread 0: decides what the block does next (pe_state d_* fields).
@@ -1278,6 +1362,8 @@ __device__ void next_action() {
       ps->d_ep = rm->ep_id;
       ps->d_arg = const_cast<unsigned char*>(env) + HDR;
       ps->d_key = i;
+      // (from the on-chip ready list; past RQ_MAX ready ones, one at a time)
+      if (p->warp_em(rm->ep_id) && batching() && !ps->rq_over) stash_batch(p, k, rm->ep_id, ps->d_arg, i);
       return;
     }
     // the inbox
@@ -1308,6 +1394,17 @@ __device__ void next_action() {
         ps->d_idx = rm->chare_idx;
         ps->d_ep = rm->ep_id;
         ps->d_arg = m + HDR;
+        if (p->warp_em(rm->ep_id) && batching()) {
+          // the first of a batch; warp 0 looks for more behind it
+          ps->d_act = ACT_CALL_BATCH;
+          ps->nb = 1;
+          ps->nb_cells = cells_for(size);
+          ps->bkey0 = ((unsigned long long)(unsigned)cid << 32) | (unsigned)rm->chare_idx;
+          ps->bp[0] = p;
+          ps->bidx[0] = rm->chare_idx;
+          ps->bep[0] = rm->ep_id;
+          ps->barg[0] = m + HDR;
+        }
       } else {
         unsigned char* dst = stash_alloc(size, cid, rm->chare_idx, rm->refnum, env->src_pe);
         if (dst) {
@@ -1327,6 +1424,87 @@ __device__ void next_action() {
     // nothing for the block to do with it: consume it here
     ps->head += ps->d_cells;
     if (ps->head - ps->head_pub >= (c_rt.ring_cells >> 3)) publish_head(ps, me);
+  }
+}
+
+// Warp 0 (all lanes): extends the batch whose first delivery thread 0
+// picked. Lane l reads the sequence words of cells l and l + 32 after the
+// first message: where a published message starts the word holds that
+// cell's ticket + 1, so one load per lane and window finds every message
+// published in the next 64 cells, and one more reads their envelopes.
+// Messages follow one another without gaps (each took its cells'
+// tickets), so the batch follows the chain from the first message's end
+// while each next message is published, is for a warp-level entry method
+// of a chare not yet in the batch, and its refnum matches; it stops at the
+// first that is not, which the scheduler then takes alone. The batch runs
+// after a barrier, so the refnums checked here are the ones the sequential
+// order would check: an entry method of the batch changes only its own
+// chare's refnum.
+struct scan_cell {
+  unsigned int cells;
+  int ok, idx, ep;
+  unsigned long long key, p, arg;
+};
+__device__ __forceinline__ scan_cell scan_one(pe_state* ps, int me, unsigned long long t) {
+  scan_cell c{0, 0, 0, 0, ~0ULL, 0, 0};
+  if (ld_acquire_x(ring_flag(me, t)) == t + 1) {
+    const unsigned char* m = ring_cell(me, t);
+    const envelope* env = reinterpret_cast<const envelope*>(m);
+    const regular_msg* rm = reinterpret_cast<const regular_msg*>(m + sizeof(envelope));
+    const unsigned long long size = env->size;
+    const int type = (int)env->type;
+    if (size >= HDR && size <= c_rt.max_msg && !(size & (ALIGN_SIZE - 1)) &&
+        (type == (int)msgtype::regular || type == (int)msgtype::user)) {
+      chare_proxy_base* q = proxy_of(ps, rm->chare_id);
+      c.idx = rm->chare_idx;
+      c.ep = rm->ep_id;
+      c.ok = q && q->valid_target(c.idx, c.ep) && q->warp_em(c.ep) && q->refnum_matches(c.idx, rm->refnum);
+      c.cells = cells_for(size);
+      c.key = ((unsigned long long)(unsigned)rm->chare_id << 32) | (unsigned)c.idx;
+      c.p = reinterpret_cast<unsigned long long>(q);
+      c.arg = reinterpret_cast<unsigned long long>(m + HDR);
+    }
+  }
+  return c;
+}
+
+__device__ void batch_extend() {
+  constexpr unsigned FULL = 0xffffffffu;
+  pe_state* ps = pes();
+  const int lane = (int)(threadIdx.x & 31);
+  const int me = ps->my_pe;
+  const int maxb = (int)(blockDim.x >> 5);
+  const unsigned long long t0 = ps->head + ps->nb_cells + (unsigned long long)lane;
+  const scan_cell lo = scan_one(ps, me, t0), hi = scan_one(ps, me, t0 + 32);
+  // lane j holds the chare of batch member j
+  unsigned long long mkey = lane == 0 ? ps->bkey0 : ~0ULL;
+  int n = ps->nb, pos = 0;
+  unsigned int total = ps->nb_cells;
+  while (n < maxb && pos < 64) {  // uniform: every lane computes the same
+    const bool w0 = pos < 32;
+    const int src = pos & 31;
+    if (!__shfl_sync(FULL, w0 ? lo.ok : hi.ok, src)) break;
+    const unsigned long long k = __shfl_sync(FULL, w0 ? lo.key : hi.key, src);
+    if (__any_sync(FULL, lane < n && mkey == k)) break;
+    const unsigned int cl = __shfl_sync(FULL, w0 ? lo.cells : hi.cells, src);
+    const unsigned long long bp = __shfl_sync(FULL, w0 ? lo.p : hi.p, src);
+    const unsigned long long ba = __shfl_sync(FULL, w0 ? lo.arg : hi.arg, src);
+    const int bi = __shfl_sync(FULL, w0 ? lo.idx : hi.idx, src);
+    const int be = __shfl_sync(FULL, w0 ? lo.ep : hi.ep, src);
+    if (lane == n) mkey = k;
+    if (lane == 0) {
+      ps->bp[n] = reinterpret_cast<chare_proxy_base*>(bp);
+      ps->barg[n] = reinterpret_cast<void*>(ba);
+      ps->bidx[n] = bi;
+      ps->bep[n] = be;
+    }
+    n++;
+    total += cl;
+    pos += (int)cl;
+  }
+  if (lane == 0) {
+    ps->nb = n;
+    ps->nb_cells = total;
   }
 }
 
@@ -1361,9 +1539,22 @@ __device__ void scheduler_loop() {
     chare_proxy_base* p = reinterpret_cast<chare_proxy_base*>(ps->d_p);
     if (call) {
       const long long c0 = clock64();
-      p->call_fn(p, ps->d_idx, ps->d_ep, ps->d_arg);
+      // a warp-level entry method outside a batch: warp 0 (of block 0)
+      if (!p->warp_em(ps->d_ep) || threadIdx.x < 32) p->call_fn(p, ps->d_idx, ps->d_ep, ps->d_arg);
       if (threadIdx.x == 0) ps->stats[ST_EM_CYC] += (unsigned long long)(clock64() - c0);
       if (group && !grid_barrier_ok()) break;  // every block is done with the message
+    } else if (act == ACT_CALL_BATCH || act == ACT_STASH_BATCH) {
+      const long long c0 = clock64();
+      if (act == ACT_CALL_BATCH) {
+        if (threadIdx.x < 32) batch_extend();
+        __syncthreads();
+      }
+      const int w = (int)(threadIdx.x >> 5);
+      if (w < ps->nb) {
+        chare_proxy_base* q = ps->bp[w];
+        q->call_fn(q, ps->bidx[w], ps->bep[w], ps->barg[w]);
+      }
+      if (threadIdx.x == 0) ps->stats[ST_EM_CYC] += (unsigned long long)(clock64() - c0);
     } else if (act == ACT_STASH_PUT) {
       copy_cooperative(ps->d_p, ps->d_arg, ps->d_bytes, threadIdx.x, blockDim.x);
     } else if (act == ACT_FLUSH) {
@@ -1384,7 +1575,8 @@ __device__ void helper_loop() {
     if (!grid_barrier_ok()) break;
     if (ld_relaxed_s32(&gs->act) != ACT_CALL_RING) break;
     chare_proxy_base* p = reinterpret_cast<chare_proxy_base*>(gl_ld_ptr(&gs->p));
-    p->call_fn(p, ld_relaxed_s32(&gs->idx), ld_relaxed_s32(&gs->ep), gl_ld_ptr(&gs->arg));
+    const int ep = ld_relaxed_s32(&gs->ep);
+    if (!p->warp_em(ep)) p->call_fn(p, ld_relaxed_s32(&gs->idx), ep, gl_ld_ptr(&gs->arg));  // warp-level: block 0's warp 0
     if (!grid_barrier_ok()) break;
   }
 }

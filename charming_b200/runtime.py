@@ -41,6 +41,7 @@ class RunStats:
     deferred: int = 0
     ticket_ms: float = 0.0
     space_ms: float = 0.0
+    batched: int = 0
 
 
 def host_collectives(group=None):
@@ -129,7 +130,8 @@ class Runtime:
         self.lib.charming_last_stats(C.byref(st))
         return RunStats(st.delivered, st.sent, st.stashed, st.revived, st.bytes_sent,
                         st.idle_polls, st.space_waits, st.kernel_ms, st.loop_ms, st.main_ms,
-                        st.status, st.idle_ms, st.em_ms, st.deferred, st.ticket_ms, st.space_ms)
+                        st.status, st.idle_ms, st.em_ms, st.deferred, st.ticket_ms, st.space_ms,
+                        st.batched)
 
     # ---- built-in programs ---------------------------------------------------
     def hello(self) -> np.ndarray:

@@ -94,9 +94,15 @@ struct chare_proxy_base {
 
   proxy_call_fn call_fn;  // direct dispatch (no virtual call on the hot path)
 
+  // Entry methods 0..63 registered with add_warp_entry_method (bit ep): one
+  // warp runs each of their deliveries.
+  unsigned long long warp_ems;
+
   __device__ chare_proxy_base() : id(-1), n_local(0), n_total(0), start_idx(-1),
   end_idx(-1), loc_map(nullptr), em_count(0), async_waits(nullptr),
-  refnum(nullptr), mismatches(nullptr), call_fn(nullptr) {}
+  refnum(nullptr), mismatches(nullptr), call_fn(nullptr), warp_ems(0) {}
+
+  __device__ bool warp_em(int ep) const { return ep >= 0 && ep < 64 && ((warp_ems >> ep) & 1ULL); }
 
   // Proxies come from the PE arena (shared memory when there is room), so
   // the scheduler's per-message reads of them stay on chip.
@@ -207,6 +213,25 @@ struct chare_proxy : chare_proxy_base {
       return;
     }
     em_fn[em_count++] = Func;
+  }
+
+  // Registers an entry method that one warp runs instead of the whole PE
+  // block (an extension; the reference has block entry methods only). The
+  // scheduler runs consecutive deliveries of such entry methods to different
+  // chares together, one per warp of the block. The entry method may use
+  // warp-level synchronisation only (no __syncthreads(), and no sends:
+  // invoke and the user-message calls are block-collective), indexes its
+  // lanes by threadIdx.x % 32, and changes the refnum of its own chare only.
+  // Single-threaded, like add_entry_method.
+  template <void Func(C&, void*)>
+  __device__ void add_warp_entry_method() {
+    if (em_count >= 64) {
+      detail::report_error(detail::ERR_TOO_MANY_EMS, id, em_count);
+      return;
+    }
+    const int ep = em_count;
+    add_entry_method<Func>();
+    if (em_count == ep + 1) warp_ems |= 1ULL << ep;
   }
 
   __device__ static bool call_static(chare_proxy_base* base, int idx, int ep, void* arg) {

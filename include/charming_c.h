@@ -179,6 +179,8 @@ typedef struct charming_stats {
                                 next: profiling builds only, else 0)     */
   double space_ms;           /* mean over PEs: then for ring space (a stale
                                 head cache refreshed, or a full ring)    */
+  uint64_t batched;          /* deliveries run beside others, one per warp,
+                                in batches of warp-level entry methods   */
 } charming_stats;
 int charming_last_stats(charming_stats* out);
 

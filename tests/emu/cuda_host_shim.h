@@ -102,6 +102,7 @@ inline void __threadfence_system() { std::atomic_thread_fence(std::memory_order_
 inline void __nanosleep(unsigned) {}
 inline bool __isLocal(const void*) { return true; }
 inline int __ffs(unsigned x) { return x ? __builtin_ffs((int)x) : 0; }
+inline int __popc(unsigned x) { return __builtin_popcount(x); }
 inline long long clock64() { return 0; }
 
 template <typename T> inline T atomicAdd(T* p, T v) { return __atomic_fetch_add(p, v, __ATOMIC_SEQ_CST); }

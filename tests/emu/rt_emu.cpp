@@ -335,6 +335,7 @@ void init_runtime(int n_blocks, size_t ring_bytes, bool gpu_level) {
 }
 
 unsigned long long g_deferred = 0;  // sends moved to an outbox in the last run
+unsigned long long g_batched = 0;   // deliveries in batches of warp-level entry methods
 
 int run_scheduler(int n_pes, int threads) {
   blockIdx = emu_dim3{0, 0, 0};
@@ -371,10 +372,12 @@ int run_scheduler(int n_pes, int threads) {
   for (auto& t : th) t.join();
   // every process's run has ended: nothing writes this one's words any more
   if (g_rdv && g_rdv->barrier() != 0) _exit(6);
-  g_deferred = 0;
+  g_deferred = g_batched = 0;
   const int n_local = charm::rt::c_rt.gpu_level ? 1 : n_pes;
-  for (int p = 0; p < n_local; p++)
+  for (int p = 0; p < n_local; p++) {
     g_deferred += charm::rt::c_rt.pe_stats[(size_t)p * charm::rt::N_STATS + charm::rt::ST_DEFERRED];
+    g_batched += charm::rt::c_rt.pe_stats[(size_t)p * charm::rt::N_STATS + charm::rt::ST_BATCHED];
+  }
   // the first error any of this process's GPUs recorded
   const int* ctl = charm::rt::c_rt.ctrl;
   const int launch_devs = g_world > 1 ? 1 : charm::rt::c_rt.n_devs;
@@ -622,8 +625,8 @@ int main(int argc, char** argv) {
       status = run_scheduler(n_pes, threads);
     }
     const int* ectl = charm::rt::c_rt.ctrl;
-    printf("status=%d chares_done=%llu deferred=%llu err_pe=%d\n", status, (unsigned long long)ctr[1], g_deferred,
-           status ? ectl[charm::rt::CTRL_ERR_PE] : -1);
+    printf("status=%d chares_done=%llu deferred=%llu err_pe=%d batched=%llu\n", status, (unsigned long long)ctr[1],
+           g_deferred, status ? ectl[charm::rt::CTRL_ERR_PE] : -1, g_batched);
     unsigned long long nrec = total;
     for (unsigned long long r = 0; r < nrec; r++) {
       printf("L");

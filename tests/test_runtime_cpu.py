@@ -78,6 +78,27 @@ def test_fanout_block_collective_paths(emus, threads, n, msgs, payload, mode, ri
     fanout(emus["rt_emu_mt"], 1, ring, n, msgs, payload, 0xC0FFEE, mode, threads)
 
 
+@pytest.mark.parametrize("threads", [64, 128])
+@pytest.mark.parametrize("n,msgs,payload,mode,ring", [
+    (40, 16, 64, 0, 1 << 18),     # FIFO: nearly every delivery in a batch
+    (40, 16, 64, 1, 1 << 18),     # refnum ladders: a mismatch ends a batch
+    (16, 8, 256, 1, 2048),        # tiny ring: batches over wrapped tickets, deferred sends
+])
+def test_warp_entry_methods_run_in_batches(emus, threads, n, msgs, payload, mode, ring):
+    """The fan-out's receive is a warp-level entry method: warp 0 scans the
+    cells after the head message and the block runs up to one delivery per
+    warp at once (2 and 4 warps, lockstep, ThreadSanitizer). The log must
+    still match the model exactly (per-pair order, refnum ladders)."""
+    r = run(emus["rt_emu_mt"], ["fanout", 1, ring, n, msgs, payload, 0xBA7 + n + mode, mode], threads)
+    head = r.stdout.splitlines()[0]
+    assert r.returncode == 0 and head.startswith("status=0"), (head, r.stderr[-2000:])
+    rows = [l.split()[1:] for l in r.stdout.splitlines() if l.startswith("L ")]
+    log = np.array([[int(x, 16) for x in row] for row in rows], dtype=np.uint32).reshape(-1, 8)
+    chk = msgmodel.check_fanout_log(log, n, msgs, payload, 0xBA7 + n + mode, mode)
+    assert chk.ok, chk.errors
+    assert int(head.split("batched=")[1].split()[0]) > 0
+
+
 @pytest.mark.parametrize("exe,n_pes,threads,ring,n,msgs,payload,mode", [
     # every PE's start entry methods send far more than the receivers'
     # rings hold, to PEs that are doing the same: each send that finds no
