@@ -823,7 +823,9 @@ def main() -> int:
                             "loop_ms": stats.loop_ms, "stashed": stats.stashed,
                             "delivered": stats.delivered},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-            "gpu_launches": 2 * args.steps, "status": stats.status,
+            # per timed step: the reset kernel, the scheduler kernel and the
+            # status latch of charming_jacobi2d_run_n
+            "gpu_launches": 3 * args.steps, "status": stats.status,
             "runtime": {k: rt.info[k] for k in ("n_pes", "threads_per_pe", "smem_bytes_per_pe",
                                                 "smem_scratch_bytes", "regs_per_thread")},
         }
