@@ -307,7 +307,8 @@ __device__ void send_halos(JBlock& c, const jac::chare_desc& d, int phase = 0) {
     bytes[n] = sizeof(jac::halo_hdr) + (size_t)e[n].nr * e[n].nc * sizeof(T);
     n++;
   }
-  charm::message msg[jac::N_DIRS];
+  static_assert(jac::N_DIRS <= charm::MSG_BATCH_MAX, "one batch holds every halo of a phase");
+  charm::message* msg = charm::block_messages();  // one copy per block, in shared memory
   CHARM_PROF(if (threadIdx.x == 0) add_pe_cyc(5, pe_clock() - t0);)
   const bool got = n > 0 && jproxy->alloc_msgs(msg, idx, bytes, n);
   CHARM_PROF(if (threadIdx.x == 0) add_pe_cyc(3, pe_clock() - t0);)

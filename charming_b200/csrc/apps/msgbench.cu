@@ -209,7 +209,7 @@ __device__ void fan_start(FanChare& c, void* arg) {
       refs[j] = mode ? k0 + j : -1;
       sizes[j] = (size_t)payload;
     }
-    charm::message m[charm::MSG_BATCH_MAX];
+    charm::message* m = charm::block_messages();  // one copy per block, in shared memory
     if (!fan_proxy->alloc_msgs(m, idx, sizes, nb)) return;  // error recorded
     for (int e = threadIdx.x; e < nb * nw; e += blockDim.x) {
       const int j = e / nw, w = e % nw, k = k0 + j;

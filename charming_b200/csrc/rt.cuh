@@ -269,6 +269,9 @@ struct pe_state {
   int bidx[MAX_THREADS / 32], bep[MAX_THREADS / 32];
   unsigned long long bstash[MAX_THREADS / 32];  // stash keys of a stash batch
   unsigned long long bkeys[MAX_THREADS / 32];   // its chares
+  // the block-shared message array of block_messages() (raw storage: the
+  // block's state is never constructed)
+  alignas(16) unsigned char bmsg[MSG_BATCH_MAX * sizeof(message)];
   // batched sends (alloc_user_msgs): per message start, ticket, bytes
   void* bm_ptr[MSG_BATCH_MAX];
   unsigned long long bm_tick[MSG_BATCH_MAX];

@@ -560,16 +560,22 @@ __device__ bool group_alloc_user_msgs(message* msgs, const int* dst_pes, const s
     }
   }
   grid_barrier();
+  // a block-shared array (block_messages()) is filled by thread 0 of each block
+  const bool fill = !__isShared(msgs) || threadIdx.x == 0;
   bool ok = true;
   for (int k = 0; k < n; k++) {
-    msgs[k].env = reinterpret_cast<envelope*>(gl_ld_ptr(&g->ptr[k]));
-    msgs[k].offset = ld_relaxed_u64(&g->u1[k]);
-    msgs[k].dst_pe = dst_pes[k];
-    const unsigned long long bytes = ld_relaxed_u64(&g->u0[k]);
-    msgs[k].cells = (int)cells_for(bytes);
-    msgs[k].capacity = msgs[k].env ? (size_t)(bytes - HDR) : 0;
-    ok = ok && msgs[k].env != nullptr;
+    envelope* env = reinterpret_cast<envelope*>(gl_ld_ptr(&g->ptr[k]));
+    if (fill) {
+      msgs[k].env = env;
+      msgs[k].offset = ld_relaxed_u64(&g->u1[k]);
+      msgs[k].dst_pe = dst_pes[k];
+      const unsigned long long bytes = ld_relaxed_u64(&g->u0[k]);
+      msgs[k].cells = (int)cells_for(bytes);
+      msgs[k].capacity = env ? (size_t)(bytes - HDR) : 0;
+    }
+    ok = ok && env != nullptr;
   }
+  if (__isShared(msgs)) __syncthreads();
   return ok;
 }
 
@@ -774,17 +780,27 @@ __device__ bool charm::alloc_user_msgs(message* msgs, const int* dst_pes,
     }
   }
   __syncthreads();
+  // every thread's own array, or a block-shared one (block_messages()) that
+  // thread 0 fills: 512 private copies of the descriptors cost each batch
+  // about 300 KB of local-memory stores
+  const bool fill = !__isShared(msgs) || threadIdx.x == 0;
   bool ok = true;
   for (int j = 0; j < n; j++) {
-    msgs[j].env = reinterpret_cast<envelope*>(ps->bm_ptr[j]);
-    msgs[j].offset = ps->bm_tick[j];
-    msgs[j].dst_pe = dst_pes[j];
-    msgs[j].cells = (int)cells_for(ps->bm_bytes[j]);
-    msgs[j].capacity = msgs[j].env ? (size_t)(ps->bm_bytes[j] - HDR) : 0;
-    ok = ok && msgs[j].env != nullptr;
+    if (fill) {
+      msgs[j].env = reinterpret_cast<envelope*>(ps->bm_ptr[j]);
+      msgs[j].offset = ps->bm_tick[j];
+      msgs[j].dst_pe = dst_pes[j];
+      msgs[j].cells = (int)cells_for(ps->bm_bytes[j]);
+      msgs[j].capacity = ps->bm_ptr[j] ? (size_t)(ps->bm_bytes[j] - HDR) : 0;
+    }
+    ok = ok && ps->bm_ptr[j] != nullptr;
   }
   __syncthreads();
   return ok;
+}
+
+__device__ charm::message* charm::block_messages() {
+  return reinterpret_cast<message*>(pes()->bmsg);
 }
 
 __device__ void charm::send_user_msgs(int chare_id, const int* chare_idx, int ep_id,
@@ -792,7 +808,9 @@ __device__ void charm::send_user_msgs(int chare_id, const int* chare_idx, int ep
   if (n > MSG_BATCH_MAX) n = MSG_BATCH_MAX;
   if (gpu_level()) {
     group_send_user_msgs(chare_id, chare_idx, ep_id, msgs, payload_sizes, refnums, n);
-    for (int j = 0; j < n; j++) msgs[j].env = nullptr;
+    if (__isShared(msgs)) __syncthreads();  // block 0's publishers are done reading it
+    if (!__isShared(msgs) || threadIdx.x == 0)
+      for (int j = 0; j < n; j++) msgs[j].env = nullptr;
     return;
   }
   pe_state* ps = pes();
@@ -816,7 +834,8 @@ __device__ void charm::send_user_msgs(int chare_id, const int* chare_idx, int ep
     publish_msg(msgs[k].dst_pe, msgs[k].offset, m);
   }
   __syncthreads();
-  for (int j = 0; j < n; j++) msgs[j].env = nullptr;
+  if (!__isShared(msgs) || threadIdx.x == 0)
+    for (int j = 0; j < n; j++) msgs[j].env = nullptr;
 }
 
 // ---------------------------------------------------------------------------

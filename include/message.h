@@ -131,6 +131,13 @@ __device__ bool alloc_user_msgs(message* msgs, const int* dst_pes, const size_t*
     int n);
 __device__ void send_user_msgs(int chare_id, const int* chare_idx, int ep_id, message* msgs,
     const size_t* payload_sizes, const int* refnums, int n);
+// MSG_BATCH_MAX message descriptors in the calling PE block's shared memory,
+// for alloc_user_msgs / send_user_msgs (an extension). Passed one of these,
+// the calls fill and clear it from thread 0 alone instead of giving every
+// thread its own copy, which saves each batch hundreds of bytes of
+// local-memory traffic per thread. One array per block: a batch must be sent
+// before the next is reserved.
+__device__ message* block_messages();
 
 // Single-threaded (called under threadIdx.x == 0 by set_refnum). Marks the
 // PE's stash for re-examination; stashed messages whose refnum now matches

@@ -157,6 +157,9 @@ inline size_t __cvta_generic_to_shared(const void* p) { return (size_t)p; }
 #ifdef EMU_RT
 extern thread_local uint64_t* s_mem_of_pe;  // set by each PE thread
 #define s_mem s_mem_of_pe
+// whether p lies in the calling PE block's stand-in shared memory
+bool emu_is_shared(const void* p);
+inline bool __isShared(const void* p) { return emu_is_shared(p); }
 #else
 extern uint64_t s_mem[];
 #endif

@@ -99,6 +99,7 @@ struct PE {
   size_t ucap = 0;
   std::vector<double> red;
   int revive = 0;
+  charm::message bmsgs[charm::MSG_BATCH_MAX];  // charm::block_messages() of the block
   alignas(128) unsigned char smem[1 << 20];  // charm::smem_scratch() of the block
 #ifdef EMU_MT
   struct Warp {
@@ -392,6 +393,12 @@ void send_reg_msg(int chare_id, int chare_idx, int ep, void* buf, size_t size, i
   if (threadIdx.x == 0) push(dst_pe, make_msg(msgtype::regular, chare_id, chare_idx, ep, refnum, buf, size));
   emu_sync(__FILE__, __LINE__);
 }
+message* block_messages() { return me_pe().bmsgs; }
+// whether msg is in the block's shared array (filled by thread 0 alone)
+static bool block_shared(const message& msg) {
+  PE& pe = me_pe();
+  return &msg >= pe.bmsgs && &msg < pe.bmsgs + MSG_BATCH_MAX;
+}
 bool alloc_user_msg(message& msg, int dst_pe, size_t size) {
   PE& pe = me_pe();
   if (threadIdx.x == 0) {
@@ -400,13 +407,16 @@ bool alloc_user_msg(message& msg, int dst_pe, size_t size) {
     pe.ucap = total - 32;
   }
   emu_sync(__FILE__, __LINE__);
-  msg.env = reinterpret_cast<envelope*>(pe.ubuf);
-  msg.offset = 0;
-  msg.dst_pe = dst_pe;
-  msg.cells = 0;
-  msg.capacity = pe.ucap;
+  unsigned char* got = pe.ubuf;
+  if (!block_shared(msg) || threadIdx.x == 0) {
+    msg.env = reinterpret_cast<envelope*>(got);
+    msg.offset = 0;
+    msg.dst_pe = dst_pe;
+    msg.cells = 0;
+    msg.capacity = pe.ucap;
+  }
   emu_sync(__FILE__, __LINE__);
-  return msg.env != nullptr;
+  return got != nullptr;
 }
 void send_user_msg(int chare_id, int chare_idx, int ep, message& msg, size_t size, int refnum) {
   if (!msg.env) return;
@@ -418,7 +428,8 @@ void send_user_msg(int chare_id, int chare_idx, int ep, message& msg, size_t siz
     delete[] p;
   }
   emu_sync(__FILE__, __LINE__);
-  msg.env = nullptr;
+  if (!block_shared(msg) || threadIdx.x == 0) msg.env = nullptr;
+  emu_sync(__FILE__, __LINE__);
 }
 bool alloc_user_msgs(message* msgs, const int* dst_pes, const size_t* sizes, int n) {
   bool ok = true;

@@ -55,6 +55,11 @@ emu_dim3 blockDim{1, 1, 1};
 emu_dim3 gridDim{1, 1, 1};
 constexpr size_t SMEM_BYTES = 1 << 16;
 thread_local uint64_t* s_mem_of_pe = nullptr;
+bool emu_is_shared(const void* p) {
+  const unsigned char* b = reinterpret_cast<const unsigned char*>(s_mem_of_pe);
+  const unsigned char* q = static_cast<const unsigned char*>(p);
+  return b && q >= b && q < b + SMEM_BYTES;
+}
 
 __global__ void charming_scheduler_kernel(int argc, char** argv, size_t* argvs);
 __global__ void charming_reset_kernel();
