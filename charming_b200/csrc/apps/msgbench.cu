@@ -200,15 +200,19 @@ __device__ void fan_start(FanChare& c, void* arg) {
   const unsigned long long seed = (unsigned long long)g_app.a[3];
   const int mode = (int)g_app.a[4];
   const int nw = (payload + 7) / 8;
+  // the batch's targets, refnums and sizes: one copy per block (per-thread
+  // arrays of them are local memory)
+  __shared__ int idx[charm::MSG_BATCH_MAX], refs[charm::MSG_BATCH_MAX];
+  __shared__ size_t sizes[charm::MSG_BATCH_MAX];
   for (int k0 = 0; k0 < msgs; k0 += charm::MSG_BATCH_MAX) {
     const int nb = msgs - k0 < charm::MSG_BATCH_MAX ? msgs - k0 : charm::MSG_BATCH_MAX;
-    int idx[charm::MSG_BATCH_MAX], refs[charm::MSG_BATCH_MAX];
-    size_t sizes[charm::MSG_BATCH_MAX];
-    for (int j = 0; j < nb; j++) {
+    // (the previous batch's send ended with a block barrier)
+    for (int j = (int)threadIdx.x; j < nb; j += (int)blockDim.x) {
       idx[j] = fan_dst(seed, c.i, k0 + j, msgs, n);
       refs[j] = mode ? k0 + j : -1;
       sizes[j] = (size_t)payload;
     }
+    __syncthreads();
     charm::message* m = charm::block_messages();  // one copy per block, in shared memory
     if (!fan_proxy->alloc_msgs(m, idx, sizes, nb)) return;  // error recorded
     for (int e = threadIdx.x; e < nb * nw; e += blockDim.x) {
