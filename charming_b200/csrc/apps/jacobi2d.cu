@@ -288,44 +288,59 @@ __device__ void count_nbrs(JBlock& c, const jac::chare_desc& d) {
 // overlap (refnum = pass in halo_mode 1). phase 0: every neighbour (the
 // one-phase exchange); 1: left and right; 2: top and bottom, with the ghost
 // columns the left/right halos of this pass filled. All threads.
-template <typename T>
-__device__ void send_halos(JBlock& c, const jac::chare_desc& d, int phase = 0) {
-  const unsigned long long t0 = threadIdx.x == 0 ? pe_clock() : 0;
+// The halos of one batch: one copy per block, written by thread 0 (a
+// private copy in every thread was local memory, about 350 bytes per thread
+// per batch).
+struct halo_batch {
   int idx[jac::N_DIRS], dirs[jac::N_DIRS], refs[jac::N_DIRS];
   size_t bytes[jac::N_DIRS];
   jac::region e[jac::N_DIRS];
-  int n = 0;
-  const bool tagged = japp::halo_mode() == 1;
-  for (int dir = 0; dir < jac::N_DIRS; dir++) {
-    if (d.nbr[dir] < 0) continue;
-    if (phase == 1 && dir != jac::LEFT && dir != jac::RIGHT) continue;
-    if (phase == 2 && dir != jac::TOP && dir != jac::BOTTOM) continue;
-    e[n] = jac::halo_edge(dir, d);
-    idx[n] = d.nbr[dir];
-    dirs[n] = dir;
-    refs[n] = tagged ? c.pass : -1;
-    bytes[n] = sizeof(jac::halo_hdr) + (size_t)e[n].nr * e[n].nc * sizeof(T);
-    n++;
+  void* vals[jac::N_DIRS];
+  int n;
+};
+__shared__ halo_batch s_halos;
+
+template <typename T>
+__device__ void send_halos(JBlock& c, const jac::chare_desc& d, int phase = 0) {
+  const unsigned long long t0 = threadIdx.x == 0 ? pe_clock() : 0;
+  halo_batch& b = s_halos;
+  __syncthreads();  // every thread is done with the last batch's record
+  if (threadIdx.x == 0) {
+    int n = 0;
+    const bool tagged = japp::halo_mode() == 1;
+    for (int dir = 0; dir < jac::N_DIRS; dir++) {
+      if (d.nbr[dir] < 0) continue;
+      if (phase == 1 && dir != jac::LEFT && dir != jac::RIGHT) continue;
+      if (phase == 2 && dir != jac::TOP && dir != jac::BOTTOM) continue;
+      b.e[n] = jac::halo_edge(dir, d);
+      b.idx[n] = d.nbr[dir];
+      b.dirs[n] = dir;
+      b.refs[n] = tagged ? c.pass : -1;
+      b.bytes[n] = sizeof(jac::halo_hdr) + (size_t)b.e[n].nr * b.e[n].nc * sizeof(T);
+      n++;
+    }
+    b.n = n;
   }
+  __syncthreads();
+  const int n = b.n;
   static_assert(jac::N_DIRS <= charm::MSG_BATCH_MAX, "one batch holds every halo of a phase");
   charm::message* msg = charm::block_messages();  // one copy per block, in shared memory
   CHARM_PROF(if (threadIdx.x == 0) add_pe_cyc(5, pe_clock() - t0);)
-  const bool got = n > 0 && jproxy->alloc_msgs(msg, idx, bytes, n);
+  const bool got = n > 0 && jproxy->alloc_msgs(msg, b.idx, b.bytes, n);
   CHARM_PROF(if (threadIdx.x == 0) add_pe_cyc(3, pe_clock() - t0);)
   if (got) {
-    T* vals[jac::N_DIRS];
-    for (int k = 0; k < n; k++)
-      vals[k] = reinterpret_cast<T*>(reinterpret_cast<char*>(msg[k].payload()) + sizeof(jac::halo_hdr));
     for (int k = (int)threadIdx.x; k < n; k += (int)blockDim.x) {  // one header per thread
       jac::halo_hdr* hh = reinterpret_cast<jac::halo_hdr*>(msg[k].payload());
-      hh->dir = jac::opposite(dirs[k]);
-      hh->len = e[k].nr * e[k].nc;
+      hh->dir = jac::opposite(b.dirs[k]);
+      hh->len = b.e[k].nr * b.e[k].nc;
       hh->pass = c.pass;
       hh->gen = c.gen;
+      b.vals[k] = reinterpret_cast<char*>(msg[k].payload()) + sizeof(jac::halo_hdr);
     }
-    copy_rects<T>(view<T>(d, c.cur), e, vals, n, false);
+    __syncthreads();
+    copy_rects<T>(view<T>(d, c.cur), b.e, reinterpret_cast<T* const*>(b.vals), n, false);
     CHARM_PROF(const unsigned long long tp = threadIdx.x == 0 ? pe_clock() : 0;)
-    jproxy->invoke_msgs(idx, EP_HALO, msg, bytes, refs, n);
+    jproxy->invoke_msgs(b.idx, EP_HALO, msg, b.bytes, b.refs, n);
     CHARM_PROF(if (threadIdx.x == 0) add_pe_cyc(4, pe_clock() - tp);)
   }
   if (threadIdx.x == 0) add_pe_cyc(1, pe_clock() - t0);
