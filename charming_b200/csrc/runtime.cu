@@ -1559,7 +1559,7 @@ __device__ void scheduler_loop() {
     if (call) {
       const long long c0 = clock64();
       // a warp-level entry method outside a batch: warp 0 (of block 0)
-      if (!p->warp_em(ps->d_ep) || threadIdx.x < 32) p->call_fn(p, ps->d_idx, ps->d_ep, ps->d_arg);
+      if (!p->warp_em(ps->d_ep) || threadIdx.x < 32) p->em_tab[ps->d_ep](p, ps->d_idx, ps->d_arg);
       if (threadIdx.x == 0) ps->stats[ST_EM_CYC] += (unsigned long long)(clock64() - c0);
       if (group && !grid_barrier_ok()) break;  // every block is done with the message
     } else if (act == ACT_CALL_BATCH || act == ACT_STASH_BATCH) {
@@ -1571,7 +1571,7 @@ __device__ void scheduler_loop() {
       const int w = (int)(threadIdx.x >> 5);
       if (w < ps->nb) {
         chare_proxy_base* q = ps->bp[w];
-        q->call_fn(q, ps->bidx[w], ps->bep[w], ps->barg[w]);
+        q->em_tab[ps->bep[w]](q, ps->bidx[w], ps->barg[w]);
       }
       if (threadIdx.x == 0) ps->stats[ST_EM_CYC] += (unsigned long long)(clock64() - c0);
     } else if (act == ACT_STASH_PUT) {
@@ -1595,7 +1595,7 @@ __device__ void helper_loop() {
     if (ld_relaxed_s32(&gs->act) != ACT_CALL_RING) break;
     chare_proxy_base* p = reinterpret_cast<chare_proxy_base*>(gl_ld_ptr(&gs->p));
     const int ep = ld_relaxed_s32(&gs->ep);
-    if (!p->warp_em(ep)) p->call_fn(p, ld_relaxed_s32(&gs->idx), ep, gl_ld_ptr(&gs->arg));  // warp-level: block 0's warp 0
+    if (!p->warp_em(ep)) p->em_tab[ep](p, ld_relaxed_s32(&gs->idx), gl_ld_ptr(&gs->arg));  // warp-level: block 0's warp 0
     if (!grid_barrier_ok()) break;
   }
 }

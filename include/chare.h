@@ -74,6 +74,9 @@ __device__ bool pe_owns(const void* p);
 struct chare_proxy_base;
 // Entry method `ep` of local chare `idx` on `arg` (all threads of the block).
 typedef bool (*proxy_call_fn)(chare_proxy_base* proxy, int idx, int ep, void* arg);
+// One registered entry method with the lookup of its chare object: the
+// scheduler reaches an entry method with this one indirect call.
+typedef void (*em_entry_fn)(chare_proxy_base* proxy, int idx, void* arg);
 
 struct chare_proxy_base {
   int id;        // Chare array ID (registration order on this PE)
@@ -93,6 +96,7 @@ struct chare_proxy_base {
   mismatch_t* mismatches;
 
   proxy_call_fn call_fn;  // direct dispatch (no virtual call on the hot path)
+  em_entry_fn* em_tab;    // the entry methods, each with its object lookup
 
   // Entry methods 0..63 registered with add_warp_entry_method (bit ep): one
   // warp runs each of their deliveries.
@@ -100,7 +104,7 @@ struct chare_proxy_base {
 
   __device__ chare_proxy_base() : id(-1), n_local(0), n_total(0), start_idx(-1),
   end_idx(-1), loc_map(nullptr), em_count(0), async_waits(nullptr),
-  refnum(nullptr), mismatches(nullptr), call_fn(nullptr), warp_ems(0) {}
+  refnum(nullptr), mismatches(nullptr), call_fn(nullptr), em_tab(nullptr), warp_ems(0) {}
 
   __device__ bool warp_em(int ep) const { return ep >= 0 && ep < 64 && ((warp_ems >> ep) & 1ULL); }
 
@@ -184,14 +188,14 @@ template <typename C>
 struct chare_proxy : chare_proxy_base {
   typedef void (*em_fn_t)(C&, void*);
   C** objects;     // Local chare objects
-  em_fn_t* em_fn;  // Entry method table: the functions themselves (the
-                   // reference keeps entry_method objects with a virtual
-                   // call operator; a function pointer saves the vtable
-                   // loads per message)
+  // Entry method table (em_tab): per entry method a function that looks up
+  // the chare object and calls the entry method, inlined into it (the
+  // reference keeps entry_method objects with a virtual call operator; one
+  // function pointer per message saves the vtable loads and a second call)
 
   // Registers this proxy in the calling PE's table (single-threaded).
   __device__ chare_proxy()
-    : chare_proxy_base(), objects(nullptr), em_fn(nullptr) {
+    : chare_proxy_base(), objects(nullptr) {
     chare_proxy_table& table = detail::my_proxy_table();
     if (table.count >= CHARE_TYPE_CNT_MAX) {
       detail::report_error(detail::ERR_TOO_MANY_TYPES, table.count, 0);
@@ -201,18 +205,24 @@ struct chare_proxy : chare_proxy_base {
     table.proxies[id] = this;
     detail::cache_proxy(id, this);
     call_fn = &chare_proxy<C>::call_static;
-    em_fn = detail::pe_array<em_fn_t>(EM_CNT_MAX);
-    if (em_fn == nullptr) detail::report_error(detail::ERR_NO_MEMORY, id, 0);
+    em_tab = detail::pe_array<em_entry_fn>(EM_CNT_MAX);
+    if (em_tab == nullptr) detail::report_error(detail::ERR_NO_MEMORY, id, 0);
+  }
+
+  template <void Func(C&, void*)>
+  __device__ static void em_entry(chare_proxy_base* base, int idx, void* arg) {
+    chare_proxy<C>* self = static_cast<chare_proxy<C>*>(base);
+    Func(*(self->objects[idx - self->start_idx]), arg);
   }
 
   // Add entry method to table (single-threaded)
   template <void Func(C&, void*)>
   __device__ void add_entry_method() {
-    if (em_fn == nullptr || em_count >= EM_CNT_MAX) {
+    if (em_tab == nullptr || em_count >= EM_CNT_MAX) {
       detail::report_error(detail::ERR_TOO_MANY_EMS, id, em_count);
       return;
     }
-    em_fn[em_count++] = Func;
+    em_tab[em_count++] = &chare_proxy<C>::em_entry<Func>;
   }
 
   // Registers an entry method that one warp runs instead of the whole PE
@@ -236,7 +246,7 @@ struct chare_proxy : chare_proxy_base {
 
   __device__ static bool call_static(chare_proxy_base* base, int idx, int ep, void* arg) {
     chare_proxy<C>* self = static_cast<chare_proxy<C>*>(base);
-    self->em_fn[ep](*(self->objects[idx - self->start_idx]), arg);
+    self->em_tab[ep](base, idx, arg);
     return true;
   }
 
@@ -302,13 +312,13 @@ struct chare_proxy : chare_proxy_base {
     detail::pe_free_array(objects);
     detail::pe_free_array(refnum);
     detail::pe_free_array(loc_map);
-    detail::pe_free_array(em_fn);
+    detail::pe_free_array(em_tab);
     detail::pe_free_array(async_waits);
     async_waits = nullptr;
     objects = nullptr;
     refnum = nullptr;
     loc_map = nullptr;
-    em_fn = nullptr;
+    em_tab = nullptr;
     n_local = 0;
     em_count = 0;
   }
